@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 path tracer on the plain-method scenes.
+
+One "step" is one complete render of the workload: every pixel traced until
+it reaches its sample budget or converges (pt_render with no wave limit),
+starting from a reset accumulator with the scene resident in HBM.
+
+  value  Msamples/s of the device-timed steps (CUDA events on the stream the
+         library launches on), summed over ranks, time = max over ranks.
+  e2e    the same metric through the public API with HOST buffers: per step
+         the mesh is uploaded from pinned host memory (and the BVH rebuilt),
+         camera and params set, the image rendered and read back to pinned
+         host memory.
+  roofline  for the closest-hit traversal kernel (the dominant kernel):
+         algorithmic bytes per ray (80 B per compressed node + 48 B per
+         triangle visited, + 32 B ray in + 16 B hit out) x rays per launch /
+         launch time.
+  cpu_baseline  the reference's own render code compiled for the host
+         (oracle/_ref, OpenMP over pixels) on a bounded pixel sample.
+
+Multi-GPU: every rank renders its own copy of the workload (pixels and
+scenes are independent; no data-path collective) -> weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import signal
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Msamples/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--config", choices=["plain-small"], default="plain-small")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name: str):
+    from lsystemeditor_b200.scene import config0_scene
+    if name == "plain-small":
+        return config0_scene()
+    raise ValueError(name)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+REASON_BITS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 4:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    smax.append(float(parts[1]))
+                    bits = int(parts[3], 16)
+                except ValueError:
+                    continue
+                for b, name in REASON_BITS.items():
+                    if bits & b and name != "gpu_idle":
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's render code on the host cores
+# ---------------------------------------------------------------------------
+def cpu_render_rate(spec, min_seconds: float = 10.0, max_pixels: int | None = None, seed: int = 0):
+    """Times the host render (reference build when present, else the oracle port) on a pixel sample."""
+    from oracle.bindings import Checker, reference_available
+    kind = "reference" if reference_available() else "port"
+    chk = Checker("ref" if kind == "reference" else "oracle")
+    sc = chk.scene(spec.mesh)
+    threads = chk.max_threads()
+    P = spec.width * spec.height
+    rng = np.random.default_rng(seed)
+    # calibrate on a small sample, then size the sample for ~min_seconds
+    n = min(P, 256)
+    pix = np.sort(rng.choice(P, n, replace=False)).astype(np.int32)
+    t0 = time.perf_counter()
+    st = sc.render(spec.camera, spec.params, spec.width, spec.height, spec.waves, pixels=pix, threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    per_pixel = dt / n
+    n = int(min(P, max(256, min_seconds / per_pixel)))
+    if max_pixels:
+        n = min(n, max_pixels)
+    pix = np.sort(rng.choice(P, n, replace=False)).astype(np.int32)
+    t0 = time.perf_counter()
+    st = sc.render(spec.camera, spec.params, spec.width, spec.height, spec.waves, pixels=pix, threads=threads)
+    dt = time.perf_counter() - t0
+    samples = int(st["counts"][pix].sum())
+    return {"value": samples / dt / 1e6, "unit": METRIC, "cores": int(threads), "kind": kind,
+            "sample": f"{n} of {P} pixels x up to {spec.waves} samples ({samples} path samples, {dt:.1f} s), "
+                      f"same scene/camera/params, PCG32 random numbers"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    spec = make_workload(args.config)
+    try:
+        from oracle.bindings import reference_available
+        kind = "reference" if reference_available() else "port"
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": f"host checker cannot be built: {e}"}))
+        return 0
+    # bounded sample per step: ~5 s of CPU work
+    for _ in range(args.warmup):
+        cpu_render_rate(spec, min_seconds=1.0)
+    rates, descr = [], None
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        r = cpu_render_rate(spec, min_seconds=5.0, seed=k + 1)
+        rates.append(r["value"])
+        descr = r
+    wall = time.perf_counter() - t0
+    value = float(np.mean(rates))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(spec, args.config),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": descr["cores"], "kind": kind,
+                         "sample": descr["sample"]},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def workload_config(spec, name):
+    m = spec.mesh
+    return {"workload": spec.name, "width": spec.width, "height": spec.height,
+            "spp": int(spec.params["max_samples_per_pixel"]), "min_spp": int(spec.params["min_samples"]),
+            "max_depth": int(spec.params["max_path_depth"]), "triangles": int(m.triangle_count),
+            "materials": int(len(m.materials)), "seed": "reference per-(pixel, sample) seed",
+            "l2": "flushed between timed steps (256 MiB write, untimed)"}
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from lsystemeditor_b200.pathtracer import PROFILE_COUNT_VISITS, PROFILE_STAGE_TIMES, PathTracer
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    spec = make_workload(args.config)
+    stream = torch.cuda.current_stream()
+    pt = PathTracer(local)
+    pt.set_stream(stream.cuda_stream)
+    pt.configure(spec.width, spec.height, spec.mesh)
+    pt.set_camera(spec.camera)
+    pt.set_params(spec.params)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        pt.reset_accumulation()
+        pt.render(0)
+
+    # warm-up (also allocates path state and sample buffers)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K device-timed renders ----------------------------
+    pt.set_profiling(PROFILE_STAGE_TIMES)
+    launches0 = pt.stats()["launches"]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ext_ms, ext_launches, ext_rays, samples = 0.0, 0, 0, 0
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        step()
+        evs[k][1].record(stream)
+        prof = pt.profile()
+        ext_ms += prof["ms_extend"]
+        ext_launches += prof["launches_extend"]
+        ext_rays += prof["rays_extend"]
+        samples += pt.stats()["samples"]
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = pt.stats()["launches"] - launches0
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(float(sum(step_ms)))
+    total_samples = sum_over_ranks(float(samples))
+    value = total_samples / (total_ms / 1e3) / 1e6
+    pt.set_profiling(0)
+
+    # ---- traversal statistics for the roofline (untimed counting pass) ----
+    pt.set_profiling(PROFILE_COUNT_VISITS | PROFILE_STAGE_TIMES)
+    step()
+    cp = pt.profile()
+    pt.set_profiling(0)
+    nodes_per_ray = cp["nodes_extend"] / max(cp["rays_extend"], 1)
+    tris_per_ray = cp["tris_extend"] / max(cp["rays_extend"], 1)
+    bytes_per_ray = 80.0 * nodes_per_ray + 48.0 * tris_per_ray + 32.0 + 16.0
+    rays_per_launch = ext_rays / max(ext_launches, 1)
+    launch_ms = ext_ms / max(ext_launches, 1)
+    achieved = bytes_per_ray * rays_per_launch / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_extend.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            t = json.load(f)
+        if t.get("workload") == spec.name and t.get("bytes_per_ray"):
+            traffic = t["bytes_per_ray"] * rays_per_launch
+
+    # ---- end to end through the public API with host buffers ---------------
+    m = spec.mesh.contiguous()
+
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(a.dtype).reshape(a.shape)
+        v[...] = a
+        return t, v
+
+    keep = []
+    pm = type(m)(*[None] * 6)
+    for field in ("positions", "normals", "uvs", "material_ids", "materials", "textures"):
+        t, v = pinned(getattr(m, field))
+        keep.append(t)
+        setattr(pm, field, v)
+    rgba_t = torch.empty((spec.height, spec.width, 4), dtype=torch.float32, pin_memory=True)
+    h2d = sum(getattr(m, f).nbytes for f in ("positions", "normals", "uvs", "material_ids", "materials",
+                                                "textures")) + 80 + 64
+    d2h = spec.width * spec.height * (16 + 4 + 1)
+
+    def e2e_step():
+        pt.set_mesh(pm)
+        pt.set_camera(spec.camera)
+        pt.set_params(spec.params)
+        pt.render(0)
+        pt.readback()
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e_samples = 0
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        e_evs[k][0].record(stream)
+        e2e_step()
+        e_evs[k][1].record(stream)
+        e_samples += pt.stats()["samples"]
+    torch.cuda.synchronize()
+    barrier()
+    e_ms = max_over_ranks(float(sum(a.elapsed_time(b) for a, b in e_evs)))
+    e_value = sum_over_ranks(float(e_samples)) / (e_ms / 1e3) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_render_rate(spec, min_seconds=12.0)
+        except Exception as e:  # the baseline must not take the GPU number down with it
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"unavailable: {e}"}
+
+    st = pt.stats()
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {**workload_config(spec, args.config), "parallelism": f"replicas{world}",
+                   "bvh_nodes": int(st["bvh_nodes"]),
+                   "mrays_per_s": (ext_rays + 0.0) / (sum(step_ms) / 1e3) / 1e6,
+                   "rays_per_sample": (cp["rays_extend"] + cp["rays_shadow"]) / max(1, spec.width * spec.height * spec.waves)},
+        "e2e": {"value": e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": (achieved / hbm_peak) if achieved else None, "traffic": traffic,
+                     "kernel": "k_extend (closest-hit traversal)",
+                     "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray, "tris_per_ray": tris_per_ray,
+                     "rays_per_launch": rays_per_launch, "launch_ms": launch_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(out))
+    pt.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,262 @@
+/*
+ * pt_b200 -- C ABI of the B200 (sm_100a) path tracer that stands in for the
+ * render path of LSystemEditor's PathTracerLib.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes.  No
+ * CUDA, Qt, OpenGL or torch types cross this boundary (streams are passed as
+ * void*).  Every entry point names the reference interface it replaces
+ * (paths are relative to the reference project root).
+ *
+ * Record layouts are byte-compatible with the reference structs, so a caller
+ * that already fills MaterialGpu / TextureDescGpu / CameraGpu / RenderParamsGpu
+ * can pass them through unchanged.
+ */
+#ifndef PT_B200_H
+#define PT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__cplusplus)
+#define PT_ALIGN16 alignas(16)
+#else
+#define PT_ALIGN16 _Alignas(16)
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes (the reference returns bool + AppLog text; PathTracer.cu:568-574). */
+enum pt_status {
+    PT_OK = 0,
+    PT_ERR_INVALID_ARGUMENT = 1, /* null handle / pointer, bad size              */
+    PT_ERR_CUDA = 2,             /* a CUDA runtime call failed                    */
+    PT_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed                      */
+    PT_ERR_NO_SCENE = 4,         /* render before a scene was set                 */
+    PT_ERR_NOT_CONFIGURED = 5,   /* render before pt_configure                    */
+    PT_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up            */
+    PT_ERR_UNSUPPORTED = 7,      /* feature not available in this build           */
+    PT_ERR_INTERNAL = 8          /* device-side consistency check failed          */
+};
+
+/* ------------------------------------------------------------------------ */
+/* Records.                                                                 */
+
+/* MaterialGpu (PathTracerLib/src/MeshAccel/MeshAccelTypes.h:49-86), 96 bytes.
+ * `sheen` occupies the reference's tail padding (no reference counterpart). */
+typedef struct PT_ALIGN16 pt_material {
+    float r, g, b;
+    float roughness;
+    float metallic;
+    float transmission;
+    float thin;
+    float ior;
+    float subsurface;
+    float emission;
+    float diffuse_roughness;
+    float scatter_radius_r, scatter_radius_g, scatter_radius_b;
+    float specular;
+    uint32_t albedo_tex, roughness_tex, metallic_tex, transmission_tex;
+    uint32_t thin_tex, ior_tex, subsurface_tex, emission_tex;
+    float sheen;
+} pt_material;
+
+/* TextureDescGpu (MeshAccelTypes.h:22-28), 64 bytes. kind: 0 constant scalar,
+ * 1 constant rgb, 2 grid 2D, 3 stripe 1D (MeshAccelTypes.h:13-19). */
+typedef struct PT_ALIGN16 pt_texture {
+    uint32_t kind;
+    uint32_t pad[3];
+    float p0[4];
+    float p1[4];
+    float p2[4];
+} pt_texture;
+
+/* CameraGpu (PathTracerLib/src/CameraGpu.h:5-16), 80 bytes. orientation is a
+ * unit quaternion (w, x, y, z); the camera looks down its local -Z. */
+typedef struct PT_ALIGN16 pt_camera {
+    float position[3];
+    float pad0;
+    float orientation[4];
+    float fov_y;
+    float aspect;
+    float near_plane;
+    float far_plane;
+    float aperture_radius;
+    float focus_distance;
+    float focus_point[3];
+    int32_t focus_valid;
+    float pad1[2];
+} pt_camera;
+
+/* RenderParamsGpu (PathTracerLib/src/RenderTypes.h:15-28): the first 44 bytes
+ * are the reference struct; the tail holds extensions whose zero value keeps
+ * the reference behaviour. 64 bytes. */
+typedef struct pt_render_params {
+    float background_r, background_g, background_b;
+    float environment_intensity;
+    int32_t max_path_depth;             /* 0 = 256 bounces, <0 = 32 (reference default) */
+    int32_t russian_roulette_min_depth; /* <0 = 3 */
+    int32_t min_samples;
+    int32_t max_samples_per_pixel;      /* <=0 = unlimited */
+    int32_t debug_overlay_mode;         /* accepted, display-only in the reference */
+    int32_t brdf_debug_flags;           /* BrdfDebugFlags (Brdf/BrdfDebug.h:6-19) */
+    float relative_error_threshold;
+    /* --- extensions --- */
+    int32_t seed_mode;          /* 0: reference seed (Sampling/RandCore.h:7-12); 1: hash(x, y, seed_value) */
+    uint32_t seed_value;
+    int32_t adaptive_criterion; /* 0: relative std-dev (reference); 1: relative std-error */
+    int32_t samples_per_launch; /* waves traced per launch; 0 = automatic */
+    int32_t reserved;
+} pt_render_params;
+
+/* Triangle soup in structure-of-arrays form: HostMesh + HostTriangle
+ * (Application/src/MeshBuilder/HostMesh.h:9-28). All pointers are HOST memory. */
+typedef struct pt_mesh {
+    uint32_t triangle_count;
+    const float* positions;      /* 9 floats per triangle: v0, v1, v2           */
+    const float* normals;        /* 9 floats per triangle: n0, n1, n2 (shading) */
+    const float* uvs;            /* 6 floats per triangle: uv0, uv1, uv2        */
+    const uint32_t* material_ids;
+    uint32_t material_count;
+    const pt_material* materials;
+    uint32_t texture_count;
+    const pt_texture* textures;
+} pt_mesh;
+
+/* Statistics of the accumulation (PathTracer.h:94-99 plus timings). */
+typedef struct pt_stats {
+    int64_t waves;              /* currentSampleCount: full-resolution waves taken */
+    int64_t active_pixels;      /* currentActivePixelCount                          */
+    int64_t samples;            /* path samples accumulated since reset             */
+    int64_t rays;               /* primary + continuation + shadow rays traced      */
+    int64_t launches;           /* device kernel launches issued                    */
+    double render_ms;           /* device time of the last pt_render call           */
+    double build_ms;            /* device time of the last scene build              */
+    int32_t budget_exhausted;   /* isSampleBudgetExhausted                          */
+    int32_t bvh_nodes;          /* compressed 8-wide nodes                          */
+    int32_t tape_underruns;     /* reserved                                         */
+    int32_t stack_overflows;    /* traversal stack overflows (rays truncated)       */
+} pt_stats;
+
+/* Per-stage device timings and traversal counters of the last pt_render call
+ * (enabled with pt_set_profiling; no reference counterpart beyond the
+ * PATHTRACER_PROFILE wait log of PathTracer.cpp:1087-1123). */
+typedef struct pt_profile {
+    double ms_generate, ms_extend, ms_shade, ms_shadow, ms_finalize, ms_accumulate, ms_compact;
+    int64_t launches_extend, launches_shadow;
+    int64_t rays_extend, rays_shadow;   /* rays traced by the closest-hit / any-hit stages */
+    int64_t nodes_extend, tris_extend;  /* compressed nodes / triangles visited (counting mode) */
+    int64_t nodes_shadow, tris_shadow;
+} pt_profile;
+
+enum pt_profile_flags {
+    PT_PROFILE_STAGE_TIMES = 1,   /* CUDA events around every stage launch */
+    PT_PROFILE_COUNT_VISITS = 2   /* count BVH nodes and triangles visited per stage */
+};
+
+typedef struct pt_renderer pt_renderer;
+
+/* ------------------------------------------------------------------------ */
+/* Renderer object: replaces class PathTracer (PathTracerLib/src/PathTracer.h:30-152). */
+
+/* PathTracer::PathTracer + cudaSetDevice.  device < 0 selects the current one. */
+int pt_create(pt_renderer** out, int device);
+/* PathTracer::~PathTracer. Releases every device buffer. */
+int pt_destroy(pt_renderer* r);
+/* Text of the last error on this renderer (never NULL). */
+const char* pt_last_error(const pt_renderer* r);
+
+/* PathTracer::configure (PathTracer.h:45-51) minus the GL PBOs: allocates the
+ * accumulation state for width x height pixels (PathTracer.cpp:323-419). */
+int pt_configure(pt_renderer* r, int width, int height);
+
+/* MeshAccelScene::build + upload (MeshAccel/MeshAccelScene.h:22-27,
+ * MeshAccelScene.cpp:141-341) and PathTracer::rebuildMeshScene (PathTracer.h:130-132):
+ * uploads the mesh and builds the acceleration structure ON THE GPU
+ * (LBVH -> compressed 8-wide BVH). Resets accumulation. */
+int pt_set_mesh(pt_renderer* r, const pt_mesh* mesh);
+
+/* PathTracer::setCamera / lastSampleCamera (PathTracer.h:101-103). */
+int pt_set_camera(pt_renderer* r, const pt_camera* camera);
+int pt_get_camera(const pt_renderer* r, pt_camera* out);
+
+/* Snapshot of the setters setMaxSamplesPerPixel, setMinSamples,
+ * setRelativeErrorThreshold, setRussianRouletteMinDepth, setBrdfDebugFlags,
+ * setClearColor, setEnvironmentIntensity (PathTracer.h:73-124) as one record
+ * (RenderParamsGpu, RenderTypes.h:15-28). Resets accumulation. */
+int pt_set_params(pt_renderer* r, const pt_render_params* params);
+int pt_get_params(const pt_renderer* r, pt_render_params* out);
+/* RenderParamsGpu{} defaults (RenderTypes.h:15-28) with a zero extension tail. */
+void pt_default_params(pt_render_params* out);
+
+/* PathTracer::setEnvironmentHdrPath (PathTracer.h:115-121) with the decoded
+ * image instead of a file: linear RGB lat-long, width x height x 3 floats
+ * (host). rgb == NULL restores the solid background. Builds the importance
+ * tables of EnvironmentMap.cpp:76-128. Resets accumulation. */
+int pt_set_environment(pt_renderer* r, int width, int height, const float* rgb);
+
+/* PathTracer::resetAccumulation + clearAccumulatorKernel (PathTracer.cu:275-303). */
+int pt_reset(pt_renderer* r);
+
+/* The render loop (PathTracer::renderLoop, PathTracer.cpp:2220-2543) as a
+ * synchronous call: traces `waves` full-resolution adaptive waves, one sample
+ * per active pixel per wave, compacting the active list as it goes. Pixels
+ * stop at max_samples_per_pixel or when converged. waves <= 0 runs until no
+ * pixel is active. */
+int pt_render(pt_renderer* r, int waves);
+
+/* Headless replacement of the PBO publish (PathTracer.cu:464-512): copies the
+ * running-mean RGBA accumulator (float4 per pixel), sample counts and the
+ * convergence mask to HOST memory. Any output pointer may be NULL. */
+int pt_readback(pt_renderer* r, float* rgba, uint32_t* counts, uint8_t* converged);
+
+/* Device pointers of the accumulation state (borrowed; valid until the next
+ * pt_configure / pt_destroy): float4 rgba[P], uint32 counts[P], uint8 converged[P]. */
+int pt_device_buffers(pt_renderer* r, void** rgba, void** counts, void** converged);
+
+/* currentSampleCount / currentActivePixelCount / isSampleBudgetExhausted
+ * (PathTracer.h:94-99) and timings. */
+int pt_get_stats(const pt_renderer* r, pt_stats* out);
+
+/* PathTracer::pickSurface (PathTracer.h:111, PathTracer.cpp:1991-2013) generalised
+ * to n rays: closest hit through the GPU BVH. All pointers HOST memory.
+ * origins/dirs: 3 floats per ray; tmin/tmax per ray. Outputs: hit flag, t,
+ * ORIGINAL triangle index, shading normal (3 floats), uv (2 floats); any
+ * output except hit may be NULL. Semantics of meshAccelTraceRay
+ * (MeshAccel/MeshAccelIntersectCore.h:110-221). */
+int pt_trace_rays(pt_renderer* r, int n, const float* origins, const float* dirs, const float* tmin,
+    const float* tmax, uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv);
+
+/* Same with DEVICE pointers on the given CUDA stream (void* = cudaStream_t). */
+int pt_trace_rays_device(pt_renderer* r, int n, const float* origins, const float* dirs, const float* tmin,
+    const float* tmax, uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, void* stream);
+
+/* Runs all work of the renderer on the caller's CUDA stream (void* =
+ * cudaStream_t; the reference's launch API takes one per call,
+ * PathTracerCuda.h:12-126). NULL restores the renderer's own stream. */
+int pt_set_stream(pt_renderer* r, void* stream);
+
+/* Profiling switches (pt_profile_flags) and the profile of the last pt_render. */
+int pt_set_profiling(pt_renderer* r, int flags);
+int pt_get_profile(const pt_renderer* r, pt_profile* out);
+
+/* Work-size tuning (no reference counterpart): paths in flight per launch
+ * (0 = default 2^21) and resident blocks per SM of the persistent stage grids
+ * (0 = from the occupancy calculator). */
+int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
+
+/* Parity hook (no reference counterpart): writes, for waves [first_wave,
+ * first_wave + waves) and every pixel, the first `stride` uniforms that the
+ * renderer's generator draws for that (pixel, sample) -- curand_init /
+ * curand_uniform with the seed of Sampling/RandCore.h:7-12 -- to HOST memory
+ * laid out [wave][pixel][stride]. The active pixels at the time of the call are
+ * assumed to have counts == first_wave (a fresh accumulation). */
+int pt_rng_tape(pt_renderer* r, int first_wave, int waves, int stride, float* out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* PT_B200_H */

@@ -1,0 +1,1057 @@
+// C ABI (include/pt_b200.h) and the host-side renderer object.
+//
+// The renderer owns every device buffer, one CUDA stream and its events, like
+// the reference's PathTracer (PathTracerLib/src/PathTracer.cpp:40-122), but
+// runs synchronously: pt_render replaces the worker thread's render loop
+// (PathTracer.cpp:2220-2543) with a loop over batches of waves.
+#include "pt_bvh.cuh"
+#include "pt_render.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace pt;
+
+namespace {
+
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    bool ensure(size_t count)
+    {
+        if (count <= n && p != nullptr) {
+            return true;
+        }
+        release();
+        if (count == 0) {
+            count = 1;
+        }
+        if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+            p = nullptr;
+            n = 0;
+            return false;
+        }
+        n = count;
+        return true;
+    }
+    void release()
+    {
+        if (p != nullptr) {
+            cudaFree(p);
+        }
+        p = nullptr;
+        n = 0;
+    }
+};
+
+} // namespace
+
+struct pt_renderer {
+    int device = 0;
+    cudaStream_t stream = nullptr;      // stream all work is issued on
+    cudaStream_t ownStream = nullptr;   // the renderer's own stream
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string lastError = "";
+    int smCount = 148;
+
+    // scene
+    DevBuf<float> positions;      // 9 floats per triangle, original order
+    DevBuf<TriShade> shade;
+    DevBuf<pt_material> materials;
+    DevBuf<pt_texture> textures;
+    DevBuf<uint32_t> emissiveIdx;
+    DevBuf<float> emissiveCdf;
+    DevBuf<float> stage;          // upload staging (normals / uvs)
+    DevBuf<uint32_t> stageIds;
+    BvhBuffers bvh;
+    BvhBuildOptions bvhOptions;
+    uint32_t triCount = 0;
+    uint32_t materialCount = 0;
+    uint32_t textureCount = 0;
+    uint32_t emissiveCount = 0;
+    bool hasScene = false;
+
+    // environment
+    DevBuf<float> envPixels, envMarginal, envRow;
+    int envW = 0, envH = 0;
+    bool envValid = false;
+
+    // accumulation
+    int width = 0, height = 0;
+    DevBuf<float4> acc;
+    DevBuf<uint32_t> counts;
+    DevBuf<float> lumMean, m2;
+    DevBuf<uint8_t> converged;
+    DevBuf<int> active0, active1, activeCount;
+    DevBuf<float4> samples;
+    int activeSel = 0;
+    int hostActive = 0;
+    int64_t wavesDone = 0;
+    int64_t samplesDone = 0;
+
+    // paths
+    int capacity = 0;
+    DevBuf<uint32_t> pPixel, pOut;
+    DevBuf<uint4> pRngA;
+    DevBuf<uint2> pRngB;
+    DevBuf<float4> pOrig, pDir, pThr, pRad, pHit, pNeeEnv, pNeeEmis;
+    DevBuf<uint8_t> pVisEnv, pVisEmis;
+    DevBuf<uint32_t> qExt0, qExt1, qFinish, qShadowPath;
+    DevBuf<float4> qShadowO, qShadowD;
+    DevBuf<unsigned int> qCounts;
+    DevBuf<unsigned long long> qRays;     // [0] extend, [1] shadow
+    DevBuf<unsigned long long> qVisits;   // [0..1] extend nodes/tris, [2..3] shadow nodes/tris
+    DevBuf<unsigned int> qOverflow;
+    int gridExtend = 0, gridShade = 0, gridShadow = 0;
+    int capacityWanted = 1 << 21;
+    int blocksPerSmOverride = 0;
+
+    // profiling
+    int profileFlags = 0;
+    pt_profile profile{};
+    std::vector<cudaEvent_t> eventPool;
+    std::vector<std::pair<int, int>> eventMarks; // (stage, first event index)
+
+    pt_camera camera{};
+    pt_render_params params{};
+
+    pt_stats stats{};
+    int64_t launches = 0;
+};
+
+namespace {
+
+int fail(pt_renderer* r, int code, const char* fmt, ...)
+{
+    if (r != nullptr) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        r->lastError = buf;
+    }
+    return code;
+}
+
+int cudaFail(pt_renderer* r, cudaError_t e, const char* what)
+{
+    return fail(r, e == cudaErrorMemoryAllocation ? PT_ERR_OUT_OF_MEMORY : PT_ERR_CUDA, "%s: %s", what,
+        cudaGetErrorString(e));
+}
+
+#define PT_CHECK(r, call)                                                                                         \
+    do {                                                                                                          \
+        cudaError_t e_ = (call);                                                                                  \
+        if (e_ != cudaSuccess) {                                                                                  \
+            return cudaFail((r), e_, #call);                                                                      \
+        }                                                                                                         \
+    } while (0)
+
+__global__ void k_build_shade(const float* nrm, const float* uv, const uint32_t* mat, uint32_t n, TriShade* out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* a = nrm + 9ull * i;
+        const float* t = uv + 6ull * i;
+        TriShade s;
+        s.a = make_float4(a[0], a[1], a[2], t[0]);
+        s.b = make_float4(a[3], a[4], a[5], t[1]);
+        s.c = make_float4(a[6], a[7], a[8], t[2]);
+        s.d = make_float4(t[3], t[4], t[5], __uint_as_float(mat[i]));
+        out[i] = s;
+    }
+}
+
+pt_material defaultMaterial()
+{
+    // MeshAccelScene.cpp:27-46 / MaterialGpu{} defaults.
+    pt_material m{};
+    m.r = m.g = m.b = 0.8f;
+    m.roughness = 0.5f;
+    m.ior = 1.5f;
+    m.diffuse_roughness = -1.0f;
+    m.specular = 1.0f;
+    return m;
+}
+
+DevScene deviceScene(const pt_renderer* r)
+{
+    DevScene s;
+    s.nodes = r->bvh.nodes;
+    s.tris = r->bvh.tris;
+    s.shade = r->shade.p;
+    s.origVerts = reinterpret_cast<const float4*>(r->positions.p);
+    s.materials = r->materials.p;
+    s.textures = r->textureCount ? r->textures.p : nullptr;
+    s.emissiveIdx = r->emissiveIdx.p;
+    s.emissiveCdf = r->emissiveCdf.p;
+    s.nodeCount = r->hasScene ? r->bvh.nodeCount : 0u;
+    s.triCount = r->triCount;
+    s.materialCount = r->materialCount;
+    s.textureCount = r->textureCount;
+    s.emissiveCount = r->emissiveCount;
+    return s;
+}
+
+int ensurePaths(pt_renderer* r, int capacity)
+{
+    if (r->capacity >= capacity) {
+        return PT_OK;
+    }
+    const size_t Q = static_cast<size_t>(capacity);
+    bool ok = r->pPixel.ensure(Q) && r->pOut.ensure(Q) && r->pRngA.ensure(Q) && r->pRngB.ensure(Q) &&
+        r->pOrig.ensure(Q) && r->pDir.ensure(Q) && r->pThr.ensure(Q) && r->pRad.ensure(Q) && r->pHit.ensure(Q) &&
+        r->pNeeEnv.ensure(Q) && r->pNeeEmis.ensure(Q) && r->pVisEnv.ensure(Q) && r->pVisEmis.ensure(Q) &&
+        r->qExt0.ensure(Q) && r->qExt1.ensure(Q) && r->qFinish.ensure(Q) && r->qShadowPath.ensure(2 * Q) &&
+        r->qShadowO.ensure(2 * Q) && r->qShadowD.ensure(2 * Q) && r->qCounts.ensure(8) && r->qRays.ensure(2) &&
+        r->qVisits.ensure(4) && r->qOverflow.ensure(1);
+    if (!ok) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "path state allocation failed for %d paths", capacity);
+    }
+    r->capacity = capacity;
+    return PT_OK;
+}
+
+LaunchCtx makeCtx(pt_renderer* r)
+{
+    LaunchCtx c{};
+    c.scene = deviceScene(r);
+    c.env.pixels = r->envPixels.p;
+    c.env.marginal = r->envMarginal.p;
+    c.env.row = r->envRow.p;
+    c.env.width = r->envW;
+    c.env.height = r->envH;
+    c.env.valid = r->envValid ? 1 : 0;
+    c.cam = r->camera;
+    c.params = r->params;
+    c.width = r->width;
+    c.height = r->height;
+    c.maxDepth = r->params.max_path_depth > 0 ? r->params.max_path_depth : (r->params.max_path_depth == 0 ? 256 : 32);
+    c.rrMinDepth = r->params.russian_roulette_min_depth >= 0 ? r->params.russian_roulette_min_depth : 3;
+    c.paths.pixel = r->pPixel.p;
+    c.paths.outIdx = r->pOut.p;
+    c.paths.rngA = r->pRngA.p;
+    c.paths.rngB = r->pRngB.p;
+    c.paths.orig = r->pOrig.p;
+    c.paths.dir = r->pDir.p;
+    c.paths.thr = r->pThr.p;
+    c.paths.rad = r->pRad.p;
+    c.paths.hit = r->pHit.p;
+    c.paths.neeEnv = r->pNeeEnv.p;
+    c.paths.neeEmis = r->pNeeEmis.p;
+    c.paths.visEnv = r->pVisEnv.p;
+    c.paths.visEmis = r->pVisEmis.p;
+    c.paths.capacity = r->capacity;
+    c.q.extend[0] = r->qExt0.p;
+    c.q.extend[1] = r->qExt1.p;
+    c.q.finish = r->qFinish.p;
+    c.q.shadowPath = r->qShadowPath.p;
+    c.q.shadowOrig = r->qShadowO.p;
+    c.q.shadowDir = r->qShadowD.p;
+    c.q.counts = r->qCounts.p;
+    c.q.rays = r->qRays.p;
+    c.q.visits = r->qVisits.p;
+    c.q.overflow = r->qOverflow.p;
+    c.acc.acc = r->acc.p;
+    c.acc.counts = r->counts.p;
+    c.acc.lumMean = r->lumMean.p;
+    c.acc.m2 = r->m2.p;
+    c.acc.converged = r->converged.p;
+    c.acc.active[0] = r->active0.p;
+    c.acc.active[1] = r->active1.p;
+    c.acc.activeCount = r->activeCount.p;
+    c.acc.samples = r->samples.p;
+    c.acc.sampleCapacity = r->samples.n;
+    c.activeSel = r->activeSel;
+    return c;
+}
+
+int resetAccum(pt_renderer* r)
+{
+    if (r->width <= 0) {
+        return PT_OK;
+    }
+    LaunchCtx c = makeCtx(r);
+    c.activeSel = 0;
+    r->activeSel = 0;
+    launchResetAccum(c, r->width * r->height, r->stream);
+    PT_CHECK(r, cudaGetLastError());
+    r->hostActive = r->width * r->height;
+    r->wavesDone = 0;
+    r->samplesDone = 0;
+    return PT_OK;
+}
+
+enum Stage { kGenerate = 0, kExtend, kShade, kShadow, kFinalize, kAccumulate, kCompact, kStageCount };
+
+// Stage timing: a pair of events around each launch when profiling is on.
+struct StageTimer {
+    pt_renderer* r;
+    int idx = -1;
+    int stage;
+    StageTimer(pt_renderer* rr, int st) : r(rr), stage(st)
+    {
+        if (!(r->profileFlags & PT_PROFILE_STAGE_TIMES)) {
+            return;
+        }
+        const size_t need = r->eventMarks.size() * 2 + 2;
+        while (r->eventPool.size() < need) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                return;
+            }
+            r->eventPool.push_back(e);
+        }
+        idx = static_cast<int>(r->eventMarks.size()) * 2;
+        cudaEventRecord(r->eventPool[idx], r->stream);
+    }
+    ~StageTimer()
+    {
+        if (idx >= 0) {
+            cudaEventRecord(r->eventPool[idx + 1], r->stream);
+            r->eventMarks.emplace_back(stage, idx);
+        }
+    }
+};
+
+void collectStageTimes(pt_renderer* r)
+{
+    double* ms[kStageCount] = {&r->profile.ms_generate, &r->profile.ms_extend, &r->profile.ms_shade,
+        &r->profile.ms_shadow, &r->profile.ms_finalize, &r->profile.ms_accumulate, &r->profile.ms_compact};
+    for (const auto& m : r->eventMarks) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, r->eventPool[m.second], r->eventPool[m.second + 1]) == cudaSuccess) {
+            *ms[m.first] += t;
+        }
+    }
+    r->eventMarks.clear();
+}
+
+// Number of waves folded into one launch (see the render loop comment).
+int chooseBatch(const pt_renderer* r, int remaining)
+{
+    const pt_render_params& p = r->params;
+    int B;
+    if (p.samples_per_launch > 0) {
+        B = p.samples_per_launch;
+    } else if (r->wavesDone < p.min_samples) {
+        B = static_cast<int>(p.min_samples - r->wavesDone); // nothing can converge before min_samples
+    } else {
+        B = 4; // convergence is tested every 4 samples: no sample is wasted
+    }
+    if (p.max_samples_per_pixel > 0) {
+        B = std::min<int64_t>(B, p.max_samples_per_pixel - r->wavesDone);
+    }
+    if (remaining > 0) {
+        B = std::min(B, remaining);
+    }
+    // cap the sample buffer at ~1 GiB
+    const int64_t cap = std::max<int64_t>(1, (int64_t(1) << 30) / (16 * std::max(1, r->hostActive)));
+    B = static_cast<int>(std::min<int64_t>(B, std::min<int64_t>(cap, 1024)));
+    return std::max(B, 1);
+}
+
+} // namespace
+
+extern "C" {
+
+int pt_create(pt_renderer** out, int device)
+{
+    if (out == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    pt_renderer* r = new pt_renderer();
+    if (device < 0) {
+        if (cudaGetDevice(&r->device) != cudaSuccess) {
+            delete r;
+            return PT_ERR_CUDA;
+        }
+    } else {
+        r->device = device;
+    }
+    if (cudaSetDevice(r->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&r->ownStream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess) {
+        delete r;
+        return PT_ERR_CUDA;
+    }
+    r->stream = r->ownStream;
+    cudaDeviceGetAttribute(&r->smCount, cudaDevAttrMultiProcessorCount, r->device);
+    pt_default_params(&r->params);
+    r->camera.orientation[0] = 1.0f;
+    r->camera.fov_y = 0.7f;
+    r->camera.aspect = 1.0f;
+    r->camera.near_plane = 0.1f;
+    r->camera.far_plane = 1000.0f;
+    int be = 1, bs = 1, bsh = 1;
+    stageOccupancy(be, bs, bsh);
+    r->gridExtend = r->smCount * std::max(be, 1);
+    r->gridShade = r->smCount * std::max(bs, 1);
+    r->gridShadow = r->smCount * std::max(bsh, 1);
+    *out = r;
+    return PT_OK;
+}
+
+int pt_destroy(pt_renderer* r)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(r->device);
+    if (r->stream) {
+        cudaStreamSynchronize(r->stream);
+    }
+    r->positions.release();
+    r->shade.release();
+    r->materials.release();
+    r->textures.release();
+    r->emissiveIdx.release();
+    r->emissiveCdf.release();
+    r->stage.release();
+    r->stageIds.release();
+    r->bvh.release();
+    r->bvh.scratch.release();
+    r->envPixels.release();
+    r->envMarginal.release();
+    r->envRow.release();
+    r->acc.release();
+    r->counts.release();
+    r->lumMean.release();
+    r->m2.release();
+    r->converged.release();
+    r->active0.release();
+    r->active1.release();
+    r->activeCount.release();
+    r->samples.release();
+    r->pPixel.release();
+    r->pOut.release();
+    r->pRngA.release();
+    r->pRngB.release();
+    r->pOrig.release();
+    r->pDir.release();
+    r->pThr.release();
+    r->pRad.release();
+    r->pHit.release();
+    r->pNeeEnv.release();
+    r->pNeeEmis.release();
+    r->pVisEnv.release();
+    r->pVisEmis.release();
+    r->qExt0.release();
+    r->qExt1.release();
+    r->qFinish.release();
+    r->qShadowPath.release();
+    r->qShadowO.release();
+    r->qShadowD.release();
+    r->qCounts.release();
+    r->qRays.release();
+    r->qVisits.release();
+    r->qOverflow.release();
+    for (cudaEvent_t e : r->eventPool) {
+        cudaEventDestroy(e);
+    }
+    if (r->ev0) {
+        cudaEventDestroy(r->ev0);
+    }
+    if (r->ev1) {
+        cudaEventDestroy(r->ev1);
+    }
+    if (r->ownStream) {
+        cudaStreamDestroy(r->ownStream);
+    }
+    delete r;
+    return PT_OK;
+}
+
+const char* pt_last_error(const pt_renderer* r)
+{
+    return r == nullptr ? "null renderer" : r->lastError.c_str();
+}
+
+void pt_default_params(pt_render_params* out)
+{
+    if (out == nullptr) {
+        return;
+    }
+    std::memset(out, 0, sizeof(*out));
+    out->background_r = out->background_g = out->background_b = 10.0f / 255.0f;
+    out->environment_intensity = 1.0f;
+    out->max_path_depth = 32;
+    out->russian_roulette_min_depth = 3;
+    out->min_samples = 16;
+    out->max_samples_per_pixel = 1024;
+    out->relative_error_threshold = 0.02f;
+}
+
+int pt_configure(pt_renderer* r, int width, int height)
+{
+    if (r == nullptr || width <= 0 || height <= 0 || static_cast<int64_t>(width) * height > (int64_t(1) << 30)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_configure: bad size %dx%d", width, height);
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const size_t P = static_cast<size_t>(width) * height;
+    if (!(r->acc.ensure(P) && r->counts.ensure(P) && r->lumMean.ensure(P) && r->m2.ensure(P) && r->converged.ensure(P) &&
+            r->active0.ensure(P) && r->active1.ensure(P) && r->activeCount.ensure(4))) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "accumulator allocation failed for %dx%d", width, height);
+    }
+    r->width = width;
+    r->height = height;
+    int st = resetAccum(r);
+    if (st != PT_OK) {
+        return st;
+    }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    return PT_OK;
+}
+
+int pt_set_mesh(pt_renderer* r, const pt_mesh* mesh)
+{
+    if (r == nullptr || mesh == nullptr) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: null argument");
+    }
+    const uint32_t n = mesh->triangle_count;
+    if (n > 0 && (mesh->positions == nullptr || mesh->normals == nullptr || mesh->uvs == nullptr ||
+                     mesh->material_ids == nullptr)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: missing per-triangle arrays");
+    }
+    if ((mesh->material_count > 0 && mesh->materials == nullptr) || (mesh->texture_count > 0 && mesh->textures == nullptr)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: missing material or texture bank");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = r->stream;
+    PT_CHECK(r, cudaEventRecord(r->ev0, s));
+    r->hasScene = false;
+    r->triCount = n;
+    // materials: MeshAccelScene::build adds one default material when none is given
+    std::vector<pt_material> mats(mesh->materials, mesh->materials + mesh->material_count);
+    if (mats.empty()) {
+        mats.push_back(defaultMaterial());
+    }
+    r->materialCount = static_cast<uint32_t>(mats.size());
+    if (!r->materials.ensure(mats.size())) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "material upload failed");
+    }
+    PT_CHECK(r, cudaMemcpyAsync(r->materials.p, mats.data(), mats.size() * sizeof(pt_material), cudaMemcpyHostToDevice, s));
+    r->textureCount = mesh->texture_count;
+    if (mesh->texture_count > 0) {
+        if (!r->textures.ensure(mesh->texture_count)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "texture upload failed");
+        }
+        PT_CHECK(r, cudaMemcpyAsync(r->textures.p, mesh->textures, mesh->texture_count * sizeof(pt_texture),
+            cudaMemcpyHostToDevice, s));
+    }
+    // emissive list + CDF: sequential float prefix sum exactly as MeshAccelScene.cpp:62-95
+    std::vector<uint32_t> eIdx;
+    std::vector<float> eCdf(1, 0.0f);
+    float total = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t mi = mesh->material_ids[i];
+        if (mi >= mats.size()) {
+            continue;
+        }
+        const pt_material& m = mats[mi];
+        const float lum = m.emission * (0.2126f * m.r + 0.7152f * m.g + 0.0722f * m.b);
+        if (lum <= 0.0f) {
+            continue;
+        }
+        const float* p = mesh->positions + 9ull * i;
+        const float e1x = p[3] - p[0], e1y = p[4] - p[1], e1z = p[5] - p[2];
+        const float e2x = p[6] - p[0], e2y = p[7] - p[1], e2z = p[8] - p[2];
+        const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+        const float area = 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
+        const float w = area * lum;
+        if (w <= 0.0f) {
+            continue;
+        }
+        eIdx.push_back(i);
+        total += w;
+        eCdf.push_back(total);
+    }
+    if (total <= 0.0f) {
+        eIdx.clear();
+        eCdf.assign(1, 0.0f);
+    }
+    r->emissiveCount = static_cast<uint32_t>(eIdx.size());
+    if (!r->emissiveIdx.ensure(std::max<size_t>(1, eIdx.size())) || !r->emissiveCdf.ensure(eCdf.size())) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list upload failed");
+    }
+    if (!eIdx.empty()) {
+        PT_CHECK(r, cudaMemcpyAsync(r->emissiveIdx.p, eIdx.data(), eIdx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    }
+    PT_CHECK(r, cudaMemcpyAsync(r->emissiveCdf.p, eCdf.data(), eCdf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    if (n > 0) {
+        if (!r->positions.ensure(9ull * n) || !r->shade.ensure(n) || !r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "mesh upload failed for %u triangles", n);
+        }
+        PT_CHECK(r, cudaMemcpyAsync(r->positions.p, mesh->positions, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p, mesh->normals, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9ull * n, mesh->uvs, 6ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stageIds.p, mesh->material_ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        const int grid = static_cast<int>(std::min<uint32_t>((n + 255) / 256, 148u * 16u));
+        k_build_shade<<<grid, 256, 0, s>>>(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, r->shade.p);
+        PT_CHECK(r, cudaGetLastError());
+        char err[256] = {0};
+        const int st = buildBvh(r->positions.p, n, r->bvh, s, r->bvhOptions, err, sizeof(err));
+        if (st != PT_OK) {
+            return fail(r, st, "BVH build: %s", err);
+        }
+    } else {
+        r->bvh.release();
+    }
+    PT_CHECK(r, cudaEventRecord(r->ev1, s));
+    PT_CHECK(r, cudaEventSynchronize(r->ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+    r->stats.build_ms = ms;
+    r->stats.bvh_nodes = static_cast<int32_t>(r->bvh.nodeCount);
+    r->hasScene = true;
+    return resetAccum(r);
+}
+
+int pt_set_camera(pt_renderer* r, const pt_camera* camera)
+{
+    if (r == nullptr || camera == nullptr) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_camera: null argument");
+    }
+    r->camera = *camera;
+    return resetAccum(r);
+}
+
+int pt_get_camera(const pt_renderer* r, pt_camera* out)
+{
+    if (r == nullptr || out == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    *out = r->camera;
+    return PT_OK;
+}
+
+int pt_set_params(pt_renderer* r, const pt_render_params* params)
+{
+    if (r == nullptr || params == nullptr) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_params: null argument");
+    }
+    r->params = *params;
+    return resetAccum(r);
+}
+
+int pt_get_params(const pt_renderer* r, pt_render_params* out)
+{
+    if (r == nullptr || out == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    *out = r->params;
+    return PT_OK;
+}
+
+int pt_set_environment(pt_renderer* r, int width, int height, const float* rgb)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    if (rgb == nullptr) {
+        r->envValid = false;
+        return resetAccum(r);
+    }
+    if (width <= 0 || height <= 0) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_environment: bad size %dx%d", width, height);
+    }
+    // importance tables, EnvironmentMap.cpp:76-128 (sequential float sums)
+    const size_t W = static_cast<size_t>(width), H = static_cast<size_t>(height);
+    std::vector<float> marginal(H + 1, 0.0f), row(H * (W + 1), 0.0f), rowW(H, 0.0f);
+    for (size_t y = 0; y < H; ++y) {
+        const float v = (static_cast<float>(y) + 0.5f) / static_cast<float>(height);
+        const float st = std::sin(v * 3.14159265f);
+        float sum = 0.0f;
+        const size_t off = y * (W + 1);
+        for (size_t x = 0; x < W; ++x) {
+            const float* px = rgb + (y * W + x) * 3;
+            const float l = std::max(px[0], std::max(px[1], px[2]));
+            sum += std::max(l, 1.0e-6f) * st;
+            row[off + x + 1] = sum;
+        }
+        if (sum > 0.0f) {
+            for (size_t x = 0; x < W; ++x) {
+                row[off + x + 1] /= sum;
+            }
+        }
+        rowW[y] = sum;
+    }
+    float total = 0.0f;
+    for (size_t y = 0; y < H; ++y) {
+        total += rowW[y];
+        marginal[y + 1] = total;
+    }
+    if (total > 0.0f) {
+        for (size_t y = 0; y < H; ++y) {
+            marginal[y + 1] /= total;
+        }
+    }
+    if (!r->envPixels.ensure(W * H * 3) || !r->envMarginal.ensure(H + 1) || !r->envRow.ensure(H * (W + 1))) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "environment upload failed");
+    }
+    PT_CHECK(r, cudaMemcpyAsync(r->envPixels.p, rgb, W * H * 3 * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PT_CHECK(r, cudaMemcpyAsync(r->envMarginal.p, marginal.data(), marginal.size() * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PT_CHECK(r, cudaMemcpyAsync(r->envRow.p, row.data(), row.size() * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    r->envW = width;
+    r->envH = height;
+    r->envValid = true;
+    return resetAccum(r);
+}
+
+int pt_reset(pt_renderer* r)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    return resetAccum(r);
+}
+
+// Render loop.  Each iteration folds B waves into one launch sequence: the
+// active pixels x B samples are generated (in chunks of the path capacity),
+// traced bounce by bounce, then folded per pixel in sample order and the
+// active list compacted.  Wave w of the reference uses globalSeed = w + 1 and
+// sampleIndex = counts[pixel] (PathTracer.cpp:2379, RandCore.h:7-12); an
+// active pixel has counts == w, so slot s of a batch starting at wave W uses
+// exactly the reference's seed for wave W + s.  Pixels that converge inside a
+// batch ignore the batch's remaining samples, which is what the reference's
+// per-wave convergence skip does.
+int pt_render(pt_renderer* r, int waves)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    if (r->width <= 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_render before pt_configure");
+    }
+    if (!r->hasScene) {
+        return fail(r, PT_ERR_NO_SCENE, "pt_render before pt_set_mesh");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = r->stream;
+    int st = ensurePaths(r, r->capacityWanted);
+    if (st != PT_OK) {
+        return st;
+    }
+    const bool countVisits = (r->profileFlags & PT_PROFILE_COUNT_VISITS) != 0;
+    r->profile = pt_profile{};
+    r->eventMarks.clear();
+    PT_CHECK(r, cudaMemsetAsync(r->qRays.p, 0, 2 * sizeof(unsigned long long), s));
+    PT_CHECK(r, cudaMemsetAsync(r->qVisits.p, 0, 4 * sizeof(unsigned long long), s));
+    PT_CHECK(r, cudaMemsetAsync(r->qOverflow.p, 0, sizeof(unsigned int), s));
+    PT_CHECK(r, cudaEventRecord(r->ev0, s));
+    int remaining = waves;
+    int64_t launches = 0;
+    const int maxDepthEff = r->params.max_path_depth > 0 ? r->params.max_path_depth : (r->params.max_path_depth == 0 ? 256 : 32);
+    while ((waves <= 0 || remaining > 0) && r->hostActive > 0) {
+        const int active = r->hostActive;
+        const int B = chooseBatch(r, waves > 0 ? remaining : 0);
+        const size_t need = static_cast<size_t>(active) * B;
+        if (!r->samples.ensure(need)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "sample buffer allocation failed (%zu samples)", need);
+        }
+        const long long jobs = static_cast<long long>(active) * B;
+        const int chunkCap = std::min(r->capacity, r->capacityWanted);
+        for (long long start = 0; start < jobs; start += chunkCap) {
+            const int chunk = static_cast<int>(std::min<long long>(chunkCap, jobs - start));
+            LaunchCtx c = makeCtx(r);
+            {
+                StageTimer tm(r, kGenerate);
+                launchGenerate(c, start, chunk, active, static_cast<uint32_t>(r->wavesDone), 0, s);
+            }
+            ++launches;
+            int sel = 0;
+            for (int depth = 0; depth <= maxDepthEff; ++depth) {
+                const bool identity = depth == 0;
+                {
+                    StageTimer tm(r, kExtend);
+                    launchExtend(c, sel, identity, r->gridExtend, countVisits, s);
+                }
+                {
+                    StageTimer tm(r, kShade);
+                    launchShade(c, sel, identity, r->gridShade, s);
+                }
+                launches += 2;
+                r->profile.launches_extend += 1;
+                if (depth < maxDepthEff) {
+                    {
+                        StageTimer tm(r, kShadow);
+                        launchShadow(c, r->gridShadow, countVisits, s);
+                    }
+                    {
+                        StageTimer tm(r, kFinalize);
+                        launchFinalize(c, r->gridShadow, s);
+                    }
+                    launches += 2;
+                    r->profile.launches_shadow += 1;
+                }
+                sel ^= 1;
+                if (depth >= 3 && (depth & 3) == 3 && depth < maxDepthEff) {
+                    unsigned int live = 0;
+                    PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p + sel, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+                    PT_CHECK(r, cudaStreamSynchronize(s));
+                    if (live == 0) {
+                        break;
+                    }
+                }
+            }
+            PT_CHECK(r, cudaGetLastError());
+        }
+        LaunchCtx c = makeCtx(r);
+        {
+            StageTimer tm(r, kAccumulate);
+            launchAccumulate(c, active, B, s);
+        }
+        PT_CHECK(r, cudaMemsetAsync(r->activeCount.p + 1, 0, sizeof(int), s));
+        {
+            StageTimer tm(r, kCompact);
+            launchCompact(c, active, s);
+        }
+        launches += 2;
+        int next = 0;
+        PT_CHECK(r, cudaMemcpyAsync(&next, r->activeCount.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PT_CHECK(r, cudaStreamSynchronize(s));
+        PT_CHECK(r, cudaGetLastError());
+        r->activeSel ^= 1;
+        r->hostActive = next;
+        r->wavesDone += B;
+        r->samplesDone += jobs;
+        if (waves > 0) {
+            remaining -= B;
+        }
+    }
+    PT_CHECK(r, cudaEventRecord(r->ev1, s));
+    PT_CHECK(r, cudaEventSynchronize(r->ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+    unsigned long long rays[2] = {0, 0};
+    unsigned long long visits[4] = {0, 0, 0, 0};
+    unsigned int overflow = 0;
+    PT_CHECK(r, cudaMemcpy(rays, r->qRays.p, sizeof(rays), cudaMemcpyDeviceToHost));
+    PT_CHECK(r, cudaMemcpy(visits, r->qVisits.p, sizeof(visits), cudaMemcpyDeviceToHost));
+    PT_CHECK(r, cudaMemcpy(&overflow, r->qOverflow.p, sizeof(overflow), cudaMemcpyDeviceToHost));
+    collectStageTimes(r);
+    r->profile.rays_extend = static_cast<int64_t>(rays[0]);
+    r->profile.rays_shadow = static_cast<int64_t>(rays[1]);
+    r->profile.nodes_extend = static_cast<int64_t>(visits[0]);
+    r->profile.tris_extend = static_cast<int64_t>(visits[1]);
+    r->profile.nodes_shadow = static_cast<int64_t>(visits[2]);
+    r->profile.tris_shadow = static_cast<int64_t>(visits[3]);
+    r->stats.render_ms = ms;
+    r->stats.rays += static_cast<int64_t>(rays[0] + rays[1]);
+    r->stats.stack_overflows += static_cast<int32_t>(overflow);
+    r->launches += launches;
+    return PT_OK;
+}
+
+int pt_readback(pt_renderer* r, float* rgba, uint32_t* counts, uint8_t* converged)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    if (r->width <= 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_readback before pt_configure");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const size_t P = static_cast<size_t>(r->width) * r->height;
+    if (rgba) {
+        PT_CHECK(r, cudaMemcpyAsync(rgba, r->acc.p, P * sizeof(float4), cudaMemcpyDeviceToHost, r->stream));
+    }
+    if (counts) {
+        PT_CHECK(r, cudaMemcpyAsync(counts, r->counts.p, P * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream));
+    }
+    if (converged) {
+        PT_CHECK(r, cudaMemcpyAsync(converged, r->converged.p, P, cudaMemcpyDeviceToHost, r->stream));
+    }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    return PT_OK;
+}
+
+int pt_device_buffers(pt_renderer* r, void** rgba, void** counts, void** converged)
+{
+    if (r == nullptr || r->width <= 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_device_buffers before pt_configure");
+    }
+    if (rgba) {
+        *rgba = r->acc.p;
+    }
+    if (counts) {
+        *counts = r->counts.p;
+    }
+    if (converged) {
+        *converged = r->converged.p;
+    }
+    return PT_OK;
+}
+
+int pt_get_stats(const pt_renderer* r, pt_stats* out)
+{
+    if (r == nullptr || out == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    *out = r->stats;
+    out->waves = r->wavesDone;
+    out->active_pixels = r->hostActive;
+    out->samples = r->samplesDone;
+    out->launches = r->launches;
+    out->budget_exhausted = r->hostActive <= 0 ? 1 : 0;
+    return PT_OK;
+}
+
+int pt_trace_rays_device(pt_renderer* r, int n, const float* origins, const float* dirs, const float* tmin,
+    const float* tmax, uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, void* stream)
+{
+    if (r == nullptr || n < 0 || (n > 0 && (origins == nullptr || dirs == nullptr || tmin == nullptr || tmax == nullptr ||
+                                              hit == nullptr))) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_trace_rays: bad arguments");
+    }
+    if (!r->hasScene) {
+        return fail(r, PT_ERR_NO_SCENE, "pt_trace_rays before pt_set_mesh");
+    }
+    if (n == 0) {
+        return PT_OK;
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : r->stream;
+    launchTraceRays(deviceScene(r), n, origins, dirs, tmin, tmax, hit, t, tri, normal, uv, s);
+    PT_CHECK(r, cudaGetLastError());
+    return PT_OK;
+}
+
+int pt_trace_rays(pt_renderer* r, int n, const float* origins, const float* dirs, const float* tmin, const float* tmax,
+    uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv)
+{
+    if (r == nullptr || n < 0 || (n > 0 && (origins == nullptr || dirs == nullptr || tmin == nullptr || tmax == nullptr ||
+                                              hit == nullptr))) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_trace_rays: bad arguments");
+    }
+    if (!r->hasScene) {
+        return fail(r, PT_ERR_NO_SCENE, "pt_trace_rays before pt_set_mesh");
+    }
+    if (n == 0) {
+        return PT_OK;
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const size_t N = static_cast<size_t>(n);
+    // one staging allocation: inputs 8 floats, outputs 1 byte + 7 words per ray
+    const size_t bytes = N * (8 * sizeof(float) + 7 * sizeof(float) + 16);
+    void* buf = nullptr;
+    PT_CHECK(r, cudaMallocAsync(&buf, bytes, r->stream));
+    float* dO = static_cast<float*>(buf);
+    float* dD = dO + 3 * N;
+    float* dTmin = dD + 3 * N;
+    float* dTmax = dTmin + N;
+    float* dT = dTmax + N;
+    uint32_t* dTri = reinterpret_cast<uint32_t*>(dT + N);
+    float* dN = reinterpret_cast<float*>(dTri + N);
+    float* dUv = dN + 3 * N;
+    uint8_t* dHit = reinterpret_cast<uint8_t*>(dUv + 2 * N);
+    cudaStream_t s = r->stream;
+    int rc = PT_OK;
+    cudaError_t e = cudaMemcpyAsync(dO, origins, 3 * N * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dD, dirs, 3 * N * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dTmin, tmin, N * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dTmax, tmax, N * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        launchTraceRays(deviceScene(r), n, dO, dD, dTmin, dTmax, dHit, dT, dTri, dN, dUv, s);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hit, dHit, N, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && t) e = cudaMemcpyAsync(t, dT, N * sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && tri) e = cudaMemcpyAsync(tri, dTri, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && normal) e = cudaMemcpyAsync(normal, dN, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && uv) e = cudaMemcpyAsync(uv, dUv, 2 * N * sizeof(float), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(buf, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) {
+        e = e2;
+    }
+    if (e != cudaSuccess) {
+        rc = cudaFail(r, e, "pt_trace_rays");
+    }
+    return rc;
+}
+
+int pt_set_stream(pt_renderer* r, void* stream)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    r->stream = stream ? static_cast<cudaStream_t>(stream) : r->ownStream;
+    return PT_OK;
+}
+
+int pt_set_profiling(pt_renderer* r, int flags)
+{
+    if (r == nullptr || (flags & ~(PT_PROFILE_STAGE_TIMES | PT_PROFILE_COUNT_VISITS)) != 0) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_profiling: unknown flags %d", flags);
+    }
+    r->profileFlags = flags;
+    return PT_OK;
+}
+
+int pt_get_profile(const pt_renderer* r, pt_profile* out)
+{
+    if (r == nullptr || out == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    *out = r->profile;
+    return PT_OK;
+}
+
+int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
+{
+    if (r == nullptr || path_capacity < 0 || blocks_per_sm < 0 || path_capacity > (1 << 26)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_tuning: bad arguments");
+    }
+    r->capacityWanted = path_capacity > 0 ? path_capacity : (1 << 21);
+    if (blocks_per_sm > 0) {
+        r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
+    } else {
+        int be = 1, bs = 1, bsh = 1;
+        stageOccupancy(be, bs, bsh);
+        r->gridExtend = r->smCount * std::max(be, 1);
+        r->gridShade = r->smCount * std::max(bs, 1);
+        r->gridShadow = r->smCount * std::max(bsh, 1);
+    }
+    return PT_OK;
+}
+
+int pt_rng_tape(pt_renderer* r, int first_wave, int waves, int stride, float* out)
+{
+    if (r == nullptr || out == nullptr || waves <= 0 || stride <= 0 || first_wave < 0) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_rng_tape: bad arguments");
+    }
+    if (r->width <= 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_rng_tape before pt_configure");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const size_t total = static_cast<size_t>(r->width) * r->height * waves * stride;
+    float* d = nullptr;
+    PT_CHECK(r, cudaMallocAsync(reinterpret_cast<void**>(&d), total * sizeof(float), r->stream));
+    launchRngTape(r->width, r->height, first_wave, waves, stride, d, r->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(out, d, total * sizeof(float), cudaMemcpyDeviceToHost, r->stream);
+    }
+    cudaFreeAsync(d, r->stream);
+    const cudaError_t e2 = cudaStreamSynchronize(r->stream);
+    if (e == cudaSuccess) {
+        e = e2;
+    }
+    if (e != cudaSuccess) {
+        return cudaFail(r, e, "pt_rng_tape");
+    }
+    return PT_OK;
+}
+
+} // extern "C"

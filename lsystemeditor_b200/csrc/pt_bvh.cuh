@@ -1,0 +1,99 @@
+// GPU BVH build interface (see pt_bvh.cu).
+#pragma once
+
+#include "pt_common.cuh"
+
+#include <cstddef>
+#include <cstdint>
+
+namespace pt {
+
+// Grow-only pool of device scratch buffers addressed by slot; reused across
+// builds so that a scene rebuild does not re-allocate.
+struct DeviceArena {
+    static constexpr int kSlots = 24;
+    void* ptr[kSlots] = {};
+    size_t bytes[kSlots] = {};
+    bool failed = false;
+
+    void* getBytes(int slot, size_t n)
+    {
+        if (n == 0) {
+            n = 16;
+        }
+        if (bytes[slot] < n) {
+            if (ptr[slot] != nullptr) {
+                cudaFree(ptr[slot]);
+                ptr[slot] = nullptr;
+                bytes[slot] = 0;
+            }
+            if (cudaMalloc(&ptr[slot], n) != cudaSuccess) {
+                ptr[slot] = nullptr;
+                failed = true;
+                return nullptr;
+            }
+            bytes[slot] = n;
+        }
+        return ptr[slot];
+    }
+    template <class T> T* get(int slot, size_t count) { return static_cast<T*>(getBytes(slot, count * sizeof(T))); }
+    bool ok() const { return !failed; }
+    void release()
+    {
+        for (int i = 0; i < kSlots; ++i) {
+            if (ptr[i] != nullptr) {
+                cudaFree(ptr[i]);
+            }
+            ptr[i] = nullptr;
+            bytes[i] = 0;
+        }
+        failed = false;
+    }
+    size_t totalBytes() const
+    {
+        size_t t = 0;
+        for (int i = 0; i < kSlots; ++i) {
+            t += bytes[i];
+        }
+        return t;
+    }
+};
+
+struct BvhBuildOptions {
+    int maxLeafSize = 3;        // triangles per compressed-node leaf (1..3)
+    int treeletPasses = 1;      // treelet SAH reordering passes (0 = plain LBVH)
+    int treeletMinLeaves = 16;  // subtrees smaller than this are left as built
+    float costTriangle = 1.0f;  // SAH cost of one triangle test
+    float costNode = 1.2f;      // SAH cost of one node visit
+};
+
+struct BvhBuffers {
+    CwNode* nodes = nullptr;
+    TriVerts* tris = nullptr;
+    uint32_t nodeCount = 0;
+    uint32_t triCount = 0;
+    int levels = 0;
+    DeviceArena scratch;
+
+    void release()
+    {
+        if (nodes != nullptr) {
+            cudaFree(nodes);
+        }
+        if (tris != nullptr) {
+            cudaFree(tris);
+        }
+        nodes = nullptr;
+        tris = nullptr;
+        nodeCount = triCount = 0;
+        levels = 0;
+    }
+};
+
+// Builds the compressed 8-wide BVH over n triangles whose positions
+// (9 floats per triangle) are already in device memory. Synchronises the
+// stream once per collapse level. Returns a pt_status code.
+int buildBvh(const float* dPositions, uint32_t n, BvhBuffers& out, cudaStream_t stream, const BvhBuildOptions& opt,
+    char* err, size_t errLen);
+
+} // namespace pt

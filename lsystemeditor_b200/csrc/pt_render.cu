@@ -1,0 +1,664 @@
+// Wavefront path-tracing pipeline for sm_100a.
+//
+// The reference runs one megakernel thread per pixel and sample
+// (sampleAdaptiveKernel, PathTracerLib/src/PathTracer.cu:186-273, body
+// tracePathRand, PathIntegratorRandCore.h:206-363).  Here the same estimator
+// is split into stages over structure-of-arrays path state:
+//
+//   generate   camera ray per (pixel, sample): curand_init with the reference
+//              seed, jitter + lens draws (PathTracer.cu:69-96)
+//   extend     closest hit for every live path            (pt_trace.cuh)
+//   shade      pending NEE resolve, miss/env MIS, emission, environment and
+//              emissive NEE (shadow rays queued), BSDF sample, throughput,
+//              subsurface tier B, Russian roulette, continuation ray
+//   shadow     any-hit occlusion for the queued shadow rays
+//   finalize   paths that ended with shadow rays in flight
+//   accumulate per pixel, the batch's samples in sample order: running mean,
+//              Welford luminance variance, convergence every 4 samples
+//              (PathTracer.cu:232-272)
+//   compact    active-pixel list without converged pixels
+//
+// Radiance is added in exactly the reference's order: emission, env NEE,
+// emissive NEE (resolved after the shadow stage), then at the next bounce the
+// miss term.  Random numbers are drawn in the reference's order from the same
+// per-(pixel, sample) XORWOW stream, so a path takes the same decisions as the
+// reference's; the state lives in registers within a stage and in the SoA
+// between stages.
+#include "pt_render.cuh"
+
+#include "pt_bsdf.cuh"
+#include "pt_trace.cuh"
+
+#include <cooperative_groups.h>
+#include <curand_kernel.h>
+
+namespace cg = cooperative_groups;
+
+namespace pt {
+
+namespace {
+
+__constant__ pt_material kFallbackMaterial = {0.8f, 0.8f, 0.8f, 0.5f, 0.0f, 0.0f, 0.0f, 1.5f, 0.0f, 0.0f, -1.0f, 0.0f,
+    0.0f, 0.0f, 1.0f, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0.0f};
+
+__device__ __forceinline__ uint32_t warpPush(unsigned int* counter)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned int base = 0;
+    if (g.thread_rank() == 0) {
+        base = atomicAdd(counter, g.size());
+    }
+    base = g.shfl(base, 0);
+    return base + g.thread_rank();
+}
+
+__device__ __forceinline__ void rngLoad(const PathSoA& P, uint32_t i, curandStateXORWOW& s)
+{
+    const uint4 a = P.rngA[i];
+    const uint2 b = P.rngB[i];
+    s.d = a.x;
+    s.v[0] = a.y;
+    s.v[1] = a.z;
+    s.v[2] = a.w;
+    s.v[3] = b.x;
+    s.v[4] = b.y;
+    s.boxmuller_flag = 0;
+    s.boxmuller_flag_double = 0;
+    s.boxmuller_extra = 0.0f;
+    s.boxmuller_extra_double = 0.0;
+}
+
+__device__ __forceinline__ void rngStore(const PathSoA& P, uint32_t i, const curandStateXORWOW& s)
+{
+    P.rngA[i] = make_uint4(s.d, s.v[0], s.v[1], s.v[2]);
+    P.rngB[i] = make_uint2(s.v[3], s.v[4]);
+}
+
+// Sampling/RandCore.h:7-12 (reference) or a hash of (x, y, seed value) (extension).
+__device__ __forceinline__ uint32_t pathSeed(const pt_render_params& p, uint32_t pixel, uint32_t width,
+    uint32_t sampleIndex, uint32_t globalSeed)
+{
+    if (p.seed_mode == 1) {
+        // PCG-style integer hash (O'Neill 2014 output permutation) of x, y, seed and sample index.
+        auto h = [](uint32_t v) {
+            const uint32_t state = v * 747796405u + 2891336453u;
+            const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+            return (word >> 22u) ^ word;
+        };
+        const uint32_t x = pixel % width, y = pixel / width;
+        return h(x ^ h(y ^ h(p.seed_value ^ h(sampleIndex))));
+    }
+    return pixel * 747796405u + sampleIndex + globalSeed * 2891336453u;
+}
+
+// PathTracer.cu:49-67.
+__device__ __forceinline__ float3 clampFirefly(float3 c)
+{
+    if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) {
+        return f3(0.0f, 0.0f, 0.0f);
+    }
+    c = f3(fmax2(0.0f, c.x), fmax2(0.0f, c.y), fmax2(0.0f, c.z));
+    const float l = __fadd_rn(__fadd_rn(__fmul_rn(c.x, 0.2126f), __fmul_rn(c.y, 0.7152f)), __fmul_rn(c.z, 0.0722f));
+    if (l <= 100.0f) {
+        return c;
+    }
+    const float k = __fdiv_rn(100.0f, l);
+    return f3(__fmul_rn(c.x, k), __fmul_rn(c.y, k), __fmul_rn(c.z, k));
+}
+
+__device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, float3 L)
+{
+    const float3 s = clampFirefly(L);
+    c.acc.samples[c.paths.outIdx[i]] = make_float4(s.x, s.y, s.z, 1.0f);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_generate(LaunchCtx c, long long jobStart, int jobCount, int activeCount,
+    uint32_t waveBase, int extendSel)
+{
+    const int* active = c.acc.active[c.activeSel];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c.q.counts[extendSel] = static_cast<unsigned int>(jobCount);
+        c.q.counts[extendSel ^ 1] = 0u;
+        c.q.counts[2] = 0u;
+        c.q.counts[3] = 0u;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < jobCount; i += gridDim.x * blockDim.x) {
+        const long long j = jobStart + i;
+        const int li = static_cast<int>(j % activeCount);
+        const uint32_t slot = static_cast<uint32_t>(j / activeCount);
+        const uint32_t pixel = static_cast<uint32_t>(active[li]);
+        const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
+        const uint32_t globalSeed = waveBase + slot + 1u;
+        curandStateXORWOW st;
+        curand_init(pathSeed(c.params, pixel, c.width, sampleIndex, globalSeed), 0ull, 0ull, &st);
+        const uint32_t x = pixel % c.width, y = pixel / c.width;
+        const float ju = curand_uniform(&st);
+        const float jv = curand_uniform(&st);
+        const float u = (static_cast<float>(x) + ju) / static_cast<float>(c.width);
+        const float v = (static_cast<float>(y) + jv) / static_cast<float>(c.height);
+        const float l1 = curand_uniform(&st);
+        const float l2 = curand_uniform(&st);
+        float3 ro, rd;
+        cameraRay(c.cam, u, v, l1, l2, ro, rd);
+        c.paths.pixel[i] = pixel;
+        c.paths.outIdx[i] = slot * static_cast<uint32_t>(activeCount) + static_cast<uint32_t>(li);
+        rngStore(c.paths, i, st);
+        c.paths.orig[i] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+        c.paths.dir[i] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+        c.paths.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        c.paths.rad[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+        c.paths.visEnv[i] = 0;
+        c.paths.visEmis[i] = 0;
+    }
+}
+
+// Closest hit for every queued path.
+template <bool Count>
+__global__ void __launch_bounds__(256) k_extend(LaunchCtx c, int sel, bool identity)
+{
+    const unsigned int count = c.q.counts[sel];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&c.q.rays[0], static_cast<unsigned long long>(count));
+        // output counters of the shade stage that follows
+        c.q.counts[sel ^ 1] = 0u;
+        c.q.counts[2] = 0u;
+        c.q.counts[3] = 0u;
+    }
+    const uint32_t* queue = c.q.extend[sel];
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t i = identity ? k : queue[k];
+        const float4 o4 = c.paths.orig[i];
+        const float4 d4 = c.paths.dir[i];
+        const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
+        HitRec h;
+        const bool hit = traceRay<false, Count>(c.scene, f3(o4.x, o4.y, o4.z), dn, o4.w, kRayTMax, h, c.q.overflow,
+            c.q.visits);
+        c.paths.hit[i] = hit ? make_float4(h.t, h.u, h.v, __uint_as_float(h.tri))
+                             : make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0xFFFFFFFFu));
+    }
+}
+
+// Shading. One thread per queued path.
+__global__ void __launch_bounds__(256) k_shade(LaunchCtx c, int sel, bool identity)
+{
+    const unsigned int count = c.q.counts[sel];
+    const uint32_t* queue = c.q.extend[sel];
+    unsigned int* nextCount = &c.q.counts[sel ^ 1];
+    uint32_t* nextQueue = c.q.extend[sel ^ 1];
+    const int debugFlags = c.params.brdf_debug_flags;
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t i = identity ? k : queue[k];
+        float4 r4 = c.paths.rad[i];
+        float3 L = f3(r4.x, r4.y, r4.z);
+        const int depth = __float_as_int(r4.w);
+        // NEE contributions of the previous bounce, in the reference's order.
+        if (depth > 0) {
+            if (c.paths.visEnv[i]) {
+                const float4 e = c.paths.neeEnv[i];
+                L = add3(L, f3(e.x, e.y, e.z));
+            }
+            if (c.paths.visEmis[i]) {
+                const float4 e = c.paths.neeEmis[i];
+                L = add3(L, f3(e.x, e.y, e.z));
+            }
+        }
+        const float4 h4 = c.paths.hit[i];
+        const uint32_t tri = __float_as_uint(h4.w);
+        const float4 d4 = c.paths.dir[i];
+        const float3 d = f3(d4.x, d4.y, d4.z);
+        bool done = false;
+        bool pendEnv = false, pendEmis = false;
+        bool cont = false;
+        if (tri == 0xFFFFFFFFu) {
+            if (depth == 0) {
+                L = envEval(c.env, c.params, d);
+            } else {
+                const float4 t4 = c.paths.thr[i];
+                const float3 Le = envEval(c.env, c.params, d);
+                const float lp = envPdf(c.env, d);
+                const float w = misBalance(d4.w, lp);
+                L = add3(L, mul3(f3(t4.x, t4.y, t4.z), scl3(Le, w)));
+            }
+            done = true;
+        } else if (depth >= c.maxDepth) {
+            done = true;
+        } else {
+            const float4 o4 = c.paths.orig[i];
+            const float4 t4 = c.paths.thr[i];
+            float3 T = f3(t4.x, t4.y, t4.z);
+            float eta = t4.w;
+            const float t = h4.x;
+            const float3 pos = xadd(f3(o4.x, o4.y, o4.z), xscl(d, t));
+            const float3 dn = xnormalize(d);
+            const TriShade sh = c.scene.shade[tri];
+            float3 n;
+            float tu, tv;
+            hitShading(sh, dn, h4.y, h4.z, n, tu, tv);
+            const uint32_t mi = __float_as_uint(sh.d.w);
+            const pt_material& srcMat =
+                (c.scene.materials != nullptr && mi < c.scene.materialCount) ? c.scene.materials[mi] : kFallbackMaterial;
+            Ctx cx;
+            cx.m = resolveMaterial(srcMat, tu, tv, c.scene.textures, c.scene.textureCount);
+            cx.w = computeLobes(cx.m);
+            cx.n = n;
+            cx.wo = scl3(d, -1.0f);
+            cx.eta = eta;
+            cx.debug = 0;
+            // emission (PathIntegratorRandCore.h:248)
+            L = add3(L, mul3(T, f3(cx.m.r * cx.m.emission, cx.m.g * cx.m.emission, cx.m.b * cx.m.emission)));
+            curandStateXORWOW st;
+            rngLoad(c.paths, i, st);
+            // environment NEE (PathIntegratorRandCore.h:65-108)
+            if (!skipsEnvNee(cx.m)) {
+                const float u1 = curand_uniform(&st);
+                const float u2 = curand_uniform(&st);
+                float lp = 0.0f;
+                const float3 wi = envSample(c.env, u1, u2, lp);
+                if (lp > kMinPdf) {
+                    const float ct = fmax2(0.0f, dot3(n, wi));
+                    if (ct > 0.0f) {
+                        const float3 Le = envEval(c.env, c.params, wi);
+                        const float3 f = bsdfEval(cx, wi);
+                        const float bp = bsdfPdf(cx, wi);
+                        const float k = misBalance(lp, bp) * ct / lp;
+                        const float3 contrib = mul3(T, mul3(f, scl3(Le, k)));
+                        c.paths.neeEnv[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                        const uint32_t s = warpPush(&c.q.counts[2]);
+                        const float3 so = add3(pos, scl3(n, kShadowBias));
+                        c.q.shadowPath[s] = i;
+                        c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
+                        c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+                        pendEnv = true;
+                    }
+                }
+            }
+            // emissive NEE (PathIntegratorRandCore.h:110-167)
+            if (c.scene.emissiveCount > 0) {
+                const float uTri = curand_uniform(&st);
+                const float u1 = curand_uniform(&st);
+                const float u2 = curand_uniform(&st);
+                float3 lpos, ln, Le;
+                float ap;
+                if (sampleEmissive(c.scene, &kFallbackMaterial, uTri, u1, u2, lpos, ln, Le, ap)) {
+                    const float3 tl = sub3(lpos, pos);
+                    const float d2 = dot3(tl, tl);
+                    if (d2 > kMinPdf) {
+                        const float3 wi = normalize3(tl);
+                        const float ct = fmax2(0.0f, dot3(n, wi));
+                        const float cl = fmax2(0.0f, dot3(ln, scl3(wi, -1.0f)));
+                        if (ct > 0.0f && cl > 0.0f) {
+                            const float lp = ap * d2 / cl;
+                            if (lp > kMinPdf) {
+                                const float3 f = bsdfEval(cx, wi);
+                                const float bp = bsdfPdf(cx, wi);
+                                const float k = misBalance(lp, bp) * ct / lp;
+                                const float3 contrib = mul3(T, mul3(f, scl3(Le, k)));
+                                c.paths.neeEmis[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                                const uint32_t s = warpPush(&c.q.counts[2]);
+                                const float3 so = add3(pos, scl3(wi, kShadowBias));
+                                c.q.shadowPath[s] = i | 0x80000000u;
+                                c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
+                                c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+                                pendEmis = true;
+                            }
+                        }
+                    }
+                }
+            }
+            // BSDF sample (PathIntegratorRandCore.h:280-321)
+            cx.debug = debugFlags;
+            const float u1 = curand_uniform(&st);
+            const float u2 = curand_uniform(&st);
+            const BsdfSample smp = bsdfSample(cx, u1, u2);
+            if (!smp.valid || smp.pdf <= kMinPdf) {
+                done = true;
+            } else {
+                const float3 f = bsdfEval(cx, smp.dir);
+                T = applyThroughput(T, cx, smp, f);
+                if (smp.sss && smp.sssSteps > 0) {
+                    // subsurface tier B (PathIntegratorRandCore.h:169-204)
+                    const float maxR = maxScatter(cx.m);
+                    if (maxR > kMinRadius) {
+                        for (int stp = 0; stp < smp.sssSteps; ++stp) {
+                            (void)curand_uniform(&st);
+                            (void)curand_uniform(&st);
+                            const float u3 = curand_uniform(&st);
+                            const float mfp = maxR * (-logf(fmax2(1.0e-8f, u3)));
+                            const float surv = expf(-mfp / maxR);
+                            T = mul3(T, scl3(f3(cx.m.r, cx.m.g, cx.m.b), surv));
+                        }
+                        const float ed = sqrtf(dot3(smp.exitOffset, smp.exitOffset));
+                        if (ed > 0.0f) {
+                            T = scl3(T, expf(-ed / maxR));
+                        }
+                    }
+                }
+                if (debugFlags & kDbgTintGlass) {
+                    T = smp.transmitted ? mul3(T, f3(0.2f, 1.0f, 0.2f)) : mul3(T, f3(1.0f, 0.2f, 0.2f));
+                }
+                const float tl = lum709(T);
+                if (!isfinite(tl) || tl <= 0.0f || tl > 1.0e8f) {
+                    done = true;
+                } else {
+                    bool survive = true;
+                    if (depth >= c.rrMinDepth) {
+                        const float surv = fmin2(0.95f, fmax2(tl, 0.05f));
+                        if (curand_uniform(&st) > surv) {
+                            survive = false;
+                        } else {
+                            T = scl3(T, 1.0f / surv);
+                        }
+                    }
+                    if (!survive) {
+                        done = true;
+                    } else {
+                        eta = smp.nextEta;
+                        const float bias = fmax2(1.0e-4f, 1.0e-3f * t);
+                        const float sign = dot3(n, smp.dir) >= 0.0f ? 1.0f : -1.0f;
+                        const float3 no = xadd(pos, xscl(n, __fmul_rn(sign, bias)));
+                        c.paths.orig[i] = make_float4(no.x, no.y, no.z, bias);
+                        c.paths.dir[i] = make_float4(smp.dir.x, smp.dir.y, smp.dir.z, smp.pdf);
+                        c.paths.thr[i] = make_float4(T.x, T.y, T.z, eta);
+                        cont = true;
+                    }
+                }
+            }
+            rngStore(c.paths, i, st);
+        }
+        c.paths.visEnv[i] = 0;
+        c.paths.visEmis[i] = 0;
+        if (cont) {
+            c.paths.rad[i] = make_float4(L.x, L.y, L.z, __int_as_float(depth + 1));
+            const uint32_t s = warpPush(nextCount);
+            nextQueue[s] = i;
+        } else if (pendEnv || pendEmis) {
+            c.paths.rad[i] = make_float4(L.x, L.y, L.z, __int_as_float(depth));
+            const uint32_t s = warpPush(&c.q.counts[3]);
+            c.q.finish[s] = i;
+        } else if (done || !cont) {
+            writeSample(c, i, L);
+        }
+    }
+}
+
+// Occlusion of the queued shadow rays (LightSamplingCore.h:187-197, 360-369).
+template <bool Count>
+__global__ void __launch_bounds__(256) k_shadow(LaunchCtx c)
+{
+    const unsigned int count = c.q.counts[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&c.q.rays[1], static_cast<unsigned long long>(count));
+    }
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t e = c.q.shadowPath[k];
+        const float4 o4 = c.q.shadowOrig[k];
+        const float4 d4 = c.q.shadowDir[k];
+        const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
+        HitRec h;
+        const bool occluded = traceRay<true, Count>(c.scene, f3(o4.x, o4.y, o4.z), dn, kShadowBias, kRayTMax, h,
+            c.q.overflow, c.q.visits + 2);
+        if (!occluded) {
+            const uint32_t i = e & 0x7FFFFFFFu;
+            if (e & 0x80000000u) {
+                c.paths.visEmis[i] = 1;
+            } else {
+                c.paths.visEnv[i] = 1;
+            }
+        }
+    }
+}
+
+// Paths that terminated while their NEE shadow rays were in flight.
+__global__ void __launch_bounds__(256) k_finalize(LaunchCtx c)
+{
+    const unsigned int count = c.q.counts[3];
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t i = c.q.finish[k];
+        const float4 r4 = c.paths.rad[i];
+        float3 L = f3(r4.x, r4.y, r4.z);
+        if (c.paths.visEnv[i]) {
+            const float4 e = c.paths.neeEnv[i];
+            L = add3(L, f3(e.x, e.y, e.z));
+        }
+        if (c.paths.visEmis[i]) {
+            const float4 e = c.paths.neeEmis[i];
+            L = add3(L, f3(e.x, e.y, e.z));
+        }
+        writeSample(c, i, L);
+    }
+}
+
+// Per pixel: fold the batch's samples in sample order (PathTracer.cu:232-272).
+__global__ void __launch_bounds__(256) k_accumulate(LaunchCtx c, int activeCount, int batch)
+{
+    const int* active = c.acc.active[c.activeSel];
+    const int maxSpp = c.params.max_samples_per_pixel;
+    const int minSpp = c.params.min_samples;
+    const float thr = c.params.relative_error_threshold;
+    const bool stdErr = c.params.adaptive_criterion == 1;
+    for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < activeCount; li += gridDim.x * blockDim.x) {
+        const int p = active[li];
+        uint8_t conv = c.acc.converged[p];
+        if (conv) {
+            continue;
+        }
+        uint32_t n = c.acc.counts[p];
+        float mean = c.acc.lumMean[p];
+        float m2 = c.acc.m2[p];
+        float4 a = c.acc.acc[p];
+        for (int s = 0; s < batch && !conv; ++s) {
+            const float4 smp = c.acc.samples[static_cast<size_t>(s) * activeCount + li];
+            const float sl =
+                __fadd_rn(__fadd_rn(__fmul_rn(smp.x, 0.2126f), __fmul_rn(smp.y, 0.7152f)), __fmul_rn(smp.z, 0.0722f));
+            const float fn1 = static_cast<float>(n + 1);
+            const float delta = __fsub_rn(sl, mean);
+            const float nm = __fadd_rn(mean, __fdiv_rn(delta, fn1));
+            m2 = __fadd_rn(m2, __fmul_rn(delta, __fsub_rn(sl, nm)));
+            mean = nm;
+            const float invN = __fdiv_rn(1.0f, fn1);
+            const float fn = static_cast<float>(n);
+            a.x = __fmul_rn(__fadd_rn(__fmul_rn(a.x, fn), smp.x), invN);
+            a.y = __fmul_rn(__fadd_rn(__fmul_rn(a.y, fn), smp.y), invN);
+            a.z = __fmul_rn(__fadd_rn(__fmul_rn(a.z, fn), smp.z), invN);
+            a.w = 1.0f;
+            ++n;
+            if (maxSpp > 0 && n >= static_cast<uint32_t>(maxSpp)) {
+                conv = 1;
+                break;
+            }
+            if ((n % 4u) != 0u) {
+                continue;
+            }
+            // isAdaptivePixelConverged (PathTracerAdaptiveSampling.h:16-40)
+            if (n >= static_cast<uint32_t>(minSpp) && n > 0 && mean >= 1.0e-5f) {
+                const float var = __fdiv_rn(m2, static_cast<float>(n));
+                float rel = __fdiv_rn(__fsqrt_rn(var), fmaxf(mean, 1.0e-4f));
+                if (stdErr) {
+                    rel = __fdiv_rn(rel, __fsqrt_rn(static_cast<float>(n)));
+                }
+                if (rel < thr) {
+                    conv = 1;
+                }
+            }
+        }
+        c.acc.counts[p] = n;
+        c.acc.lumMean[p] = mean;
+        c.acc.m2[p] = m2;
+        c.acc.acc[p] = a;
+        c.acc.converged[p] = conv;
+    }
+}
+
+// Ordered-within-block compaction of the active list (compactActiveListKernel,
+// PathTracer.cu:372-411, without per-element atomics).
+__global__ void __launch_bounds__(256) k_compact(LaunchCtx c, int activeCount)
+{
+    const int* in = c.acc.active[c.activeSel];
+    int* out = c.acc.active[c.activeSel ^ 1];
+    const int maxSpp = c.params.max_samples_per_pixel;
+    __shared__ int warpCounts[8];
+    __shared__ int blockBase;
+    for (int base = blockIdx.x * blockDim.x; base < activeCount; base += gridDim.x * blockDim.x) {
+        const int li = base + threadIdx.x;
+        int p = -1;
+        bool keep = false;
+        if (li < activeCount) {
+            p = in[li];
+            keep = c.acc.converged[p] == 0 && !(maxSpp > 0 && c.acc.counts[p] >= static_cast<uint32_t>(maxSpp));
+        }
+        const unsigned int ballot = __ballot_sync(0xffffffffu, keep);
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) {
+            warpCounts[w] = __popc(ballot);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int total = 0;
+            for (int k = 0; k < 8; ++k) {
+                const int t = warpCounts[k];
+                warpCounts[k] = total;
+                total += t;
+            }
+            blockBase = total ? static_cast<int>(atomicAdd(&c.acc.activeCount[1], total)) : 0;
+        }
+        __syncthreads();
+        if (keep) {
+            out[blockBase + warpCounts[w] + __popc(ballot & ((1u << lane) - 1u))] = p;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_reset(LaunchCtx c, int pixels)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pixels; i += gridDim.x * blockDim.x) {
+        c.acc.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        c.acc.counts[i] = 0;
+        c.acc.lumMean[i] = 0.0f;
+        c.acc.m2[i] = 0.0f;
+        c.acc.converged[i] = 0;
+        c.acc.active[0][i] = i;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c.acc.activeCount[0] = pixels;
+        c.acc.activeCount[1] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_trace_rays(DevScene S, int n, const float* o, const float* d, const float* tmin,
+    const float* tmax, uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float3 ro = f3(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
+        const float3 dn = xnormalize(f3(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
+        HitRec h;
+        const bool ok = traceRay<false>(S, ro, dn, tmin[i], tmax[i], h);
+        hit[i] = ok ? 1 : 0;
+        float3 nn = f3(0.0f, 0.0f, 0.0f);
+        float tu = 0.0f, tv = 0.0f;
+        if (ok) {
+            hitShading(S.shade[h.tri], dn, h.u, h.v, nn, tu, tv);
+        }
+        if (t) {
+            t[i] = ok ? h.t : 0.0f;
+        }
+        if (tri) {
+            tri[i] = ok ? h.tri : 0u;
+        }
+        if (normal) {
+            normal[3 * i] = nn.x;
+            normal[3 * i + 1] = nn.y;
+            normal[3 * i + 2] = nn.z;
+        }
+        if (uv) {
+            uv[2 * i] = tu;
+            uv[2 * i + 1] = tv;
+        }
+    }
+}
+
+__global__ void k_rng_tape(int width, int height, int firstWave, int waves, int stride, float* out)
+{
+    const long long P = static_cast<long long>(width) * height;
+    const long long total = P * waves;
+    for (long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; k < total;
+         k += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const uint32_t w = static_cast<uint32_t>(k / P);
+        const uint32_t p = static_cast<uint32_t>(k % P);
+        const uint32_t wave = static_cast<uint32_t>(firstWave) + w;
+        const uint32_t seed = p * 747796405u + wave + (wave + 1u) * 2891336453u;
+        curandStateXORWOW st;
+        curand_init(seed, 0ull, 0ull, &st);
+        float* row = out + k * stride;
+        for (int j = 0; j < stride; ++j) {
+            row[j] = curand_uniform(&st);
+        }
+    }
+}
+
+inline int gridFor(long long n, int block = 256, int cap = 148 * 16)
+{
+    long long g = (n + block - 1) / block;
+    if (g < 1) {
+        g = 1;
+    }
+    return static_cast<int>(g < cap ? g : cap);
+}
+
+} // namespace
+
+void launchGenerate(const LaunchCtx& c, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
+    int extendSel, cudaStream_t s)
+{
+    k_generate<<<gridFor(jobCount), 256, 0, s>>>(c, jobStart, jobCount, activeCount, waveBase, extendSel);
+}
+void launchExtend(const LaunchCtx& c, int sel, bool identity, int grid, bool count, cudaStream_t s)
+{
+    if (count) {
+        k_extend<true><<<grid, 256, 0, s>>>(c, sel, identity);
+    } else {
+        k_extend<false><<<grid, 256, 0, s>>>(c, sel, identity);
+    }
+}
+void launchShade(const LaunchCtx& c, int sel, bool identity, int grid, cudaStream_t s)
+{
+    k_shade<<<grid, 256, 0, s>>>(c, sel, identity);
+}
+void launchShadow(const LaunchCtx& c, int grid, bool count, cudaStream_t s)
+{
+    if (count) {
+        k_shadow<true><<<grid, 256, 0, s>>>(c);
+    } else {
+        k_shadow<false><<<grid, 256, 0, s>>>(c);
+    }
+}
+void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
+{
+    extendBlocks = shadeBlocks = shadowBlocks = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extendBlocks, k_extend<false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadeBlocks, k_shade, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadowBlocks, k_shadow<false>, 256, 0);
+}
+void launchFinalize(const LaunchCtx& c, int grid, cudaStream_t s) { k_finalize<<<grid, 256, 0, s>>>(c); }
+void launchAccumulate(const LaunchCtx& c, int activeCount, int batch, cudaStream_t s)
+{
+    k_accumulate<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount, batch);
+}
+void launchCompact(const LaunchCtx& c, int activeCount, cudaStream_t s)
+{
+    k_compact<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount);
+}
+void launchResetAccum(const LaunchCtx& c, int pixels, cudaStream_t s) { k_reset<<<gridFor(pixels), 256, 0, s>>>(c, pixels); }
+void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,
+    uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s)
+{
+    k_trace_rays<<<gridFor(n), 256, 0, s>>>(S, n, o, d, tmin, tmax, hit, t, tri, normal, uv);
+}
+void launchRngTape(int width, int height, int firstWave, int waves, int stride, float* out, cudaStream_t s)
+{
+    k_rng_tape<<<gridFor(static_cast<long long>(width) * height * waves), 256, 0, s>>>(width, height, firstWave, waves,
+        stride, out);
+}
+
+} // namespace pt

@@ -1,0 +1,82 @@
+// Wavefront render pipeline: device buffers and launchers (see pt_render.cu).
+#pragma once
+
+#include "pt_common.cuh"
+
+namespace pt {
+
+// Structure-of-arrays path state, capacity `capacity` paths.
+struct PathSoA {
+    uint32_t* pixel = nullptr;   // pixel index
+    uint32_t* outIdx = nullptr;  // slot * activeCount + listIndex into the sample buffer
+    uint4* rngA = nullptr;       // XORWOW d, v0, v1, v2
+    uint2* rngB = nullptr;       // XORWOW v3, v4
+    float4* orig = nullptr;      // ray origin, tMin
+    float4* dir = nullptr;       // ray direction (as produced, not renormalised), pdf of the sampled direction
+    float4* thr = nullptr;       // throughput, medium IOR
+    float4* rad = nullptr;       // radiance, depth (int bits)
+    float4* hit = nullptr;       // t, u, v, triangle (uint bits, 0xFFFFFFFF = miss)
+    float4* neeEnv = nullptr;    // pending environment-NEE contribution
+    float4* neeEmis = nullptr;   // pending emissive-NEE contribution
+    uint8_t* visEnv = nullptr;   // 1 = that contribution is unoccluded
+    uint8_t* visEmis = nullptr;
+    int capacity = 0;
+};
+
+struct QueueSet {
+    uint32_t* extend[2] = {nullptr, nullptr}; // path indices, ping-pong
+    uint32_t* finish = nullptr;               // paths that ended with shadow rays in flight
+    uint32_t* shadowPath = nullptr;           // path index | kind << 31
+    float4* shadowOrig = nullptr;
+    float4* shadowDir = nullptr;
+    // counters: [0],[1] extend ping-pong, [2] shadow, [3] finish
+    unsigned int* counts = nullptr;
+    unsigned long long* rays = nullptr;       // [0] closest-hit rays, [1] shadow rays
+    unsigned long long* visits = nullptr;     // [0..1] extend nodes/tris, [2..3] shadow nodes/tris
+    unsigned int* overflow = nullptr;         // traversal stack overflows
+};
+
+struct AccumState {
+    float4* acc = nullptr;
+    uint32_t* counts = nullptr;
+    float* lumMean = nullptr;
+    float* m2 = nullptr;
+    uint8_t* converged = nullptr;
+    int* active[2] = {nullptr, nullptr};
+    int* activeCount = nullptr; // [0] current, [1] next
+    float4* samples = nullptr;  // per-batch sample buffer
+    size_t sampleCapacity = 0;
+};
+
+struct LaunchCtx {
+    DevScene scene;
+    DevEnv env;
+    pt_camera cam;
+    pt_render_params params;
+    int width;
+    int height;
+    int maxDepth;     // effective (0 -> 256, <0 -> 32)
+    int rrMinDepth;   // effective
+    PathSoA paths;
+    QueueSet q;
+    AccumState acc;
+    int activeSel;    // which active[] list is current
+};
+
+// Launchers. `grid` is a persistent-style grid; kernels loop over device-side counts.
+void launchGenerate(const LaunchCtx& c, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
+    int extendSel, cudaStream_t s);
+void launchExtend(const LaunchCtx& c, int sel, bool identity, int grid, bool count, cudaStream_t s);
+void launchShade(const LaunchCtx& c, int sel, bool identity, int grid, cudaStream_t s);
+void launchShadow(const LaunchCtx& c, int grid, bool count, cudaStream_t s);
+void launchFinalize(const LaunchCtx& c, int grid, cudaStream_t s);
+void launchAccumulate(const LaunchCtx& c, int activeCount, int batch, cudaStream_t s);
+void launchCompact(const LaunchCtx& c, int activeCount, cudaStream_t s);
+void launchResetAccum(const LaunchCtx& c, int pixels, cudaStream_t s);
+void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,
+    uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s);
+// Resident blocks per SM of the stage kernels (occupancy calculator).
+void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks);
+void launchRngTape(int width, int height, int firstWave, int waves, int stride, float* out, cudaStream_t s);
+
+} // namespace pt

@@ -1,0 +1,341 @@
+// Ray traversal of the compressed 8-wide BVH: closest hit and any hit.
+//
+// Semantics follow meshAccelTraceRay (PathTracerLib/src/MeshAccel/
+// MeshAccelIntersectCore.h:110-221):
+//   * the direction is normalised first (zero length -> (0, 0, -1));
+//   * triangles are intersected with the reference's Moller-Trumbore
+//     (:52-108), rounded exactly like the reference (no FMA contraction), and
+//     accepted when tMin <= t <= closest (a later equal-t hit replaces the
+//     earlier one);
+//   * a hit is reported only if the final t < tMax;
+//   * quirk Q1: a direction component with |d| <= 1e-8 gets a zero reciprocal
+//     in the reference, which turns every slab test into "does the box contain
+//     the origin in the other axes" and fails all boxes when tMin > 0.  The
+//     reference's leaves are single triangles with exact bounds, so this is
+//     reproduced independently of the tree by testing only triangles whose
+//     exact bounds contain the origin in the non-degenerate axes (traceQ1).
+// Child boxes are quantised outward, so the tree is conservative; the slab
+// test widens tExit by 2^-21 relative to absorb its own rounding.
+#pragma once
+
+#include "pt_common.cuh"
+
+namespace pt {
+
+constexpr int kTraversalStack = 32;
+constexpr float kSlabWiden = 1.0000005f;
+
+struct HitRec {
+    float t;
+    float u;
+    float v;
+    uint32_t tri; // original triangle index, 0xFFFFFFFF = miss
+};
+
+// Moller-Trumbore, MeshAccelIntersectCore.h:52-93, exact rounding.
+__device__ __forceinline__ bool intersectTriExact(
+    float3 o, float3 d, float3 v0, float3 v1, float3 v2, float tMin, float tMax, float& t, float& u, float& v)
+{
+    const float3 e1 = xsub(v1, v0);
+    const float3 e2 = xsub(v2, v0);
+    const float3 p = xcross(d, e2);
+    const float det = xdot(e1, p);
+    if (fabsf(det) < 1.0e-8f) {
+        return false;
+    }
+    const float invDet = __fdiv_rn(1.0f, det);
+    const float3 tv = xsub(o, v0);
+    const float bu = __fmul_rn(xdot(tv, p), invDet);
+    if (bu < 0.0f || bu > 1.0f) {
+        return false;
+    }
+    const float3 q = xcross(tv, e1);
+    const float bv = __fmul_rn(xdot(d, q), invDet);
+    if (bv < 0.0f || __fadd_rn(bu, bv) > 1.0f) {
+        return false;
+    }
+    const float tt = __fmul_rn(xdot(e2, q), invDet);
+    if (tt < tMin || tt > tMax) {
+        return false;
+    }
+    t = tt;
+    u = bu;
+    v = bv;
+    return true;
+}
+
+// Shading normal and uv at a hit (MeshAccelIntersectCore.h:95-106 and the
+// final renormalisation at :215), exact rounding.
+__device__ __forceinline__ void hitShading(const TriShade& s, float3 dn, float bu, float bv, float3& n, float& tu, float& tv)
+{
+    const float bw = __fsub_rn(__fsub_rn(1.0f, bu), bv);
+    const float3 n0 = f3(s.a.x, s.a.y, s.a.z), n1 = f3(s.b.x, s.b.y, s.b.z), n2 = f3(s.c.x, s.c.y, s.c.z);
+    float3 m = xnormalize(xadd(xadd(xscl(n0, bw), xscl(n1, bu)), xscl(n2, bv)));
+    if (xdot(m, dn) > 0.0f) {
+        m = xscl(m, -1.0f);
+    }
+    n = xnormalize(m);
+    tu = __fadd_rn(__fadd_rn(__fmul_rn(s.a.w, bw), __fmul_rn(s.c.w, bu)), __fmul_rn(s.d.y, bv));
+    tv = __fadd_rn(__fadd_rn(__fmul_rn(s.b.w, bw), __fmul_rn(s.d.x, bu)), __fmul_rn(s.d.z, bv));
+}
+
+__device__ __forceinline__ bool isDegenerateDir(float3 dn)
+{
+    return !(fabsf(dn.x) > 1.0e-8f) || !(fabsf(dn.y) > 1.0e-8f) || !(fabsf(dn.z) > 1.0e-8f);
+}
+
+// Intersects the ray with the eight quantised child boxes of a node.
+// Returns the hit mask: bits 24..31 internal children (slot ^ octinv), bits
+// 0..23 leaf triangles (node-local offsets).
+__device__ __forceinline__ uint32_t intersectChildren(const CwNode* __restrict__ nodes, uint32_t idx, float3 o,
+    float3 idir, uint32_t octinv, float tMin, float tMax, uint32_t& childBase, uint32_t& triBase, uint32_t& imask)
+{
+    const uint4* np = reinterpret_cast<const uint4*>(nodes + idx);
+    const uint4 w0 = __ldg(np + 0);
+    const uint4 w1 = __ldg(np + 1);
+    const uint4 w2 = __ldg(np + 2);
+    const uint4 w3 = __ldg(np + 3);
+    const uint4 w4 = __ldg(np + 4);
+    const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    const uint32_t ex = w0.w & 0xffu, ey = (w0.w >> 8) & 0xffu, ez = (w0.w >> 16) & 0xffu;
+    imask = w0.w >> 24;
+    childBase = w1.x;
+    triBase = w1.y;
+    const float ax = __uint_as_float(ex << 23) * idir.x;
+    const float ay = __uint_as_float(ey << 23) * idir.y;
+    const float az = __uint_as_float(ez << 23) * idir.z;
+    const float bx = (px - o.x) * idir.x;
+    const float by = (py - o.y) * idir.y;
+    const float bz = (pz - o.z) * idir.z;
+    // near/far plane words per axis (quantised lo/hi swapped for negative directions)
+    const bool sx = idir.x < 0.0f, sy = idir.y < 0.0f, sz = idir.z < 0.0f;
+    const uint32_t nearX[2] = {sx ? w3.z : w2.x, sx ? w3.w : w2.y};
+    const uint32_t farX[2] = {sx ? w2.x : w3.z, sx ? w2.y : w3.w};
+    const uint32_t nearY[2] = {sy ? w4.x : w2.z, sy ? w4.y : w2.w};
+    const uint32_t farY[2] = {sy ? w2.z : w4.x, sy ? w2.w : w4.y};
+    const uint32_t nearZ[2] = {sz ? w4.z : w3.x, sz ? w4.w : w3.y};
+    const uint32_t farZ[2] = {sz ? w3.x : w4.z, sz ? w3.y : w4.w};
+    const uint32_t meta[2] = {w1.z, w1.w};
+    uint32_t hitmask = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int sh = 8 * j;
+            const float t0x = fmaf(static_cast<float>((nearX[h] >> sh) & 0xffu), ax, bx);
+            const float t0y = fmaf(static_cast<float>((nearY[h] >> sh) & 0xffu), ay, by);
+            const float t0z = fmaf(static_cast<float>((nearZ[h] >> sh) & 0xffu), az, bz);
+            const float t1x = fmaf(static_cast<float>((farX[h] >> sh) & 0xffu), ax, bx);
+            const float t1y = fmaf(static_cast<float>((farY[h] >> sh) & 0xffu), ay, by);
+            const float t1z = fmaf(static_cast<float>((farZ[h] >> sh) & 0xffu), az, bz);
+            const float tEnter = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, tMin));
+            const float tExit = fminf(fminf(t1x, t1y), fminf(t1z, tMax)) * kSlabWiden;
+            const uint32_t m = (meta[h] >> sh) & 0xffu;
+            if (tEnter <= tExit) {
+                const uint32_t inner = ((m & 0x18u) == 0x18u) ? octinv : 0u;
+                hitmask |= (m >> 5) << ((m ^ inner) & 0x1fu);
+            }
+        }
+    }
+    return hitmask;
+}
+
+// Slow path for quirk Q1 (degenerate direction components); see the file comment.
+__device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, bool anyHit,
+    HitRec& out)
+{
+    out.tri = 0xFFFFFFFFu;
+    if (tMin > 0.0f || S.nodeCount == 0) {
+        return false;
+    }
+    const bool useX = fabsf(dn.x) > 1.0e-8f, useY = fabsf(dn.y) > 1.0e-8f, useZ = fabsf(dn.z) > 1.0e-8f;
+    uint32_t stack[kTraversalStack * 2];
+    int sp = 0;
+    stack[sp++] = 0;
+    float closest = tMax;
+    uint32_t best = 0xFFFFFFFFu;
+    float bu = 0.0f, bv = 0.0f;
+    while (sp > 0) {
+        const uint32_t idx = stack[--sp];
+        const uint4* np = reinterpret_cast<const uint4*>(S.nodes + idx);
+        const uint4 w0 = np[0], w1 = np[1], w2 = np[2], w3 = np[3], w4 = np[4];
+        const float p[3] = {__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z)};
+        const float sc[3] = {__uint_as_float((w0.w & 0xffu) << 23), __uint_as_float(((w0.w >> 8) & 0xffu) << 23),
+            __uint_as_float(((w0.w >> 16) & 0xffu) << 23)};
+        const uint32_t imask = w0.w >> 24;
+        const uint64_t qlo[3] = {w2.x | (uint64_t(w2.y) << 32), w2.z | (uint64_t(w2.w) << 32),
+            w3.x | (uint64_t(w3.y) << 32)};
+        const uint64_t qhi[3] = {w3.z | (uint64_t(w3.w) << 32), w4.x | (uint64_t(w4.y) << 32),
+            w4.z | (uint64_t(w4.w) << 32)};
+        const uint64_t meta = w1.z | (uint64_t(w1.w) << 32);
+        const float oo[3] = {o.x, o.y, o.z};
+        const bool use[3] = {useX, useY, useZ};
+        int rank = 0;
+        for (int s = 0; s < 8; ++s) {
+            const uint32_t m = static_cast<uint32_t>(meta >> (8 * s)) & 0xffu;
+            const bool inner = (imask >> s) & 1u;
+            bool pass = m != 0u;
+            for (int a = 0; a < 3 && pass; ++a) {
+                if (!use[a]) {
+                    continue;
+                }
+                const float lo = fmaf(static_cast<float>((qlo[a] >> (8 * s)) & 0xffu), sc[a], p[a]);
+                const float hi = fmaf(static_cast<float>((qhi[a] >> (8 * s)) & 0xffu), sc[a], p[a]);
+                pass = lo <= oo[a] && oo[a] <= hi;
+            }
+            if (inner) {
+                if (pass && sp < kTraversalStack * 2) {
+                    stack[sp++] = w1.x + rank;
+                }
+                ++rank;
+                continue;
+            }
+            if (!pass) {
+                continue;
+            }
+            const int cnt = __popc(m >> 5);
+            const int off = m & 0x1f;
+            for (int k = 0; k < cnt; ++k) {
+                const TriVerts tv = S.tris[w1.y + off + k];
+                const float3 v0 = f3(tv.v0.x, tv.v0.y, tv.v0.z), v1 = f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                             v2 = f3(tv.v2.x, tv.v2.y, tv.v2.z);
+                const float lo3[3] = {fminf(fminf(v0.x, v1.x), v2.x), fminf(fminf(v0.y, v1.y), v2.y),
+                    fminf(fminf(v0.z, v1.z), v2.z)};
+                const float hi3[3] = {fmaxf(fmaxf(v0.x, v1.x), v2.x), fmaxf(fmaxf(v0.y, v1.y), v2.y),
+                    fmaxf(fmaxf(v0.z, v1.z), v2.z)};
+                bool inside = true;
+                for (int a = 0; a < 3; ++a) {
+                    if (use[a] && !(lo3[a] <= oo[a] && oo[a] <= hi3[a])) {
+                        inside = false;
+                    }
+                }
+                float t, u, v;
+                if (inside && intersectTriExact(o, dn, v0, v1, v2, tMin, closest, t, u, v)) {
+                    if (anyHit && t < tMax) {
+                        out.t = t;
+                        out.u = u;
+                        out.v = v;
+                        out.tri = __float_as_uint(tv.v0.w);
+                        return true;
+                    }
+                    closest = t;
+                    best = w1.y + off + k;
+                    bu = u;
+                    bv = v;
+                }
+            }
+        }
+    }
+    if (best != 0xFFFFFFFFu && closest < tMax) {
+        out.t = closest;
+        out.u = bu;
+        out.v = bv;
+        out.tri = __float_as_uint(S.tris[best].v0.w);
+        return true;
+    }
+    return false;
+}
+
+// Closest hit (AnyHit = false) or occlusion (AnyHit = true) for a normalised
+// direction dn. Returns true on a hit; out.tri is the ORIGINAL triangle index.
+// Count = true adds the nodes and triangles visited to visits[0] / visits[1].
+template <bool AnyHit, bool Count = false>
+__device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, HitRec& out,
+    unsigned int* overflowCounter = nullptr, unsigned long long* visits = nullptr)
+{
+    out.tri = 0xFFFFFFFFu;
+    if (S.nodeCount == 0) {
+        return false;
+    }
+    if (isDegenerateDir(dn)) {
+        return traceQ1(S, o, dn, tMin, tMax, AnyHit, out);
+    }
+    const float3 idir = f3(__frcp_rn(dn.x), __frcp_rn(dn.y), __frcp_rn(dn.z));
+    const uint32_t oct = (dn.x < 0.0f ? 4u : 0u) | (dn.y < 0.0f ? 2u : 0u) | (dn.z < 0.0f ? 1u : 0u);
+    const uint32_t octinv = 7u - oct;
+    uint2 stack[kTraversalStack];
+    int sp = 0;
+    uint2 ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
+    float closest = tMax;
+    uint32_t best = 0xFFFFFFFFu;
+    float bu = 0.0f, bv = 0.0f;
+    bool overflow = false;
+    uint32_t nodeVisits = 0, triVisits = 0;
+    while (true) {
+        // descend into the nearest remaining child of the current node group
+        if (ngroup.y > 0x00FFFFFFu) {
+            const uint32_t bit = 31u - __clz(ngroup.y);
+            ngroup.y &= ~(1u << bit);
+            const uint32_t slot = (bit - 24u) ^ octinv;
+            const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
+            if (ngroup.y > 0x00FFFFFFu) {
+                if (sp < kTraversalStack) {
+                    stack[sp++] = ngroup;
+                } else {
+                    overflow = true;
+                }
+            }
+            uint32_t childBase, triBase, imask;
+            const uint32_t hits = intersectChildren(S.nodes, child, o, idir, octinv, tMin, closest, childBase, triBase,
+                imask);
+            if (Count) {
+                ++nodeVisits;
+            }
+            ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
+            uint32_t tmask = hits & 0x00FFFFFFu;
+            while (tmask != 0u) {
+                const int k = __ffs(tmask) - 1;
+                tmask &= tmask - 1u;
+                const TriVerts tv = S.tris[triBase + k];
+                float t, u, v;
+                if (Count) {
+                    ++triVisits;
+                }
+                if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                        f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
+                    if (AnyHit) {
+                        if (t < tMax) {
+                            if (Count) {
+                                atomicAdd(&visits[0], static_cast<unsigned long long>(nodeVisits));
+                                atomicAdd(&visits[1], static_cast<unsigned long long>(triVisits));
+                            }
+                            out.t = t;
+                            out.u = u;
+                            out.v = v;
+                            out.tri = __float_as_uint(tv.v0.w);
+                            return true;
+                        }
+                    } else {
+                        closest = t;
+                        best = triBase + k;
+                        bu = u;
+                        bv = v;
+                    }
+                }
+            }
+        }
+        if (ngroup.y <= 0x00FFFFFFu) {
+            if (sp == 0) {
+                break;
+            }
+            ngroup = stack[--sp];
+        }
+    }
+    if (overflow && overflowCounter != nullptr) {
+        atomicAdd(overflowCounter, 1u);
+    }
+    if (Count) {
+        atomicAdd(&visits[0], static_cast<unsigned long long>(nodeVisits));
+        atomicAdd(&visits[1], static_cast<unsigned long long>(triVisits));
+    }
+    if (!AnyHit && best != 0xFFFFFFFFu && closest < tMax) {
+        out.t = closest;
+        out.u = bu;
+        out.v = bv;
+        out.tri = __float_as_uint(__ldg(&S.tris[best].v0.w));
+        return true;
+    }
+    return false;
+}
+
+} // namespace pt

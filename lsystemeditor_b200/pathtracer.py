@@ -1,0 +1,316 @@
+"""Python host API over the C ABI (include/pt_b200.h).
+
+``PathTracer`` mirrors the reference renderer object
+(PathTracerLib/src/PathTracer.h:30-152) minus Qt/OpenGL: configure, setters,
+mesh rebuild, camera, render, headless readback, statistics and surface
+picking.  Every call goes through ``libpt_b200.so``; there is no CPU fallback
+-- construction fails if the library or a CUDA device is unavailable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _build
+from .records import CAMERA_DTYPE, MATERIAL_DTYPE, PARAMS_DTYPE, TEXTURE_DTYPE
+from .scene import HostMesh
+
+PT_OK = 0
+STATUS_NAMES = {0: "PT_OK", 1: "PT_ERR_INVALID_ARGUMENT", 2: "PT_ERR_CUDA", 3: "PT_ERR_OUT_OF_MEMORY",
+                4: "PT_ERR_NO_SCENE", 5: "PT_ERR_NOT_CONFIGURED", 6: "PT_ERR_TIMEOUT", 7: "PT_ERR_UNSUPPORTED",
+                8: "PT_ERR_INTERNAL"}
+
+_fp = C.POINTER(C.c_float)
+_u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class PtMesh(C.Structure):
+    _fields_ = [("triangle_count", C.c_uint32), ("positions", _fp), ("normals", _fp), ("uvs", _fp),
+                ("material_ids", _u32p), ("material_count", C.c_uint32), ("materials", C.c_void_p),
+                ("texture_count", C.c_uint32), ("textures", C.c_void_p)]
+
+
+class PtProfile(C.Structure):
+    _fields_ = [("ms_generate", C.c_double), ("ms_extend", C.c_double), ("ms_shade", C.c_double),
+                ("ms_shadow", C.c_double), ("ms_finalize", C.c_double), ("ms_accumulate", C.c_double),
+                ("ms_compact", C.c_double), ("launches_extend", C.c_int64), ("launches_shadow", C.c_int64),
+                ("rays_extend", C.c_int64), ("rays_shadow", C.c_int64), ("nodes_extend", C.c_int64),
+                ("tris_extend", C.c_int64), ("nodes_shadow", C.c_int64), ("tris_shadow", C.c_int64)]
+
+
+PROFILE_STAGE_TIMES = 1
+PROFILE_COUNT_VISITS = 2
+
+
+class PtStats(C.Structure):
+    _fields_ = [("waves", C.c_int64), ("active_pixels", C.c_int64), ("samples", C.c_int64), ("rays", C.c_int64),
+                ("launches", C.c_int64), ("render_ms", C.c_double), ("build_ms", C.c_double),
+                ("budget_exhausted", C.c_int32), ("bvh_nodes", C.c_int32), ("tape_underruns", C.c_int32),
+                ("stack_overflows", C.c_int32)]
+
+
+EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", "pt_set_mesh", "pt_set_camera",
+                    "pt_get_camera", "pt_set_params", "pt_get_params", "pt_default_params", "pt_set_environment",
+                    "pt_reset", "pt_render", "pt_readback", "pt_device_buffers", "pt_get_stats", "pt_trace_rays",
+                    "pt_trace_rays_device", "pt_rng_tape", "pt_set_stream", "pt_set_profiling", "pt_get_profile",
+                    "pt_set_tuning"]
+
+_LIB: Optional[C.CDLL] = None
+
+
+def load_library(build_if_missing: bool = True) -> C.CDLL:
+    """Loads libpt_b200.so (building it with nvcc first when it is missing or stale)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.LIB
+    if build_if_missing and _build.needs_build():
+        _build.build()
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing; run lsystemeditor_b200._build.build()")
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.pt_create.argtypes = [C.POINTER(vp), C.c_int]
+    L.pt_destroy.argtypes = [vp]
+    L.pt_last_error.argtypes = [vp]
+    L.pt_last_error.restype = C.c_char_p
+    L.pt_configure.argtypes = [vp, C.c_int, C.c_int]
+    L.pt_set_mesh.argtypes = [vp, C.POINTER(PtMesh)]
+    L.pt_set_camera.argtypes = [vp, vp]
+    L.pt_get_camera.argtypes = [vp, vp]
+    L.pt_set_params.argtypes = [vp, vp]
+    L.pt_get_params.argtypes = [vp, vp]
+    L.pt_default_params.argtypes = [vp]
+    L.pt_default_params.restype = None
+    L.pt_set_environment.argtypes = [vp, C.c_int, C.c_int, _fp]
+    L.pt_reset.argtypes = [vp]
+    L.pt_render.argtypes = [vp, C.c_int]
+    L.pt_readback.argtypes = [vp, _fp, _u32p, _u8p]
+    L.pt_device_buffers.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]
+    L.pt_get_stats.argtypes = [vp, C.POINTER(PtStats)]
+    L.pt_trace_rays.argtypes = [vp, C.c_int, _fp, _fp, _fp, _fp, _u8p, _fp, _u32p, _fp, _fp]
+    L.pt_trace_rays_device.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.pt_rng_tape.argtypes = [vp, C.c_int, C.c_int, C.c_int, _fp]
+    L.pt_set_stream.argtypes = [vp, vp]
+    L.pt_set_profiling.argtypes = [vp, C.c_int]
+    L.pt_get_profile.argtypes = [vp, C.POINTER(PtProfile)]
+    L.pt_set_tuning.argtypes = [vp, C.c_int, C.c_int]
+    _LIB = L
+    return L
+
+
+class PathTracerError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def _ptr(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+class PathTracer:
+    """Renderer object (reference: class PathTracer, PathTracer.h:30-152)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        h = C.c_void_p()
+        rc = self._lib.pt_create(C.byref(h), int(device))
+        if rc != PT_OK:
+            raise PathTracerError(rc, "pt_create failed (is a CUDA device available?)")
+        self._h = h
+        self._mesh_keepalive = None
+        self.width = 0
+        self.height = 0
+        self._params = np.zeros((), PARAMS_DTYPE)
+        self._lib.pt_default_params(C.c_void_p(self._params.ctypes.data))
+
+    # -- lifetime -------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.pt_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != PT_OK:
+            msg = self._lib.pt_last_error(self._h)
+            raise PathTracerError(rc, msg.decode() if msg else "")
+
+    # -- configure / scene ------------------------------------------------
+    def configure(self, width: int, height: int, mesh: Optional[HostMesh] = None):
+        """PathTracer::configure (PathTracer.h:45-51) without GL surfaces."""
+        self._check(self._lib.pt_configure(self._h, int(width), int(height)))
+        self.width, self.height = int(width), int(height)
+        if mesh is not None:
+            self.set_mesh(mesh)
+
+    def set_mesh(self, mesh: HostMesh):
+        """MeshAccelScene::build + upload / PathTracer::rebuildMeshScene: GPU BVH build."""
+        m = mesh.contiguous()
+        s = PtMesh(m.triangle_count, _ptr(m.positions, _fp), _ptr(m.normals, _fp), _ptr(m.uvs, _fp),
+                   _ptr(m.material_ids, _u32p), len(m.materials),
+                   C.c_void_p(m.materials.ctypes.data) if len(m.materials) else None, len(m.textures),
+                   C.c_void_p(m.textures.ctypes.data) if len(m.textures) else None)
+        self._check(self._lib.pt_set_mesh(self._h, C.byref(s)))
+        self._mesh_keepalive = m
+
+    rebuild_mesh_scene = set_mesh
+
+    def set_camera(self, camera: np.ndarray):
+        cam = np.ascontiguousarray(camera, CAMERA_DTYPE)
+        self._check(self._lib.pt_set_camera(self._h, C.c_void_p(cam.ctypes.data)))
+
+    def last_sample_camera(self) -> np.ndarray:
+        cam = np.zeros((), CAMERA_DTYPE)
+        self._check(self._lib.pt_get_camera(self._h, C.c_void_p(cam.ctypes.data)))
+        return cam
+
+    def set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, PARAMS_DTYPE)
+        self._check(self._lib.pt_set_params(self._h, C.c_void_p(p.ctypes.data)))
+        self._params = p.copy()
+
+    def params(self) -> np.ndarray:
+        p = np.zeros((), PARAMS_DTYPE)
+        self._check(self._lib.pt_get_params(self._h, C.c_void_p(p.ctypes.data)))
+        return p
+
+    def _set(self, **kw):
+        p = self.params()
+        for k, v in kw.items():
+            p[k] = v
+        self.set_params(p)
+
+    # Setters of the reference (PathTracer.h:73-124); values are clamped the
+    # way PathTracer.cpp:126-190 clamps them.
+    def set_max_samples_per_pixel(self, n: int):
+        self._set(max_samples_per_pixel=int(min(max(n, 0), 1_000_000)))
+
+    def set_min_samples(self, n: int):
+        self._set(min_samples=int(min(max(n, 1), 10_000)))
+
+    def set_relative_error_threshold(self, t: float):
+        self._set(relative_error_threshold=float(min(max(t, 0.001), 1.0)))
+
+    def set_russian_roulette_min_depth(self, d: int):
+        self._set(russian_roulette_min_depth=int(max(d, 0)))
+
+    def set_brdf_debug_flags(self, flags: int):
+        self._set(brdf_debug_flags=int(flags))
+
+    def set_debug_overlay_mode(self, mode: int):
+        self._set(debug_overlay_mode=int(mode))
+
+    def set_clear_color(self, r: float, g: float, b: float):
+        self._set(background_r=r, background_g=g, background_b=b)
+
+    def set_environment_intensity(self, k: float):
+        self._set(environment_intensity=float(k))
+
+    def set_max_path_depth(self, d: int):
+        self._set(max_path_depth=int(d))
+
+    def set_environment(self, rgb: Optional[np.ndarray]):
+        """Lat-long linear RGB (H, W, 3) or None for the solid background."""
+        if rgb is None:
+            self._check(self._lib.pt_set_environment(self._h, 0, 0, None))
+            return
+        a = np.ascontiguousarray(rgb, np.float32)
+        self._check(self._lib.pt_set_environment(self._h, a.shape[1], a.shape[0], _ptr(a, _fp)))
+
+    # -- rendering --------------------------------------------------------
+    def reset_accumulation(self):
+        self._check(self._lib.pt_reset(self._h))
+
+    def render(self, waves: int = 0):
+        """Traces `waves` full-resolution adaptive waves (<= 0: until every pixel is done)."""
+        self._check(self._lib.pt_render(self._h, int(waves)))
+
+    def readback(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        P = self.width * self.height
+        rgba = np.empty((self.height, self.width, 4), np.float32)
+        counts = np.empty((self.height, self.width), np.uint32)
+        conv = np.empty((self.height, self.width), np.uint8)
+        self._check(self._lib.pt_readback(self._h, _ptr(rgba, _fp), _ptr(counts, _u32p), _ptr(conv, _u8p)))
+        assert rgba.size == 4 * P
+        return rgba, counts, conv
+
+    def device_buffers(self) -> Tuple[int, int, int]:
+        a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        self._check(self._lib.pt_device_buffers(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def stats(self) -> dict:
+        s = PtStats()
+        self._check(self._lib.pt_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in PtStats._fields_}
+
+    def current_sample_count(self) -> int:
+        return int(self.stats()["waves"])
+
+    def current_active_pixel_count(self) -> int:
+        return int(self.stats()["active_pixels"])
+
+    def is_sample_budget_exhausted(self) -> bool:
+        return bool(self.stats()["budget_exhausted"])
+
+    def sample_budget_total_iterations(self) -> int:
+        """PathTracerSampleBudget.h:8-14 with no preview levels."""
+        m = int(self.params()["max_samples_per_pixel"])
+        return -1 if m <= 0 else m
+
+    # -- queries ----------------------------------------------------------
+    def trace_rays(self, origins, dirs, tmin=None, tmax=None) -> dict:
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        tmin = np.zeros(n, np.float32) if tmin is None else np.ascontiguousarray(np.broadcast_to(tmin, (n,)), np.float32)
+        tmax = np.full(n, 1.0e6, np.float32) if tmax is None else np.ascontiguousarray(np.broadcast_to(tmax, (n,)), np.float32)
+        hit = np.zeros(n, np.uint8); t = np.zeros(n, np.float32); tri = np.zeros(n, np.uint32)
+        nrm = np.zeros((n, 3), np.float32); uv = np.zeros((n, 2), np.float32)
+        self._check(self._lib.pt_trace_rays(self._h, n, _ptr(o, _fp), _ptr(d, _fp), _ptr(tmin, _fp), _ptr(tmax, _fp),
+                                            _ptr(hit, _u8p), _ptr(t, _fp), _ptr(tri, _u32p), _ptr(nrm, _fp),
+                                            _ptr(uv, _fp)))
+        return dict(hit=hit.astype(bool), t=t, tri=tri, normal=nrm, uv=uv)
+
+    def pick_surface(self, origin, direction):
+        """PathTracer::pickSurface (PathTracer.cpp:1991-2013): tMin 0.001, tMax 1e30."""
+        r = self.trace_rays(np.asarray(origin)[None], np.asarray(direction)[None], 0.001, 1.0e30)
+        return {k: v[0] for k, v in r.items()}
+
+    # -- runtime plumbing ---------------------------------------------------
+    def set_stream(self, stream_handle: Optional[int]):
+        """Issue all work on a caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._check(self._lib.pt_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def set_profiling(self, flags: int):
+        self._check(self._lib.pt_set_profiling(self._h, int(flags)))
+
+    def profile(self) -> dict:
+        p = PtProfile()
+        self._check(self._lib.pt_get_profile(self._h, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in PtProfile._fields_}
+
+    def set_tuning(self, path_capacity: int = 0, blocks_per_sm: int = 0):
+        self._check(self._lib.pt_set_tuning(self._h, int(path_capacity), int(blocks_per_sm)))
+
+    def rng_tape(self, first_wave: int, waves: int, stride: int) -> np.ndarray:
+        out = np.zeros((waves, self.width * self.height, stride), np.float32)
+        self._check(self._lib.pt_rng_tape(self._h, int(first_wave), int(waves), int(stride), _ptr(out, _fp)))
+        return out

@@ -1,0 +1,332 @@
+"""Host-side mesh container and the procedural scene generator for the benchmark scenes.
+
+``HostMesh`` is the flat structure-of-arrays form of the reference's
+``HostMesh`` (Application/src/MeshBuilder/HostMesh.h:9-28): per triangle three
+positions, three shading normals, three uvs and a material index, plus the
+material and texture banks.
+
+The generator is a small L-system rewriter + turtle + tube loft that produces
+the benchmark scenes.  It follows the reference's turtle conventions
+(Application/src/Procedural/Turtle.cpp:12-282): the turtle starts at the
+origin heading -Z with up +Y, ``Yaw`` turns about up, ``Pitch`` about
+right = up x tangent, ``Roll`` about the tangent, ``F`` appends a state and
+brackets / ``f`` close the current segment.  Each segment is lofted as an
+n-gon tube with rings at its states and flat caps (Loft.cpp:108-155).  It is a
+scene generator only; the path tracer consumes whatever mesh it is given.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .records import MATERIAL_DTYPE, TEXTURE_DTYPE, default_material, default_params, look_at_camera
+
+
+@dataclasses.dataclass
+class HostMesh:
+    positions: np.ndarray        # (N, 3, 3) float32
+    normals: np.ndarray          # (N, 3, 3) float32
+    uvs: np.ndarray              # (N, 3, 2) float32
+    material_ids: np.ndarray     # (N,) uint32
+    materials: np.ndarray        # (M,) MATERIAL_DTYPE
+    textures: np.ndarray         # (K,) TEXTURE_DTYPE
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.positions.shape[0])
+
+    @staticmethod
+    def empty() -> "HostMesh":
+        return HostMesh(np.zeros((0, 3, 3), np.float32), np.zeros((0, 3, 3), np.float32),
+                        np.zeros((0, 3, 2), np.float32), np.zeros((0,), np.uint32),
+                        np.zeros((0,), MATERIAL_DTYPE), np.zeros((0,), TEXTURE_DTYPE))
+
+    def contiguous(self) -> "HostMesh":
+        return HostMesh(np.ascontiguousarray(self.positions, np.float32),
+                        np.ascontiguousarray(self.normals, np.float32),
+                        np.ascontiguousarray(self.uvs, np.float32),
+                        np.ascontiguousarray(self.material_ids, np.uint32),
+                        np.ascontiguousarray(self.materials, MATERIAL_DTYPE),
+                        np.ascontiguousarray(self.textures, TEXTURE_DTYPE))
+
+    @staticmethod
+    def concat(parts: Sequence["HostMesh"]) -> "HostMesh":
+        """Appends meshes like hostMeshAppend (HostMesh.h:77-117): material ids are offset."""
+        pos, nrm, uv, mid, mats, texs = [], [], [], [], [], []
+        mat_off = 0
+        for p in parts:
+            pos.append(p.positions)
+            nrm.append(p.normals)
+            uv.append(p.uvs)
+            mid.append(p.material_ids.astype(np.uint32) + np.uint32(mat_off))
+            mats.append(p.materials)
+            texs.append(p.textures)
+            mat_off += len(p.materials)
+        return HostMesh(np.concatenate(pos).astype(np.float32), np.concatenate(nrm).astype(np.float32),
+                        np.concatenate(uv).astype(np.float32), np.concatenate(mid).astype(np.uint32),
+                        np.concatenate(mats), np.concatenate(texs))
+
+    def bounds(self) -> Tuple[np.ndarray, np.ndarray]:
+        p = self.positions.reshape(-1, 3)
+        return p.min(axis=0), p.max(axis=0)
+
+
+def quad_mesh(center, u_axis, v_axis, material: np.ndarray, normal=None) -> HostMesh:
+    """Two-triangle rectangle spanning center +- u_axis/2 +- v_axis/2."""
+    c = np.asarray(center, np.float32)
+    u = np.asarray(u_axis, np.float32) * 0.5
+    v = np.asarray(v_axis, np.float32) * 0.5
+    p00, p10, p11, p01 = c - u - v, c + u - v, c + u + v, c - u + v
+    n = np.cross(u, v) if normal is None else np.asarray(normal, np.float32)
+    n = (n / np.linalg.norm(n)).astype(np.float32)
+    pos = np.array([[p00, p10, p11], [p00, p11, p01]], np.float32)
+    nrm = np.broadcast_to(n, (2, 3, 3)).astype(np.float32)
+    uvs = np.array([[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]], np.float32)
+    return HostMesh(pos, nrm, uvs, np.zeros(2, np.uint32), np.atleast_1d(material).astype(MATERIAL_DTYPE),
+                    np.zeros(0, TEXTURE_DTYPE))
+
+
+# ---------------------------------------------------------------------------
+# L-system rewriting.  A module is (name, args); rules map a name to a
+# function of (args, rng) returning the successor module list.
+# ---------------------------------------------------------------------------
+Module = Tuple[str, Tuple[float, ...]]
+Rule = Callable[[Tuple[float, ...], np.random.Generator], List[Module]]
+
+
+def expand(axiom: List[Module], rules: Dict[str, Rule], iterations: int, seed: int = 0) -> List[Module]:
+    rng = np.random.default_rng(seed)
+    word = list(axiom)
+    for _ in range(iterations):
+        out: List[Module] = []
+        for name, args in word:
+            rule = rules.get(name)
+            if rule is None:
+                out.append((name, args))
+            else:
+                out.extend(rule(args, rng))
+        word = out
+    return word
+
+
+# ---------------------------------------------------------------------------
+# Turtle (Turtle.cpp:110-282).
+# ---------------------------------------------------------------------------
+def _rotate(v: np.ndarray, axis: np.ndarray, deg: float) -> np.ndarray:
+    n = axis / np.linalg.norm(axis)
+    a = math.radians(deg)
+    c, s = math.cos(a), math.sin(a)
+    return v * c + np.cross(n, v) * s + n * np.dot(n, v) * (1.0 - c)
+
+
+@dataclasses.dataclass
+class Segment:
+    points: List[np.ndarray]
+    tangents: List[np.ndarray]
+    radii: List[float]
+    material: int
+    tag: int  # caller-defined (branch depth for leaves, etc.)
+
+
+def turtle(word: List[Module], start_tangent=(0.0, 0.0, -1.0), start_up=(0.0, 1.0, 0.0),
+           default_step: float = 1.0, default_radius: float = 0.1,
+           leaf_symbol: Optional[str] = None) -> Tuple[List[Segment], List[Tuple[np.ndarray, np.ndarray, np.ndarray, float]]]:
+    """Runs the turtle; returns tube segments and leaf frames (position, tangent, up, size)."""
+    pos = np.zeros(3)
+    tan = np.asarray(start_tangent, np.float64)
+    up = np.asarray(start_up, np.float64)
+    stack: List[Tuple[np.ndarray, np.ndarray, np.ndarray, int]] = []
+    states: List[Tuple[np.ndarray, np.ndarray, float]] = []
+    segments: List[Segment] = []
+    leaves: List[Tuple[np.ndarray, np.ndarray, np.ndarray, float]] = []
+    material = 0
+
+    def flush():
+        nonlocal states
+        if not states:
+            return
+        last_r = states[-1][2]
+        states.append((pos.copy(), tan.copy(), last_r))
+        segments.append(Segment([s[0] for s in states], [s[1] for s in states], [s[2] for s in states],
+                                material, len(stack)))
+        states = []
+
+    for name, args in word:
+        if name == "[":
+            flush()
+            stack.append((pos.copy(), tan.copy(), up.copy(), material))
+        elif name == "]":
+            flush()
+            if stack:
+                pos, tan, up, material = stack.pop()
+        elif name == "F":
+            step = args[0] if args else default_step
+            radius = args[1] if len(args) > 1 else (args[0] if args else default_radius)
+            states.append((pos.copy(), tan.copy(), float(radius)))
+            pos = pos + tan * step
+        elif name == "f":
+            flush()
+            pos = pos + tan * (args[0] if args else default_step)
+        elif name == "Yaw":
+            tan = _rotate(tan, up, args[0]); up = _rotate(up, up, args[0])
+            tan /= np.linalg.norm(tan); up /= np.linalg.norm(up)
+        elif name in ("Pitch", "Pich"):
+            right = np.cross(up, tan); right /= np.linalg.norm(right)
+            tan = _rotate(tan, right, args[0]); up = _rotate(up, right, args[0])
+            tan /= np.linalg.norm(tan); up /= np.linalg.norm(up)
+        elif name == "Roll":
+            up = _rotate(up, tan, args[0]); up /= np.linalg.norm(up)
+        elif name == "Mat":
+            material = int(args[0])
+        elif leaf_symbol is not None and name == leaf_symbol:
+            leaves.append((pos.copy(), tan.copy(), up.copy(), float(args[0]) if args else 1.0))
+    flush()
+    return segments, leaves
+
+
+# ---------------------------------------------------------------------------
+# Loft (Loft.cpp:108-155): rings at every state, side quads as two triangles,
+# flat caps at both ends.  Vectorised over all segments that have the same
+# number of rings.
+# ---------------------------------------------------------------------------
+def _perp_frames(tangents: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    t = tangents / np.linalg.norm(tangents, axis=-1, keepdims=True)
+    ref = np.where(np.abs(t[..., 1:2]) < 0.99, np.array([0.0, 1.0, 0.0]), np.array([1.0, 0.0, 0.0]))
+    a = np.cross(ref, t)
+    a /= np.linalg.norm(a, axis=-1, keepdims=True)
+    b = np.cross(t, a)
+    return a, b
+
+
+def loft(segments: Sequence[Segment], sides: int = 8, material_ids: Optional[Sequence[int]] = None) -> HostMesh:
+    groups: Dict[int, List[int]] = {}
+    for i, s in enumerate(segments):
+        groups.setdefault(len(s.points), []).append(i)
+    parts_pos, parts_nrm, parts_uv, parts_mid = [], [], [], []
+    ang = np.arange(sides + 1) * (2.0 * math.pi / sides)
+    cs, sn = np.cos(ang), np.sin(ang)
+    for rings, idxs in groups.items():
+        P = np.array([[segments[i].points[k] for k in range(rings)] for i in idxs])      # (S, R, 3)
+        T = np.array([[segments[i].tangents[k] for k in range(rings)] for i in idxs])
+        Rr = np.array([[segments[i].radii[k] for k in range(rings)] for i in idxs])     # (S, R)
+        T[:, -1] = T[:, -2] if rings > 1 else T[:, -1]
+        A, B = _perp_frames(T)
+        # Parallel-transport-free approximation: per-ring frame from the ring tangent.
+        dirs = A[:, :, None, :] * cs[None, None, :, None] + B[:, :, None, :] * sn[None, None, :, None]  # (S,R,C+1,3)
+        ringp = P[:, :, None, :] + dirs * Rr[:, :, None, None]
+        S = len(idxs)
+        tris_pos, tris_nrm, tris_uv = [], [], []
+        for r in range(rings - 1):
+            v0, v1 = r / max(rings - 1, 1), (r + 1) / max(rings - 1, 1)
+            for k in range(sides):
+                a00, a01 = ringp[:, r, k], ringp[:, r, k + 1]
+                a10, a11 = ringp[:, r + 1, k], ringp[:, r + 1, k + 1]
+                n00, n01 = dirs[:, r, k], dirs[:, r, k + 1]
+                n10, n11 = dirs[:, r + 1, k], dirs[:, r + 1, k + 1]
+                u0, u1 = k / sides, (k + 1) / sides
+                tris_pos += [np.stack([a00, a01, a10], 1), np.stack([a01, a11, a10], 1)]
+                tris_nrm += [np.stack([n00, n01, n10], 1), np.stack([n01, n11, n10], 1)]
+                uvq = np.array([[[u0, v0], [u1, v0], [u0, v1]], [[u1, v0], [u1, v1], [u0, v1]]], np.float32)
+                tris_uv += [np.broadcast_to(uvq[0], (S, 3, 2)), np.broadcast_to(uvq[1], (S, 3, 2))]
+        # caps
+        for end, sign in ((0, -1.0), (rings - 1, 1.0)):
+            tn = T[:, end] / np.linalg.norm(T[:, end], axis=-1, keepdims=True) * sign
+            c = P[:, end]
+            for k in range(sides):
+                r0, r1 = ringp[:, end, k], ringp[:, end, k + 1]
+                tri = np.stack([c, r1, r0] if sign < 0 else [c, r0, r1], 1)
+                tris_pos.append(tri)
+                tris_nrm.append(np.broadcast_to(tn[:, None, :], (S, 3, 3)))
+                tris_uv.append(np.broadcast_to(np.array([[0.5, 0.5], [1.0, 0.0], [0.0, 1.0]], np.float32), (S, 3, 2)))
+        pos = np.stack(tris_pos, 1).reshape(-1, 3, 3)     # segment-major
+        nrm = np.stack(tris_nrm, 1).reshape(-1, 3, 3)
+        uv = np.stack(tris_uv, 1).reshape(-1, 3, 2)
+        per = len(tris_pos)
+        mids = np.repeat(np.array([segments[i].material if material_ids is None else material_ids[i]
+                                   for i in idxs], np.uint32), per)
+        parts_pos.append(pos); parts_nrm.append(nrm); parts_uv.append(uv); parts_mid.append(mids)
+    if not parts_pos:
+        return HostMesh.empty()
+    return HostMesh(np.concatenate(parts_pos).astype(np.float32), np.concatenate(parts_nrm).astype(np.float32),
+                    np.concatenate(parts_uv).astype(np.float32), np.concatenate(parts_mid).astype(np.uint32),
+                    np.zeros(0, MATERIAL_DTYPE), np.zeros(0, TEXTURE_DTYPE))
+
+
+def leaf_quads(leaves, size: float, material: int) -> HostMesh:
+    """One two-triangle quad per leaf frame, spanning the leaf's up/tangent plane."""
+    if not leaves:
+        return HostMesh.empty()
+    P = np.array([l[0] for l in leaves]); T = np.array([l[1] for l in leaves]); U = np.array([l[2] for l in leaves])
+    s = np.array([l[3] for l in leaves])[:, None] * size
+    w = np.cross(T, U)
+    w /= np.linalg.norm(w, axis=-1, keepdims=True)
+    p00, p10 = P - w * s * 0.5, P + w * s * 0.5
+    p01, p11 = p00 + T * s, p10 + T * s
+    n = U / np.linalg.norm(U, axis=-1, keepdims=True)
+    pos = np.stack([np.stack([p00, p10, p11], 1), np.stack([p00, p11, p01], 1)], 1).reshape(-1, 3, 3)
+    nrm = np.repeat(n[:, None, None, :], 2, 1).repeat(3, 2).reshape(-1, 3, 3)
+    uv1 = np.array([[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]], np.float32)
+    uvs = np.broadcast_to(uv1, (len(leaves), 2, 3, 2)).reshape(-1, 3, 2)
+    return HostMesh(pos.astype(np.float32), nrm.astype(np.float32), uvs.astype(np.float32),
+                    np.full(len(leaves) * 2, material, np.uint32), np.zeros(0, MATERIAL_DTYPE),
+                    np.zeros(0, TEXTURE_DTYPE))
+
+
+# ---------------------------------------------------------------------------
+# Benchmark scenes.
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class SceneSpec:
+    name: str
+    mesh: HostMesh
+    camera: np.ndarray
+    params: np.ndarray
+    width: int
+    height: int
+    waves: int  # number of full-resolution waves a complete render takes (upper bound)
+
+
+def bracketed_ol_tree(iterations: int = 4, angle: float = 25.7, length: float = 0.1, radius: float = 0.02,
+                      sides: int = 8) -> HostMesh:
+    """F(h,r) -> F(h,r)[Yaw(a)F(h,r)]F(h,r)[Yaw(-a)F(h,r)]F(h,r) in the XY plane (5^n segments).
+
+    The turtle heads +Y with up +Z so that Yaw bends the branches in the XY plane
+    (the reference reaches the same orientation with a +90 degree instance pitch).
+    """
+    def rule(args, _rng):
+        h, r = args
+        F = ("F", (h, r))
+        return [F, ("[", ()), ("Yaw", (angle,)), F, ("]", ()), F, ("[", ()), ("Yaw", (-angle,)), F, ("]", ()), F]
+    word = expand([("F", (length, radius))], {"F": rule}, iterations)
+    segs, _ = turtle(word, start_tangent=(0.0, 1.0, 0.0), start_up=(0.0, 0.0, 1.0))
+    return loft(segs, sides)
+
+
+def config0_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> SceneSpec:
+    """Plain method, small: 625-segment bracketed tree, ground, one area light, pinhole 40 deg.
+
+    Bark (0.35, 0.22, 0.12) roughness 0.8; ground 0.5 grey roughness 1; a 1x1
+    light at height 5 (emission 10, white) offset 1.5 units in z so that the trunk
+    does not pass through it; black background; 64 spp fixed (min = max); max depth 8.
+    """
+    tree = bracketed_ol_tree()
+    tree.materials = np.array([default_material(r=0.35, g=0.22, b=0.12, roughness=0.8, metallic=0.0)],
+                              MATERIAL_DTYPE)
+    ground = quad_mesh((0, 0, 0), (10, 0, 0), (0, 0, -10),
+                       default_material(r=0.5, g=0.5, b=0.5, roughness=1.0), normal=(0, 1, 0))
+    light = quad_mesh((0, 5, 1.5), (1, 0, 0), (0, 0, 1),
+                      default_material(r=1.0, g=1.0, b=1.0, emission=10.0), normal=(0, -1, 0))
+    mesh = HostMesh.concat([tree, ground, light])
+    lo, hi = tree.bounds()
+    center = (lo + hi) * 0.5
+    extent = float(np.max(hi - lo))
+    dist = extent * 0.5 / math.tan(math.radians(20.0)) * 1.15
+    cam = look_at_camera((center[0], center[1], center[2] + dist), center, fov_y_deg=40.0,
+                         aspect=width / height)
+    params = default_params(background_r=0.0, background_g=0.0, background_b=0.0, max_path_depth=max_depth,
+                            russian_roulette_min_depth=3, min_samples=spp, max_samples_per_pixel=spp)
+    return SceneSpec("plain-small: 2D bracketed OL-system, 625 segments, 256x256, 64 spp, depth 8",
+                     mesh, cam, params, width, height, spp)

@@ -1,0 +1,302 @@
+"""ctypes bindings for the two CPU checkers (test infrastructure).
+
+* ``Checker("oracle")`` loads oracle/libpt_oracle.so -- this project's C++
+  restatement of the reference render path (FP32 ``orc_*`` and FP64 ``orc64_*``).
+* ``Checker("ref")`` loads oracle/_ref/libptref.so -- the reference's own
+  hot-path code compiled for the host (only where it could be built).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  Both libraries expose the same entry points, so a test can run
+one case through either and compare.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libpt_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libptref.so")
+REF_ROOT = "/root/reference"
+
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+_u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
+_i32p = C.POINTER(C.c_int32)
+
+
+def _ptr(a: Optional[np.ndarray], t):
+    if a is None:
+        return None
+    return a.ctypes.data_as(t)
+
+
+def _vp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return C.c_void_p(a.ctypes.data)
+
+
+def build_oracle(force: bool = False) -> str:
+    """Compiles the restatement with make (gcc; no reference tree needed)."""
+    src = [os.path.join(HERE, f) for f in ("pt_oracle.cpp", "pt_oracle.h")]
+    if force or not os.path.exists(ORACLE_SO) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_SO) for s in src):
+        subprocess.run(["make", "-C", HERE, "liboracle"], check=True, stdout=subprocess.DEVNULL)
+    return ORACLE_SO
+
+
+def build_ref() -> Optional[str]:
+    """Compiles the reference's own sources for the host where the reference tree exists."""
+    if os.path.exists(REF_SO) and not os.path.isdir(REF_ROOT):
+        return REF_SO
+    if not os.path.isdir(REF_ROOT):
+        return None
+    src = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "ref_shim", "curand_kernel.h")]
+    if not os.path.exists(REF_SO) or any(os.path.getmtime(s) > os.path.getmtime(REF_SO) for s in src):
+        subprocess.run(["make", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"], check=True, stdout=subprocess.DEVNULL)
+    return REF_SO
+
+
+class Checker:
+    def __init__(self, kind: str = "oracle"):
+        if kind == "oracle":
+            path, self.p = build_oracle(), "orc_"
+        elif kind == "ref":
+            path = build_ref()
+            if path is None or not os.path.exists(path):
+                raise FileNotFoundError("reference host build unavailable")
+            self.p = "ref_"
+        else:
+            raise ValueError(kind)
+        self.kind = kind
+        self.lib = C.CDLL(path)
+        L, p = self.lib, self.p
+        L[p + "scene_create"].restype = C.c_void_p
+        L[p + "scene_create"].argtypes = [C.c_int, _fp, _fp, _fp, _u32p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        L[p + "scene_destroy"].argtypes = [C.c_void_p]
+        L[p + "scene_bvh_node_count"].argtypes = [C.c_void_p]
+        L[p + "scene_emissive"].argtypes = [C.c_void_p, _u32p, _fp]
+        L[p + "trace_rays"].argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp, _u8p, _fp, _u32p, _fp, _fp]
+        L[p + "env_create"].restype = C.c_void_p
+        L[p + "env_create"].argtypes = [C.c_int, C.c_int, _fp]
+        L[p + "env_destroy"].argtypes = [C.c_void_p]
+        L[p + "env_tables"].argtypes = [C.c_void_p, _fp, _fp]
+        L[p + "render"].argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                    C.c_uint, _fp, C.c_int, _i32p, C.c_int, _fp, _u32p, _fp, _fp, _u8p, C.c_int]
+        L[p + "trace_pixel"].argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                         C.c_int, C.c_int, C.c_uint, _fp, C.c_int, _fp]
+        L[p + "brdf_eval"].argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, _fp, _fp]
+        L[p + "brdf_pdf"].restype = C.c_float
+        L[p + "brdf_pdf"].argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, _fp]
+        L[p + "brdf_sample"].argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, C.c_float, C.c_float, _fp, _fp,
+                                         _fp, _fp, _i32p]
+        L[p + "brdf_apply_throughput"].argtypes = [_fp, _fp, _fp, C.c_void_p, C.c_float, C.c_float, C.c_float, _fp]
+        L[p + "camera_ray"].argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_float, _fp, _fp]
+        L[p + "env_sample"].argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, _fp, _fp]
+        L[p + "env_pdf"].restype = C.c_float
+        L[p + "env_pdf"].argtypes = [C.c_void_p, C.c_void_p, _fp]
+        L[p + "env_eval"].argtypes = [C.c_void_p, C.c_void_p, _fp, _fp]
+        L[p + "sample_emissive"].argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, _fp, _fp, _fp, _fp]
+        L[p + "is_converged"].argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_int, C.c_float]
+        if kind == "oracle":
+            L.orc64_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                       C.c_uint, _fp, C.c_int, _i32p, C.c_int, _dp, _u32p, _dp, _dp, _u8p, C.c_int]
+            L.orc_trace_rays_bruteforce.argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp, _u8p, _fp, _u32p]
+            L.orc_reference_seed.restype = C.c_uint
+            L.orc_reference_seed.argtypes = [C.c_int, C.c_int, C.c_uint]
+
+    def fn(self, name):
+        return self.lib[self.p + name]
+
+    def max_threads(self) -> int:
+        return int(self.fn("max_threads")())
+
+    # -- scene ------------------------------------------------------------
+    def scene(self, mesh) -> "CheckerScene":
+        return CheckerScene(self, mesh)
+
+    def env(self, rgb: np.ndarray) -> "CheckerEnv":
+        return CheckerEnv(self, rgb)
+
+    # -- BSDF / lights / camera ------------------------------------------
+    def brdf_eval(self, normal, wo, material, eta, wi, debug=0):
+        out = np.zeros(3, np.float32)
+        self.fn("brdf_eval")(_ptr(np.ascontiguousarray(normal, np.float32), _fp),
+                             _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material), C.c_float(eta),
+                             int(debug), _ptr(np.ascontiguousarray(wi, np.float32), _fp), _ptr(out, _fp))
+        return out
+
+    def brdf_pdf(self, normal, wo, material, eta, wi, debug=0) -> float:
+        return float(self.fn("brdf_pdf")(_ptr(np.ascontiguousarray(normal, np.float32), _fp),
+                                         _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material),
+                                         C.c_float(eta), int(debug),
+                                         _ptr(np.ascontiguousarray(wi, np.float32), _fp)))
+
+    def brdf_sample(self, normal, wo, material, eta, u1, u2, debug=0):
+        d = np.zeros(3, np.float32); pdf = np.zeros(1, np.float32); ne = np.zeros(1, np.float32)
+        off = np.zeros(3, np.float32); flags = np.zeros(1, np.int32)
+        steps = self.fn("brdf_sample")(_ptr(np.ascontiguousarray(normal, np.float32), _fp),
+                                       _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material),
+                                       C.c_float(eta), int(debug), C.c_float(u1), C.c_float(u2), _ptr(d, _fp),
+                                       _ptr(pdf, _fp), _ptr(ne, _fp), _ptr(off, _fp), _ptr(flags, _i32p))
+        f = int(flags[0])
+        return dict(direction=d, pdf=float(pdf[0]), valid=bool(f & 1), transmitted=bool(f & 2),
+                    subsurface=bool(f & 4), next_eta=float(ne[0]), exit_offset=off, steps=int(steps))
+
+    def brdf_apply_throughput(self, throughput, normal, wo, material, eta, u1, u2):
+        out = np.zeros(3, np.float32)
+        self.fn("brdf_apply_throughput")(_ptr(np.ascontiguousarray(throughput, np.float32), _fp),
+                                         _ptr(np.ascontiguousarray(normal, np.float32), _fp),
+                                         _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material),
+                                         C.c_float(eta), C.c_float(u1), C.c_float(u2), _ptr(out, _fp))
+        return out
+
+    def camera_ray(self, camera, u, v, l1, l2):
+        o = np.zeros(3, np.float32); d = np.zeros(3, np.float32)
+        self.fn("camera_ray")(_vp(camera), C.c_float(u), C.c_float(v), C.c_float(l1), C.c_float(l2),
+                              _ptr(o, _fp), _ptr(d, _fp))
+        return o, d
+
+    def is_converged(self, n, mean, m2, min_samples, thr) -> bool:
+        return bool(self.fn("is_converged")(int(n), C.c_float(mean), C.c_float(m2), int(min_samples),
+                                            C.c_float(thr)))
+
+
+class CheckerScene:
+    def __init__(self, chk: Checker, mesh):
+        self.chk = chk
+        m = mesh.contiguous()
+        self.mesh = m
+        self.h = chk.fn("scene_create")(m.triangle_count, _ptr(m.positions, _fp), _ptr(m.normals, _fp),
+                                        _ptr(m.uvs, _fp), _ptr(m.material_ids, _u32p), len(m.materials),
+                                        _vp(m.materials) if len(m.materials) else None, len(m.textures),
+                                        _vp(m.textures) if len(m.textures) else None)
+        if not self.h:
+            raise RuntimeError("scene build failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.chk.fn("scene_destroy")(self.h)
+            self.h = None
+
+    def bvh_node_count(self) -> int:
+        return int(self.chk.fn("scene_bvh_node_count")(self.h))
+
+    def emissive(self):
+        n = int(self.chk.fn("scene_emissive")(self.h, None, None))
+        idx = np.zeros(max(n, 1), np.uint32)
+        cdf = np.zeros(n + 1, np.float32)
+        self.chk.fn("scene_emissive")(self.h, _ptr(idx, _u32p), _ptr(cdf, _fp))
+        return idx[:n], cdf
+
+    def trace(self, origins, dirs, tmin=None, tmax=None):
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        n = o.shape[0]
+        tmin = np.zeros(n, np.float32) if tmin is None else np.ascontiguousarray(
+            np.broadcast_to(tmin, (n,)), np.float32)
+        tmax = np.full(n, 1.0e6, np.float32) if tmax is None else np.ascontiguousarray(
+            np.broadcast_to(tmax, (n,)), np.float32)
+        hit = np.zeros(n, np.uint8); t = np.zeros(n, np.float32); tri = np.zeros(n, np.uint32)
+        nrm = np.zeros((n, 3), np.float32); uv = np.zeros((n, 2), np.float32)
+        self.chk.fn("trace_rays")(self.h, n, _ptr(o, _fp), _ptr(d, _fp), _ptr(tmin, _fp), _ptr(tmax, _fp),
+                                  _ptr(hit, _u8p), _ptr(t, _fp), _ptr(tri, _u32p), _ptr(nrm, _fp), _ptr(uv, _fp))
+        return dict(hit=hit.astype(bool), t=t, tri=tri, normal=nrm, uv=uv)
+
+    def trace_bruteforce(self, origins, dirs, tmin=None, tmax=None):
+        assert self.chk.kind == "oracle"
+        o = np.ascontiguousarray(origins, np.float32)
+        d = np.ascontiguousarray(dirs, np.float32)
+        n = o.shape[0]
+        tmin = np.zeros(n, np.float32) if tmin is None else np.ascontiguousarray(
+            np.broadcast_to(tmin, (n,)), np.float32)
+        tmax = np.full(n, 1.0e6, np.float32) if tmax is None else np.ascontiguousarray(
+            np.broadcast_to(tmax, (n,)), np.float32)
+        hit = np.zeros(n, np.uint8); t = np.zeros(n, np.float32); tri = np.zeros(n, np.uint32)
+        self.chk.lib.orc_trace_rays_bruteforce(self.h, n, _ptr(o, _fp), _ptr(d, _fp), _ptr(tmin, _fp),
+                                               _ptr(tmax, _fp), _ptr(hit, _u8p), _ptr(t, _fp), _ptr(tri, _u32p))
+        return dict(hit=hit.astype(bool), t=t, tri=tri)
+
+    def sample_emissive(self, u_tri, u1, u2):
+        p = np.zeros(3, np.float32); n = np.zeros(3, np.float32); L = np.zeros(3, np.float32)
+        pdf = np.zeros(1, np.float32)
+        ok = self.chk.fn("sample_emissive")(self.h, C.c_float(u_tri), C.c_float(u1), C.c_float(u2), _ptr(p, _fp),
+                                            _ptr(n, _fp), _ptr(L, _fp), _ptr(pdf, _fp))
+        return bool(ok), p, n, L, float(pdf[0])
+
+    def render(self, camera, params, width, height, waves, seed_base=1, tape=None, tape_stride=0, env=None,
+               pixels=None, state=None, threads=0, fp64=False):
+        """Runs adaptive waves like the reference render loop; returns the accumulation state."""
+        P = width * height
+        ft = np.float64 if fp64 else np.float32
+        if state is None:
+            state = dict(acc=np.zeros((P, 4), ft), counts=np.zeros(P, np.uint32), lum_mean=np.zeros(P, ft),
+                         m2=np.zeros(P, ft), converged=np.zeros(P, np.uint8))
+        pix = None if pixels is None else np.ascontiguousarray(pixels, np.int32)
+        tp = None if tape is None else np.ascontiguousarray(tape, np.float32)
+        args = (self.h, env.h if env is not None else None, _vp(camera), _vp(params), width, height, waves,
+                C.c_uint(seed_base), _ptr(tp, _fp), int(tape_stride), _ptr(pix, _i32p),
+                0 if pix is None else len(pix))
+        if fp64:
+            assert self.chk.kind == "oracle"
+            err = self.chk.lib.orc64_render(*args, _ptr(state["acc"], _dp), _ptr(state["counts"], _u32p),
+                                            _ptr(state["lum_mean"], _dp), _ptr(state["m2"], _dp),
+                                            _ptr(state["converged"], _u8p), int(threads))
+        else:
+            err = self.chk.fn("render")(*args, _ptr(state["acc"], _fp), _ptr(state["counts"], _u32p),
+                                        _ptr(state["lum_mean"], _fp), _ptr(state["m2"], _fp),
+                                        _ptr(state["converged"], _u8p), int(threads))
+        state["tape_errors"] = int(err)
+        return state
+
+    def trace_pixel(self, camera, params, width, height, idx, sample_index, global_seed, tape_row, env=None):
+        out = np.zeros(3, np.float32)
+        row = np.ascontiguousarray(tape_row, np.float32)
+        used = self.chk.fn("trace_pixel")(self.h, env.h if env is not None else None, _vp(camera), _vp(params),
+                                          width, height, idx, sample_index, C.c_uint(global_seed),
+                                          _ptr(row, _fp), len(row), _ptr(out, _fp))
+        return out, int(used)
+
+
+class CheckerEnv:
+    def __init__(self, chk: Checker, rgb: np.ndarray):
+        self.chk = chk
+        self.rgb = np.ascontiguousarray(rgb, np.float32)
+        self.height, self.width = self.rgb.shape[:2]
+        self.h = chk.fn("env_create")(self.width, self.height, _ptr(self.rgb, _fp))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.chk.fn("env_destroy")(self.h)
+            self.h = None
+
+    def tables(self):
+        marg = np.zeros(self.height + 1, np.float32)
+        row = np.zeros(self.height * (self.width + 1), np.float32)
+        self.chk.fn("env_tables")(self.h, _ptr(marg, _fp), _ptr(row, _fp))
+        return marg, row
+
+    def sample(self, params, u1, u2):
+        d = np.zeros(3, np.float32); pdf = np.zeros(1, np.float32)
+        self.chk.fn("env_sample")(self.h, _vp(params), C.c_float(u1), C.c_float(u2), _ptr(d, _fp), _ptr(pdf, _fp))
+        return d, float(pdf[0])
+
+    def pdf(self, params, d):
+        return float(self.chk.fn("env_pdf")(self.h, _vp(params), _ptr(np.ascontiguousarray(d, np.float32), _fp)))
+
+    def eval(self, params, d):
+        out = np.zeros(3, np.float32)
+        self.chk.fn("env_eval")(self.h, _vp(params), _ptr(np.ascontiguousarray(d, np.float32), _fp), _ptr(out, _fp))
+        return out
+
+
+def reference_available() -> bool:
+    try:
+        return build_ref() is not None and os.path.exists(REF_SO)
+    except Exception:
+        return False
