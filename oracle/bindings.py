@@ -39,7 +39,15 @@ def _ptr(a: Optional[np.ndarray], t):
 def _vp(a: Optional[np.ndarray]):
     if a is None:
         return None
+    assert isinstance(a, np.ndarray), "pass records through _rec() so that they stay alive during the call"
     return C.c_void_p(a.ctypes.data)
+
+
+def _rec(a):
+    """Contiguous array form of a record (np.void rows included); keep the result alive across the call."""
+    if a is None:
+        return None
+    return np.ascontiguousarray(np.array(a) if isinstance(a, np.void) else a)
 
 
 def build_oracle(force: bool = False) -> str:
@@ -76,33 +84,37 @@ class Checker:
         self.kind = kind
         self.lib = C.CDLL(path)
         L, p = self.lib, self.p
-        L[p + "scene_create"].restype = C.c_void_p
-        L[p + "scene_create"].argtypes = [C.c_int, _fp, _fp, _fp, _u32p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
-        L[p + "scene_destroy"].argtypes = [C.c_void_p]
-        L[p + "scene_bvh_node_count"].argtypes = [C.c_void_p]
-        L[p + "scene_emissive"].argtypes = [C.c_void_p, _u32p, _fp]
-        L[p + "trace_rays"].argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp, _u8p, _fp, _u32p, _fp, _fp]
-        L[p + "env_create"].restype = C.c_void_p
-        L[p + "env_create"].argtypes = [C.c_int, C.c_int, _fp]
-        L[p + "env_destroy"].argtypes = [C.c_void_p]
-        L[p + "env_tables"].argtypes = [C.c_void_p, _fp, _fp]
-        L[p + "render"].argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+        getattr(L, p + "scene_create").restype = C.c_void_p
+        getattr(L, p + "scene_create").argtypes = [C.c_int, _fp, _fp, _fp, _u32p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        getattr(L, p + "scene_destroy").argtypes = [C.c_void_p]
+        getattr(L, p + "scene_bvh_node_count").argtypes = [C.c_void_p]
+        getattr(L, p + "scene_emissive").argtypes = [C.c_void_p, _u32p, _fp]
+        getattr(L, p + "trace_rays").argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp, _u8p, _fp, _u32p, _fp, _fp]
+        getattr(L, p + "env_create").restype = C.c_void_p
+        getattr(L, p + "env_create").argtypes = [C.c_int, C.c_int, _fp]
+        getattr(L, p + "env_destroy").argtypes = [C.c_void_p]
+        getattr(L, p + "env_tables").argtypes = [C.c_void_p, _fp, _fp]
+        getattr(L, p + "render").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                     C.c_uint, _fp, C.c_int, _i32p, C.c_int, _fp, _u32p, _fp, _fp, _u8p, C.c_int]
-        L[p + "trace_pixel"].argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+        getattr(L, p + "trace_pixel").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                          C.c_int, C.c_int, C.c_uint, _fp, C.c_int, _fp]
-        L[p + "brdf_eval"].argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, _fp, _fp]
-        L[p + "brdf_pdf"].restype = C.c_float
-        L[p + "brdf_pdf"].argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, _fp]
-        L[p + "brdf_sample"].argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, C.c_float, C.c_float, _fp, _fp,
+        getattr(L, p + "brdf_eval").argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, _fp, _fp]
+        getattr(L, p + "brdf_pdf").restype = C.c_float
+        getattr(L, p + "brdf_pdf").argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, _fp]
+        getattr(L, p + "brdf_sample").argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, C.c_float, C.c_float, _fp, _fp,
                                          _fp, _fp, _i32p]
-        L[p + "brdf_apply_throughput"].argtypes = [_fp, _fp, _fp, C.c_void_p, C.c_float, C.c_float, C.c_float, _fp]
-        L[p + "camera_ray"].argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_float, _fp, _fp]
-        L[p + "env_sample"].argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, _fp, _fp]
-        L[p + "env_pdf"].restype = C.c_float
-        L[p + "env_pdf"].argtypes = [C.c_void_p, C.c_void_p, _fp]
-        L[p + "env_eval"].argtypes = [C.c_void_p, C.c_void_p, _fp, _fp]
-        L[p + "sample_emissive"].argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, _fp, _fp, _fp, _fp]
-        L[p + "is_converged"].argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_int, C.c_float]
+        getattr(L, p + "brdf_apply_throughput").argtypes = [_fp, _fp, _fp, C.c_void_p, C.c_float, C.c_float, C.c_float, _fp]
+        getattr(L, p + "camera_ray").argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_float, _fp, _fp]
+        getattr(L, p + "env_sample").argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_float, _fp, _fp]
+        getattr(L, p + "env_pdf").restype = C.c_float
+        getattr(L, p + "env_pdf").argtypes = [C.c_void_p, C.c_void_p, _fp]
+        getattr(L, p + "env_eval").argtypes = [C.c_void_p, C.c_void_p, _fp, _fp]
+        getattr(L, p + "sample_emissive").argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float, _fp, _fp, _fp, _fp]
+        getattr(L, p + "is_converged").argtypes = [C.c_uint32, C.c_float, C.c_float, C.c_int, C.c_float]
+        getattr(L, p + "brdf_sample_transmit").argtypes = [_fp, _fp, C.c_void_p, C.c_float, C.c_int, C.c_float, C.c_float,
+                                                  _fp, _fp, _fp, _i32p]
+        getattr(L, p + "lobe_weights").argtypes = [C.c_void_p, _fp]
+        getattr(L, p + "resolve_material").argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_int, _fp]
         if kind == "oracle":
             L.orc64_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                        C.c_uint, _fp, C.c_int, _i32p, C.c_int, _dp, _u32p, _dp, _dp, _u8p, C.c_int]
@@ -111,7 +123,8 @@ class Checker:
             L.orc_reference_seed.argtypes = [C.c_int, C.c_int, C.c_uint]
 
     def fn(self, name):
-        return self.lib[self.p + name]
+        # attribute access caches the function object, so argtypes/restype set in __init__ stick
+        return getattr(self.lib, self.p + name)
 
     def max_threads(self) -> int:
         return int(self.fn("max_threads")())
@@ -125,42 +138,90 @@ class Checker:
 
     # -- BSDF / lights / camera ------------------------------------------
     def brdf_eval(self, normal, wo, material, eta, wi, debug=0):
+        material_ = _rec(material)
         out = np.zeros(3, np.float32)
         self.fn("brdf_eval")(_ptr(np.ascontiguousarray(normal, np.float32), _fp),
-                             _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material), C.c_float(eta),
+                             _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material_), C.c_float(eta),
                              int(debug), _ptr(np.ascontiguousarray(wi, np.float32), _fp), _ptr(out, _fp))
         return out
 
     def brdf_pdf(self, normal, wo, material, eta, wi, debug=0) -> float:
+        material_ = _rec(material)
         return float(self.fn("brdf_pdf")(_ptr(np.ascontiguousarray(normal, np.float32), _fp),
-                                         _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material),
+                                         _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material_),
                                          C.c_float(eta), int(debug),
                                          _ptr(np.ascontiguousarray(wi, np.float32), _fp)))
 
     def brdf_sample(self, normal, wo, material, eta, u1, u2, debug=0):
+        material_ = _rec(material)
         d = np.zeros(3, np.float32); pdf = np.zeros(1, np.float32); ne = np.zeros(1, np.float32)
         off = np.zeros(3, np.float32); flags = np.zeros(1, np.int32)
         steps = self.fn("brdf_sample")(_ptr(np.ascontiguousarray(normal, np.float32), _fp),
-                                       _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material),
+                                       _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material_),
                                        C.c_float(eta), int(debug), C.c_float(u1), C.c_float(u2), _ptr(d, _fp),
                                        _ptr(pdf, _fp), _ptr(ne, _fp), _ptr(off, _fp), _ptr(flags, _i32p))
         f = int(flags[0])
         return dict(direction=d, pdf=float(pdf[0]), valid=bool(f & 1), transmitted=bool(f & 2),
                     subsurface=bool(f & 4), next_eta=float(ne[0]), exit_offset=off, steps=int(steps))
 
+    def brdf_sample_transmit(self, normal, wo, material, eta, u1, u2, debug=0):
+        material_ = _rec(material)
+        d = np.zeros(3, np.float32); pdf = np.zeros(1, np.float32); ne = np.zeros(1, np.float32)
+        flags = np.zeros(1, np.int32)
+        self.fn("brdf_sample_transmit")(_ptr(np.ascontiguousarray(normal, np.float32), _fp),
+                                        _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material_),
+                                        C.c_float(eta), int(debug), C.c_float(u1), C.c_float(u2), _ptr(d, _fp),
+                                        _ptr(pdf, _fp), _ptr(ne, _fp), _ptr(flags, _i32p))
+        f = int(flags[0])
+        return dict(direction=d, pdf=float(pdf[0]), valid=bool(f & 1), transmitted=bool(f & 2),
+                    subsurface=bool(f & 4), next_eta=float(ne[0]))
+
+    def lobe_weights(self, material):
+        material_ = _rec(material)
+        out = np.zeros(4, np.float32)
+        self.fn("lobe_weights")(_vp(material_), _ptr(out, _fp))
+        return out
+
+    def resolve_material(self, material, u, v, textures=None):
+        material_ = _rec(material)
+        out = np.zeros(15, np.float32)
+        tex = None if textures is None or len(textures) == 0 else np.ascontiguousarray(textures)
+        self.fn("resolve_material")(_vp(material_), C.c_float(u), C.c_float(v), _vp(tex),
+                                    0 if tex is None else len(tex), _ptr(out, _fp))
+        return out
+
     def brdf_apply_throughput(self, throughput, normal, wo, material, eta, u1, u2):
+        material_ = _rec(material)
         out = np.zeros(3, np.float32)
         self.fn("brdf_apply_throughput")(_ptr(np.ascontiguousarray(throughput, np.float32), _fp),
                                          _ptr(np.ascontiguousarray(normal, np.float32), _fp),
-                                         _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material),
+                                         _ptr(np.ascontiguousarray(wo, np.float32), _fp), _vp(material_),
                                          C.c_float(eta), C.c_float(u1), C.c_float(u2), _ptr(out, _fp))
         return out
 
     def camera_ray(self, camera, u, v, l1, l2):
+        camera_ = _rec(camera)
         o = np.zeros(3, np.float32); d = np.zeros(3, np.float32)
-        self.fn("camera_ray")(_vp(camera), C.c_float(u), C.c_float(v), C.c_float(l1), C.c_float(l2),
+        self.fn("camera_ray")(_vp(camera_), C.c_float(u), C.c_float(v), C.c_float(l1), C.c_float(l2),
                               _ptr(o, _fp), _ptr(d, _fp))
         return o, d
+
+    # solid background (no environment map): LightSamplingCore.h:56-77, 149-159
+    def env_sample_solid(self, params, u1, u2):
+        params_ = _rec(params)
+        d = np.zeros(3, np.float32); pdf = np.zeros(1, np.float32)
+        self.fn("env_sample")(None, _vp(params_), C.c_float(u1), C.c_float(u2), _ptr(d, _fp), _ptr(pdf, _fp))
+        return d, float(pdf[0])
+
+    def env_pdf_solid(self, params, d):
+        params_ = _rec(params)
+        return float(self.fn("env_pdf")(None, _vp(params_), _ptr(np.ascontiguousarray(d, np.float32), _fp)))
+
+    def env_eval_solid(self, params, d):
+        params_ = _rec(params)
+        out = np.zeros(3, np.float32)
+        self.fn("env_eval")(None, _vp(params_), _ptr(np.ascontiguousarray(d, np.float32), _fp), _ptr(out, _fp))
+        return out
 
     def is_converged(self, n, mean, m2, min_samples, thr) -> bool:
         return bool(self.fn("is_converged")(int(n), C.c_float(mean), C.c_float(m2), int(min_samples),
@@ -232,6 +293,7 @@ class CheckerScene:
     def render(self, camera, params, width, height, waves, seed_base=1, tape=None, tape_stride=0, env=None,
                pixels=None, state=None, threads=0, fp64=False):
         """Runs adaptive waves like the reference render loop; returns the accumulation state."""
+        camera_, params_ = _rec(camera), _rec(params)
         P = width * height
         ft = np.float64 if fp64 else np.float32
         if state is None:
@@ -239,7 +301,7 @@ class CheckerScene:
                          m2=np.zeros(P, ft), converged=np.zeros(P, np.uint8))
         pix = None if pixels is None else np.ascontiguousarray(pixels, np.int32)
         tp = None if tape is None else np.ascontiguousarray(tape, np.float32)
-        args = (self.h, env.h if env is not None else None, _vp(camera), _vp(params), width, height, waves,
+        args = (self.h, env.h if env is not None else None, _vp(camera_), _vp(params_), width, height, waves,
                 C.c_uint(seed_base), _ptr(tp, _fp), int(tape_stride), _ptr(pix, _i32p),
                 0 if pix is None else len(pix))
         if fp64:
@@ -255,9 +317,11 @@ class CheckerScene:
         return state
 
     def trace_pixel(self, camera, params, width, height, idx, sample_index, global_seed, tape_row, env=None):
+        camera_ = _rec(camera)
+        params_ = _rec(params)
         out = np.zeros(3, np.float32)
         row = np.ascontiguousarray(tape_row, np.float32)
-        used = self.chk.fn("trace_pixel")(self.h, env.h if env is not None else None, _vp(camera), _vp(params),
+        used = self.chk.fn("trace_pixel")(self.h, env.h if env is not None else None, _vp(camera_), _vp(params_),
                                           width, height, idx, sample_index, C.c_uint(global_seed),
                                           _ptr(row, _fp), len(row), _ptr(out, _fp))
         return out, int(used)
@@ -282,16 +346,19 @@ class CheckerEnv:
         return marg, row
 
     def sample(self, params, u1, u2):
+        params_ = _rec(params)
         d = np.zeros(3, np.float32); pdf = np.zeros(1, np.float32)
-        self.chk.fn("env_sample")(self.h, _vp(params), C.c_float(u1), C.c_float(u2), _ptr(d, _fp), _ptr(pdf, _fp))
+        self.chk.fn("env_sample")(self.h, _vp(params_), C.c_float(u1), C.c_float(u2), _ptr(d, _fp), _ptr(pdf, _fp))
         return d, float(pdf[0])
 
     def pdf(self, params, d):
-        return float(self.chk.fn("env_pdf")(self.h, _vp(params), _ptr(np.ascontiguousarray(d, np.float32), _fp)))
+        params_ = _rec(params)
+        return float(self.chk.fn("env_pdf")(self.h, _vp(params_), _ptr(np.ascontiguousarray(d, np.float32), _fp)))
 
     def eval(self, params, d):
+        params_ = _rec(params)
         out = np.zeros(3, np.float32)
-        self.chk.fn("env_eval")(self.h, _vp(params), _ptr(np.ascontiguousarray(d, np.float32), _fp), _ptr(out, _fp))
+        self.chk.fn("env_eval")(self.h, _vp(params_), _ptr(np.ascontiguousarray(d, np.float32), _fp), _ptr(out, _fp))
         return out
 
 

@@ -465,6 +465,43 @@ int orc_sample_emissive(void* scene, float uTri, float u1, float u2, float* outP
     return ok ? 1 : 0;
 }
 
+int orc_brdf_sample_transmit(const float* normal, const float* wo, const void* material, float eta, int debug,
+    float u1, float u2, float* outDir, float* outPdf, float* outNextEta, int* outFlags)
+{
+    const Sample<float> r = sampleTransmit(makeCtx(normal, wo, material, eta, debug), u1, u2);
+    outDir[0] = r.dir.x;
+    outDir[1] = r.dir.y;
+    outDir[2] = r.dir.z;
+    *outPdf = r.pdf;
+    *outNextEta = r.nextEta;
+    *outFlags = (r.valid ? 1 : 0) | (r.transmitted ? 2 : 0) | (r.sss ? 4 : 0);
+    return r.sssSteps;
+}
+
+void orc_lobe_weights(const void* material, float* out)
+{
+    const float zero[3] = {0.0f, 0.0f, 1.0f};
+    const Lobes<float> w = lobes(makeCtx(zero, zero, material, 1.0f, 0));
+    out[0] = w.diffuse;
+    out[1] = w.specular;
+    out[2] = w.transmit;
+    out[3] = w.subsurface;
+}
+
+void orc_resolve_material(const void* material, float u, float v, const void* textures, int textureCount, float* out)
+{
+    MaterialRec m;
+    std::memcpy(&m, material, sizeof(m));
+    std::vector<TextureRec> bank(static_cast<size_t>(textureCount > 0 ? textureCount : 0));
+    if (textureCount > 0) {
+        std::memcpy(bank.data(), textures, sizeof(TextureRec) * static_cast<size_t>(textureCount));
+    }
+    const Mat<float> r = resolve<float>(m, V2<float>{u, v}, bank);
+    const float vals[15] = {r.r, r.g, r.b, r.roughness, r.metallic, r.transmission, r.thin, r.ior, r.subsurface,
+        r.emission, r.diffuseRoughness, r.scatterR, r.scatterG, r.scatterB, r.specular};
+    std::memcpy(out, vals, sizeof(vals));
+}
+
 int orc_is_converged(uint32_t n, float mean, float m2, int minSamples, float thr)
 {
     return isConverged(n, mean, m2, minSamples, thr) ? 1 : 0;

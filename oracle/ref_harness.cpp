@@ -590,6 +590,50 @@ int ref_sample_emissive(void* sceneHandle, float uTri, float u1, float u2, float
     return ok ? 1 : 0;
 }
 
+// PrincipledBrdf::sampleTransmit alone (PrincipledBrdf.h:476-551).
+int ref_brdf_sample_transmit(const float* normal, const float* wo, const void* material, float etaMedium,
+    int debugFlags, float u1, float u2, float* outDir, float* outPdf, float* outNextEta, int* outFlags)
+{
+    BrdfContext ctx{};
+    ctx.normal = vecMake3(normal[0], normal[1], normal[2]);
+    ctx.wo = vecMake3(wo[0], wo[1], wo[2]);
+    std::memcpy(&ctx.material, material, sizeof(MaterialGpu));
+    ctx.etaMedium = etaMedium;
+    ctx.debugFlags = debugFlags;
+    const BrdfSampleResult r = PrincipledBrdf{}.sampleTransmit(ctx, u1, u2);
+    outDir[0] = r.direction.x;
+    outDir[1] = r.direction.y;
+    outDir[2] = r.direction.z;
+    *outPdf = r.pdf;
+    *outNextEta = r.nextMediumEta;
+    *outFlags = (r.valid ? 1 : 0) | (r.transmitted ? 2 : 0) | (r.subsurfaceScatter ? 4 : 0);
+    return r.subsurfaceInternalSteps;
+}
+
+// Lobe weights (PrincipledBrdf.h:75-100): diffuse, specular, transmit, subsurface.
+void ref_lobe_weights(const void* material, float* out)
+{
+    BrdfContext ctx{};
+    std::memcpy(&ctx.material, material, sizeof(MaterialGpu));
+    const PrincipledDetail::LobeWeights w = PrincipledDetail::computeLobeWeights(ctx);
+    out[0] = w.diffuse;
+    out[1] = w.specular;
+    out[2] = w.transmit;
+    out[3] = w.subsurface;
+}
+
+// Texture bank resolve (Texture/ProceduralTexture.h:138-207); writes the 15
+// MaterialGpu float fields of the resolved material.
+void ref_resolve_material(const void* material, float u, float v, const void* textures, int textureCount, float* out)
+{
+    MaterialGpu m{};
+    std::memcpy(&m, material, sizeof(MaterialGpu));
+    const TextureEvalContext ctx{Vec2{u, v}, u};
+    const MaterialGpu r = materialFromResolved(resolveMaterial(m, ctx,
+        textureCount > 0 ? static_cast<const TextureDescGpu*>(textures) : nullptr, static_cast<uint32_t>(textureCount)));
+    std::memcpy(out, &r, 15 * sizeof(float));
+}
+
 // Adaptive convergence predicate (PathTracerAdaptiveSampling.h:16-40).
 int ref_is_converged(uint32_t count, float lumMean, float m2, int minSamples, float threshold)
 {
