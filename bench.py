@@ -49,15 +49,17 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--config", choices=["plain-small"], default="plain-small")
+    ap.add_argument("--config", choices=["plain-small", "plain-large"], default="plain-small")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
 def make_workload(name: str):
-    from lsystemeditor_b200.scene import config0_scene
+    from lsystemeditor_b200.scene import config0_scene, config1_scene
     if name == "plain-small":
         return config0_scene()
+    if name == "plain-large":
+        return config1_scene()
     raise ValueError(name)
 
 
@@ -139,13 +141,20 @@ def cpu_render_rate(spec, min_seconds: float = 10.0, max_pixels: int | None = No
     if max_pixels:
         n = min(n, max_pixels)
     pix = np.sort(rng.choice(P, n, replace=False)).astype(np.int32)
+    # whole frames when the image is small: repeat (fresh accumulation, new seeds) until min_seconds
+    samples, reps = 0, 0
     t0 = time.perf_counter()
-    st = sc.render(spec.camera, spec.params, spec.width, spec.height, spec.waves, pixels=pix, threads=threads)
-    dt = time.perf_counter() - t0
-    samples = int(st["counts"][pix].sum())
+    while True:
+        st = sc.render(spec.camera, spec.params, spec.width, spec.height, spec.waves, pixels=pix, threads=threads,
+                       seed_base=1 + reps * spec.waves)
+        samples += int(st["counts"][pix].sum())
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt >= min_seconds or reps >= 1000:
+            break
     return {"value": samples / dt / 1e6, "unit": METRIC, "cores": int(threads), "kind": kind,
-            "sample": f"{n} of {P} pixels x up to {spec.waves} samples ({samples} path samples, {dt:.1f} s), "
-                      f"same scene/camera/params, PCG32 random numbers"}
+            "sample": f"{n} of {P} pixels x up to {spec.waves} samples, {reps} frame(s) ({samples} path samples, "
+                      f"{dt:.1f} s), same scene/camera/params, PCG32 random numbers"}
 
 
 def run_reference(args):
@@ -187,6 +196,8 @@ def workload_config(spec, name):
     m = spec.mesh
     return {"workload": spec.name, "width": spec.width, "height": spec.height,
             "spp": int(spec.params["max_samples_per_pixel"]), "min_spp": int(spec.params["min_samples"]),
+            "adaptive": ("relative std-error" if int(spec.params["adaptive_criterion"]) == 1 else "relative std-dev")
+            + f" < {float(spec.params['relative_error_threshold']):g}",
             "max_depth": int(spec.params["max_path_depth"]), "triangles": int(m.triangle_count),
             "materials": int(len(m.materials)), "seed": "reference per-(pixel, sample) seed",
             "l2": "flushed between timed steps (256 MiB write, untimed)"}
@@ -246,10 +257,9 @@ def run_b200(args):
     torch.cuda.synchronize()
 
     # ---- timed region: K device-timed renders ----------------------------
-    pt.set_profiling(PROFILE_STAGE_TIMES)
     launches0 = pt.stats()["launches"]
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    ext_ms, ext_launches, ext_rays, samples = 0.0, 0, 0, 0
+    samples = 0
     barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -259,10 +269,6 @@ def run_b200(args):
         evs[k][0].record(stream)
         step()
         evs[k][1].record(stream)
-        prof = pt.profile()
-        ext_ms += prof["ms_extend"]
-        ext_launches += prof["launches_extend"]
-        ext_rays += prof["rays_extend"]
         samples += pt.stats()["samples"]
     torch.cuda.synchronize()
     barrier()
@@ -272,6 +278,22 @@ def run_b200(args):
     total_ms = max_over_ranks(float(sum(step_ms)))
     total_samples = sum_over_ranks(float(samples))
     value = total_samples / (total_ms / 1e3) / 1e6
+
+    # ---- the same K renders again with CUDA events around every stage launch
+    # (on the launch stream) for the kernel durations of the roofline ---------
+    pt.set_profiling(PROFILE_STAGE_TIMES)
+    stages = {}
+    ext_ms, ext_launches, ext_rays = 0.0, 0, 0
+    for k in range(args.steps):
+        flush.zero_()
+        step()
+        prof = pt.profile()
+        for key, v in prof.items():
+            if key.startswith("ms_"):
+                stages[key[3:]] = stages.get(key[3:], 0.0) + v / args.steps
+        ext_ms += prof["ms_extend"]
+        ext_launches += prof["launches_extend"]
+        ext_rays += prof["rays_extend"]
     pt.set_profiling(0)
 
     # ---- traversal statistics for the roofline (untimed counting pass) ----
@@ -360,7 +382,8 @@ def run_b200(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**workload_config(spec, args.config), "parallelism": f"replicas{world}",
                    "bvh_nodes": int(st["bvh_nodes"]),
-                   "mrays_per_s": (ext_rays + 0.0) / (sum(step_ms) / 1e3) / 1e6,
+                   "mrays_per_s": (cp["rays_extend"] + cp["rays_shadow"]) / (total_ms / args.steps / 1e3) / 1e6,
+                   "stage_ms_per_step": {k: round(v, 4) for k, v in stages.items()},
                    "rays_per_sample": (cp["rays_extend"] + cp["rays_shadow"]) / max(1, spec.width * spec.height * spec.waves)},
         "e2e": {"value": e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",

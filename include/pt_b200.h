@@ -243,7 +243,7 @@ int pt_set_profiling(pt_renderer* r, int flags);
 int pt_get_profile(const pt_renderer* r, pt_profile* out);
 
 /* Work-size tuning (no reference counterpart): paths in flight per launch
- * (0 = default 2^21) and resident blocks per SM of the persistent stage grids
+ * (0 = default 2^23) and resident blocks per SM of the persistent stage grids
  * (0 = from the occupancy calculator). */
 int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
 

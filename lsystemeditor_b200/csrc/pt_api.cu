@@ -101,15 +101,17 @@ struct pt_renderer {
     DevBuf<uint2> pRngB;
     DevBuf<float4> pOrig, pDir, pThr, pRad, pHit, pNeeEnv, pNeeEmis;
     DevBuf<uint8_t> pVisEnv, pVisEmis;
-    DevBuf<uint32_t> qExt0, qExt1, qFinish, qShadowPath;
+    DevBuf<uint32_t> qExt0, qExt1, qFinish, qShadowPath, qMiss, qHit;
     DevBuf<float4> qShadowO, qShadowD;
     DevBuf<unsigned int> qCounts;
     DevBuf<unsigned long long> qRays;     // [0] extend, [1] shadow
     DevBuf<unsigned long long> qVisits;   // [0..1] extend nodes/tris, [2..3] shadow nodes/tris
     DevBuf<unsigned int> qOverflow;
     int gridExtend = 0, gridShade = 0, gridShadow = 0;
-    int capacityWanted = 1 << 21;
+    int capacityWanted = 1 << 23;     // paths in flight per launch (one chunk for most frames)
     int blocksPerSmOverride = 0;
+
+    DevBuf<LaunchCtx> dctx;               // device copy of the launch context
 
     // profiling
     int profileFlags = 0;
@@ -208,6 +210,7 @@ int ensurePaths(pt_renderer* r, int capacity)
         r->pOrig.ensure(Q) && r->pDir.ensure(Q) && r->pThr.ensure(Q) && r->pRad.ensure(Q) && r->pHit.ensure(Q) &&
         r->pNeeEnv.ensure(Q) && r->pNeeEmis.ensure(Q) && r->pVisEnv.ensure(Q) && r->pVisEmis.ensure(Q) &&
         r->qExt0.ensure(Q) && r->qExt1.ensure(Q) && r->qFinish.ensure(Q) && r->qShadowPath.ensure(2 * Q) &&
+        r->qMiss.ensure(Q) && r->qHit.ensure(Q) &&
         r->qShadowO.ensure(2 * Q) && r->qShadowD.ensure(2 * Q) && r->qCounts.ensure(8) && r->qRays.ensure(2) &&
         r->qVisits.ensure(4) && r->qOverflow.ensure(1);
     if (!ok) {
@@ -250,6 +253,8 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.q.extend[0] = r->qExt0.p;
     c.q.extend[1] = r->qExt1.p;
     c.q.finish = r->qFinish.p;
+    c.q.missQueue = r->qMiss.p;
+    c.q.hitQueue = r->qHit.p;
     c.q.shadowPath = r->qShadowPath.p;
     c.q.shadowOrig = r->qShadowO.p;
     c.q.shadowDir = r->qShadowD.p;
@@ -271,15 +276,30 @@ LaunchCtx makeCtx(pt_renderer* r)
     return c;
 }
 
+// Uploads the current launch context; returns its device address (nullptr on failure).
+const LaunchCtx* uploadCtx(pt_renderer* r)
+{
+    if (!r->dctx.ensure(1)) {
+        return nullptr;
+    }
+    const LaunchCtx c = makeCtx(r);
+    if (cudaMemcpyAsync(r->dctx.p, &c, sizeof(LaunchCtx), cudaMemcpyHostToDevice, r->stream) != cudaSuccess) {
+        return nullptr;
+    }
+    return r->dctx.p;
+}
+
 int resetAccum(pt_renderer* r)
 {
     if (r->width <= 0) {
         return PT_OK;
     }
-    LaunchCtx c = makeCtx(r);
-    c.activeSel = 0;
     r->activeSel = 0;
-    launchResetAccum(c, r->width * r->height, r->stream);
+    const LaunchCtx* dc = uploadCtx(r);
+    if (dc == nullptr) {
+        return fail(r, PT_ERR_CUDA, "launch context upload failed");
+    }
+    launchResetAccum(dc, r->width * r->height, r->stream);
     PT_CHECK(r, cudaGetLastError());
     r->hostActive = r->width * r->height;
     r->wavesDone = 0;
@@ -288,6 +308,7 @@ int resetAccum(pt_renderer* r)
 }
 
 enum Stage { kGenerate = 0, kExtend, kShade, kShadow, kFinalize, kAccumulate, kCompact, kStageCount };
+// (the miss-shading kernel is accounted to kShade)
 
 // Stage timing: a pair of events around each launch when profiling is on.
 struct StageTimer {
@@ -445,6 +466,8 @@ int pt_destroy(pt_renderer* r)
     r->qExt0.release();
     r->qExt1.release();
     r->qFinish.release();
+    r->qMiss.release();
+    r->qHit.release();
     r->qShadowPath.release();
     r->qShadowO.release();
     r->qShadowD.release();
@@ -452,6 +475,7 @@ int pt_destroy(pt_renderer* r)
     r->qRays.release();
     r->qVisits.release();
     r->qOverflow.release();
+    r->dctx.release();
     for (cudaEvent_t e : r->eventPool) {
         cudaEventDestroy(e);
     }
@@ -737,9 +761,15 @@ int pt_render(pt_renderer* r, int waves)
     }
     PT_CHECK(r, cudaSetDevice(r->device));
     cudaStream_t s = r->stream;
-    int st = ensurePaths(r, r->capacityWanted);
-    if (st != PT_OK) {
-        return st;
+    {
+        // path state for min(cap, pixels x first batch) paths
+        const int B0 = chooseBatch(r, waves > 0 ? waves : 0);
+        const long long jobs0 = static_cast<long long>(std::max(r->hostActive, 1)) * B0;
+        const int want = static_cast<int>(std::min<long long>(r->capacityWanted, std::max<long long>(jobs0, 1 << 16)));
+        int st = ensurePaths(r, want);
+        if (st != PT_OK) {
+            return st;
+        }
     }
     const bool countVisits = (r->profileFlags & PT_PROFILE_COUNT_VISITS) != 0;
     r->profile = pt_profile{};
@@ -762,7 +792,10 @@ int pt_render(pt_renderer* r, int waves)
         const int chunkCap = std::min(r->capacity, r->capacityWanted);
         for (long long start = 0; start < jobs; start += chunkCap) {
             const int chunk = static_cast<int>(std::min<long long>(chunkCap, jobs - start));
-            LaunchCtx c = makeCtx(r);
+            const LaunchCtx* c = uploadCtx(r);
+            if (c == nullptr) {
+                return fail(r, PT_ERR_CUDA, "launch context upload failed");
+            }
             {
                 StageTimer tm(r, kGenerate);
                 launchGenerate(c, start, chunk, active, static_cast<uint32_t>(r->wavesDone), 0, s);
@@ -773,13 +806,14 @@ int pt_render(pt_renderer* r, int waves)
                 const bool identity = depth == 0;
                 {
                     StageTimer tm(r, kExtend);
-                    launchExtend(c, sel, identity, r->gridExtend, countVisits, s);
+                    launchExtend(c, sel, identity, depth, r->gridExtend, countVisits, s);
                 }
                 {
                     StageTimer tm(r, kShade);
-                    launchShade(c, sel, identity, r->gridShade, s);
+                    launchShadeMiss(c, depth, r->gridShade, s);
+                    launchShade(c, sel, depth, r->gridShade, s);
                 }
-                launches += 2;
+                launches += 3;
                 r->profile.launches_extend += 1;
                 if (depth < maxDepthEff) {
                     {
@@ -805,7 +839,7 @@ int pt_render(pt_renderer* r, int waves)
             }
             PT_CHECK(r, cudaGetLastError());
         }
-        LaunchCtx c = makeCtx(r);
+        const LaunchCtx* c = r->dctx.p;
         {
             StageTimer tm(r, kAccumulate);
             launchAccumulate(c, active, B, s);
@@ -1013,7 +1047,7 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
     if (r == nullptr || path_capacity < 0 || blocks_per_sm < 0 || path_capacity > (1 << 26)) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_tuning: bad arguments");
     }
-    r->capacityWanted = path_capacity > 0 ? path_capacity : (1 << 21);
+    r->capacityWanted = path_capacity > 0 ? path_capacity : (1 << 23);
     if (blocks_per_sm > 0) {
         r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
     } else {

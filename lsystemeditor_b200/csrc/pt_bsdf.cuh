@@ -860,7 +860,7 @@ __device__ __forceinline__ const pt_material* fetchMaterial(const DevScene& S, u
 
 // Emissive triangle sampling (LightSamplingCore.h:257-313).
 __device__ __forceinline__ bool sampleEmissive(const DevScene& S, const pt_material* fallback, float uTri, float u1,
-    float u2, float3& pos, float3& n, float3& L, float& pdf)
+    float u2, float3& pos, float3& n, float3& L, float& pdf, float3& v0, float3& v1, float3& v2)
 {
     pdf = 0.0f;
     const uint32_t E = S.emissiveCount;
@@ -880,7 +880,9 @@ __device__ __forceinline__ bool sampleEmissive(const DevScene& S, const pt_mater
     }
     const uint32_t tri = S.emissiveIdx[lo];
     const pt_material& m = *fetchMaterial(S, tri, fallback);
-    const float3 v0 = loadOrigVertex(S, tri, 0), v1 = loadOrigVertex(S, tri, 1), v2 = loadOrigVertex(S, tri, 2);
+    v0 = loadOrigVertex(S, tri, 0);
+    v1 = loadOrigVertex(S, tri, 1);
+    v2 = loadOrigVertex(S, tri, 2);
     const float su = sqrtf(fmax2(0.0f, u1));
     const float b0 = 1.0f - su;
     const float b1 = u2 * su;

@@ -113,15 +113,18 @@ __device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, floa
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_generate(LaunchCtx c, long long jobStart, int jobCount, int activeCount,
+__global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ cp, long long jobStart, int jobCount, int activeCount,
     uint32_t waveBase, int extendSel)
 {
+    const LaunchCtx& c = *cp;
     const int* active = c.acc.active[c.activeSel];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         c.q.counts[extendSel] = static_cast<unsigned int>(jobCount);
         c.q.counts[extendSel ^ 1] = 0u;
         c.q.counts[2] = 0u;
         c.q.counts[3] = 0u;
+        c.q.counts[4] = 0u;
+        c.q.counts[5] = 0u;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < jobCount; i += gridDim.x * blockDim.x) {
         const long long j = jobStart + i;
@@ -153,17 +156,25 @@ __global__ void __launch_bounds__(256) k_generate(LaunchCtx c, long long jobStar
     }
 }
 
-// Closest hit for every queued path.
+// Closest hit for every queued path; each path is then routed to the miss or
+// the hit queue of this bounce so that the two shade kernels run coherent work.
+// Counters: [4 + 2p] misses and [5 + 2p] hits of bounce parity p; this kernel
+// zeroes the other parity's pair for the next bounce.
 template <bool Count>
-__global__ void __launch_bounds__(256) k_extend(LaunchCtx c, int sel, bool identity)
+__global__ void __launch_bounds__(256, 4) k_extend(const LaunchCtx* __restrict__ cp, int sel, bool identity, int depth)
 {
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
     const unsigned int count = c.q.counts[sel];
+    const int par = depth & 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&c.q.rays[0], static_cast<unsigned long long>(count));
-        // output counters of the shade stage that follows
+        // output counters of the shade stage that follows, and next bounce's routing counters
         c.q.counts[sel ^ 1] = 0u;
         c.q.counts[2] = 0u;
         c.q.counts[3] = 0u;
+        c.q.counts[4 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[5 + 2 * (par ^ 1)] = 0u;
     }
     const uint32_t* queue = c.q.extend[sel];
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
@@ -173,25 +184,68 @@ __global__ void __launch_bounds__(256) k_extend(LaunchCtx c, int sel, bool ident
         const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
         HitRec h;
         const bool hit = traceRay<false, Count>(c.scene, f3(o4.x, o4.y, o4.z), dn, o4.w, kRayTMax, h, c.q.overflow,
-            c.q.visits);
-        c.paths.hit[i] = hit ? make_float4(h.t, h.u, h.v, __uint_as_float(h.tri))
-                             : make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0xFFFFFFFFu));
+            c.q.visits, smemStack + threadIdx.x, blockDim.x);
+        if (hit) {
+            c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+            const uint32_t s = warpPush(&c.q.counts[5 + 2 * par]);
+            c.q.hitQueue[s] = i;
+        } else {
+            const uint32_t s = warpPush(&c.q.counts[4 + 2 * par]);
+            c.q.missQueue[s] = i;
+        }
     }
 }
 
-// Shading. One thread per queued path.
-__global__ void __launch_bounds__(256) k_shade(LaunchCtx c, int sel, bool identity)
+// Paths whose ray left the scene: previous bounce's NEE, then the
+// environment / background term (PathIntegratorRandCore.h:215-216, 338-346).
+__global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict__ cp, int depth)
 {
-    const unsigned int count = c.q.counts[sel];
-    const uint32_t* queue = c.q.extend[sel];
+    const LaunchCtx& c = *cp;
+    const unsigned int count = c.q.counts[4 + 2 * (depth & 1)];
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t i = c.q.missQueue[k];
+        const float4 d4 = c.paths.dir[i];
+        const float3 d = f3(d4.x, d4.y, d4.z);
+        float3 L;
+        if (depth == 0) {
+            L = envEval(c.env, c.params, d);
+        } else {
+            const float4 r4 = c.paths.rad[i];
+            L = f3(r4.x, r4.y, r4.z);
+            if (c.paths.visEnv[i]) {
+                const float4 e = c.paths.neeEnv[i];
+                L = add3(L, f3(e.x, e.y, e.z));
+            }
+            if (c.paths.visEmis[i]) {
+                const float4 e = c.paths.neeEmis[i];
+                L = add3(L, f3(e.x, e.y, e.z));
+            }
+            const float4 t4 = c.paths.thr[i];
+            const float3 Le = envEval(c.env, c.params, d);
+            const float lp = envPdf(c.env, d);
+            const float w = misBalance(d4.w, lp);
+            L = add3(L, mul3(f3(t4.x, t4.y, t4.z), scl3(Le, w)));
+        }
+        writeSample(c, i, L);
+    }
+}
+
+// Shading of the paths that hit a triangle. One thread per queued path.
+__global__ void __launch_bounds__(256) k_shade(const LaunchCtx* __restrict__ cp, int sel, int depth)
+{
+    const LaunchCtx& c = *cp;
+    const unsigned int count = c.q.counts[5 + 2 * (depth & 1)];
+    const uint32_t* queue = c.q.hitQueue;
     unsigned int* nextCount = &c.q.counts[sel ^ 1];
     uint32_t* nextQueue = c.q.extend[sel ^ 1];
     const int debugFlags = c.params.brdf_debug_flags;
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-        const uint32_t i = identity ? k : queue[k];
-        float4 r4 = c.paths.rad[i];
-        float3 L = f3(r4.x, r4.y, r4.z);
-        const int depth = __float_as_int(r4.w);
+        const uint32_t i = queue[k];
+        float3 L = f3(0.0f, 0.0f, 0.0f);
+        if (depth > 0) {
+            const float4 r4 = c.paths.rad[i];
+            L = f3(r4.x, r4.y, r4.z);
+        }
         // NEE contributions of the previous bounce, in the reference's order.
         if (depth > 0) {
             if (c.paths.visEnv[i]) {
@@ -210,24 +264,17 @@ __global__ void __launch_bounds__(256) k_shade(LaunchCtx c, int sel, bool identi
         bool done = false;
         bool pendEnv = false, pendEmis = false;
         bool cont = false;
-        if (tri == 0xFFFFFFFFu) {
-            if (depth == 0) {
-                L = envEval(c.env, c.params, d);
-            } else {
-                const float4 t4 = c.paths.thr[i];
-                const float3 Le = envEval(c.env, c.params, d);
-                const float lp = envPdf(c.env, d);
-                const float w = misBalance(d4.w, lp);
-                L = add3(L, mul3(f3(t4.x, t4.y, t4.z), scl3(Le, w)));
-            }
-            done = true;
-        } else if (depth >= c.maxDepth) {
+        if (depth >= c.maxDepth) {
             done = true;
         } else {
             const float4 o4 = c.paths.orig[i];
-            const float4 t4 = c.paths.thr[i];
-            float3 T = f3(t4.x, t4.y, t4.z);
-            float eta = t4.w;
+            float3 T = f3(1.0f, 1.0f, 1.0f);
+            float eta = 1.0f;
+            if (depth > 0) {
+                const float4 t4 = c.paths.thr[i];
+                T = f3(t4.x, t4.y, t4.z);
+                eta = t4.w;
+            }
             const float t = h4.x;
             const float3 pos = xadd(f3(o4.x, o4.y, o4.z), xscl(d, t));
             const float3 dn = xnormalize(d);
@@ -263,13 +310,17 @@ __global__ void __launch_bounds__(256) k_shade(LaunchCtx c, int sel, bool identi
                         const float bp = bsdfPdf(cx, wi);
                         const float k = misBalance(lp, bp) * ct / lp;
                         const float3 contrib = mul3(T, mul3(f, scl3(Le, k)));
-                        c.paths.neeEnv[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
-                        const uint32_t s = warpPush(&c.q.counts[2]);
-                        const float3 so = add3(pos, scl3(n, kShadowBias));
-                        c.q.shadowPath[s] = i;
-                        c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
-                        c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, 0.0f);
-                        pendEnv = true;
+                        // A contribution of exactly zero adds nothing whether or not the light
+                        // is occluded, so its shadow ray is not traced (black backgrounds).
+                        if (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f) {
+                            c.paths.neeEnv[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                            const uint32_t s = warpPush(&c.q.counts[2]);
+                            const float3 so = add3(pos, scl3(n, kShadowBias));
+                            c.q.shadowPath[s] = i;
+                            c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
+                            c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+                            pendEnv = true;
+                        }
                     }
                 }
             }
@@ -278,9 +329,9 @@ __global__ void __launch_bounds__(256) k_shade(LaunchCtx c, int sel, bool identi
                 const float uTri = curand_uniform(&st);
                 const float u1 = curand_uniform(&st);
                 const float u2 = curand_uniform(&st);
-                float3 lpos, ln, Le;
+                float3 lpos, ln, Le, ev0, ev1, ev2;
                 float ap;
-                if (sampleEmissive(c.scene, &kFallbackMaterial, uTri, u1, u2, lpos, ln, Le, ap)) {
+                if (sampleEmissive(c.scene, &kFallbackMaterial, uTri, u1, u2, lpos, ln, Le, ap, ev0, ev1, ev2)) {
                     const float3 tl = sub3(lpos, pos);
                     const float d2 = dot3(tl, tl);
                     if (d2 > kMinPdf) {
@@ -294,13 +345,28 @@ __global__ void __launch_bounds__(256) k_shade(LaunchCtx c, int sel, bool identi
                                 const float bp = bsdfPdf(cx, wi);
                                 const float k = misBalance(lp, bp) * ct / lp;
                                 const float3 contrib = mul3(T, mul3(f, scl3(Le, k)));
-                                c.paths.neeEmis[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
-                                const uint32_t s = warpPush(&c.q.counts[2]);
+                                // The reference's emissive shadow ray runs to tMax = 1e6
+                                // (LightSamplingCore.h:360-369), so the sampled emitter triangle
+                                // itself occludes it whenever the ray hits that triangle.  An
+                                // any-hit query is true as soon as one triangle is hit, so testing
+                                // the emitter first (same origin, direction and rounding as the
+                                // shadow stage) decides those rays without a traversal.
                                 const float3 so = add3(pos, scl3(wi, kShadowBias));
-                                c.q.shadowPath[s] = i | 0x80000000u;
-                                c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
-                                c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, 0.0f);
-                                pendEmis = true;
+                                const float3 sdn = xnormalize(wi);
+                                bool occludedBySelf = false;
+                                if (!isDegenerateDir(sdn)) {
+                                    float th, tu2, tv2;
+                                    occludedBySelf = intersectTriExact(so, sdn, ev0, ev1, ev2, kShadowBias, kRayTMax, th,
+                                                         tu2, tv2) && th < kRayTMax;
+                                }
+                                if (!occludedBySelf && (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f)) {
+                                    c.paths.neeEmis[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                                    const uint32_t s = warpPush(&c.q.counts[2]);
+                                    c.q.shadowPath[s] = i | 0x80000000u;
+                                    c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
+                                    c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+                                    pendEmis = true;
+                                }
                             }
                         }
                     }
@@ -384,8 +450,10 @@ __global__ void __launch_bounds__(256) k_shade(LaunchCtx c, int sel, bool identi
 
 // Occlusion of the queued shadow rays (LightSamplingCore.h:187-197, 360-369).
 template <bool Count>
-__global__ void __launch_bounds__(256) k_shadow(LaunchCtx c)
+__global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__ cp)
 {
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
     const unsigned int count = c.q.counts[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&c.q.rays[1], static_cast<unsigned long long>(count));
@@ -397,7 +465,7 @@ __global__ void __launch_bounds__(256) k_shadow(LaunchCtx c)
         const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
         HitRec h;
         const bool occluded = traceRay<true, Count>(c.scene, f3(o4.x, o4.y, o4.z), dn, kShadowBias, kRayTMax, h,
-            c.q.overflow, c.q.visits + 2);
+            c.q.overflow, c.q.visits + 2, smemStack + threadIdx.x, blockDim.x);
         if (!occluded) {
             const uint32_t i = e & 0x7FFFFFFFu;
             if (e & 0x80000000u) {
@@ -410,8 +478,9 @@ __global__ void __launch_bounds__(256) k_shadow(LaunchCtx c)
 }
 
 // Paths that terminated while their NEE shadow rays were in flight.
-__global__ void __launch_bounds__(256) k_finalize(LaunchCtx c)
+__global__ void __launch_bounds__(256) k_finalize(const LaunchCtx* __restrict__ cp)
 {
+    const LaunchCtx& c = *cp;
     const unsigned int count = c.q.counts[3];
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = c.q.finish[k];
@@ -430,8 +499,9 @@ __global__ void __launch_bounds__(256) k_finalize(LaunchCtx c)
 }
 
 // Per pixel: fold the batch's samples in sample order (PathTracer.cu:232-272).
-__global__ void __launch_bounds__(256) k_accumulate(LaunchCtx c, int activeCount, int batch)
+__global__ void __launch_bounds__(256) k_accumulate(const LaunchCtx* __restrict__ cp, int activeCount, int batch)
 {
+    const LaunchCtx& c = *cp;
     const int* active = c.acc.active[c.activeSel];
     const int maxSpp = c.params.max_samples_per_pixel;
     const int minSpp = c.params.min_samples;
@@ -492,8 +562,9 @@ __global__ void __launch_bounds__(256) k_accumulate(LaunchCtx c, int activeCount
 
 // Ordered-within-block compaction of the active list (compactActiveListKernel,
 // PathTracer.cu:372-411, without per-element atomics).
-__global__ void __launch_bounds__(256) k_compact(LaunchCtx c, int activeCount)
+__global__ void __launch_bounds__(256) k_compact(const LaunchCtx* __restrict__ cp, int activeCount)
 {
+    const LaunchCtx& c = *cp;
     const int* in = c.acc.active[c.activeSel];
     int* out = c.acc.active[c.activeSel ^ 1];
     const int maxSpp = c.params.max_samples_per_pixel;
@@ -530,8 +601,9 @@ __global__ void __launch_bounds__(256) k_compact(LaunchCtx c, int activeCount)
     }
 }
 
-__global__ void k_reset(LaunchCtx c, int pixels)
+__global__ void k_reset(const LaunchCtx* __restrict__ cp, int pixels)
 {
+    const LaunchCtx& c = *cp;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < pixels; i += gridDim.x * blockDim.x) {
         c.acc.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         c.acc.counts[i] = 0;
@@ -608,48 +680,55 @@ inline int gridFor(long long n, int block = 256, int cap = 148 * 16)
 
 } // namespace
 
-void launchGenerate(const LaunchCtx& c, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
+void launchGenerate(const LaunchCtx* d, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
     int extendSel, cudaStream_t s)
 {
-    k_generate<<<gridFor(jobCount), 256, 0, s>>>(c, jobStart, jobCount, activeCount, waveBase, extendSel);
+    k_generate<<<gridFor(jobCount), 256, 0, s>>>(d, jobStart, jobCount, activeCount, waveBase, extendSel);
 }
-void launchExtend(const LaunchCtx& c, int sel, bool identity, int grid, bool count, cudaStream_t s)
+void launchExtend(const LaunchCtx* c, int sel, bool identity, int depth, int grid, bool count, cudaStream_t s)
 {
+    const size_t smem = sizeof(uint2) * kSharedStack * 256;
     if (count) {
-        k_extend<true><<<grid, 256, 0, s>>>(c, sel, identity);
+        k_extend<true><<<grid, 256, smem, s>>>(c, sel, identity, depth);
     } else {
-        k_extend<false><<<grid, 256, 0, s>>>(c, sel, identity);
+        k_extend<false><<<grid, 256, smem, s>>>(c, sel, identity, depth);
     }
 }
-void launchShade(const LaunchCtx& c, int sel, bool identity, int grid, cudaStream_t s)
+void launchShadeMiss(const LaunchCtx* c, int depth, int grid, cudaStream_t s)
 {
-    k_shade<<<grid, 256, 0, s>>>(c, sel, identity);
+    k_shade_miss<<<grid, 256, 0, s>>>(c, depth);
 }
-void launchShadow(const LaunchCtx& c, int grid, bool count, cudaStream_t s)
+void launchShade(const LaunchCtx* c, int sel, int depth, int grid, cudaStream_t s)
 {
+    k_shade<<<grid, 256, 0, s>>>(c, sel, depth);
+}
+void launchShadow(const LaunchCtx* c, int grid, bool count, cudaStream_t s)
+{
+    const size_t smem = sizeof(uint2) * kSharedStack * 256;
     if (count) {
-        k_shadow<true><<<grid, 256, 0, s>>>(c);
+        k_shadow<true><<<grid, 256, smem, s>>>(c);
     } else {
-        k_shadow<false><<<grid, 256, 0, s>>>(c);
+        k_shadow<false><<<grid, 256, smem, s>>>(c);
     }
 }
 void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
 {
     extendBlocks = shadeBlocks = shadowBlocks = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extendBlocks, k_extend<false>, 256, 0);
+    const size_t smem = sizeof(uint2) * kSharedStack * 256;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extendBlocks, k_extend<false>, 256, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadeBlocks, k_shade, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadowBlocks, k_shadow<false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadowBlocks, k_shadow<false>, 256, smem);
 }
-void launchFinalize(const LaunchCtx& c, int grid, cudaStream_t s) { k_finalize<<<grid, 256, 0, s>>>(c); }
-void launchAccumulate(const LaunchCtx& c, int activeCount, int batch, cudaStream_t s)
+void launchFinalize(const LaunchCtx* c, int grid, cudaStream_t s) { k_finalize<<<grid, 256, 0, s>>>(c); }
+void launchAccumulate(const LaunchCtx* c, int activeCount, int batch, cudaStream_t s)
 {
     k_accumulate<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount, batch);
 }
-void launchCompact(const LaunchCtx& c, int activeCount, cudaStream_t s)
+void launchCompact(const LaunchCtx* c, int activeCount, cudaStream_t s)
 {
     k_compact<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount);
 }
-void launchResetAccum(const LaunchCtx& c, int pixels, cudaStream_t s) { k_reset<<<gridFor(pixels), 256, 0, s>>>(c, pixels); }
+void launchResetAccum(const LaunchCtx* c, int pixels, cudaStream_t s) { k_reset<<<gridFor(pixels), 256, 0, s>>>(c, pixels); }
 void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,
     uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s)
 {

@@ -26,10 +26,13 @@ struct PathSoA {
 struct QueueSet {
     uint32_t* extend[2] = {nullptr, nullptr}; // path indices, ping-pong
     uint32_t* finish = nullptr;               // paths that ended with shadow rays in flight
+    uint32_t* missQueue = nullptr;            // paths whose last ray left the scene
+    uint32_t* hitQueue = nullptr;             // paths whose last ray hit a triangle
     uint32_t* shadowPath = nullptr;           // path index | kind << 31
     float4* shadowOrig = nullptr;
     float4* shadowDir = nullptr;
-    // counters: [0],[1] extend ping-pong, [2] shadow, [3] finish
+    // counters: [0],[1] extend ping-pong, [2] shadow, [3] finish,
+    // [4 + 2p] misses / [5 + 2p] hits of bounce parity p
     unsigned int* counts = nullptr;
     unsigned long long* rays = nullptr;       // [0] closest-hit rays, [1] shadow rays
     unsigned long long* visits = nullptr;     // [0..1] extend nodes/tris, [2..3] shadow nodes/tris
@@ -63,16 +66,20 @@ struct LaunchCtx {
     int activeSel;    // which active[] list is current
 };
 
-// Launchers. `grid` is a persistent-style grid; kernels loop over device-side counts.
-void launchGenerate(const LaunchCtx& c, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
+// Launchers. The LaunchCtx lives in DEVICE memory (one per renderer) and is
+// passed by pointer: a large by-value kernel parameter whose members are
+// taken by reference would be copied to local memory by every thread.
+// `grid` is a persistent-style grid; kernels loop over device-side counts.
+void launchGenerate(const LaunchCtx* d, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
     int extendSel, cudaStream_t s);
-void launchExtend(const LaunchCtx& c, int sel, bool identity, int grid, bool count, cudaStream_t s);
-void launchShade(const LaunchCtx& c, int sel, bool identity, int grid, cudaStream_t s);
-void launchShadow(const LaunchCtx& c, int grid, bool count, cudaStream_t s);
-void launchFinalize(const LaunchCtx& c, int grid, cudaStream_t s);
-void launchAccumulate(const LaunchCtx& c, int activeCount, int batch, cudaStream_t s);
-void launchCompact(const LaunchCtx& c, int activeCount, cudaStream_t s);
-void launchResetAccum(const LaunchCtx& c, int pixels, cudaStream_t s);
+void launchExtend(const LaunchCtx* d, int sel, bool identity, int depth, int grid, bool count, cudaStream_t s);
+void launchShadeMiss(const LaunchCtx* d, int depth, int grid, cudaStream_t s);
+void launchShade(const LaunchCtx* d, int sel, int depth, int grid, cudaStream_t s);
+void launchShadow(const LaunchCtx* d, int grid, bool count, cudaStream_t s);
+void launchFinalize(const LaunchCtx* d, int grid, cudaStream_t s);
+void launchAccumulate(const LaunchCtx* d, int activeCount, int batch, cudaStream_t s);
+void launchCompact(const LaunchCtx* d, int activeCount, cudaStream_t s);
+void launchResetAccum(const LaunchCtx* d, int pixels, cudaStream_t s);
 void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,
     uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s);
 // Resident blocks per SM of the stage kernels (occupancy calculator).

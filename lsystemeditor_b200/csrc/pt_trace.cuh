@@ -22,7 +22,8 @@
 
 namespace pt {
 
-constexpr int kTraversalStack = 32;
+constexpr int kTraversalStack = 32;   // entries of the local-memory stack (fallback / Q1 path)
+constexpr int kSharedStack = 20;      // entries per thread of the shared-memory stack
 constexpr float kSlabWiden = 1.0000005f;
 
 struct HitRec {
@@ -239,9 +240,13 @@ __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 dn, flo
 // Closest hit (AnyHit = false) or occlusion (AnyHit = true) for a normalised
 // direction dn. Returns true on a hit; out.tri is the ORIGINAL triangle index.
 // Count = true adds the nodes and triangles visited to visits[0] / visits[1].
+// The traversal stack lives in shared memory when `sstack` is given (this
+// thread's column of a [kSharedStack][blockDim] array, so that consecutive
+// threads hit consecutive banks), spilling to a local array beyond that.
 template <bool AnyHit, bool Count = false>
 __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, HitRec& out,
-    unsigned int* overflowCounter = nullptr, unsigned long long* visits = nullptr)
+    unsigned int* overflowCounter = nullptr, unsigned long long* visits = nullptr, uint2* sstack = nullptr,
+    int sstride = 0)
 {
     out.tri = 0xFFFFFFFFu;
     if (S.nodeCount == 0) {
@@ -269,8 +274,12 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
             const uint32_t slot = (bit - 24u) ^ octinv;
             const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
             if (ngroup.y > 0x00FFFFFFu) {
-                if (sp < kTraversalStack) {
-                    stack[sp++] = ngroup;
+                if (sstack != nullptr && sp < kSharedStack) {
+                    sstack[sp * sstride] = ngroup;
+                    ++sp;
+                } else if (sp < (sstack != nullptr ? kSharedStack : 0) + kTraversalStack) {
+                    stack[sp - (sstack != nullptr ? kSharedStack : 0)] = ngroup;
+                    ++sp;
                 } else {
                     overflow = true;
                 }
@@ -318,7 +327,12 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
             if (sp == 0) {
                 break;
             }
-            ngroup = stack[--sp];
+            --sp;
+            if (sstack != nullptr && sp < kSharedStack) {
+                ngroup = sstack[sp * sstride];
+            } else {
+                ngroup = stack[sp - (sstack != nullptr ? kSharedStack : 0)];
+            }
         }
     }
     if (overflow && overflowCounter != nullptr) {

@@ -305,6 +305,86 @@ def bracketed_ol_tree(iterations: int = 4, angle: float = 25.7, length: float = 
     return loft(segs, sides)
 
 
+def stochastic_tree(iterations: int = 7, seed: int = 7, angle: float = 22.5, jitter: float = 5.0,
+                    length: float = 0.8, radius: float = 0.08, length_decay: float = 0.9, radius_decay: float = 0.7):
+    """3D stochastic L-system tree: axiom A,
+        A -> F [&+A] [&-A] [^A]   (p = 0.6)
+        A -> F [&A] [^/A]         (p = 0.4)
+    with + / - = Yaw(+-a), & / ^ = Pitch(+-a), / = Roll(a), a = angle +- uniform jitter
+    (drawn per symbol from a seeded generator and baked into the successor), segment
+    length x length_decay and radius x radius_decay per depth.  Terminal A's carry
+    a leaf.  Returns (segments, leaves) from the turtle (heading +Y, up +Z).
+    """
+    def rot(name, rng, sign=1.0):
+        return (name, (sign * (angle + rng.uniform(-jitter, jitter)),))
+
+    def rule(args, rng):
+        depth = args[0]
+        h = length * length_decay ** depth
+        r = radius * radius_decay ** depth
+        F = ("F", (h, r))
+        A = ("A", (depth + 1,))
+        if rng.uniform() < 0.6:
+            return [F, ("[", ()), rot("Pitch", rng), rot("Yaw", rng), A, ("]", ()),
+                    ("[", ()), rot("Pitch", rng), rot("Yaw", rng, -1.0), A, ("]", ()),
+                    ("[", ()), rot("Pitch", rng, -1.0), A, ("]", ())]
+        return [F, ("[", ()), rot("Pitch", rng), A, ("]", ()),
+                ("[", ()), rot("Pitch", rng, -1.0), rot("Roll", rng), A, ("]", ())]
+
+    word = expand([("A", (0,))], {"A": rule}, iterations, seed=seed)
+    word = [("Leaf", (1.0,)) if name == "A" else (name, a) for name, a in word]
+    return turtle(word, start_tangent=(0.0, 1.0, 0.0), start_up=(0.0, 0.0, 1.0), leaf_symbol="Leaf")
+
+
+def refine_segments(segments: Sequence[Segment], rings: int, taper: float) -> List[Segment]:
+    """Resamples every two-state segment into `rings` states with a linear radius taper."""
+    out = []
+    for s in segments:
+        p0, p1 = s.points[0], s.points[-1]
+        r0 = s.radii[0]
+        pts = [p0 + (p1 - p0) * (k / (rings - 1)) for k in range(rings)]
+        tans = [s.tangents[0]] * rings
+        radii = [r0 * (1.0 - (1.0 - taper) * k / (rings - 1)) for k in range(rings)]
+        out.append(Segment(pts, tans, radii, s.material, s.tag))
+    return out
+
+
+def config1_scene(width: int = 1024, height: int = 1024, sides: int = 64, rings: int = 16,
+                  max_depth: int = 12) -> SceneSpec:
+    """Plain method, large: the 3D stochastic tree (7 iterations, seed 7) with leaf quads.
+
+    The grammar yields ~500 branch segments and ~800 leaves; to reach the ~1M
+    triangles of the workload each branch is lofted as a 64-gon tube with 16
+    tapered rings.  Bark (0.35, 0.22, 0.12) roughness 0.8; leaves (0.1, 0.4,
+    0.08) roughness 0.5, transmission 0.3, thin; the light and ground of the
+    plain-small scene.  1024^2, adaptive 16..1024 spp stopping at a relative
+    standard error of 1e-2, max depth 12.
+    """
+    segs, leaves = stochastic_tree()
+    segs = refine_segments(segs, rings, taper=0.85)
+    tree = loft(segs, sides)
+    tree.materials = np.array([default_material(r=0.35, g=0.22, b=0.12, roughness=0.8)], MATERIAL_DTYPE)
+    leaf = leaf_quads(leaves, size=0.18, material=0)
+    leaf.materials = np.array([default_material(r=0.1, g=0.4, b=0.08, roughness=0.5, transmission=0.3, thin=1.0)],
+                              MATERIAL_DTYPE)
+    ground = quad_mesh((0, 0, 0), (10, 0, 0), (0, 0, -10),
+                       default_material(r=0.5, g=0.5, b=0.5, roughness=1.0), normal=(0, 1, 0))
+    light = quad_mesh((0, 5, 1.5), (1, 0, 0), (0, 0, 1),
+                      default_material(r=1.0, g=1.0, b=1.0, emission=10.0), normal=(0, -1, 0))
+    mesh = HostMesh.concat([tree, leaf, ground, light])
+    lo, hi = HostMesh.concat([tree, leaf]).bounds()
+    center = (lo + hi) * 0.5
+    extent = float(np.max(hi - lo))
+    dist = extent * 0.5 / math.tan(math.radians(20.0)) * 1.2
+    cam = look_at_camera((center[0], center[1], center[2] + dist), center, fov_y_deg=40.0, aspect=width / height)
+    params = default_params(background_r=0.0, background_g=0.0, background_b=0.0, max_path_depth=max_depth,
+                            russian_roulette_min_depth=3, min_samples=16, max_samples_per_pixel=1024,
+                            relative_error_threshold=0.01, adaptive_criterion=1)
+    return SceneSpec(f"plain-large: 3D stochastic L-system tree, {mesh.triangle_count} triangles, 1024x1024, "
+                     "adaptive 16-1024 spp to relative std-error 1e-2, depth 12", mesh, cam, params, width, height,
+                     1024)
+
+
 def config0_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> SceneSpec:
     """Plain method, small: 625-segment bracketed tree, ground, one area light, pinhole 40 deg.
 
