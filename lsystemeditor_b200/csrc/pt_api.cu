@@ -112,6 +112,9 @@ struct pt_renderer {
     int blocksPerSmOverride = 0;
 
     DevBuf<LaunchCtx> dctx;               // device copy of the launch context
+    DevBuf<BatchInfo> dbatch;             // current batch of jobs
+    BatchInfo hbatch{};                   // host staging of dbatch
+    double lastStopRate = 1.0;            // fraction of active pixels that stopped per 4 waves
 
     // profiling
     int profileFlags = 0;
@@ -211,8 +214,8 @@ int ensurePaths(pt_renderer* r, int capacity)
         r->pNeeEnv.ensure(Q) && r->pNeeEmis.ensure(Q) && r->pVisEnv.ensure(Q) && r->pVisEmis.ensure(Q) &&
         r->qExt0.ensure(Q) && r->qExt1.ensure(Q) && r->qFinish.ensure(Q) && r->qShadowPath.ensure(2 * Q) &&
         r->qMiss.ensure(Q) && r->qHit.ensure(Q) &&
-        r->qShadowO.ensure(2 * Q) && r->qShadowD.ensure(2 * Q) && r->qCounts.ensure(8) && r->qRays.ensure(2) &&
-        r->qVisits.ensure(4) && r->qOverflow.ensure(1);
+        r->qShadowO.ensure(2 * Q) && r->qShadowD.ensure(2 * Q) && r->qCounts.ensure(16) && r->qRays.ensure(2) &&
+        r->qVisits.ensure(4) && r->qOverflow.ensure(1) && r->dbatch.ensure(1);
     if (!ok) {
         return fail(r, PT_ERR_OUT_OF_MEMORY, "path state allocation failed for %d paths", capacity);
     }
@@ -260,6 +263,7 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.q.shadowDir = r->qShadowD.p;
     c.q.counts = r->qCounts.p;
     c.q.rays = r->qRays.p;
+    c.q.batch = r->dbatch.p;
     c.q.visits = r->qVisits.p;
     c.q.overflow = r->qOverflow.p;
     c.acc.acc = r->acc.p;
@@ -302,6 +306,7 @@ int resetAccum(pt_renderer* r)
     launchResetAccum(dc, r->width * r->height, r->stream);
     PT_CHECK(r, cudaGetLastError());
     r->hostActive = r->width * r->height;
+    r->lastStopRate = 1.0;
     r->wavesDone = 0;
     r->samplesDone = 0;
     return PT_OK;
@@ -353,28 +358,31 @@ void collectStageTimes(pt_renderer* r)
     r->eventMarks.clear();
 }
 
-// Number of waves folded into one launch (see the render loop comment).
+// Number of waves folded into one batch (see the render loop comment).
+// Results do not depend on it; a pixel that converges inside a batch leaves
+// the rest of the batch's samples unused, so the batch grows when few pixels
+// stopped during the previous one.
 int chooseBatch(const pt_renderer* r, int remaining)
 {
     const pt_render_params& p = r->params;
-    int B;
+    int64_t B;
     if (p.samples_per_launch > 0) {
         B = p.samples_per_launch;
     } else if (r->wavesDone < p.min_samples) {
-        B = static_cast<int>(p.min_samples - r->wavesDone); // nothing can converge before min_samples
+        B = p.min_samples - r->wavesDone; // nothing can converge before min_samples
     } else {
-        B = 4; // convergence is tested every 4 samples: no sample is wasted
+        B = r->lastStopRate > 0.02 ? 4 : (r->lastStopRate > 0.005 ? 16 : 64);
     }
     if (p.max_samples_per_pixel > 0) {
         B = std::min<int64_t>(B, p.max_samples_per_pixel - r->wavesDone);
     }
     if (remaining > 0) {
-        B = std::min(B, remaining);
+        B = std::min<int64_t>(B, remaining);
     }
     // cap the sample buffer at ~1 GiB
     const int64_t cap = std::max<int64_t>(1, (int64_t(1) << 30) / (16 * std::max(1, r->hostActive)));
-    B = static_cast<int>(std::min<int64_t>(B, std::min<int64_t>(cap, 1024)));
-    return std::max(B, 1);
+    B = std::min<int64_t>(B, std::min<int64_t>(cap, 1024));
+    return static_cast<int>(std::max<int64_t>(B, 1));
 }
 
 } // namespace
@@ -476,6 +484,7 @@ int pt_destroy(pt_renderer* r)
     r->qVisits.release();
     r->qOverflow.release();
     r->dctx.release();
+    r->dbatch.release();
     for (cudaEvent_t e : r->eventPool) {
         cudaEventDestroy(e);
     }
@@ -789,57 +798,62 @@ int pt_render(pt_renderer* r, int waves)
             return fail(r, PT_ERR_OUT_OF_MEMORY, "sample buffer allocation failed (%zu samples)", need);
         }
         const long long jobs = static_cast<long long>(active) * B;
-        const int chunkCap = std::min(r->capacity, r->capacityWanted);
-        for (long long start = 0; start < jobs; start += chunkCap) {
-            const int chunk = static_cast<int>(std::min<long long>(chunkCap, jobs - start));
-            const LaunchCtx* c = uploadCtx(r);
-            if (c == nullptr) {
-                return fail(r, PT_ERR_CUDA, "launch context upload failed");
+        const int slots = static_cast<int>(std::min<long long>(std::min(r->capacity, r->capacityWanted), jobs));
+        r->hbatch.jobs = static_cast<unsigned long long>(jobs);
+        r->hbatch.nextJob = static_cast<unsigned long long>(slots);
+        r->hbatch.activeCount = active;
+        r->hbatch.waveBase = static_cast<uint32_t>(r->wavesDone);
+        PT_CHECK(r, cudaMemcpyAsync(r->dbatch.p, &r->hbatch, sizeof(BatchInfo), cudaMemcpyHostToDevice, s));
+        const LaunchCtx* c = uploadCtx(r);
+        if (c == nullptr) {
+            return fail(r, PT_ERR_CUDA, "launch context upload failed");
+        }
+        {
+            StageTimer tm(r, kGenerate);
+            launchGenerate(c, slots, 0, s);
+        }
+        ++launches;
+        // Every live path advances one bounce per iteration and a finished path's
+        // slot takes the next job, so iterations <= bounce-steps / slots + drain.
+        const long long maxIters =
+            (jobs * (maxDepthEff + 1) + slots - 1) / std::max(slots, 1) + maxDepthEff + 8;
+        int sel = 0;
+        for (long long it = 0;; ++it) {
+            if (it > maxIters) {
+                return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
+            }
+            const int iter = static_cast<int>(it & 0x7fffffff);
+            {
+                StageTimer tm(r, kExtend);
+                launchExtend(c, sel, it == 0, iter, r->gridExtend, countVisits, s);
             }
             {
-                StageTimer tm(r, kGenerate);
-                launchGenerate(c, start, chunk, active, static_cast<uint32_t>(r->wavesDone), 0, s);
+                StageTimer tm(r, kShade);
+                launchShadeMiss(c, iter, sel, r->gridShade, s);
+                launchShade(c, sel, iter, r->gridShade, s);
             }
-            ++launches;
-            int sel = 0;
-            for (int depth = 0; depth <= maxDepthEff; ++depth) {
-                const bool identity = depth == 0;
-                {
-                    StageTimer tm(r, kExtend);
-                    launchExtend(c, sel, identity, depth, r->gridExtend, countVisits, s);
-                }
-                {
-                    StageTimer tm(r, kShade);
-                    launchShadeMiss(c, depth, r->gridShade, s);
-                    launchShade(c, sel, depth, r->gridShade, s);
-                }
-                launches += 3;
-                r->profile.launches_extend += 1;
-                if (depth < maxDepthEff) {
-                    {
-                        StageTimer tm(r, kShadow);
-                        launchShadow(c, r->gridShadow, countVisits, s);
-                    }
-                    {
-                        StageTimer tm(r, kFinalize);
-                        launchFinalize(c, r->gridShadow, s);
-                    }
-                    launches += 2;
-                    r->profile.launches_shadow += 1;
-                }
-                sel ^= 1;
-                if (depth >= 3 && (depth & 3) == 3 && depth < maxDepthEff) {
-                    unsigned int live = 0;
-                    PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p + sel, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-                    PT_CHECK(r, cudaStreamSynchronize(s));
-                    if (live == 0) {
-                        break;
-                    }
+            {
+                StageTimer tm(r, kShadow);
+                launchShadow(c, iter, r->gridShadow, countVisits, s);
+            }
+            {
+                StageTimer tm(r, kFinalize);
+                launchFinalize(c, sel, r->gridShadow, s);
+            }
+            launches += 5;
+            r->profile.launches_extend += 1;
+            r->profile.launches_shadow += 1;
+            sel ^= 1;
+            if ((it & 3) == 3) {
+                unsigned int live = 0;
+                PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p + sel, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+                PT_CHECK(r, cudaStreamSynchronize(s));
+                if (live == 0) {
+                    break;
                 }
             }
-            PT_CHECK(r, cudaGetLastError());
         }
-        const LaunchCtx* c = r->dctx.p;
+        PT_CHECK(r, cudaGetLastError());
         {
             StageTimer tm(r, kAccumulate);
             launchAccumulate(c, active, B, s);
@@ -854,6 +868,7 @@ int pt_render(pt_renderer* r, int waves)
         PT_CHECK(r, cudaMemcpyAsync(&next, r->activeCount.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
         PT_CHECK(r, cudaStreamSynchronize(s));
         PT_CHECK(r, cudaGetLastError());
+        r->lastStopRate = static_cast<double>(active - next) / active / std::max(1.0, B / 4.0);
         r->activeSel ^= 1;
         r->hostActive = next;
         r->wavesDone += B;

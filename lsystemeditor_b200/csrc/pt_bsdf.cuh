@@ -536,7 +536,11 @@ __device__ __forceinline__ float pdfSubsurface(const Ctx& c, float3 wi)
     return c.w.subsurface * fmax2(cp, burleyPdf(disk, mr) * 0.5f);
 }
 
-__device__ __forceinline__ float3 bsdfEval(const Ctx& c, float3 wi)
+// The BSDF is evaluated at up to four call sites per shading point (two NEE
+// estimators, the sampled direction, and the pdf inside sampling).  Keeping one
+// out-of-line copy of eval, pdf and sample keeps the shade kernel small enough
+// for the instruction cache (inlining every site made it fetch-bound).
+__device__ __forceinline__ float3 bsdfEvalImpl(const Ctx& c, float3 wi)
 {
     const float3 d = evalDiffuse(c, wi);
     const float3 s = evalSpecular(c, wi);
@@ -549,7 +553,7 @@ __device__ __forceinline__ float3 bsdfEval(const Ctx& c, float3 wi)
     return r;
 }
 
-__device__ __forceinline__ float bsdfPdf(const Ctx& c, float3 wi)
+__device__ __forceinline__ float bsdfPdfImpl(const Ctx& c, float3 wi)
 {
     float p = pdfDiffuse(c, wi) + pdfSpecular(c, wi);
     if (c.w.transmit != 0.0f) {
@@ -560,6 +564,9 @@ __device__ __forceinline__ float bsdfPdf(const Ctx& c, float3 wi)
     }
     return p;
 }
+
+__device__ __noinline__ float3 bsdfEval(const Ctx& c, float3 wi) { return bsdfEvalImpl(c, wi); }
+__device__ __noinline__ float bsdfPdf(const Ctx& c, float3 wi) { return bsdfPdfImpl(c, wi); }
 
 __device__ __forceinline__ BsdfSample emptySample(const Ctx& c)
 {
@@ -695,7 +702,7 @@ __device__ __noinline__ BsdfSample sampleTransmit(const Ctx& c, float u1, float 
     return s;
 }
 
-__device__ __forceinline__ BsdfSample bsdfSample(const Ctx& c, float u1, float u2)
+__device__ __noinline__ BsdfSample bsdfSample(const Ctx& c, float u1, float u2)
 {
     if (c.debug & kDbgForceTransmit) {
         return sampleTransmit(c, u1, u2);

@@ -52,6 +52,18 @@ __device__ __forceinline__ uint32_t warpPush(unsigned int* counter)
     return base + g.thread_rank();
 }
 
+// Warp-granular work distribution: each warp takes the next 32 queue entries
+// from a per-launch counter, so warps that drew cheap rays keep working
+// instead of idling while others finish (no static grid-stride split).
+__device__ __forceinline__ unsigned int warpFetch(unsigned int* counter)
+{
+    unsigned int base = 0;
+    if ((threadIdx.x & 31) == 0) {
+        base = atomicAdd(counter, 32u);
+    }
+    return __shfl_sync(0xffffffffu, base, 0) + (threadIdx.x & 31);
+}
+
 __device__ __forceinline__ void rngLoad(const PathSoA& P, uint32_t i, curandStateXORWOW& s)
 {
     const uint4 a = P.rngA[i];
@@ -112,47 +124,75 @@ __device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, floa
     c.acc.samples[c.paths.outIdx[i]] = make_float4(s.x, s.y, s.z, 1.0f);
 }
 
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ cp, long long jobStart, int jobCount, int activeCount,
-    uint32_t waveBase, int extendSel)
+// Camera path for job j of the current batch (PathTracer.cu:69-96): job
+// j = slot * activeCount + listIndex draws sample `counts[pixel] + slot` of
+// pixel active[listIndex] with the reference seed for wave waveBase + slot.
+__device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigned long long j)
+{
+    const BatchInfo& bt = *c.q.batch;
+    const int activeCount = bt.activeCount;
+    const int* active = c.acc.active[c.activeSel];
+    const int li = static_cast<int>(j % static_cast<unsigned long long>(activeCount));
+    const uint32_t slot = static_cast<uint32_t>(j / static_cast<unsigned long long>(activeCount));
+    const uint32_t pixel = static_cast<uint32_t>(active[li]);
+    const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
+    const uint32_t globalSeed = bt.waveBase + slot + 1u;
+    curandStateXORWOW st;
+    curand_init(pathSeed(c.params, pixel, c.width, sampleIndex, globalSeed), 0ull, 0ull, &st);
+    const uint32_t x = pixel % c.width, y = pixel / c.width;
+    const float ju = curand_uniform(&st);
+    const float jv = curand_uniform(&st);
+    const float u = (static_cast<float>(x) + ju) / static_cast<float>(c.width);
+    const float v = (static_cast<float>(y) + jv) / static_cast<float>(c.height);
+    const float l1 = curand_uniform(&st);
+    const float l2 = curand_uniform(&st);
+    float3 ro, rd;
+    cameraRay(c.cam, u, v, l1, l2, ro, rd);
+    c.paths.pixel[i] = pixel;
+    c.paths.outIdx[i] = static_cast<uint32_t>(j); // == slot * activeCount + listIndex
+    rngStore(c.paths, i, st);
+    c.paths.orig[i] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+    c.paths.dir[i] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+    c.paths.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+    c.paths.rad[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+    c.paths.visEnv[i] = 0;
+    c.paths.visEmis[i] = 0;
+}
+
+// A terminated path's slot takes the batch's next job, if any, and joins the
+// next extend queue: launches stay full until the batch drains.
+__device__ __forceinline__ void recyclePath(const LaunchCtx& c, uint32_t i, unsigned int* nextCount, uint32_t* nextQueue)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) {
+        base = atomicAdd(&c.q.batch->nextJob, static_cast<unsigned long long>(g.size()));
+    }
+    base = g.shfl(base, 0);
+    const unsigned long long j = base + g.thread_rank();
+    if (j < c.q.batch->jobs) {
+        initPath(c, i, j);
+        const uint32_t s = warpPush(nextCount);
+        nextQueue[s] = i;
+    }
+}
+
+// First `count` jobs of a batch into slots 0..count-1 (extend queue = identity).
+__global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ cp, int count, int extendSel)
 {
     const LaunchCtx& c = *cp;
-    const int* active = c.acc.active[c.activeSel];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        c.q.counts[extendSel] = static_cast<unsigned int>(jobCount);
+        c.q.counts[extendSel] = static_cast<unsigned int>(count);
         c.q.counts[extendSel ^ 1] = 0u;
         c.q.counts[2] = 0u;
         c.q.counts[3] = 0u;
         c.q.counts[4] = 0u;
         c.q.counts[5] = 0u;
+        c.q.counts[8] = 0u;  // fetch counters of the first extend and shadow stages
+        c.q.counts[10] = 0u;
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < jobCount; i += gridDim.x * blockDim.x) {
-        const long long j = jobStart + i;
-        const int li = static_cast<int>(j % activeCount);
-        const uint32_t slot = static_cast<uint32_t>(j / activeCount);
-        const uint32_t pixel = static_cast<uint32_t>(active[li]);
-        const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
-        const uint32_t globalSeed = waveBase + slot + 1u;
-        curandStateXORWOW st;
-        curand_init(pathSeed(c.params, pixel, c.width, sampleIndex, globalSeed), 0ull, 0ull, &st);
-        const uint32_t x = pixel % c.width, y = pixel / c.width;
-        const float ju = curand_uniform(&st);
-        const float jv = curand_uniform(&st);
-        const float u = (static_cast<float>(x) + ju) / static_cast<float>(c.width);
-        const float v = (static_cast<float>(y) + jv) / static_cast<float>(c.height);
-        const float l1 = curand_uniform(&st);
-        const float l2 = curand_uniform(&st);
-        float3 ro, rd;
-        cameraRay(c.cam, u, v, l1, l2, ro, rd);
-        c.paths.pixel[i] = pixel;
-        c.paths.outIdx[i] = slot * static_cast<uint32_t>(activeCount) + static_cast<uint32_t>(li);
-        rngStore(c.paths, i, st);
-        c.paths.orig[i] = make_float4(ro.x, ro.y, ro.z, 0.0f);
-        c.paths.dir[i] = make_float4(rd.x, rd.y, rd.z, 0.0f);
-        c.paths.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        c.paths.rad[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
-        c.paths.visEnv[i] = 0;
-        c.paths.visEmis[i] = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        initPath(c, static_cast<uint32_t>(i), static_cast<unsigned long long>(i));
     }
 }
 
@@ -161,12 +201,12 @@ __global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ 
 // Counters: [4 + 2p] misses and [5 + 2p] hits of bounce parity p; this kernel
 // zeroes the other parity's pair for the next bounce.
 template <bool Count>
-__global__ void __launch_bounds__(256, 4) k_extend(const LaunchCtx* __restrict__ cp, int sel, bool identity, int depth)
+__global__ void __launch_bounds__(256, 4) k_extend(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
 {
     const LaunchCtx& c = *cp;
     extern __shared__ uint2 smemStack[];
     const unsigned int count = c.q.counts[sel];
-    const int par = depth & 1;
+    const int par = iter & 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&c.q.rays[0], static_cast<unsigned long long>(count));
         // output counters of the shade stage that follows, and next bounce's routing counters
@@ -175,9 +215,18 @@ __global__ void __launch_bounds__(256, 4) k_extend(const LaunchCtx* __restrict__
         c.q.counts[3] = 0u;
         c.q.counts[4 + 2 * (par ^ 1)] = 0u;
         c.q.counts[5 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[8 + (par ^ 1)] = 0u; // next extend's fetch counter
     }
     const uint32_t* queue = c.q.extend[sel];
-    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    unsigned int* fetch = &c.q.counts[8 + par];
+    for (;;) {
+        const unsigned int k = warpFetch(fetch);
+        if (__shfl_sync(0xffffffffu, k, 0) >= count) {
+            break;
+        }
+        if (k >= count) {
+            continue;
+        }
         const uint32_t i = identity ? k : queue[k];
         const float4 o4 = c.paths.orig[i];
         const float4 d4 = c.paths.dir[i];
@@ -198,19 +247,22 @@ __global__ void __launch_bounds__(256, 4) k_extend(const LaunchCtx* __restrict__
 
 // Paths whose ray left the scene: previous bounce's NEE, then the
 // environment / background term (PathIntegratorRandCore.h:215-216, 338-346).
-__global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict__ cp, int depth)
+__global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict__ cp, int iter, int sel)
 {
     const LaunchCtx& c = *cp;
-    const unsigned int count = c.q.counts[4 + 2 * (depth & 1)];
+    const unsigned int count = c.q.counts[4 + 2 * (iter & 1)];
+    unsigned int* nextCount = &c.q.counts[sel ^ 1];
+    uint32_t* nextQueue = c.q.extend[sel ^ 1];
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = c.q.missQueue[k];
         const float4 d4 = c.paths.dir[i];
         const float3 d = f3(d4.x, d4.y, d4.z);
+        const float4 r4 = c.paths.rad[i];
+        const int depth = __float_as_int(r4.w);
         float3 L;
         if (depth == 0) {
             L = envEval(c.env, c.params, d);
         } else {
-            const float4 r4 = c.paths.rad[i];
             L = f3(r4.x, r4.y, r4.z);
             if (c.paths.visEnv[i]) {
                 const float4 e = c.paths.neeEnv[i];
@@ -227,35 +279,33 @@ __global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict_
             L = add3(L, mul3(f3(t4.x, t4.y, t4.z), scl3(Le, w)));
         }
         writeSample(c, i, L);
+        recyclePath(c, i, nextCount, nextQueue);
     }
 }
 
 // Shading of the paths that hit a triangle. One thread per queued path.
-__global__ void __launch_bounds__(256) k_shade(const LaunchCtx* __restrict__ cp, int sel, int depth)
+__global__ void __launch_bounds__(256, 3) k_shade(const LaunchCtx* __restrict__ cp, int sel, int iter)
 {
     const LaunchCtx& c = *cp;
-    const unsigned int count = c.q.counts[5 + 2 * (depth & 1)];
+    const unsigned int count = c.q.counts[5 + 2 * (iter & 1)];
     const uint32_t* queue = c.q.hitQueue;
     unsigned int* nextCount = &c.q.counts[sel ^ 1];
     uint32_t* nextQueue = c.q.extend[sel ^ 1];
     const int debugFlags = c.params.brdf_debug_flags;
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = queue[k];
-        float3 L = f3(0.0f, 0.0f, 0.0f);
-        if (depth > 0) {
-            const float4 r4 = c.paths.rad[i];
-            L = f3(r4.x, r4.y, r4.z);
+        const float4 r4 = c.paths.rad[i];
+        float3 L = f3(r4.x, r4.y, r4.z);
+        const int depth = __float_as_int(r4.w);
+        // NEE contributions of the previous bounce, in the reference's order
+        // (the flags are clear for a path that starts at this bounce).
+        if (c.paths.visEnv[i]) {
+            const float4 e = c.paths.neeEnv[i];
+            L = add3(L, f3(e.x, e.y, e.z));
         }
-        // NEE contributions of the previous bounce, in the reference's order.
-        if (depth > 0) {
-            if (c.paths.visEnv[i]) {
-                const float4 e = c.paths.neeEnv[i];
-                L = add3(L, f3(e.x, e.y, e.z));
-            }
-            if (c.paths.visEmis[i]) {
-                const float4 e = c.paths.neeEmis[i];
-                L = add3(L, f3(e.x, e.y, e.z));
-            }
+        if (c.paths.visEmis[i]) {
+            const float4 e = c.paths.neeEmis[i];
+            L = add3(L, f3(e.x, e.y, e.z));
         }
         const float4 h4 = c.paths.hit[i];
         const uint32_t tri = __float_as_uint(h4.w);
@@ -268,13 +318,9 @@ __global__ void __launch_bounds__(256) k_shade(const LaunchCtx* __restrict__ cp,
             done = true;
         } else {
             const float4 o4 = c.paths.orig[i];
-            float3 T = f3(1.0f, 1.0f, 1.0f);
-            float eta = 1.0f;
-            if (depth > 0) {
-                const float4 t4 = c.paths.thr[i];
-                T = f3(t4.x, t4.y, t4.z);
-                eta = t4.w;
-            }
+            const float4 t4 = c.paths.thr[i];
+            float3 T = f3(t4.x, t4.y, t4.z);
+            float eta = t4.w;
             const float t = h4.x;
             const float3 pos = xadd(f3(o4.x, o4.y, o4.z), xscl(d, t));
             const float3 dn = xnormalize(d);
@@ -442,23 +488,34 @@ __global__ void __launch_bounds__(256) k_shade(const LaunchCtx* __restrict__ cp,
             c.paths.rad[i] = make_float4(L.x, L.y, L.z, __int_as_float(depth));
             const uint32_t s = warpPush(&c.q.counts[3]);
             c.q.finish[s] = i;
-        } else if (done || !cont) {
+        } else {
             writeSample(c, i, L);
+            recyclePath(c, i, nextCount, nextQueue);
         }
     }
 }
 
 // Occlusion of the queued shadow rays (LightSamplingCore.h:187-197, 360-369).
 template <bool Count>
-__global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__ cp)
+__global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__ cp, int iter)
 {
     const LaunchCtx& c = *cp;
     extern __shared__ uint2 smemStack[];
     const unsigned int count = c.q.counts[2];
+    const int par = iter & 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&c.q.rays[1], static_cast<unsigned long long>(count));
+        c.q.counts[10 + (par ^ 1)] = 0u; // next shadow stage's fetch counter
     }
-    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    unsigned int* fetch = &c.q.counts[10 + par];
+    for (;;) {
+        const unsigned int k = warpFetch(fetch);
+        if (__shfl_sync(0xffffffffu, k, 0) >= count) {
+            break;
+        }
+        if (k >= count) {
+            continue;
+        }
         const uint32_t e = c.q.shadowPath[k];
         const float4 o4 = c.q.shadowOrig[k];
         const float4 d4 = c.q.shadowDir[k];
@@ -478,10 +535,12 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__
 }
 
 // Paths that terminated while their NEE shadow rays were in flight.
-__global__ void __launch_bounds__(256) k_finalize(const LaunchCtx* __restrict__ cp)
+__global__ void __launch_bounds__(256) k_finalize(const LaunchCtx* __restrict__ cp, int sel)
 {
     const LaunchCtx& c = *cp;
     const unsigned int count = c.q.counts[3];
+    unsigned int* nextCount = &c.q.counts[sel ^ 1];
+    uint32_t* nextQueue = c.q.extend[sel ^ 1];
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = c.q.finish[k];
         const float4 r4 = c.paths.rad[i];
@@ -495,6 +554,7 @@ __global__ void __launch_bounds__(256) k_finalize(const LaunchCtx* __restrict__ 
             L = add3(L, f3(e.x, e.y, e.z));
         }
         writeSample(c, i, L);
+        recyclePath(c, i, nextCount, nextQueue);
     }
 }
 
@@ -680,35 +740,34 @@ inline int gridFor(long long n, int block = 256, int cap = 148 * 16)
 
 } // namespace
 
-void launchGenerate(const LaunchCtx* d, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
-    int extendSel, cudaStream_t s)
+void launchGenerate(const LaunchCtx* d, int count, int extendSel, cudaStream_t s)
 {
-    k_generate<<<gridFor(jobCount), 256, 0, s>>>(d, jobStart, jobCount, activeCount, waveBase, extendSel);
+    k_generate<<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
 }
-void launchExtend(const LaunchCtx* c, int sel, bool identity, int depth, int grid, bool count, cudaStream_t s)
+void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid, bool count, cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
     if (count) {
-        k_extend<true><<<grid, 256, smem, s>>>(c, sel, identity, depth);
+        k_extend<true><<<grid, 256, smem, s>>>(c, sel, identity, iter);
     } else {
-        k_extend<false><<<grid, 256, smem, s>>>(c, sel, identity, depth);
+        k_extend<false><<<grid, 256, smem, s>>>(c, sel, identity, iter);
     }
 }
-void launchShadeMiss(const LaunchCtx* c, int depth, int grid, cudaStream_t s)
+void launchShadeMiss(const LaunchCtx* c, int iter, int sel, int grid, cudaStream_t s)
 {
-    k_shade_miss<<<grid, 256, 0, s>>>(c, depth);
+    k_shade_miss<<<grid, 256, 0, s>>>(c, iter, sel);
 }
-void launchShade(const LaunchCtx* c, int sel, int depth, int grid, cudaStream_t s)
+void launchShade(const LaunchCtx* c, int sel, int iter, int grid, cudaStream_t s)
 {
-    k_shade<<<grid, 256, 0, s>>>(c, sel, depth);
+    k_shade<<<grid, 256, 0, s>>>(c, sel, iter);
 }
-void launchShadow(const LaunchCtx* c, int grid, bool count, cudaStream_t s)
+void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
     if (count) {
-        k_shadow<true><<<grid, 256, smem, s>>>(c);
+        k_shadow<true><<<grid, 256, smem, s>>>(c, iter);
     } else {
-        k_shadow<false><<<grid, 256, smem, s>>>(c);
+        k_shadow<false><<<grid, 256, smem, s>>>(c, iter);
     }
 }
 void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
@@ -719,7 +778,7 @@ void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadeBlocks, k_shade, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadowBlocks, k_shadow<false>, 256, smem);
 }
-void launchFinalize(const LaunchCtx* c, int grid, cudaStream_t s) { k_finalize<<<grid, 256, 0, s>>>(c); }
+void launchFinalize(const LaunchCtx* c, int sel, int grid, cudaStream_t s) { k_finalize<<<grid, 256, 0, s>>>(c, sel); }
 void launchAccumulate(const LaunchCtx* c, int activeCount, int batch, cudaStream_t s)
 {
     k_accumulate<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount, batch);

@@ -23,6 +23,15 @@ struct PathSoA {
     int capacity = 0;
 };
 
+// Current batch of (pixel, sample) jobs (device memory; written by the host at
+// batch start, nextJob advanced by the kernels that recycle path slots).
+struct BatchInfo {
+    unsigned long long jobs;     // activeCount x waves in this batch
+    unsigned long long nextJob;  // first job not yet handed to a path slot
+    int activeCount;
+    uint32_t waveBase;
+};
+
 struct QueueSet {
     uint32_t* extend[2] = {nullptr, nullptr}; // path indices, ping-pong
     uint32_t* finish = nullptr;               // paths that ended with shadow rays in flight
@@ -32,11 +41,13 @@ struct QueueSet {
     float4* shadowOrig = nullptr;
     float4* shadowDir = nullptr;
     // counters: [0],[1] extend ping-pong, [2] shadow, [3] finish,
-    // [4 + 2p] misses / [5 + 2p] hits of bounce parity p
+    // [4 + 2p] misses / [5 + 2p] hits of bounce parity p, [8 + p] extend and
+    // [10 + p] shadow work-fetch counters
     unsigned int* counts = nullptr;
     unsigned long long* rays = nullptr;       // [0] closest-hit rays, [1] shadow rays
     unsigned long long* visits = nullptr;     // [0..1] extend nodes/tris, [2..3] shadow nodes/tris
     unsigned int* overflow = nullptr;         // traversal stack overflows
+    BatchInfo* batch = nullptr;
 };
 
 struct AccumState {
@@ -70,13 +81,12 @@ struct LaunchCtx {
 // passed by pointer: a large by-value kernel parameter whose members are
 // taken by reference would be copied to local memory by every thread.
 // `grid` is a persistent-style grid; kernels loop over device-side counts.
-void launchGenerate(const LaunchCtx* d, long long jobStart, int jobCount, int activeCount, uint32_t waveBase,
-    int extendSel, cudaStream_t s);
-void launchExtend(const LaunchCtx* d, int sel, bool identity, int depth, int grid, bool count, cudaStream_t s);
-void launchShadeMiss(const LaunchCtx* d, int depth, int grid, cudaStream_t s);
-void launchShade(const LaunchCtx* d, int sel, int depth, int grid, cudaStream_t s);
-void launchShadow(const LaunchCtx* d, int grid, bool count, cudaStream_t s);
-void launchFinalize(const LaunchCtx* d, int grid, cudaStream_t s);
+void launchGenerate(const LaunchCtx* d, int count, int extendSel, cudaStream_t s);
+void launchExtend(const LaunchCtx* d, int sel, bool identity, int iter, int grid, bool count, cudaStream_t s);
+void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, cudaStream_t s);
+void launchShade(const LaunchCtx* d, int sel, int iter, int grid, cudaStream_t s);
+void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, cudaStream_t s);
+void launchFinalize(const LaunchCtx* d, int sel, int grid, cudaStream_t s);
 void launchAccumulate(const LaunchCtx* d, int activeCount, int batch, cudaStream_t s);
 void launchCompact(const LaunchCtx* d, int activeCount, cudaStream_t s);
 void launchResetAccum(const LaunchCtx* d, int pixels, cudaStream_t s);

@@ -24,6 +24,7 @@ namespace pt {
 
 constexpr int kTraversalStack = 32;   // entries of the local-memory stack (fallback / Q1 path)
 constexpr int kSharedStack = 20;      // entries per thread of the shared-memory stack
+constexpr int kPostponeLanes = 8;     // postpone triangle tests when fewer lanes want them
 constexpr float kSlabWiden = 1.0000005f;
 
 struct HitRec {
@@ -266,23 +267,27 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
     float bu = 0.0f, bv = 0.0f;
     bool overflow = false;
     uint32_t nodeVisits = 0, triVisits = 0;
+    uint2 tgroup = make_uint2(0u, 0u);
+    auto push = [&](uint2 g) -> bool {
+        if (sstack != nullptr && sp < kSharedStack) {
+            sstack[sp * sstride] = g;
+        } else if (sp < (sstack != nullptr ? kSharedStack : 0) + kTraversalStack) {
+            stack[sp - (sstack != nullptr ? kSharedStack : 0)] = g;
+        } else {
+            return false;
+        }
+        ++sp;
+        return true;
+    };
     while (true) {
-        // descend into the nearest remaining child of the current node group
         if (ngroup.y > 0x00FFFFFFu) {
+            // descend into the nearest remaining child of the current node group
             const uint32_t bit = 31u - __clz(ngroup.y);
             ngroup.y &= ~(1u << bit);
             const uint32_t slot = (bit - 24u) ^ octinv;
             const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
-            if (ngroup.y > 0x00FFFFFFu) {
-                if (sstack != nullptr && sp < kSharedStack) {
-                    sstack[sp * sstride] = ngroup;
-                    ++sp;
-                } else if (sp < (sstack != nullptr ? kSharedStack : 0) + kTraversalStack) {
-                    stack[sp - (sstack != nullptr ? kSharedStack : 0)] = ngroup;
-                    ++sp;
-                } else {
-                    overflow = true;
-                }
+            if (ngroup.y > 0x00FFFFFFu && !push(ngroup)) {
+                overflow = true;
             }
             uint32_t childBase, triBase, imask;
             const uint32_t hits = intersectChildren(S.nodes, child, o, idir, octinv, tMin, closest, childBase, triBase,
@@ -291,35 +296,45 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
                 ++nodeVisits;
             }
             ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
-            uint32_t tmask = hits & 0x00FFFFFFu;
-            while (tmask != 0u) {
-                const int k = __ffs(tmask) - 1;
-                tmask &= tmask - 1u;
-                const TriVerts tv = S.tris[triBase + k];
-                float t, u, v;
-                if (Count) {
-                    ++triVisits;
-                }
-                if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
-                        f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
-                    if (AnyHit) {
-                        if (t < tMax) {
-                            if (Count) {
-                                atomicAdd(&visits[0], static_cast<unsigned long long>(nodeVisits));
-                                atomicAdd(&visits[1], static_cast<unsigned long long>(triVisits));
-                            }
-                            out.t = t;
-                            out.u = u;
-                            out.v = v;
-                            out.tri = __float_as_uint(tv.v0.w);
-                            return true;
+            tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
+        } else {
+            // a group popped without node hits holds postponed triangles
+            tgroup = ngroup;
+            ngroup = make_uint2(0u, 0u);
+        }
+        while (tgroup.y != 0u) {
+            // Postpone the triangle tests while few lanes of the warp have any and this
+            // lane can keep descending (Ylitie, Karras & Laine 2017); they are retried
+            // from the stack, so SIMT lanes test triangles together.
+            if (ngroup.y > 0x00FFFFFFu && __popc(__activemask()) < kPostponeLanes && push(tgroup)) {
+                break;
+            }
+            const int k = __ffs(tgroup.y) - 1;
+            tgroup.y &= tgroup.y - 1u;
+            const TriVerts tv = S.tris[tgroup.x + k];
+            float t, u, v;
+            if (Count) {
+                ++triVisits;
+            }
+            if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                    f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
+                if (AnyHit) {
+                    if (t < tMax) {
+                        if (Count) {
+                            atomicAdd(&visits[0], static_cast<unsigned long long>(nodeVisits));
+                            atomicAdd(&visits[1], static_cast<unsigned long long>(triVisits));
                         }
-                    } else {
-                        closest = t;
-                        best = triBase + k;
-                        bu = u;
-                        bv = v;
+                        out.t = t;
+                        out.u = u;
+                        out.v = v;
+                        out.tri = __float_as_uint(tv.v0.w);
+                        return true;
                     }
+                } else {
+                    closest = t;
+                    best = tgroup.x + k;
+                    bu = u;
+                    bv = v;
                 }
             }
         }
