@@ -255,6 +255,31 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
  * assumed to have counts == first_wave (a fresh accumulation). */
 int pt_rng_tape(pt_renderer* r, int first_wave, int waves, int stride, float* out);
 
+/* Largest triangle count pt_trace_soup_noalloc accepts. */
+#define PT_NOALLOC_MAX_TRIANGLES 16384u
+
+/* Closest-hit queries against a small triangle soup that allocates no device
+ * memory (no counterpart in the reference).  For callers that cannot allocate:
+ * hosts whose allocator owns the whole device and hands out every byte itself
+ * (a cudaMalloc behind its back can fail or break its accounting), and
+ * latency-critical callbacks such as a viewport's surface pick, for which
+ * cudaMalloc/cudaFree cost an implicit device synchronisation each time.  Every input and output
+ * is a DEVICE pointer supplied by the caller (positions 9 floats/triangle;
+ * normals and uvs may be NULL; results as in pt_trace_rays); work runs on
+ * `stream` (NULL = default stream) of the current device and the call returns
+ * after the work is enqueued (the BVH build synchronises the stream once per
+ * tree level).  All temporaries live in one 8 MiB device array that the
+ * library reserves on every GPU it is loaded on, for the life of the process;
+ * up to PT_NOALLOC_MAX_TRIANGLES triangles (larger inputs are rejected with
+ * PT_ERR_INVALID_ARGUMENT and a message).  The first call on a device looks up
+ * that array's device address -- make it before any stream capture.  Calls
+ * share the array, so calls whose GPU work overlaps race and must be
+ * serialised by the caller.  error_message (may be NULL) receives the reason
+ * of a failure. */
+int pt_trace_soup_noalloc(uint32_t triangle_count, const float* positions, const float* normals, const float* uvs,
+    int n, const float* origins, const float* dirs, const float* tmin, const float* tmax, uint8_t* hit, float* t,
+    uint32_t* tri, float* normal, float* uv, void* stream, char* error_message, size_t error_capacity);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libpt_b200.so")
-SOURCES = ["pt_bvh.cu", "pt_render.cu", "pt_api.cu"]
+SOURCES = ["pt_bvh.cu", "pt_render.cu", "pt_api.cu", "pt_noalloc.cu"]
 HEADERS = ["pt_common.cuh", "pt_bvh.cuh", "pt_render.cuh", "pt_trace.cuh", "pt_bsdf.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--cudart", "static",

@@ -744,3 +744,89 @@ int buildBvh(const float* dPositions, uint32_t n, BvhBuffers& out, cudaStream_t 
 }
 
 } // namespace pt
+
+namespace pt {
+
+size_t bvhSortTempBytes(uint32_t n)
+{
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+        static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 30);
+    return bytes;
+}
+
+// Same build as buildBvh, into caller-provided buffers: nothing is allocated.
+int buildBvhInto(const float* dPositions, uint32_t n, const BvhScratch& sc, CwNode* outNodes, TriVerts* outTris,
+    uint32_t* outNodeCount, cudaStream_t stream, const BvhBuildOptions& opt, char* err, size_t errLen)
+{
+    if (n == 0) {
+        *outNodeCount = 0;
+        return PT_OK;
+    }
+    const int N = static_cast<int>(n);
+    const int nodesBin = 2 * N - 1;
+    const unsigned int init[8] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0u, 0u};
+    PT_TRY(cudaMemcpyAsync(sc.cbounds, init, sizeof(init), cudaMemcpyHostToDevice, stream));
+    k_prepare<<<gridFor(n), kBlock, 0, stream>>>(dPositions, n, sc.triLo, sc.triHi, sc.cbounds);
+    k_morton<<<gridFor(n), kBlock, 0, stream>>>(sc.triLo, sc.triHi, n, sc.cbounds, sc.keys, sc.vals);
+    size_t tempBytes = 0;
+    PT_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, sc.keys, sc.keysSorted, sc.vals, sc.valsSorted, N, 0, 30,
+        stream));
+    if (tempBytes > sc.sortTempBytes) {
+        std::snprintf(err, errLen, "radix sort needs %zu scratch bytes, %zu reserved", tempBytes, sc.sortTempBytes);
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    PT_TRY(cub::DeviceRadixSort::SortPairs(sc.sortTemp, tempBytes, sc.keys, sc.keysSorted, sc.vals, sc.valsSorted, N, 0,
+        30, stream));
+    PT_TRY(cudaMemsetAsync(sc.parent, 0xff, sizeof(int) * nodesBin, stream));
+    if (N > 1) {
+        k_karras<<<gridFor(N - 1), kBlock, 0, stream>>>(sc.keysSorted, N, sc.child, sc.parent);
+        PT_TRY(cudaMemsetAsync(sc.visits, 0, sizeof(int) * (N - 1), stream));
+    }
+    k_refit<<<gridFor(N), kBlock, 0, stream>>>(sc.valsSorted, sc.triLo, sc.triHi, N, sc.child, sc.parent, sc.nodeLo,
+        sc.nodeHi, sc.visits);
+    if (N > 1 && opt.treeletPasses > 0) {
+        for (int pass = 0; pass < opt.treeletPasses; ++pass) {
+            PT_TRY(cudaMemsetAsync(sc.visits, 0, sizeof(int) * (N - 1), stream));
+            k_treelet<<<gridFor(static_cast<long long>(N) * 32), kBlock, 0, stream>>>(N, sc.child, sc.parent, sc.nodeLo,
+                sc.nodeHi, sc.visits, sc.subCost, opt.treeletMinLeaves, opt.costTriangle, opt.costNode);
+        }
+    }
+    PT_TRY(cudaGetLastError());
+    const unsigned int cinit[4] = {1u, 0u, 0u, 0u};
+    PT_TRY(cudaMemcpyAsync(sc.counters, cinit, sizeof(cinit), cudaMemcpyHostToDevice, stream));
+    const int2 rootTask = make_int2(0, 0);
+    PT_TRY(cudaMemcpyAsync(sc.taskA, &rootTask, sizeof(int2), cudaMemcpyHostToDevice, stream));
+    CollapseArgs ca{N, sc.child, sc.nodeLo, sc.nodeHi, sc.valsSorted, dPositions, outNodes, outTris, sc.counters,
+        opt.maxLeafSize};
+    int2* taskA = sc.taskA;
+    int2* taskB = sc.taskB;
+    int taskCount = 1;
+    int levels = 0;
+    while (taskCount > 0) {
+        PT_TRY(cudaMemsetAsync(sc.counters + 2, 0, sizeof(unsigned int), stream));
+        k_collapse<<<gridFor(taskCount, 64), 64, 0, stream>>>(ca, taskA, taskCount, taskB, sc.counters + 2);
+        unsigned int next = 0;
+        PT_TRY(cudaMemcpyAsync(&next, sc.counters + 2, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
+        PT_TRY(cudaStreamSynchronize(stream));
+        taskCount = static_cast<int>(next);
+        int2* t = taskA;
+        taskA = taskB;
+        taskB = t;
+        if (++levels > 256) {
+            std::snprintf(err, errLen, "BVH collapse did not terminate");
+            return PT_ERR_INTERNAL;
+        }
+    }
+    unsigned int finalCounts[2] = {0, 0};
+    PT_TRY(cudaMemcpyAsync(finalCounts, sc.counters, sizeof(finalCounts), cudaMemcpyDeviceToHost, stream));
+    PT_TRY(cudaStreamSynchronize(stream));
+    if (finalCounts[1] != n) {
+        std::snprintf(err, errLen, "BVH collapse placed %u of %u triangles", finalCounts[1], n);
+        return PT_ERR_INTERNAL;
+    }
+    *outNodeCount = finalCounts[0];
+    return PT_OK;
+}
+
+} // namespace pt

@@ -90,6 +90,39 @@ struct BvhBuffers {
     }
 };
 
+// Caller-provided scratch for buildBvhInto (n = triangle count):
+//   triLo, triHi: n float4; cbounds: 8; keys, vals, keysSorted, valsSorted: n;
+//   child: n int2; parent: 2n int; nodeLo, nodeHi: 2n float4; visits: n;
+//   subCost: 2n; taskA, taskB: n + 1 int2; counters: 4; sortTemp: sortTempBytes.
+struct BvhScratch {
+    float4* triLo;
+    float4* triHi;
+    unsigned int* cbounds;
+    uint32_t* keys;
+    uint32_t* vals;
+    uint32_t* keysSorted;
+    uint32_t* valsSorted;
+    int2* child;
+    int* parent;
+    float4* nodeLo;
+    float4* nodeHi;
+    int* visits;
+    float* subCost;
+    int2* taskA;
+    int2* taskB;
+    unsigned int* counters;
+    void* sortTemp;
+    size_t sortTempBytes;
+};
+
+// Radix-sort scratch bytes for n keys (a size query; nothing is launched).
+size_t bvhSortTempBytes(uint32_t n);
+
+// The build of buildBvh into caller-provided buffers (outNodes: n + 1 nodes,
+// outTris: n records); performs no device allocation.
+int buildBvhInto(const float* dPositions, uint32_t n, const BvhScratch& scratch, CwNode* outNodes, TriVerts* outTris,
+    uint32_t* outNodeCount, cudaStream_t stream, const BvhBuildOptions& opt, char* err, size_t errLen);
+
 // Builds the compressed 8-wide BVH over n triangles whose positions
 // (9 floats per triangle) are already in device memory. Synchronises the
 // stream once per collapse level. Returns a pt_status code.

@@ -143,7 +143,7 @@ __device__ __forceinline__ uint32_t intersectChildren(const CwNode* __restrict__
 }
 
 // Slow path for quirk Q1 (degenerate direction components); see the file comment.
-__device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, bool anyHit,
+static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, bool anyHit,
     HitRec& out)
 {
     out.tri = 0xFFFFFFFFu;

@@ -57,7 +57,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_get_camera", "pt_set_params", "pt_get_params", "pt_default_params", "pt_set_environment",
                     "pt_reset", "pt_render", "pt_readback", "pt_device_buffers", "pt_get_stats", "pt_trace_rays",
                     "pt_trace_rays_device", "pt_rng_tape", "pt_set_stream", "pt_set_profiling", "pt_get_profile",
-                    "pt_set_tuning"]
+                    "pt_set_tuning", "pt_trace_soup_noalloc"]
 
 _LIB: Optional[C.CDLL] = None
 
