@@ -3,7 +3,10 @@
 
 One "step" is one complete render of the workload: every pixel traced until
 it reaches its sample budget or converges (pt_render with no wave limit),
-starting from a reset accumulator with the scene resident in HBM.
+starting from a reset accumulator with the scene resident in HBM.  The
+default workload is plain-large (972k-triangle stochastic tree, 1024x1024,
+adaptive 16-1024 spp, depth 12); --config plain-small selects the 20k-triangle
+2D tree at 256x256, 64 spp.
 
   value  Msamples/s of the device-timed steps (CUDA events on the stream the
          library launches on), summed over ranks, time = max over ranks.
@@ -46,10 +49,10 @@ L2_FLUSH_BYTES = 256 << 20
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--config", choices=["plain-small", "plain-large"], default="plain-small")
+    ap.add_argument("--config", choices=["plain-small", "plain-large"], default="plain-large")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -314,12 +317,13 @@ def run_b200(args):
     except OSError:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    # DRAM bytes per k_extend ray from an ncu capture (profiles/), scaled to a launch
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_extend.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            t = json.load(f)
-        if t.get("workload") == spec.name and t.get("bytes_per_ray"):
+            t = json.load(f).get(args.config, {})
+        if t.get("bytes_per_ray"):
             traffic = t["bytes_per_ray"] * rays_per_launch
 
     # ---- end to end through the public API with host buffers ---------------
