@@ -255,6 +255,21 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
  * assumed to have counts == first_wave (a fresh accumulation). */
 int pt_rng_tape(pt_renderer* r, int first_wave, int waves, int stride, float* out);
 
+/* ---- Batched form (no counterpart in the reference) ----------------------
+ * One renderer can hold several independent scenes (meshes, cameras, image
+ * sizes) that pt_render advances together: their pixels form one work queue,
+ * so small scenes fill the GPU jointly instead of one launch sequence each.
+ * Every scene renders exactly as it would alone (seeds and film coordinates
+ * use the pixel's index within its own image); the render parameters and the
+ * environment are shared.  pt_configure returns a renderer to one scene; the
+ * single-scene calls (pt_set_mesh, pt_set_camera, pt_readback, pt_trace_rays)
+ * address scene 0, and pt_device_buffers returns the concatenated pixels of
+ * all scenes (scene after scene). */
+int pt_batch_configure(pt_renderer* r, int scene_count, const int* widths, const int* heights);
+int pt_batch_set_mesh(pt_renderer* r, int scene, const pt_mesh* mesh);
+int pt_batch_set_camera(pt_renderer* r, int scene, const pt_camera* camera);
+int pt_batch_readback(pt_renderer* r, int scene, float* rgba, uint32_t* counts, uint8_t* converged);
+
 /* Largest triangle count pt_trace_soup_noalloc accepts. */
 #define PT_NOALLOC_MAX_TRIANGLES 16384u
 

@@ -49,6 +49,41 @@ template <class T> struct DevBuf {
     }
 };
 
+// One scene: geometry on the device, its image size, camera and first pixel
+// in the renderer's concatenated pixel range.  A plain renderer has one
+// scene; a batch has several that render together.
+struct SceneSlot {
+    DevBuf<float> positions;      // 9 floats per triangle, original order
+    DevBuf<TriShade> shade;
+    DevBuf<pt_material> materials;
+    DevBuf<pt_texture> textures;
+    DevBuf<uint32_t> emissiveIdx;
+    DevBuf<float> emissiveCdf;
+    BvhBuffers bvh;
+    uint32_t triCount = 0;
+    uint32_t materialCount = 0;
+    uint32_t textureCount = 0;
+    uint32_t emissiveCount = 0;
+    bool hasScene = false;
+    int width = 0;
+    int height = 0;
+    uint32_t pixelBase = 0;
+    pt_camera camera{};
+
+    void release()
+    {
+        positions.release();
+        shade.release();
+        materials.release();
+        textures.release();
+        emissiveIdx.release();
+        emissiveCdf.release();
+        bvh.release();
+        bvh.scratch.release();
+        hasScene = false;
+    }
+};
+
 } // namespace
 
 struct pt_renderer {
@@ -59,30 +94,22 @@ struct pt_renderer {
     std::string lastError = "";
     int smCount = 148;
 
-    // scene
-    DevBuf<float> positions;      // 9 floats per triangle, original order
-    DevBuf<TriShade> shade;
-    DevBuf<pt_material> materials;
-    DevBuf<pt_texture> textures;
-    DevBuf<uint32_t> emissiveIdx;
-    DevBuf<float> emissiveCdf;
+    // scenes (scenes[0] is the one the single-scene calls address)
+    std::vector<SceneSlot> scenes = std::vector<SceneSlot>(1);
+    DevBuf<DevScene> dScenes;             // device copies for batches
+    DevBuf<SceneView> dViews;
     DevBuf<float> stage;          // upload staging (normals / uvs)
     DevBuf<uint32_t> stageIds;
-    BvhBuffers bvh;
     BvhBuildOptions bvhOptions;
-    uint32_t triCount = 0;
-    uint32_t materialCount = 0;
-    uint32_t textureCount = 0;
-    uint32_t emissiveCount = 0;
-    bool hasScene = false;
 
     // environment
     DevBuf<float> envPixels, envMarginal, envRow;
     int envW = 0, envH = 0;
     bool envValid = false;
 
-    // accumulation
-    int width = 0, height = 0;
+    // accumulation over the concatenated pixels of all scenes
+    int width = 0, height = 0;            // scene 0
+    size_t pixelCount = 0;
     DevBuf<float4> acc;
     DevBuf<uint32_t> counts;
     DevBuf<float> lumMean, m2;
@@ -101,6 +128,7 @@ struct pt_renderer {
     DevBuf<uint2> pRngB;
     DevBuf<float4> pOrig, pDir, pThr, pRad, pHit, pNeeEnv, pNeeEmis;
     DevBuf<uint8_t> pVisEnv, pVisEmis;
+    DevBuf<uint16_t> pScene;
     DevBuf<uint32_t> qExt0, qExt1, qFinish, qShadowPath, qMiss, qHit;
     DevBuf<float4> qShadowO, qShadowD;
     DevBuf<unsigned int> qCounts;
@@ -112,6 +140,9 @@ struct pt_renderer {
     int blocksPerSmOverride = 0;
 
     DevBuf<LaunchCtx> dctx;               // device copy of the launch context
+    LaunchCtx hostCtx{};                  // its host staging (lives until the copy has run)
+    std::vector<DevScene> hostScenes;     // host staging of dScenes / dViews
+    std::vector<SceneView> hostViews;
     DevBuf<BatchInfo> dbatch;             // current batch of jobs
     BatchInfo hbatch{};                   // host staging of dbatch
     double lastStopRate = 1.0;            // fraction of active pixels that stopped per 4 waves
@@ -122,7 +153,6 @@ struct pt_renderer {
     std::vector<cudaEvent_t> eventPool;
     std::vector<std::pair<int, int>> eventMarks; // (stage, first event index)
 
-    pt_camera camera{};
     pt_render_params params{};
 
     pt_stats stats{};
@@ -172,6 +202,17 @@ __global__ void k_build_shade(const float* nrm, const float* uv, const uint32_t*
     }
 }
 
+pt_camera defaultCamera()
+{
+    pt_camera c{};
+    c.orientation[0] = 1.0f;
+    c.fov_y = 0.7f;
+    c.aspect = 1.0f;
+    c.near_plane = 0.1f;
+    c.far_plane = 1000.0f;
+    return c;
+}
+
 pt_material defaultMaterial()
 {
     // MeshAccelScene.cpp:27-46 / MaterialGpu{} defaults.
@@ -184,7 +225,7 @@ pt_material defaultMaterial()
     return m;
 }
 
-DevScene deviceScene(const pt_renderer* r)
+DevScene deviceScene(const SceneSlot* r)
 {
     DevScene s;
     s.nodes = r->bvh.nodes;
@@ -211,7 +252,7 @@ int ensurePaths(pt_renderer* r, int capacity)
     const size_t Q = static_cast<size_t>(capacity);
     bool ok = r->pPixel.ensure(Q) && r->pOut.ensure(Q) && r->pRngA.ensure(Q) && r->pRngB.ensure(Q) &&
         r->pOrig.ensure(Q) && r->pDir.ensure(Q) && r->pThr.ensure(Q) && r->pRad.ensure(Q) && r->pHit.ensure(Q) &&
-        r->pNeeEnv.ensure(Q) && r->pNeeEmis.ensure(Q) && r->pVisEnv.ensure(Q) && r->pVisEmis.ensure(Q) &&
+        r->pNeeEnv.ensure(Q) && r->pNeeEmis.ensure(Q) && r->pVisEnv.ensure(Q) && r->pVisEmis.ensure(Q) && r->pScene.ensure(Q) &&
         r->qExt0.ensure(Q) && r->qExt1.ensure(Q) && r->qFinish.ensure(Q) && r->qShadowPath.ensure(2 * Q) &&
         r->qMiss.ensure(Q) && r->qHit.ensure(Q) &&
         r->qShadowO.ensure(2 * Q) && r->qShadowD.ensure(2 * Q) && r->qCounts.ensure(16) && r->qRays.ensure(2) &&
@@ -226,17 +267,20 @@ int ensurePaths(pt_renderer* r, int capacity)
 LaunchCtx makeCtx(pt_renderer* r)
 {
     LaunchCtx c{};
-    c.scene = deviceScene(r);
+    c.scene = deviceScene(&r->scenes[0]);
     c.env.pixels = r->envPixels.p;
     c.env.marginal = r->envMarginal.p;
     c.env.row = r->envRow.p;
     c.env.width = r->envW;
     c.env.height = r->envH;
     c.env.valid = r->envValid ? 1 : 0;
-    c.cam = r->camera;
+    c.cam = r->scenes[0].camera;
     c.params = r->params;
     c.width = r->width;
     c.height = r->height;
+    c.sceneCount = static_cast<int>(r->scenes.size());
+    c.scenes = r->dScenes.p;
+    c.views = r->dViews.p;
     c.maxDepth = r->params.max_path_depth > 0 ? r->params.max_path_depth : (r->params.max_path_depth == 0 ? 256 : 32);
     c.rrMinDepth = r->params.russian_roulette_min_depth >= 0 ? r->params.russian_roulette_min_depth : 3;
     c.paths.pixel = r->pPixel.p;
@@ -252,6 +296,7 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.paths.neeEmis = r->pNeeEmis.p;
     c.paths.visEnv = r->pVisEnv.p;
     c.paths.visEmis = r->pVisEmis.p;
+    c.paths.scene = r->pScene.p;
     c.paths.capacity = r->capacity;
     c.q.extend[0] = r->qExt0.p;
     c.q.extend[1] = r->qExt1.p;
@@ -286,8 +331,32 @@ const LaunchCtx* uploadCtx(pt_renderer* r)
     if (!r->dctx.ensure(1)) {
         return nullptr;
     }
-    const LaunchCtx c = makeCtx(r);
-    if (cudaMemcpyAsync(r->dctx.p, &c, sizeof(LaunchCtx), cudaMemcpyHostToDevice, r->stream) != cudaSuccess) {
+    if (r->scenes.size() > 1) {
+        const size_t n = r->scenes.size();
+        if (!r->dScenes.ensure(n) || !r->dViews.ensure(n)) {
+            return nullptr;
+        }
+        r->hostScenes.resize(n);
+        r->hostViews.resize(n);
+        for (size_t k = 0; k < n; ++k) {
+            const SceneSlot& sl = r->scenes[k];
+            r->hostScenes[k] = deviceScene(&sl);
+            SceneView v{};
+            v.cam = sl.camera;
+            v.width = sl.width;
+            v.height = sl.height;
+            v.pixelBase = sl.pixelBase;
+            r->hostViews[k] = v;
+        }
+        if (cudaMemcpyAsync(r->dScenes.p, r->hostScenes.data(), n * sizeof(DevScene), cudaMemcpyHostToDevice,
+                r->stream) != cudaSuccess ||
+            cudaMemcpyAsync(r->dViews.p, r->hostViews.data(), n * sizeof(SceneView), cudaMemcpyHostToDevice,
+                r->stream) != cudaSuccess) {
+            return nullptr;
+        }
+    }
+    r->hostCtx = makeCtx(r);
+    if (cudaMemcpyAsync(r->dctx.p, &r->hostCtx, sizeof(LaunchCtx), cudaMemcpyHostToDevice, r->stream) != cudaSuccess) {
         return nullptr;
     }
     return r->dctx.p;
@@ -303,9 +372,9 @@ int resetAccum(pt_renderer* r)
     if (dc == nullptr) {
         return fail(r, PT_ERR_CUDA, "launch context upload failed");
     }
-    launchResetAccum(dc, r->width * r->height, r->stream);
+    launchResetAccum(dc, static_cast<int>(r->pixelCount), r->stream);
     PT_CHECK(r, cudaGetLastError());
-    r->hostActive = r->width * r->height;
+    r->hostActive = static_cast<int>(r->pixelCount);
     r->lastStopRate = 1.0;
     r->wavesDone = 0;
     r->samplesDone = 0;
@@ -387,6 +456,157 @@ int chooseBatch(const pt_renderer* r, int remaining)
 
 } // namespace
 
+namespace {
+
+// Image sizes of scenes 0..n-1 (n = scenes.size()): pixel ranges laid out
+// scene after scene, accumulators sized for all of them, accumulation reset.
+int configureLayout(pt_renderer* r, const int* widths, const int* heights)
+{
+    const size_t n = r->scenes.size();
+    size_t total = 0;
+    for (size_t k = 0; k < n; ++k) {
+        if (widths[k] <= 0 || heights[k] <= 0) {
+            return fail(r, PT_ERR_INVALID_ARGUMENT, "bad image size %dx%d for scene %zu", widths[k], heights[k], k);
+        }
+        total += static_cast<size_t>(widths[k]) * heights[k];
+    }
+    if (total > (size_t(1) << 30)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "%zu pixels in total exceed 2^30", total);
+    }
+    if (!(r->acc.ensure(total) && r->counts.ensure(total) && r->lumMean.ensure(total) && r->m2.ensure(total) &&
+            r->converged.ensure(total) && r->active0.ensure(total) && r->active1.ensure(total) &&
+            r->activeCount.ensure(4))) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "accumulator allocation failed for %zu pixels", total);
+    }
+    size_t base = 0;
+    for (size_t k = 0; k < n; ++k) {
+        SceneSlot& sl = r->scenes[k];
+        sl.width = widths[k];
+        sl.height = heights[k];
+        sl.pixelBase = static_cast<uint32_t>(base);
+        base += static_cast<size_t>(widths[k]) * heights[k];
+    }
+    r->pixelCount = total;
+    r->width = r->scenes[0].width;
+    r->height = r->scenes[0].height;
+    int st = resetAccum(r);
+    if (st != PT_OK) {
+        return st;
+    }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    return PT_OK;
+}
+
+// Uploads a mesh into a scene slot and builds its BVH (MeshAccelScene::build +
+// upload, MeshAccelScene.cpp:141-341).
+int setSceneMesh(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
+{
+    const uint32_t n = mesh->triangle_count;
+    if (n > 0 && (mesh->positions == nullptr || mesh->normals == nullptr || mesh->uvs == nullptr ||
+                     mesh->material_ids == nullptr)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: missing per-triangle arrays");
+    }
+    if ((mesh->material_count > 0 && mesh->materials == nullptr) || (mesh->texture_count > 0 && mesh->textures == nullptr)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: missing material or texture bank");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = r->stream;
+    PT_CHECK(r, cudaEventRecord(r->ev0, s));
+    sl.hasScene = false;
+    sl.triCount = n;
+    // materials: MeshAccelScene::build adds one default material when none is given
+    std::vector<pt_material> mats(mesh->materials, mesh->materials + mesh->material_count);
+    if (mats.empty()) {
+        mats.push_back(defaultMaterial());
+    }
+    sl.materialCount = static_cast<uint32_t>(mats.size());
+    if (!sl.materials.ensure(mats.size())) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "material upload failed");
+    }
+    PT_CHECK(r, cudaMemcpyAsync(sl.materials.p, mats.data(), mats.size() * sizeof(pt_material), cudaMemcpyHostToDevice, s));
+    sl.textureCount = mesh->texture_count;
+    if (mesh->texture_count > 0) {
+        if (!sl.textures.ensure(mesh->texture_count)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "texture upload failed");
+        }
+        PT_CHECK(r, cudaMemcpyAsync(sl.textures.p, mesh->textures, mesh->texture_count * sizeof(pt_texture),
+            cudaMemcpyHostToDevice, s));
+    }
+    // emissive list + CDF: sequential float prefix sum exactly as MeshAccelScene.cpp:62-95
+    std::vector<uint32_t> eIdx;
+    std::vector<float> eCdf(1, 0.0f);
+    float total = 0.0f;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t mi = mesh->material_ids[i];
+        if (mi >= mats.size()) {
+            continue;
+        }
+        const pt_material& m = mats[mi];
+        const float lum = m.emission * (0.2126f * m.r + 0.7152f * m.g + 0.0722f * m.b);
+        if (lum <= 0.0f) {
+            continue;
+        }
+        const float* p = mesh->positions + 9ull * i;
+        const float e1x = p[3] - p[0], e1y = p[4] - p[1], e1z = p[5] - p[2];
+        const float e2x = p[6] - p[0], e2y = p[7] - p[1], e2z = p[8] - p[2];
+        const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+        const float area = 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
+        const float w = area * lum;
+        if (w <= 0.0f) {
+            continue;
+        }
+        eIdx.push_back(i);
+        total += w;
+        eCdf.push_back(total);
+    }
+    if (total <= 0.0f) {
+        eIdx.clear();
+        eCdf.assign(1, 0.0f);
+    }
+    sl.emissiveCount = static_cast<uint32_t>(eIdx.size());
+    if (!sl.emissiveIdx.ensure(std::max<size_t>(1, eIdx.size())) || !sl.emissiveCdf.ensure(eCdf.size())) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list upload failed");
+    }
+    if (!eIdx.empty()) {
+        PT_CHECK(r, cudaMemcpyAsync(sl.emissiveIdx.p, eIdx.data(), eIdx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    }
+    PT_CHECK(r, cudaMemcpyAsync(sl.emissiveCdf.p, eCdf.data(), eCdf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    if (n > 0) {
+        if (!sl.positions.ensure(9ull * n) || !sl.shade.ensure(n) || !r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "mesh upload failed for %u triangles", n);
+        }
+        PT_CHECK(r, cudaMemcpyAsync(sl.positions.p, mesh->positions, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p, mesh->normals, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9ull * n, mesh->uvs, 6ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stageIds.p, mesh->material_ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        const int grid = static_cast<int>(std::min<uint32_t>((n + 255) / 256, 148u * 16u));
+        k_build_shade<<<grid, 256, 0, s>>>(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, sl.shade.p);
+        PT_CHECK(r, cudaGetLastError());
+        char err[256] = {0};
+        const int st = buildBvh(sl.positions.p, n, sl.bvh, s, r->bvhOptions, err, sizeof(err));
+        if (st != PT_OK) {
+            return fail(r, st, "BVH build: %s", err);
+        }
+    } else {
+        sl.bvh.release();
+    }
+    PT_CHECK(r, cudaEventRecord(r->ev1, s));
+    PT_CHECK(r, cudaEventSynchronize(r->ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+    r->stats.build_ms = ms;
+    sl.hasScene = true;
+    uint32_t nodes = 0;
+    for (const SceneSlot& x : r->scenes) {
+        nodes += x.hasScene ? x.bvh.nodeCount : 0u;
+    }
+    r->stats.bvh_nodes = static_cast<int32_t>(nodes);
+    return resetAccum(r);
+}
+
+} // namespace
+
+
 extern "C" {
 
 int pt_create(pt_renderer** out, int device)
@@ -413,11 +633,7 @@ int pt_create(pt_renderer** out, int device)
     r->stream = r->ownStream;
     cudaDeviceGetAttribute(&r->smCount, cudaDevAttrMultiProcessorCount, r->device);
     pt_default_params(&r->params);
-    r->camera.orientation[0] = 1.0f;
-    r->camera.fov_y = 0.7f;
-    r->camera.aspect = 1.0f;
-    r->camera.near_plane = 0.1f;
-    r->camera.far_plane = 1000.0f;
+    r->scenes[0].camera = defaultCamera();
     int be = 1, bs = 1, bsh = 1;
     stageOccupancy(be, bs, bsh);
     r->gridExtend = r->smCount * std::max(be, 1);
@@ -436,16 +652,13 @@ int pt_destroy(pt_renderer* r)
     if (r->stream) {
         cudaStreamSynchronize(r->stream);
     }
-    r->positions.release();
-    r->shade.release();
-    r->materials.release();
-    r->textures.release();
-    r->emissiveIdx.release();
-    r->emissiveCdf.release();
+    for (SceneSlot& sl : r->scenes) {
+        sl.release();
+    }
+    r->dScenes.release();
+    r->dViews.release();
     r->stage.release();
     r->stageIds.release();
-    r->bvh.release();
-    r->bvh.scratch.release();
     r->envPixels.release();
     r->envMarginal.release();
     r->envRow.release();
@@ -471,6 +684,7 @@ int pt_destroy(pt_renderer* r)
     r->pNeeEmis.release();
     r->pVisEnv.release();
     r->pVisEmis.release();
+    r->pScene.release();
     r->qExt0.release();
     r->qExt1.release();
     r->qFinish.release();
@@ -527,19 +741,12 @@ int pt_configure(pt_renderer* r, int width, int height)
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_configure: bad size %dx%d", width, height);
     }
     PT_CHECK(r, cudaSetDevice(r->device));
-    const size_t P = static_cast<size_t>(width) * height;
-    if (!(r->acc.ensure(P) && r->counts.ensure(P) && r->lumMean.ensure(P) && r->m2.ensure(P) && r->converged.ensure(P) &&
-            r->active0.ensure(P) && r->active1.ensure(P) && r->activeCount.ensure(4))) {
-        return fail(r, PT_ERR_OUT_OF_MEMORY, "accumulator allocation failed for %dx%d", width, height);
+    // back to a single scene: drop the geometry of any further batch scenes
+    for (size_t k = 1; k < r->scenes.size(); ++k) {
+        r->scenes[k].release();
     }
-    r->width = width;
-    r->height = height;
-    int st = resetAccum(r);
-    if (st != PT_OK) {
-        return st;
-    }
-    PT_CHECK(r, cudaStreamSynchronize(r->stream));
-    return PT_OK;
+    r->scenes.resize(1);
+    return configureLayout(r, &width, &height);
 }
 
 int pt_set_mesh(pt_renderer* r, const pt_mesh* mesh)
@@ -547,103 +754,7 @@ int pt_set_mesh(pt_renderer* r, const pt_mesh* mesh)
     if (r == nullptr || mesh == nullptr) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: null argument");
     }
-    const uint32_t n = mesh->triangle_count;
-    if (n > 0 && (mesh->positions == nullptr || mesh->normals == nullptr || mesh->uvs == nullptr ||
-                     mesh->material_ids == nullptr)) {
-        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: missing per-triangle arrays");
-    }
-    if ((mesh->material_count > 0 && mesh->materials == nullptr) || (mesh->texture_count > 0 && mesh->textures == nullptr)) {
-        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_mesh: missing material or texture bank");
-    }
-    PT_CHECK(r, cudaSetDevice(r->device));
-    cudaStream_t s = r->stream;
-    PT_CHECK(r, cudaEventRecord(r->ev0, s));
-    r->hasScene = false;
-    r->triCount = n;
-    // materials: MeshAccelScene::build adds one default material when none is given
-    std::vector<pt_material> mats(mesh->materials, mesh->materials + mesh->material_count);
-    if (mats.empty()) {
-        mats.push_back(defaultMaterial());
-    }
-    r->materialCount = static_cast<uint32_t>(mats.size());
-    if (!r->materials.ensure(mats.size())) {
-        return fail(r, PT_ERR_OUT_OF_MEMORY, "material upload failed");
-    }
-    PT_CHECK(r, cudaMemcpyAsync(r->materials.p, mats.data(), mats.size() * sizeof(pt_material), cudaMemcpyHostToDevice, s));
-    r->textureCount = mesh->texture_count;
-    if (mesh->texture_count > 0) {
-        if (!r->textures.ensure(mesh->texture_count)) {
-            return fail(r, PT_ERR_OUT_OF_MEMORY, "texture upload failed");
-        }
-        PT_CHECK(r, cudaMemcpyAsync(r->textures.p, mesh->textures, mesh->texture_count * sizeof(pt_texture),
-            cudaMemcpyHostToDevice, s));
-    }
-    // emissive list + CDF: sequential float prefix sum exactly as MeshAccelScene.cpp:62-95
-    std::vector<uint32_t> eIdx;
-    std::vector<float> eCdf(1, 0.0f);
-    float total = 0.0f;
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t mi = mesh->material_ids[i];
-        if (mi >= mats.size()) {
-            continue;
-        }
-        const pt_material& m = mats[mi];
-        const float lum = m.emission * (0.2126f * m.r + 0.7152f * m.g + 0.0722f * m.b);
-        if (lum <= 0.0f) {
-            continue;
-        }
-        const float* p = mesh->positions + 9ull * i;
-        const float e1x = p[3] - p[0], e1y = p[4] - p[1], e1z = p[5] - p[2];
-        const float e2x = p[6] - p[0], e2y = p[7] - p[1], e2z = p[8] - p[2];
-        const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
-        const float area = 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
-        const float w = area * lum;
-        if (w <= 0.0f) {
-            continue;
-        }
-        eIdx.push_back(i);
-        total += w;
-        eCdf.push_back(total);
-    }
-    if (total <= 0.0f) {
-        eIdx.clear();
-        eCdf.assign(1, 0.0f);
-    }
-    r->emissiveCount = static_cast<uint32_t>(eIdx.size());
-    if (!r->emissiveIdx.ensure(std::max<size_t>(1, eIdx.size())) || !r->emissiveCdf.ensure(eCdf.size())) {
-        return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list upload failed");
-    }
-    if (!eIdx.empty()) {
-        PT_CHECK(r, cudaMemcpyAsync(r->emissiveIdx.p, eIdx.data(), eIdx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-    }
-    PT_CHECK(r, cudaMemcpyAsync(r->emissiveCdf.p, eCdf.data(), eCdf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
-    if (n > 0) {
-        if (!r->positions.ensure(9ull * n) || !r->shade.ensure(n) || !r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
-            return fail(r, PT_ERR_OUT_OF_MEMORY, "mesh upload failed for %u triangles", n);
-        }
-        PT_CHECK(r, cudaMemcpyAsync(r->positions.p, mesh->positions, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
-        PT_CHECK(r, cudaMemcpyAsync(r->stage.p, mesh->normals, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
-        PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9ull * n, mesh->uvs, 6ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
-        PT_CHECK(r, cudaMemcpyAsync(r->stageIds.p, mesh->material_ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-        const int grid = static_cast<int>(std::min<uint32_t>((n + 255) / 256, 148u * 16u));
-        k_build_shade<<<grid, 256, 0, s>>>(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, r->shade.p);
-        PT_CHECK(r, cudaGetLastError());
-        char err[256] = {0};
-        const int st = buildBvh(r->positions.p, n, r->bvh, s, r->bvhOptions, err, sizeof(err));
-        if (st != PT_OK) {
-            return fail(r, st, "BVH build: %s", err);
-        }
-    } else {
-        r->bvh.release();
-    }
-    PT_CHECK(r, cudaEventRecord(r->ev1, s));
-    PT_CHECK(r, cudaEventSynchronize(r->ev1));
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
-    r->stats.build_ms = ms;
-    r->stats.bvh_nodes = static_cast<int32_t>(r->bvh.nodeCount);
-    r->hasScene = true;
-    return resetAccum(r);
+    return setSceneMesh(r, r->scenes[0], mesh);
 }
 
 int pt_set_camera(pt_renderer* r, const pt_camera* camera)
@@ -651,7 +762,7 @@ int pt_set_camera(pt_renderer* r, const pt_camera* camera)
     if (r == nullptr || camera == nullptr) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_camera: null argument");
     }
-    r->camera = *camera;
+    r->scenes[0].camera = *camera;
     return resetAccum(r);
 }
 
@@ -660,7 +771,7 @@ int pt_get_camera(const pt_renderer* r, pt_camera* out)
     if (r == nullptr || out == nullptr) {
         return PT_ERR_INVALID_ARGUMENT;
     }
-    *out = r->camera;
+    *out = r->scenes[0].camera;
     return PT_OK;
 }
 
@@ -765,8 +876,10 @@ int pt_render(pt_renderer* r, int waves)
     if (r->width <= 0) {
         return fail(r, PT_ERR_NOT_CONFIGURED, "pt_render before pt_configure");
     }
-    if (!r->hasScene) {
-        return fail(r, PT_ERR_NO_SCENE, "pt_render before pt_set_mesh");
+    for (size_t k = 0; k < r->scenes.size(); ++k) {
+        if (!r->scenes[k].hasScene) {
+            return fail(r, PT_ERR_NO_SCENE, "pt_render before the mesh of scene %zu was set", k);
+        }
     }
     PT_CHECK(r, cudaSetDevice(r->device));
     cudaStream_t s = r->stream;
@@ -962,7 +1075,7 @@ int pt_trace_rays_device(pt_renderer* r, int n, const float* origins, const floa
                                               hit == nullptr))) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_trace_rays: bad arguments");
     }
-    if (!r->hasScene) {
+    if (!r->scenes[0].hasScene) {
         return fail(r, PT_ERR_NO_SCENE, "pt_trace_rays before pt_set_mesh");
     }
     if (n == 0) {
@@ -970,7 +1083,7 @@ int pt_trace_rays_device(pt_renderer* r, int n, const float* origins, const floa
     }
     PT_CHECK(r, cudaSetDevice(r->device));
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : r->stream;
-    launchTraceRays(deviceScene(r), n, origins, dirs, tmin, tmax, hit, t, tri, normal, uv, s);
+    launchTraceRays(deviceScene(&r->scenes[0]), n, origins, dirs, tmin, tmax, hit, t, tri, normal, uv, s);
     PT_CHECK(r, cudaGetLastError());
     return PT_OK;
 }
@@ -982,7 +1095,7 @@ int pt_trace_rays(pt_renderer* r, int n, const float* origins, const float* dirs
                                               hit == nullptr))) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_trace_rays: bad arguments");
     }
-    if (!r->hasScene) {
+    if (!r->scenes[0].hasScene) {
         return fail(r, PT_ERR_NO_SCENE, "pt_trace_rays before pt_set_mesh");
     }
     if (n == 0) {
@@ -1010,7 +1123,7 @@ int pt_trace_rays(pt_renderer* r, int n, const float* origins, const float* dirs
     if (e == cudaSuccess) e = cudaMemcpyAsync(dTmin, tmin, N * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dTmax, tmax, N * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-        launchTraceRays(deviceScene(r), n, dO, dD, dTmin, dTmax, dHit, dT, dTri, dN, dUv, s);
+        launchTraceRays(deviceScene(&r->scenes[0]), n, dO, dD, dTmin, dTmax, dHit, dT, dTri, dN, dUv, s);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(hit, dHit, N, cudaMemcpyDeviceToHost, s);
@@ -1100,6 +1213,68 @@ int pt_rng_tape(pt_renderer* r, int first_wave, int waves, int stride, float* ou
     if (e != cudaSuccess) {
         return cudaFail(r, e, "pt_rng_tape");
     }
+    return PT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: several scenes in one render (no reference counterpart)
+// ---------------------------------------------------------------------------
+int pt_batch_configure(pt_renderer* r, int scene_count, const int* widths, const int* heights)
+{
+    if (r == nullptr || scene_count < 1 || scene_count > 65535 || widths == nullptr || heights == nullptr) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_configure: bad arguments");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    for (SceneSlot& sl : r->scenes) {
+        sl.release();
+    }
+    r->scenes.assign(static_cast<size_t>(scene_count), SceneSlot{});
+    for (SceneSlot& sl : r->scenes) {
+        sl.camera = defaultCamera();
+    }
+    return configureLayout(r, widths, heights);
+}
+
+int pt_batch_set_mesh(pt_renderer* r, int scene, const pt_mesh* mesh)
+{
+    if (r == nullptr || mesh == nullptr || scene < 0 || static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_mesh: bad scene %d or null mesh", scene);
+    }
+    return setSceneMesh(r, r->scenes[static_cast<size_t>(scene)], mesh);
+}
+
+int pt_batch_set_camera(pt_renderer* r, int scene, const pt_camera* camera)
+{
+    if (r == nullptr || camera == nullptr || scene < 0 || static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_camera: bad scene %d or null camera", scene);
+    }
+    r->scenes[static_cast<size_t>(scene)].camera = *camera;
+    return resetAccum(r);
+}
+
+int pt_batch_readback(pt_renderer* r, int scene, float* rgba, uint32_t* counts, uint8_t* converged)
+{
+    if (r == nullptr || scene < 0 || static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_readback: bad scene %d", scene);
+    }
+    if (r->pixelCount == 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_batch_readback before pt_batch_configure");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
+    const size_t P = static_cast<size_t>(sl.width) * sl.height;
+    const size_t o = sl.pixelBase;
+    if (rgba) {
+        PT_CHECK(r, cudaMemcpyAsync(rgba, r->acc.p + o, P * sizeof(float4), cudaMemcpyDeviceToHost, r->stream));
+    }
+    if (counts) {
+        PT_CHECK(r, cudaMemcpyAsync(counts, r->counts.p + o, P * sizeof(uint32_t), cudaMemcpyDeviceToHost, r->stream));
+    }
+    if (converged) {
+        PT_CHECK(r, cudaMemcpyAsync(converged, r->converged.p + o, P, cudaMemcpyDeviceToHost, r->stream));
+    }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
     return PT_OK;
 }
 

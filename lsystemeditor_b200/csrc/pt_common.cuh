@@ -119,7 +119,7 @@ struct DevScene {
     const CwNode* nodes = nullptr;
     const TriVerts* tris = nullptr;      // leaf order
     const TriShade* shade = nullptr;     // original order
-    const float4* origVerts = nullptr;   // original order, 3 float4 per triangle (emissive sampling, Q1 path)
+    const float4* origVerts = nullptr;   // original order, 9 floats per triangle (emissive sampling)
     const pt_material* materials = nullptr;
     const pt_texture* textures = nullptr;
     const uint32_t* emissiveIdx = nullptr;

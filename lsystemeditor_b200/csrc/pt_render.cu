@@ -86,6 +86,12 @@ __device__ __forceinline__ void rngStore(const PathSoA& P, uint32_t i, const cur
     P.rngB[i] = make_uint2(s.v[3], s.v[4]);
 }
 
+// Geometry of path i's scene.
+__device__ __forceinline__ const DevScene& sceneOf(const LaunchCtx& c, uint32_t i)
+{
+    return c.sceneCount > 1 ? c.scenes[c.paths.scene[i]] : c.scene;
+}
+
 // Sampling/RandCore.h:7-12 (reference) or a hash of (x, y, seed value) (extension).
 __device__ __forceinline__ uint32_t pathSeed(const pt_render_params& p, uint32_t pixel, uint32_t width,
     uint32_t sampleIndex, uint32_t globalSeed)
@@ -137,17 +143,39 @@ __device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigne
     const uint32_t pixel = static_cast<uint32_t>(active[li]);
     const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
     const uint32_t globalSeed = bt.waveBase + slot + 1u;
+    // scene of the pixel; seeds and film coordinates use the pixel's index
+    // within its own image, so a scene renders the same in a batch as alone
+    uint32_t local = pixel;
+    const pt_camera* cam = &c.cam;
+    uint32_t width = static_cast<uint32_t>(c.width), height = static_cast<uint32_t>(c.height);
+    if (c.sceneCount > 1) {
+        int lo = 0, hi = c.sceneCount - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (c.views[mid].pixelBase <= pixel) {
+                lo = mid;
+            } else {
+                hi = mid - 1;
+            }
+        }
+        const SceneView& sv = c.views[lo];
+        local = pixel - sv.pixelBase;
+        cam = &sv.cam;
+        width = static_cast<uint32_t>(sv.width);
+        height = static_cast<uint32_t>(sv.height);
+        c.paths.scene[i] = static_cast<uint16_t>(lo);
+    }
     curandStateXORWOW st;
-    curand_init(pathSeed(c.params, pixel, c.width, sampleIndex, globalSeed), 0ull, 0ull, &st);
-    const uint32_t x = pixel % c.width, y = pixel / c.width;
+    curand_init(pathSeed(c.params, local, width, sampleIndex, globalSeed), 0ull, 0ull, &st);
+    const uint32_t x = local % width, y = local / width;
     const float ju = curand_uniform(&st);
     const float jv = curand_uniform(&st);
-    const float u = (static_cast<float>(x) + ju) / static_cast<float>(c.width);
-    const float v = (static_cast<float>(y) + jv) / static_cast<float>(c.height);
+    const float u = (static_cast<float>(x) + ju) / static_cast<float>(width);
+    const float v = (static_cast<float>(y) + jv) / static_cast<float>(height);
     const float l1 = curand_uniform(&st);
     const float l2 = curand_uniform(&st);
     float3 ro, rd;
-    cameraRay(c.cam, u, v, l1, l2, ro, rd);
+    cameraRay(*cam, u, v, l1, l2, ro, rd);
     c.paths.pixel[i] = pixel;
     c.paths.outIdx[i] = static_cast<uint32_t>(j); // == slot * activeCount + listIndex
     rngStore(c.paths, i, st);
@@ -232,7 +260,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(const LaunchCtx* __restrict__
         const float4 d4 = c.paths.dir[i];
         const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
         HitRec h;
-        const bool hit = traceRay<false, Count>(c.scene, f3(o4.x, o4.y, o4.z), dn, o4.w, kRayTMax, h, c.q.overflow,
+        const bool hit = traceRay<false, Count>(sceneOf(c, i), f3(o4.x, o4.y, o4.z), dn, o4.w, kRayTMax, h, c.q.overflow,
             c.q.visits, smemStack + threadIdx.x, blockDim.x);
         if (hit) {
             c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
@@ -294,6 +322,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(const LaunchCtx* __restrict__ 
     const int debugFlags = c.params.brdf_debug_flags;
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = queue[k];
+        const DevScene& S = sceneOf(c, i);
         const float4 r4 = c.paths.rad[i];
         float3 L = f3(r4.x, r4.y, r4.z);
         const int depth = __float_as_int(r4.w);
@@ -324,15 +353,15 @@ __global__ void __launch_bounds__(256, 3) k_shade(const LaunchCtx* __restrict__ 
             const float t = h4.x;
             const float3 pos = xadd(f3(o4.x, o4.y, o4.z), xscl(d, t));
             const float3 dn = xnormalize(d);
-            const TriShade sh = c.scene.shade[tri];
+            const TriShade sh = S.shade[tri];
             float3 n;
             float tu, tv;
             hitShading(sh, dn, h4.y, h4.z, n, tu, tv);
             const uint32_t mi = __float_as_uint(sh.d.w);
             const pt_material& srcMat =
-                (c.scene.materials != nullptr && mi < c.scene.materialCount) ? c.scene.materials[mi] : kFallbackMaterial;
+                (S.materials != nullptr && mi < S.materialCount) ? S.materials[mi] : kFallbackMaterial;
             Ctx cx;
-            cx.m = resolveMaterial(srcMat, tu, tv, c.scene.textures, c.scene.textureCount);
+            cx.m = resolveMaterial(srcMat, tu, tv, S.textures, S.textureCount);
             cx.w = computeLobes(cx.m);
             cx.n = n;
             cx.wo = scl3(d, -1.0f);
@@ -371,13 +400,13 @@ __global__ void __launch_bounds__(256, 3) k_shade(const LaunchCtx* __restrict__ 
                 }
             }
             // emissive NEE (PathIntegratorRandCore.h:110-167)
-            if (c.scene.emissiveCount > 0) {
+            if (S.emissiveCount > 0) {
                 const float uTri = curand_uniform(&st);
                 const float u1 = curand_uniform(&st);
                 const float u2 = curand_uniform(&st);
                 float3 lpos, ln, Le, ev0, ev1, ev2;
                 float ap;
-                if (sampleEmissive(c.scene, &kFallbackMaterial, uTri, u1, u2, lpos, ln, Le, ap, ev0, ev1, ev2)) {
+                if (sampleEmissive(S, &kFallbackMaterial, uTri, u1, u2, lpos, ln, Le, ap, ev0, ev1, ev2)) {
                     const float3 tl = sub3(lpos, pos);
                     const float d2 = dot3(tl, tl);
                     if (d2 > kMinPdf) {
@@ -521,7 +550,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__
         const float4 d4 = c.q.shadowDir[k];
         const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
         HitRec h;
-        const bool occluded = traceRay<true, Count>(c.scene, f3(o4.x, o4.y, o4.z), dn, kShadowBias, kRayTMax, h,
+        const bool occluded = traceRay<true, Count>(sceneOf(c, e & 0x7FFFFFFFu), f3(o4.x, o4.y, o4.z), dn, kShadowBias, kRayTMax, h,
             c.q.overflow, c.q.visits + 2, smemStack + threadIdx.x, blockDim.x);
         if (!occluded) {
             const uint32_t i = e & 0x7FFFFFFFu;

@@ -20,6 +20,7 @@ struct PathSoA {
     float4* neeEmis = nullptr;   // pending emissive-NEE contribution
     uint8_t* visEnv = nullptr;   // 1 = that contribution is unoccluded
     uint8_t* visEmis = nullptr;
+    uint16_t* scene = nullptr;   // scene of the path (written only when more than one scene is rendered)
     int capacity = 0;
 };
 
@@ -62,13 +63,28 @@ struct AccumState {
     size_t sampleCapacity = 0;
 };
 
-struct LaunchCtx {
-    DevScene scene;
-    DevEnv env;
+// One scene of a batch: its camera, image size and first pixel in the batch's
+// concatenated pixel range.
+struct SceneView {
     pt_camera cam;
-    pt_render_params params;
     int width;
     int height;
+    uint32_t pixelBase;
+    uint32_t pad;
+};
+
+struct LaunchCtx {
+    DevScene scene;           // scene 0
+    DevEnv env;
+    pt_camera cam;            // scene 0
+    pt_render_params params;
+    int width;                // scene 0
+    int height;
+    // batch of several scenes (sceneCount > 1): per-scene geometry and views;
+    // pixels are numbered scene after scene
+    int sceneCount;
+    const DevScene* scenes;
+    const SceneView* views;
     int maxDepth;     // effective (0 -> 256, <0 -> 32)
     int rrMinDepth;   // effective
     PathSoA paths;

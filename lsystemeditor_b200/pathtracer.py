@@ -57,7 +57,8 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_get_camera", "pt_set_params", "pt_get_params", "pt_default_params", "pt_set_environment",
                     "pt_reset", "pt_render", "pt_readback", "pt_device_buffers", "pt_get_stats", "pt_trace_rays",
                     "pt_trace_rays_device", "pt_rng_tape", "pt_set_stream", "pt_set_profiling", "pt_get_profile",
-                    "pt_set_tuning", "pt_trace_soup_noalloc"]
+                    "pt_set_tuning", "pt_trace_soup_noalloc", "pt_batch_configure", "pt_batch_set_mesh",
+                    "pt_batch_set_camera", "pt_batch_readback"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -99,6 +100,10 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_set_profiling.argtypes = [vp, C.c_int]
     L.pt_get_profile.argtypes = [vp, C.POINTER(PtProfile)]
     L.pt_set_tuning.argtypes = [vp, C.c_int, C.c_int]
+    L.pt_batch_configure.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.pt_batch_set_mesh.argtypes = [vp, C.c_int, C.POINTER(PtMesh)]
+    L.pt_batch_set_camera.argtypes = [vp, C.c_int, vp]
+    L.pt_batch_readback.argtypes = [vp, C.c_int, _fp, _u32p, _u8p]
     _LIB = L
     return L
 
@@ -160,13 +165,18 @@ class PathTracer:
         if mesh is not None:
             self.set_mesh(mesh)
 
-    def set_mesh(self, mesh: HostMesh):
-        """MeshAccelScene::build + upload / PathTracer::rebuildMeshScene: GPU BVH build."""
+    @staticmethod
+    def _pt_mesh(mesh: HostMesh):
         m = mesh.contiguous()
         s = PtMesh(m.triangle_count, _ptr(m.positions, _fp), _ptr(m.normals, _fp), _ptr(m.uvs, _fp),
                    _ptr(m.material_ids, _u32p), len(m.materials),
                    C.c_void_p(m.materials.ctypes.data) if len(m.materials) else None, len(m.textures),
                    C.c_void_p(m.textures.ctypes.data) if len(m.textures) else None)
+        return m, s
+
+    def set_mesh(self, mesh: HostMesh):
+        """MeshAccelScene::build + upload / PathTracer::rebuildMeshScene: GPU BVH build."""
+        m, s = self._pt_mesh(mesh)
         self._check(self._lib.pt_set_mesh(self._h, C.byref(s)))
         self._mesh_keepalive = m
 
@@ -274,6 +284,33 @@ class PathTracer:
         """PathTracerSampleBudget.h:8-14 with no preview levels."""
         m = int(self.params()["max_samples_per_pixel"])
         return -1 if m <= 0 else m
+
+    # -- batched form (no reference counterpart) -------------------------------
+    def batch_configure(self, sizes):
+        """Several independent scenes rendered together; sizes = [(width, height), ...].
+        The single-scene calls then address scene 0."""
+        w = (C.c_int * len(sizes))(*[int(a) for a, _ in sizes])
+        h = (C.c_int * len(sizes))(*[int(b) for _, b in sizes])
+        self._check(self._lib.pt_batch_configure(self._h, len(sizes), w, h))
+        self.batch_sizes = [(int(a), int(b)) for a, b in sizes]
+        self.width, self.height = self.batch_sizes[0]
+
+    def batch_set_mesh(self, scene: int, mesh: HostMesh):
+        m, s = self._pt_mesh(mesh)
+        self._check(self._lib.pt_batch_set_mesh(self._h, int(scene), C.byref(s)))
+
+    def batch_set_camera(self, scene: int, camera: np.ndarray):
+        cam = np.ascontiguousarray(camera, CAMERA_DTYPE)
+        self._check(self._lib.pt_batch_set_camera(self._h, int(scene), C.c_void_p(cam.ctypes.data)))
+
+    def batch_readback(self, scene: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        w, h = self.batch_sizes[scene]
+        rgba = np.empty((h, w, 4), np.float32)
+        counts = np.empty((h, w), np.uint32)
+        conv = np.empty((h, w), np.uint8)
+        self._check(self._lib.pt_batch_readback(self._h, int(scene), _ptr(rgba, _fp), _ptr(counts, _u32p),
+                                                _ptr(conv, _u8p)))
+        return rgba, counts, conv
 
     # -- queries ----------------------------------------------------------
     def trace_rays(self, origins, dirs, tmin=None, tmax=None) -> dict:
