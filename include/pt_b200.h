@@ -270,6 +270,57 @@ int pt_batch_set_mesh(pt_renderer* r, int scene, const pt_mesh* mesh);
 int pt_batch_set_camera(pt_renderer* r, int scene, const pt_camera* camera);
 int pt_batch_readback(pt_renderer* r, int scene, float* rgba, uint32_t* counts, uint8_t* converged);
 
+/* ---- Scene generation on the device (no reference counterpart) ----------
+ * Turtle output as tubes and leaves, lofted into triangles on the GPU and fed
+ * straight to the BVH build (replaces the host loft of
+ * Application/src/Procedural/Loft.cpp:108-155 and the HostMesh upload).  Tube
+ * t spans rings ring_start[t] .. ring_start[t + 1] - 1 (each ring: centre,
+ * tangent, radius, in double); every ring contributes 2 * sides triangles
+ * (side quads to the next ring, a flat cap at each tube end) and every leaf a
+ * two-triangle quad of size leaf_size * leaf[9] spanning (tangent x up) and
+ * the tangent.  The mesh is [tubes in order, leaves in order, extra]; all
+ * material ids index the material bank of `extra`.  cos_sin may be NULL (the
+ * library then tabulates cos / sin of k * 2 pi / sides itself). */
+typedef struct pt_tubes {
+    uint32_t tube_count;
+    uint32_t sides;
+    const uint32_t* ring_start;   /* tube_count + 1 offsets, ring_start[0] = 0 */
+    const double* points;         /* 3 per ring */
+    const double* tangents;       /* 3 per ring */
+    const double* radii;          /* 1 per ring */
+    const uint32_t* materials;    /* 1 per tube */
+    const double* cos_sin;        /* 2 * (sides + 1) or NULL */
+    uint32_t leaf_count;
+    const double* leaves;         /* 10 per leaf: position, tangent, up, size */
+    double leaf_size;
+    uint32_t leaf_material;
+} pt_tubes;
+
+/* Builds scene `scene` (0 for a single-scene renderer) from tubes, leaves and
+ * an extra triangle soup (ground, lights; may have no triangles but carries
+ * the material bank). */
+int pt_batch_set_tubes(pt_renderer* r, int scene, const pt_tubes* tubes, const pt_mesh* extra);
+
+/* Copies scene `scene`'s triangles back to host memory in their original
+ * order (for OBJ export; MeshAccelWavefrontExport.cpp:64-142 exports from the
+ * host mesh instead): 9 + 9 + 6 floats and 1 material id per triangle.  Any
+ * output may be NULL; *triangle_count receives the count. */
+int pt_export_mesh(pt_renderer* r, int scene, uint32_t* triangle_count, float* positions, float* normals,
+    float* uvs, uint32_t* material_ids);
+
+/* Headless display output: replaces the GL publish path
+ * (PathTracer::publishDisplayFrame, PathTracer.cu:421-512 writeDisplayToPboKernel
+ * without downscale).  Writes scene `scene`'s image as 8-bit RGBA to HOST memory
+ * (width x height x 4 bytes): background colour where a pixel has no sample,
+ * rgb x exposure, Reinhard x / (1 + x), clamp to [0, 1], x 255 truncated; with
+ * debug_overlay_mode 2 the adaptive-sampling overlay (green converged, red
+ * active). */
+int pt_tonemap(pt_renderer* r, int scene, float exposure, uint8_t* rgba8);
+
+/* PhysicalCamera::exposureMultiplier (PhysicalCamera.cpp:392-397):
+ * shutter x (max(iso, 1) / 100) / max(f_stop, 0.1)^2. */
+float pt_exposure_multiplier(float f_stop, float shutter_seconds, float iso);
+
 /* Largest triangle count pt_trace_soup_noalloc accepts. */
 #define PT_NOALLOC_MAX_TRIANGLES 16384u
 

@@ -6,6 +6,8 @@
 // (PathTracer.cpp:2220-2543) with a loop over batches of waves.
 #include "pt_bvh.cuh"
 #include "pt_render.cuh"
+#include "pt_output.cuh"
+#include "pt_scene.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -100,6 +102,15 @@ struct pt_renderer {
     DevBuf<SceneView> dViews;
     DevBuf<float> stage;          // upload staging (normals / uvs)
     DevBuf<uint32_t> stageIds;
+    // scene-build scratch: emissive selection, tube loft inputs
+    DevBuf<float> eWeights;
+    DevBuf<uint8_t> eFlags;
+    DevBuf<uint32_t> eIdx;
+    DevBuf<float> eCdf;
+    DevBuf<uint32_t> eOut;
+    DevBuf<unsigned char> eTemp;
+    DevBuf<uint32_t> tRingStart, tMaterials;
+    DevBuf<double> tPoints, tTangents, tRadii, tCosSin, tLeaves, tFrames;
     BvhBuildOptions bvhOptions;
 
     // environment
@@ -116,6 +127,10 @@ struct pt_renderer {
     DevBuf<uint8_t> converged;
     DevBuf<int> active0, active1, activeCount;
     DevBuf<float4> samples;
+    DevBuf<uint8_t> displayBuf;           // RGBA8 output of pt_tonemap
+    DevBuf<unsigned char> compactTemp;    // scratch of the active-list compaction
+    DevBuf<uint32_t> sceneActiveStart;    // batches: per-scene active ranges
+    DevBuf<unsigned long long> sceneJobStart;
     int activeSel = 0;
     int hostActive = 0;
     int64_t wavesDone = 0;
@@ -187,20 +202,6 @@ int cudaFail(pt_renderer* r, cudaError_t e, const char* what)
             return cudaFail((r), e_, #call);                                                                      \
         }                                                                                                         \
     } while (0)
-
-__global__ void k_build_shade(const float* nrm, const float* uv, const uint32_t* mat, uint32_t n, TriShade* out)
-{
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float* a = nrm + 9ull * i;
-        const float* t = uv + 6ull * i;
-        TriShade s;
-        s.a = make_float4(a[0], a[1], a[2], t[0]);
-        s.b = make_float4(a[3], a[4], a[5], t[1]);
-        s.c = make_float4(a[6], a[7], a[8], t[2]);
-        s.d = make_float4(t[3], t[4], t[5], __uint_as_float(mat[i]));
-        out[i] = s;
-    }
-}
 
 pt_camera defaultCamera()
 {
@@ -281,6 +282,8 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.sceneCount = static_cast<int>(r->scenes.size());
     c.scenes = r->dScenes.p;
     c.views = r->dViews.p;
+    c.sceneActiveStart = r->sceneActiveStart.p;
+    c.sceneJobStart = r->sceneJobStart.p;
     c.maxDepth = r->params.max_path_depth > 0 ? r->params.max_path_depth : (r->params.max_path_depth == 0 ? 256 : 32);
     c.rrMinDepth = r->params.russian_roulette_min_depth >= 0 ? r->params.russian_roulette_min_depth : 3;
     c.paths.pixel = r->pPixel.p;
@@ -333,7 +336,8 @@ const LaunchCtx* uploadCtx(pt_renderer* r)
     }
     if (r->scenes.size() > 1) {
         const size_t n = r->scenes.size();
-        if (!r->dScenes.ensure(n) || !r->dViews.ensure(n)) {
+        if (!r->dScenes.ensure(n) || !r->dViews.ensure(n) || !r->sceneActiveStart.ensure(n + 1) ||
+            !r->sceneJobStart.ensure(n + 1)) {
             return nullptr;
         }
         r->hostScenes.resize(n);
@@ -497,6 +501,88 @@ int configureLayout(pt_renderer* r, const int* widths, const int* heights)
     return PT_OK;
 }
 
+// Material and texture banks of a scene; MeshAccelScene::build adds one
+// default material when none is given.
+int uploadBank(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
+{
+    cudaStream_t s = r->stream;
+    std::vector<pt_material> mats(mesh->materials, mesh->materials + mesh->material_count);
+    if (mats.empty()) {
+        mats.push_back(defaultMaterial());
+    }
+    sl.materialCount = static_cast<uint32_t>(mats.size());
+    if (!sl.materials.ensure(mats.size())) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "material upload failed");
+    }
+    // (a copy from pageable memory has read the source when the call returns)
+    PT_CHECK(r, cudaMemcpyAsync(sl.materials.p, mats.data(), mats.size() * sizeof(pt_material), cudaMemcpyHostToDevice, s));
+    sl.textureCount = mesh->texture_count;
+    if (mesh->texture_count > 0) {
+        if (!sl.textures.ensure(mesh->texture_count)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "texture upload failed");
+        }
+        PT_CHECK(r, cudaMemcpyAsync(sl.textures.p, mesh->textures, mesh->texture_count * sizeof(pt_texture),
+            cudaMemcpyHostToDevice, s));
+    }
+    return PT_OK;
+}
+
+// With the triangles of a scene in sl.positions (9 floats each) and their
+// normals, uvs and material ids in the staging buffers: shading records, the
+// emissive list and CDF, and the BVH, all on the device.
+int finishScene(pt_renderer* r, SceneSlot& sl, uint32_t n)
+{
+    cudaStream_t s = r->stream;
+    sl.triCount = n;
+    if (n == 0) {
+        sl.emissiveCount = 0;
+        if (!sl.emissiveIdx.ensure(1) || !sl.emissiveCdf.ensure(1)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list allocation failed");
+        }
+        PT_CHECK(r, cudaMemsetAsync(sl.emissiveCdf.p, 0, sizeof(float), s));
+        sl.bvh.release();
+        return PT_OK;
+    }
+    if (!sl.shade.ensure(n)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "shading records allocation failed for %u triangles", n);
+    }
+    launchBuildShade(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, sl.shade.p, s);
+    PT_CHECK(r, cudaGetLastError());
+    // emissive triangles (MeshAccelScene.cpp:62-95), selected and summed on the device
+    const size_t tempBytes = emissiveSelectTempBytes(n);
+    if (!r->eWeights.ensure(n) || !r->eFlags.ensure(n) || !r->eIdx.ensure(n) || !r->eCdf.ensure(n + 1ull) ||
+        !r->eOut.ensure(4) || !r->eTemp.ensure(tempBytes)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive scratch allocation failed for %u triangles", n);
+    }
+    launchEmissiveWeights(sl.positions.p, r->stageIds.p, n, sl.materials.p, sl.materialCount, r->eWeights.p,
+        r->eFlags.p, s);
+    PT_CHECK(r, emissiveSelect(r->eTemp.p, tempBytes, r->eFlags.p, n, r->eIdx.p, r->eOut.p + 2, s));
+    launchEmissiveCdf(r->eWeights.p, r->eIdx.p, r->eOut.p + 2, r->eCdf.p, r->eOut.p, s);
+    PT_CHECK(r, cudaGetLastError());
+    uint32_t out[2] = {0, 0};
+    PT_CHECK(r, cudaMemcpyAsync(out, r->eOut.p, sizeof(out), cudaMemcpyDeviceToHost, s));
+    PT_CHECK(r, cudaStreamSynchronize(s));
+    float total;
+    std::memcpy(&total, &out[1], sizeof(float));
+    const uint32_t count = total <= 0.0f ? 0u : out[0];
+    sl.emissiveCount = count;
+    if (!sl.emissiveIdx.ensure(std::max<uint32_t>(1u, count)) || !sl.emissiveCdf.ensure(count + 1ull)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list allocation failed");
+    }
+    if (count > 0) {
+        PT_CHECK(r, cudaMemcpyAsync(sl.emissiveIdx.p, r->eIdx.p, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(sl.emissiveCdf.p, r->eCdf.p, (count + 1ull) * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    } else {
+        PT_CHECK(r, cudaMemsetAsync(sl.emissiveCdf.p, 0, sizeof(float), s));
+    }
+    char err[256] = {0};
+    const int st = buildBvh(sl.positions.p, n, sl.bvh, s, r->bvhOptions, err, sizeof(err));
+    if (st != PT_OK) {
+        return fail(r, st, "BVH build: %s", err);
+    }
+    return PT_OK;
+}
+
 // Uploads a mesh into a scene slot and builds its BVH (MeshAccelScene::build +
 // upload, MeshAccelScene.cpp:141-341).
 int setSceneMesh(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
@@ -514,81 +600,26 @@ int setSceneMesh(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
     PT_CHECK(r, cudaEventRecord(r->ev0, s));
     sl.hasScene = false;
     sl.triCount = n;
-    // materials: MeshAccelScene::build adds one default material when none is given
-    std::vector<pt_material> mats(mesh->materials, mesh->materials + mesh->material_count);
-    if (mats.empty()) {
-        mats.push_back(defaultMaterial());
-    }
-    sl.materialCount = static_cast<uint32_t>(mats.size());
-    if (!sl.materials.ensure(mats.size())) {
-        return fail(r, PT_ERR_OUT_OF_MEMORY, "material upload failed");
-    }
-    PT_CHECK(r, cudaMemcpyAsync(sl.materials.p, mats.data(), mats.size() * sizeof(pt_material), cudaMemcpyHostToDevice, s));
-    sl.textureCount = mesh->texture_count;
-    if (mesh->texture_count > 0) {
-        if (!sl.textures.ensure(mesh->texture_count)) {
-            return fail(r, PT_ERR_OUT_OF_MEMORY, "texture upload failed");
+    {
+        const int st = uploadBank(r, sl, mesh);
+        if (st != PT_OK) {
+            return st;
         }
-        PT_CHECK(r, cudaMemcpyAsync(sl.textures.p, mesh->textures, mesh->texture_count * sizeof(pt_texture),
-            cudaMemcpyHostToDevice, s));
     }
-    // emissive list + CDF: sequential float prefix sum exactly as MeshAccelScene.cpp:62-95
-    std::vector<uint32_t> eIdx;
-    std::vector<float> eCdf(1, 0.0f);
-    float total = 0.0f;
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t mi = mesh->material_ids[i];
-        if (mi >= mats.size()) {
-            continue;
-        }
-        const pt_material& m = mats[mi];
-        const float lum = m.emission * (0.2126f * m.r + 0.7152f * m.g + 0.0722f * m.b);
-        if (lum <= 0.0f) {
-            continue;
-        }
-        const float* p = mesh->positions + 9ull * i;
-        const float e1x = p[3] - p[0], e1y = p[4] - p[1], e1z = p[5] - p[2];
-        const float e2x = p[6] - p[0], e2y = p[7] - p[1], e2z = p[8] - p[2];
-        const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
-        const float area = 0.5f * std::sqrt(cx * cx + cy * cy + cz * cz);
-        const float w = area * lum;
-        if (w <= 0.0f) {
-            continue;
-        }
-        eIdx.push_back(i);
-        total += w;
-        eCdf.push_back(total);
-    }
-    if (total <= 0.0f) {
-        eIdx.clear();
-        eCdf.assign(1, 0.0f);
-    }
-    sl.emissiveCount = static_cast<uint32_t>(eIdx.size());
-    if (!sl.emissiveIdx.ensure(std::max<size_t>(1, eIdx.size())) || !sl.emissiveCdf.ensure(eCdf.size())) {
-        return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list upload failed");
-    }
-    if (!eIdx.empty()) {
-        PT_CHECK(r, cudaMemcpyAsync(sl.emissiveIdx.p, eIdx.data(), eIdx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-    }
-    PT_CHECK(r, cudaMemcpyAsync(sl.emissiveCdf.p, eCdf.data(), eCdf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     if (n > 0) {
-        if (!sl.positions.ensure(9ull * n) || !sl.shade.ensure(n) || !r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
+        if (!sl.positions.ensure(9ull * n) || !r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
             return fail(r, PT_ERR_OUT_OF_MEMORY, "mesh upload failed for %u triangles", n);
         }
         PT_CHECK(r, cudaMemcpyAsync(sl.positions.p, mesh->positions, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
         PT_CHECK(r, cudaMemcpyAsync(r->stage.p, mesh->normals, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
         PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9ull * n, mesh->uvs, 6ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
         PT_CHECK(r, cudaMemcpyAsync(r->stageIds.p, mesh->material_ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-        const int grid = static_cast<int>(std::min<uint32_t>((n + 255) / 256, 148u * 16u));
-        k_build_shade<<<grid, 256, 0, s>>>(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, sl.shade.p);
-        PT_CHECK(r, cudaGetLastError());
-        char err[256] = {0};
-        const int st = buildBvh(sl.positions.p, n, sl.bvh, s, r->bvhOptions, err, sizeof(err));
+    }
+    {
+        const int st = finishScene(r, sl, n);
         if (st != PT_OK) {
-            return fail(r, st, "BVH build: %s", err);
+            return st;
         }
-    } else {
-        sl.bvh.release();
     }
     PT_CHECK(r, cudaEventRecord(r->ev1, s));
     PT_CHECK(r, cudaEventSynchronize(r->ev1));
@@ -659,6 +690,20 @@ int pt_destroy(pt_renderer* r)
     r->dViews.release();
     r->stage.release();
     r->stageIds.release();
+    r->eWeights.release();
+    r->eFlags.release();
+    r->eIdx.release();
+    r->eCdf.release();
+    r->eOut.release();
+    r->eTemp.release();
+    r->tRingStart.release();
+    r->tMaterials.release();
+    r->tPoints.release();
+    r->tTangents.release();
+    r->tRadii.release();
+    r->tCosSin.release();
+    r->tLeaves.release();
+    r->tFrames.release();
     r->envPixels.release();
     r->envMarginal.release();
     r->envRow.release();
@@ -671,6 +716,10 @@ int pt_destroy(pt_renderer* r)
     r->active1.release();
     r->activeCount.release();
     r->samples.release();
+    r->displayBuf.release();
+    r->compactTemp.release();
+    r->sceneActiveStart.release();
+    r->sceneJobStart.release();
     r->pPixel.release();
     r->pOut.release();
     r->pRngA.release();
@@ -921,6 +970,10 @@ int pt_render(pt_renderer* r, int waves)
         if (c == nullptr) {
             return fail(r, PT_ERR_CUDA, "launch context upload failed");
         }
+        if (r->scenes.size() > 1) {
+            launchSceneJobs(c, static_cast<int>(r->scenes.size()), B, s);
+            ++launches;
+        }
         {
             StageTimer tm(r, kGenerate);
             launchGenerate(c, slots, 0, s);
@@ -974,7 +1027,13 @@ int pt_render(pt_renderer* r, int waves)
         PT_CHECK(r, cudaMemsetAsync(r->activeCount.p + 1, 0, sizeof(int), s));
         {
             StageTimer tm(r, kCompact);
-            launchCompact(c, active, s);
+            const size_t tb = compactTempBytes(active);
+            if (!r->compactTemp.ensure(tb)) {
+                return fail(r, PT_ERR_OUT_OF_MEMORY, "compaction scratch allocation failed");
+            }
+            int* lists[2] = {r->active0.p, r->active1.p};
+            PT_CHECK(r, launchCompactStable(lists[r->activeSel], lists[r->activeSel ^ 1], r->activeCount.p + 1, active,
+                r->converged.p, r->counts.p, r->params.max_samples_per_pixel, r->compactTemp.p, tb, s));
         }
         launches += 2;
         int next = 0;
@@ -1274,6 +1333,198 @@ int pt_batch_readback(pt_renderer* r, int scene, float* rgba, uint32_t* counts, 
     if (converged) {
         PT_CHECK(r, cudaMemcpyAsync(converged, r->converged.p + o, P, cudaMemcpyDeviceToHost, r->stream));
     }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    return PT_OK;
+}
+
+int pt_batch_set_tubes(pt_renderer* r, int scene, const pt_tubes* tubes, const pt_mesh* extra)
+{
+    if (r == nullptr || tubes == nullptr || extra == nullptr || scene < 0 ||
+        static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_tubes: bad scene %d or null argument", scene);
+    }
+    const uint32_t T = tubes->tube_count, S = tubes->sides, Lc = tubes->leaf_count;
+    if (T > 0 && (S < 3 || tubes->ring_start == nullptr || tubes->points == nullptr || tubes->tangents == nullptr ||
+                     tubes->radii == nullptr || tubes->materials == nullptr)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_tubes: missing tube arrays or sides < 3");
+    }
+    if (Lc > 0 && tubes->leaves == nullptr) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_tubes: missing leaf array");
+    }
+    const uint32_t rings = T > 0 ? tubes->ring_start[T] : 0u;
+    if (T > 0) {
+        if (tubes->ring_start[0] != 0u) {
+            return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_tubes: ring_start[0] must be 0");
+        }
+        for (uint32_t t = 0; t < T; ++t) {
+            if (tubes->ring_start[t + 1] <= tubes->ring_start[t]) {
+                return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_tubes: tube %u has no ring", t);
+            }
+        }
+    }
+    const uint64_t gen = tubeTriangles(S, rings, Lc);
+    const uint64_t total = gen + extra->triangle_count;
+    if (total > 0xFFFFFFFFull / 2) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_tubes: %llu triangles are too many",
+            static_cast<unsigned long long>(total));
+    }
+    const uint32_t n = static_cast<uint32_t>(total);
+    const pt_mesh* m = extra;
+    if (m->triangle_count > 0 && (m->positions == nullptr || m->normals == nullptr || m->uvs == nullptr ||
+                                     m->material_ids == nullptr)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_set_tubes: missing extra triangle arrays");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = r->stream;
+    SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
+    PT_CHECK(r, cudaEventRecord(r->ev0, s));
+    sl.hasScene = false;
+    int st = uploadBank(r, sl, extra);
+    if (st != PT_OK) {
+        return st;
+    }
+    if (n > 0 && (!sl.positions.ensure(9ull * n) || !r->stage.ensure(15ull * n) || !r->stageIds.ensure(n))) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "mesh allocation failed for %u triangles", n);
+    }
+    if (gen > 0) {
+        std::vector<double> cs;
+        const double* csp = tubes->cos_sin;
+        if (csp == nullptr && S > 0) {
+            cs.resize(2ull * (S + 1));
+            const double step = 2.0 * 3.14159265358979323846 / static_cast<double>(S);
+            for (uint32_t k = 0; k <= S; ++k) {
+                cs[2 * k] = std::cos(static_cast<double>(k) * step);
+                cs[2 * k + 1] = std::sin(static_cast<double>(k) * step);
+            }
+            csp = cs.data();
+        }
+        const size_t R = rings;
+        if (!r->tRingStart.ensure(T + 1ull) || !r->tMaterials.ensure(std::max<uint32_t>(T, 1)) ||
+            !r->tPoints.ensure(3 * R + 1) || !r->tTangents.ensure(3 * R + 1) || !r->tRadii.ensure(R + 1) ||
+            !r->tCosSin.ensure(2ull * (S + 1)) || !r->tLeaves.ensure(10ull * Lc + 1) || !r->tFrames.ensure(9 * R + 1)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "tube upload failed (%u rings, %u leaves)", rings, Lc);
+        }
+        if (T > 0) {
+            PT_CHECK(r, cudaMemcpyAsync(r->tRingStart.p, tubes->ring_start, (T + 1ull) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+            PT_CHECK(r, cudaMemcpyAsync(r->tMaterials.p, tubes->materials, T * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+            PT_CHECK(r, cudaMemcpyAsync(r->tPoints.p, tubes->points, 3 * R * sizeof(double), cudaMemcpyHostToDevice, s));
+            PT_CHECK(r, cudaMemcpyAsync(r->tTangents.p, tubes->tangents, 3 * R * sizeof(double), cudaMemcpyHostToDevice, s));
+            PT_CHECK(r, cudaMemcpyAsync(r->tRadii.p, tubes->radii, R * sizeof(double), cudaMemcpyHostToDevice, s));
+            PT_CHECK(r, cudaMemcpyAsync(r->tCosSin.p, csp, 2ull * (S + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
+        if (Lc > 0) {
+            PT_CHECK(r, cudaMemcpyAsync(r->tLeaves.p, tubes->leaves, 10ull * Lc * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
+        TubeSetDev d;
+        d.tubeCount = T;
+        d.sides = S;
+        d.ringCount = rings;
+        d.ringStart = r->tRingStart.p;
+        d.points = r->tPoints.p;
+        d.tangents = r->tTangents.p;
+        d.radii = r->tRadii.p;
+        d.materials = r->tMaterials.p;
+        d.cosSin = r->tCosSin.p;
+        d.leafCount = Lc;
+        d.leaves = r->tLeaves.p;
+        d.leafSize = tubes->leaf_size;
+        d.leafMaterial = tubes->leaf_material;
+        launchRingFrames(d, r->tFrames.p, s);
+        launchLoft(d, r->tFrames.p, sl.positions.p, r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, s);
+        PT_CHECK(r, cudaGetLastError());
+    }
+    if (m->triangle_count > 0) {
+        const size_t e = m->triangle_count;
+        PT_CHECK(r, cudaMemcpyAsync(sl.positions.p + 9 * gen, m->positions, 9 * e * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9 * gen, m->normals, 9 * e * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9ull * n + 6 * gen, m->uvs, 6 * e * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stageIds.p + gen, m->material_ids, e * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    }
+    st = finishScene(r, sl, n);
+    if (st != PT_OK) {
+        return st;
+    }
+    PT_CHECK(r, cudaEventRecord(r->ev1, s));
+    PT_CHECK(r, cudaEventSynchronize(r->ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+    r->stats.build_ms = ms;
+    sl.hasScene = true;
+    uint32_t nodes = 0;
+    for (const SceneSlot& x : r->scenes) {
+        nodes += x.hasScene ? x.bvh.nodeCount : 0u;
+    }
+    r->stats.bvh_nodes = static_cast<int32_t>(nodes);
+    return resetAccum(r);
+}
+
+int pt_export_mesh(pt_renderer* r, int scene, uint32_t* triangle_count, float* positions, float* normals,
+    float* uvs, uint32_t* material_ids)
+{
+    if (r == nullptr || scene < 0 || static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_export_mesh: bad scene %d", scene);
+    }
+    const SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
+    if (!sl.hasScene) {
+        return fail(r, PT_ERR_NO_SCENE, "pt_export_mesh: scene %d has no mesh", scene);
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = r->stream;
+    const uint32_t n = sl.triCount;
+    if (triangle_count != nullptr) {
+        *triangle_count = n;
+    }
+    if (n == 0) {
+        return PT_OK;
+    }
+    if (positions != nullptr) {
+        PT_CHECK(r, cudaMemcpyAsync(positions, sl.positions.p, 9ull * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    if (normals != nullptr || uvs != nullptr || material_ids != nullptr) {
+        if (!r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "export staging allocation failed");
+        }
+        launchUnpackShade(sl.shade.p, n, r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, s);
+        PT_CHECK(r, cudaGetLastError());
+        if (normals != nullptr) {
+            PT_CHECK(r, cudaMemcpyAsync(normals, r->stage.p, 9ull * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+        }
+        if (uvs != nullptr) {
+            PT_CHECK(r, cudaMemcpyAsync(uvs, r->stage.p + 9ull * n, 6ull * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+        }
+        if (material_ids != nullptr) {
+            PT_CHECK(r, cudaMemcpyAsync(material_ids, r->stageIds.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        }
+    }
+    PT_CHECK(r, cudaStreamSynchronize(s));
+    return PT_OK;
+}
+
+float pt_exposure_multiplier(float f_stop, float shutter_seconds, float iso)
+{
+    const float f = f_stop < 0.1f ? 0.1f : f_stop;
+    const float i = iso < 1.0f ? 1.0f : iso;
+    return shutter_seconds * (i / 100.0f) / (f * f);
+}
+
+int pt_tonemap(pt_renderer* r, int scene, float exposure, uint8_t* rgba8)
+{
+    if (r == nullptr || rgba8 == nullptr || scene < 0 || static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_tonemap: bad scene %d or null output", scene);
+    }
+    if (r->pixelCount == 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_tonemap before pt_configure");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
+    const size_t P = static_cast<size_t>(sl.width) * sl.height;
+    if (!r->displayBuf.ensure(4 * P)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "display buffer allocation failed");
+    }
+    launchTonemap(r->acc.p + sl.pixelBase, r->counts.p + sl.pixelBase, r->converged.p + sl.pixelBase,
+        static_cast<int>(P), r->params, exposure, r->displayBuf.p, r->stream);
+    PT_CHECK(r, cudaGetLastError());
+    PT_CHECK(r, cudaMemcpyAsync(rgba8, r->displayBuf.p, 4 * P, cudaMemcpyDeviceToHost, r->stream));
     PT_CHECK(r, cudaStreamSynchronize(r->stream));
     return PT_OK;
 }

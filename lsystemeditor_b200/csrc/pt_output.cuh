@@ -1,0 +1,13 @@
+// Headless display output (tone map of the accumulator).
+#pragma once
+
+#include "pt_common.cuh"
+
+namespace pt {
+
+// RGBA8 of `pixels` accumulator entries: background for pixels without
+// samples, exposure, Reinhard, 8-bit; or the adaptive-sampling overlay.
+void launchTonemap(const float4* acc, const uint32_t* counts, const uint8_t* converged, int pixels,
+    const pt_render_params& params, float exposure, uint8_t* out, cudaStream_t s);
+
+} // namespace pt

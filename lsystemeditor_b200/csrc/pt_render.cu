@@ -30,6 +30,7 @@
 #include "pt_trace.cuh"
 
 #include <cooperative_groups.h>
+#include <cub/device/device_select.cuh>
 #include <curand_kernel.h>
 
 namespace cg = cooperative_groups;
@@ -138,33 +139,46 @@ __device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigne
     const BatchInfo& bt = *c.q.batch;
     const int activeCount = bt.activeCount;
     const int* active = c.acc.active[c.activeSel];
-    const int li = static_cast<int>(j % static_cast<unsigned long long>(activeCount));
-    const uint32_t slot = static_cast<uint32_t>(j / static_cast<unsigned long long>(activeCount));
-    const uint32_t pixel = static_cast<uint32_t>(active[li]);
-    const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
-    const uint32_t globalSeed = bt.waveBase + slot + 1u;
-    // scene of the pixel; seeds and film coordinates use the pixel's index
-    // within its own image, so a scene renders the same in a batch as alone
-    uint32_t local = pixel;
+    int li;
+    uint32_t slot;
+    uint32_t local;
     const pt_camera* cam = &c.cam;
     uint32_t width = static_cast<uint32_t>(c.width), height = static_cast<uint32_t>(c.height);
+    uint32_t pixel;
     if (c.sceneCount > 1) {
+        // scene-major job order: all of a scene's jobs before the next scene's,
+        // so that the paths in flight share few scenes' geometry
         int lo = 0, hi = c.sceneCount - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (c.views[mid].pixelBase <= pixel) {
+            if (c.sceneJobStart[mid] <= j) {
                 lo = mid;
             } else {
                 hi = mid - 1;
             }
         }
+        const uint32_t a0 = c.sceneActiveStart[lo];
+        const uint32_t n = c.sceneActiveStart[lo + 1] - a0;
+        const unsigned long long q = j - c.sceneJobStart[lo];
+        slot = static_cast<uint32_t>(q / n);
+        li = static_cast<int>(a0 + static_cast<uint32_t>(q % n));
+        pixel = static_cast<uint32_t>(active[li]);
         const SceneView& sv = c.views[lo];
+        // seeds and film coordinates use the pixel's index within its own
+        // image, so a scene renders the same in a batch as alone
         local = pixel - sv.pixelBase;
         cam = &sv.cam;
         width = static_cast<uint32_t>(sv.width);
         height = static_cast<uint32_t>(sv.height);
         c.paths.scene[i] = static_cast<uint16_t>(lo);
+    } else {
+        li = static_cast<int>(j % static_cast<unsigned long long>(activeCount));
+        slot = static_cast<uint32_t>(j / static_cast<unsigned long long>(activeCount));
+        pixel = static_cast<uint32_t>(active[li]);
+        local = pixel;
     }
+    const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
+    const uint32_t globalSeed = bt.waveBase + slot + 1u;
     curandStateXORWOW st;
     curand_init(pathSeed(c.params, local, width, sampleIndex, globalSeed), 0ull, 0ull, &st);
     const uint32_t x = local % width, y = local / width;
@@ -177,7 +191,7 @@ __device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigne
     float3 ro, rd;
     cameraRay(*cam, u, v, l1, l2, ro, rd);
     c.paths.pixel[i] = pixel;
-    c.paths.outIdx[i] = static_cast<uint32_t>(j); // == slot * activeCount + listIndex
+    c.paths.outIdx[i] = slot * static_cast<uint32_t>(activeCount) + static_cast<uint32_t>(li);
     rngStore(c.paths, i, st);
     c.paths.orig[i] = make_float4(ro.x, ro.y, ro.z, 0.0f);
     c.paths.dir[i] = make_float4(rd.x, rd.y, rd.z, 0.0f);
@@ -651,44 +665,53 @@ __global__ void __launch_bounds__(256) k_accumulate(const LaunchCtx* __restrict_
 
 // Ordered-within-block compaction of the active list (compactActiveListKernel,
 // PathTracer.cu:372-411, without per-element atomics).
-__global__ void __launch_bounds__(256) k_compact(const LaunchCtx* __restrict__ cp, int activeCount)
+// Per-scene active ranges (the active list is sorted by pixel) and job
+// offsets of the current batch: scene s owns active entries
+// [sceneActiveStart[s], sceneActiveStart[s + 1]) and jobs
+// [sceneJobStart[s], sceneJobStart[s + 1]).
+__global__ void k_scene_jobs(const LaunchCtx* __restrict__ cp, int sceneCount, int waves)
 {
     const LaunchCtx& c = *cp;
-    const int* in = c.acc.active[c.activeSel];
-    int* out = c.acc.active[c.activeSel ^ 1];
-    const int maxSpp = c.params.max_samples_per_pixel;
-    __shared__ int warpCounts[8];
-    __shared__ int blockBase;
-    for (int base = blockIdx.x * blockDim.x; base < activeCount; base += gridDim.x * blockDim.x) {
-        const int li = base + threadIdx.x;
-        int p = -1;
-        bool keep = false;
-        if (li < activeCount) {
-            p = in[li];
-            keep = c.acc.converged[p] == 0 && !(maxSpp > 0 && c.acc.counts[p] >= static_cast<uint32_t>(maxSpp));
-        }
-        const unsigned int ballot = __ballot_sync(0xffffffffu, keep);
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        if (lane == 0) {
-            warpCounts[w] = __popc(ballot);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int total = 0;
-            for (int k = 0; k < 8; ++k) {
-                const int t = warpCounts[k];
-                warpCounts[k] = total;
-                total += t;
+    const int n = c.q.batch->activeCount;
+    const int* active = c.acc.active[c.activeSel];
+    for (int s = threadIdx.x; s <= sceneCount; s += blockDim.x) {
+        uint32_t pos = static_cast<uint32_t>(n);
+        if (s < sceneCount) {
+            const int key = static_cast<int>(c.views[s].pixelBase);
+            int lo = 0, hi = n; // first entry >= key
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (active[mid] < key) {
+                    lo = mid + 1;
+                } else {
+                    hi = mid;
+                }
             }
-            blockBase = total ? static_cast<int>(atomicAdd(&c.acc.activeCount[1], total)) : 0;
+            pos = static_cast<uint32_t>(lo);
         }
-        __syncthreads();
-        if (keep) {
-            out[blockBase + warpCounts[w] + __popc(ballot & ((1u << lane) - 1u))] = p;
+        c.sceneActiveStart[s] = pos;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long acc = 0;
+        for (int s = 0; s < sceneCount; ++s) {
+            c.sceneJobStart[s] = acc;
+            acc += static_cast<unsigned long long>(c.sceneActiveStart[s + 1] - c.sceneActiveStart[s]) *
+                static_cast<unsigned long long>(waves);
         }
-        __syncthreads();
+        c.sceneJobStart[sceneCount] = acc;
     }
 }
+
+struct KeepActive {
+    const uint8_t* converged;
+    const uint32_t* counts;
+    int maxSpp;
+    __device__ __forceinline__ bool operator()(int p) const
+    {
+        return converged[p] == 0 && !(maxSpp > 0 && counts[p] >= static_cast<uint32_t>(maxSpp));
+    }
+};
 
 __global__ void k_reset(const LaunchCtx* __restrict__ cp, int pixels)
 {
@@ -812,9 +835,21 @@ void launchAccumulate(const LaunchCtx* c, int activeCount, int batch, cudaStream
 {
     k_accumulate<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount, batch);
 }
-void launchCompact(const LaunchCtx* c, int activeCount, cudaStream_t s)
+size_t compactTempBytes(int n)
 {
-    k_compact<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount);
+    size_t bytes = 0;
+    cub::DeviceSelect::If(nullptr, bytes, static_cast<const int*>(nullptr), static_cast<int*>(nullptr),
+        static_cast<int*>(nullptr), n, KeepActive{nullptr, nullptr, 0});
+    return bytes;
+}
+cudaError_t launchCompactStable(const int* in, int* out, int* outCount, int n, const uint8_t* converged,
+    const uint32_t* counts, int maxSpp, void* temp, size_t tempBytes, cudaStream_t s)
+{
+    return cub::DeviceSelect::If(temp, tempBytes, in, out, outCount, n, KeepActive{converged, counts, maxSpp}, s);
+}
+void launchSceneJobs(const LaunchCtx* c, int sceneCount, int waves, cudaStream_t s)
+{
+    k_scene_jobs<<<1, 1024, 0, s>>>(c, sceneCount, waves);
 }
 void launchResetAccum(const LaunchCtx* c, int pixels, cudaStream_t s) { k_reset<<<gridFor(pixels), 256, 0, s>>>(c, pixels); }
 void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,

@@ -85,6 +85,10 @@ struct LaunchCtx {
     int sceneCount;
     const DevScene* scenes;
     const SceneView* views;
+    // per batch: first active-list entry of each scene (sceneCount + 1) and
+    // first job of each scene (sceneCount + 1); jobs are taken scene by scene
+    uint32_t* sceneActiveStart;
+    unsigned long long* sceneJobStart;
     int maxDepth;     // effective (0 -> 256, <0 -> 32)
     int rrMinDepth;   // effective
     PathSoA paths;
@@ -104,7 +108,14 @@ void launchShade(const LaunchCtx* d, int sel, int iter, int grid, cudaStream_t s
 void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, cudaStream_t s);
 void launchFinalize(const LaunchCtx* d, int sel, int grid, cudaStream_t s);
 void launchAccumulate(const LaunchCtx* d, int activeCount, int batch, cudaStream_t s);
-void launchCompact(const LaunchCtx* d, int activeCount, cudaStream_t s);
+// Stable compaction of the active list (pixels neither converged nor at the
+// sample cap), so that the list stays sorted by pixel and thereby by scene.
+size_t compactTempBytes(int n);
+cudaError_t launchCompactStable(const int* in, int* out, int* outCount, int n, const uint8_t* converged,
+    const uint32_t* counts, int maxSpp, void* temp, size_t tempBytes, cudaStream_t s);
+// Batches of several scenes: the per-scene active ranges and job offsets of
+// the current batch (B waves).
+void launchSceneJobs(const LaunchCtx* d, int sceneCount, int waves, cudaStream_t s);
 void launchResetAccum(const LaunchCtx* d, int pixels, cudaStream_t s);
 void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,
     uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s);

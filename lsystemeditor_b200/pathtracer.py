@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _build
 from .records import CAMERA_DTYPE, MATERIAL_DTYPE, PARAMS_DTYPE, TEXTURE_DTYPE
-from .scene import HostMesh
+from .scene import HostMesh, TubeSet
 
 PT_OK = 0
 STATUS_NAMES = {0: "PT_OK", 1: "PT_ERR_INVALID_ARGUMENT", 2: "PT_ERR_CUDA", 3: "PT_ERR_OUT_OF_MEMORY",
@@ -32,6 +32,13 @@ class PtMesh(C.Structure):
     _fields_ = [("triangle_count", C.c_uint32), ("positions", _fp), ("normals", _fp), ("uvs", _fp),
                 ("material_ids", _u32p), ("material_count", C.c_uint32), ("materials", C.c_void_p),
                 ("texture_count", C.c_uint32), ("textures", C.c_void_p)]
+
+
+class PtTubes(C.Structure):
+    _fields_ = [("tube_count", C.c_uint32), ("sides", C.c_uint32), ("ring_start", C.c_void_p),
+                ("points", C.c_void_p), ("tangents", C.c_void_p), ("radii", C.c_void_p), ("materials", C.c_void_p),
+                ("cos_sin", C.c_void_p), ("leaf_count", C.c_uint32), ("leaves", C.c_void_p),
+                ("leaf_size", C.c_double), ("leaf_material", C.c_uint32)]
 
 
 class PtProfile(C.Structure):
@@ -58,7 +65,8 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_reset", "pt_render", "pt_readback", "pt_device_buffers", "pt_get_stats", "pt_trace_rays",
                     "pt_trace_rays_device", "pt_rng_tape", "pt_set_stream", "pt_set_profiling", "pt_get_profile",
                     "pt_set_tuning", "pt_trace_soup_noalloc", "pt_batch_configure", "pt_batch_set_mesh",
-                    "pt_batch_set_camera", "pt_batch_readback"]
+                    "pt_batch_set_camera", "pt_batch_readback", "pt_batch_set_tubes", "pt_export_mesh",
+                    "pt_tonemap", "pt_exposure_multiplier"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -104,6 +112,11 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_batch_set_mesh.argtypes = [vp, C.c_int, C.POINTER(PtMesh)]
     L.pt_batch_set_camera.argtypes = [vp, C.c_int, vp]
     L.pt_batch_readback.argtypes = [vp, C.c_int, _fp, _u32p, _u8p]
+    L.pt_batch_set_tubes.argtypes = [vp, C.c_int, C.POINTER(PtTubes), C.POINTER(PtMesh)]
+    L.pt_export_mesh.argtypes = [vp, C.c_int, _u32p, _fp, _fp, _fp, _u32p]
+    L.pt_tonemap.argtypes = [vp, C.c_int, C.c_float, _u8p]
+    L.pt_exposure_multiplier.argtypes = [C.c_float, C.c_float, C.c_float]
+    L.pt_exposure_multiplier.restype = C.c_float
     _LIB = L
     return L
 
@@ -162,6 +175,7 @@ class PathTracer:
         """PathTracer::configure (PathTracer.h:45-51) without GL surfaces."""
         self._check(self._lib.pt_configure(self._h, int(width), int(height)))
         self.width, self.height = int(width), int(height)
+        self.batch_sizes = [(self.width, self.height)]
         if mesh is not None:
             self.set_mesh(mesh)
 
@@ -311,6 +325,48 @@ class PathTracer:
         self._check(self._lib.pt_batch_readback(self._h, int(scene), _ptr(rgba, _fp), _ptr(counts, _u32p),
                                                 _ptr(conv, _u8p)))
         return rgba, counts, conv
+
+    # -- scene generation on the device, export, display --------------------
+    def batch_set_tubes(self, scene: int, tubes: TubeSet):
+        """Lofts tubes and leaves on the GPU (pt_batch_set_tubes) and builds scene `scene`."""
+        rs = np.ascontiguousarray(tubes.ring_start, np.uint32)
+        pts = np.ascontiguousarray(tubes.points, np.float64)
+        tan = np.ascontiguousarray(tubes.tangents, np.float64)
+        rad = np.ascontiguousarray(tubes.radii, np.float64)
+        mat = np.ascontiguousarray(tubes.materials, np.uint32)
+        cs = np.ascontiguousarray(tubes.cos_sin(), np.float64)
+        lv = np.ascontiguousarray(tubes.leaves, np.float64)
+        addr = lambda a: C.c_void_p(a.ctypes.data) if a.size else None
+        t = PtTubes(len(mat), int(tubes.sides), addr(rs), addr(pts), addr(tan), addr(rad), addr(mat), addr(cs),
+                    len(lv), addr(lv), float(tubes.leaf_size), int(tubes.leaf_material))
+        m, ms = self._pt_mesh(tubes.extra)
+        self._check(self._lib.pt_batch_set_tubes(self._h, int(scene), C.byref(t), C.byref(ms)))
+
+    def export_mesh(self, scene: int = 0) -> HostMesh:
+        """The scene's triangles as built on the device (original order); material bank not included."""
+        n = C.c_uint32()
+        self._check(self._lib.pt_export_mesh(self._h, int(scene), C.byref(n), None, None, None, None))
+        N = int(n.value)
+        pos = np.empty((N, 3, 3), np.float32); nrm = np.empty((N, 3, 3), np.float32)
+        uv = np.empty((N, 3, 2), np.float32); mid = np.empty(N, np.uint32)
+        if N:
+            self._check(self._lib.pt_export_mesh(self._h, int(scene), C.byref(n), _ptr(pos, _fp), _ptr(nrm, _fp),
+                                                 _ptr(uv, _fp), _ptr(mid, _u32p)))
+        from .records import MATERIAL_DTYPE as _M, TEXTURE_DTYPE as _T
+        return HostMesh(pos, nrm, uv, mid, np.zeros(0, _M), np.zeros(0, _T))
+
+    def tonemap(self, scene: int = 0, exposure: float = 1.0) -> np.ndarray:
+        """8-bit RGBA display image (reference display pipeline), (height, width, 4) uint8."""
+        w, h = (self.batch_sizes[scene] if getattr(self, "batch_sizes", None) and scene > 0
+                else (self.width, self.height))
+        out = np.empty((h, w, 4), np.uint8)
+        self._check(self._lib.pt_tonemap(self._h, int(scene), float(exposure), _ptr(out, _u8p)))
+        return out
+
+    @staticmethod
+    def exposure_multiplier(f_stop: float, shutter_seconds: float, iso: float) -> float:
+        """PhysicalCamera::exposureMultiplier (PhysicalCamera.cpp:392-397)."""
+        return float(load_library().pt_exposure_multiplier(float(f_stop), float(shutter_seconds), float(iso)))
 
     # -- queries ----------------------------------------------------------
     def trace_rays(self, origins, dirs, tmin=None, tmax=None) -> dict:

@@ -276,6 +276,84 @@ def leaf_quads(leaves, size: float, material: int) -> HostMesh:
 
 
 # ---------------------------------------------------------------------------
+# Tube sets: turtle output in the form the device loft takes (pt_tubes).
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class TubeSet:
+    """Branch tubes + leaf frames + extra triangles, lofted on the GPU by
+    pt_batch_set_tubes; ``host_mesh`` is the same loft on the host (the
+    device result is bit-identical when every tube has the same ring count)."""
+    ring_start: np.ndarray   # (T + 1,) uint32
+    points: np.ndarray       # (R, 3) float64 ring centres
+    tangents: np.ndarray     # (R, 3) float64
+    radii: np.ndarray        # (R,) float64
+    materials: np.ndarray    # (T,) uint32, index into extra.materials
+    sides: int
+    leaves: np.ndarray       # (L, 10) float64: position, tangent, up, size
+    leaf_size: float
+    leaf_material: int
+    extra: HostMesh          # appended triangles; its material bank is the scene's
+
+    @staticmethod
+    def from_turtle(segments: Sequence[Segment], leaves, sides: int, leaf_size: float, leaf_material: int,
+                    extra: HostMesh, tube_material_offset: int = 0) -> "TubeSet":
+        counts = np.array([len(sg.points) for sg in segments], np.int64)
+        ring_start = np.zeros(len(segments) + 1, np.uint32)
+        ring_start[1:] = np.cumsum(counts)
+        if segments:
+            pts = np.array([p for sg in segments for p in sg.points], np.float64).reshape(-1, 3)
+            tans = np.array([t for sg in segments for t in sg.tangents], np.float64).reshape(-1, 3)
+            rad = np.array([r for sg in segments for r in sg.radii], np.float64)
+        else:
+            pts = np.zeros((0, 3)); tans = np.zeros((0, 3)); rad = np.zeros(0)
+        mats = np.array([sg.material + tube_material_offset for sg in segments], np.uint32)
+        lv = np.array([np.concatenate([l[0], l[1], l[2], [l[3]]]) for l in leaves], np.float64).reshape(-1, 10)
+        return TubeSet(ring_start, pts, tans, rad, mats, int(sides), lv, float(leaf_size), int(leaf_material),
+                       extra)
+
+    @property
+    def triangle_count(self) -> int:
+        return 2 * self.sides * len(self.radii) + 2 * len(self.leaves) + self.extra.triangle_count
+
+    def cos_sin(self) -> np.ndarray:
+        """The loft's angle table (same expression as ``loft``)."""
+        ang = np.arange(self.sides + 1) * (2.0 * math.pi / self.sides)
+        return np.stack([np.cos(ang), np.sin(ang)], -1).reshape(-1)
+
+    def segments(self) -> List[Segment]:
+        out = []
+        for t in range(len(self.materials)):
+            a, b = int(self.ring_start[t]), int(self.ring_start[t + 1])
+            out.append(Segment(list(self.points[a:b]), list(self.tangents[a:b]), list(self.radii[a:b]),
+                               int(self.materials[t]), 0))
+        return out
+
+    def host_mesh(self) -> HostMesh:
+        """The same mesh built on the host: tubes, leaves, extra."""
+        segs = self.segments()
+        tube = loft(segs, self.sides, material_ids=[int(m) for m in self.materials]) if segs else HostMesh.empty()
+        lv = [(r[0:3], r[3:6], r[6:9], float(r[9])) for r in self.leaves]
+        leaf = leaf_quads(lv, self.leaf_size, self.leaf_material)
+        parts = [tube, leaf, self.extra]
+        return HostMesh(np.concatenate([q.positions for q in parts]).astype(np.float32),
+                        np.concatenate([q.normals for q in parts]).astype(np.float32),
+                        np.concatenate([q.uvs for q in parts]).astype(np.float32),
+                        np.concatenate([q.material_ids for q in parts]).astype(np.uint32),
+                        self.extra.materials, self.extra.textures)
+
+    def bounds(self) -> Tuple[np.ndarray, np.ndarray]:
+        """Bounds of the ring centres padded by the radii and of the leaf bases (a conservative estimate)."""
+        lo = np.full(3, np.inf); hi = np.full(3, -np.inf)
+        if len(self.radii):
+            lo = np.minimum(lo, (self.points - self.radii[:, None]).min(0))
+            hi = np.maximum(hi, (self.points + self.radii[:, None]).max(0))
+        if len(self.leaves):
+            lo = np.minimum(lo, self.leaves[:, 0:3].min(0) - self.leaf_size)
+            hi = np.maximum(hi, self.leaves[:, 0:3].max(0) + self.leaf_size)
+        return lo, hi
+
+
+# ---------------------------------------------------------------------------
 # Benchmark scenes.
 # ---------------------------------------------------------------------------
 @dataclasses.dataclass
@@ -287,6 +365,7 @@ class SceneSpec:
     width: int
     height: int
     waves: int  # number of full-resolution waves a complete render takes (upper bound)
+    tubes: Optional["TubeSet"] = None  # the same scene as tubes + leaves + extra triangles (device loft)
 
 
 def bracketed_ol_tree(iterations: int = 4, angle: float = 25.7, length: float = 0.1, radius: float = 0.02,
@@ -349,6 +428,31 @@ def refine_segments(segments: Sequence[Segment], rings: int, taper: float) -> Li
     return out
 
 
+def _bank(materials) -> HostMesh:
+    """A mesh without triangles that carries a material bank (for HostMesh.concat)."""
+    e = HostMesh.empty()
+    e.materials = np.array(list(materials), MATERIAL_DTYPE)
+    return e
+
+
+BARK = dict(r=0.35, g=0.22, b=0.12, roughness=0.8)
+LEAF = dict(r=0.1, g=0.4, b=0.08, roughness=0.5, transmission=0.3, thin=1.0)
+
+
+def tree_tubes(iterations: int = 7, seed: int = 7, sides: int = 64, rings: int = 16, taper: float = 0.85,
+               leaf_size: float = 0.18) -> TubeSet:
+    """The stochastic tree as a TubeSet: bark tubes (material 0), leaf quads
+    (material 1), the ground (2) and the light (3) of the plain scenes."""
+    segs, leaves = stochastic_tree(iterations=iterations, seed=seed)
+    segs = refine_segments(segs, rings, taper=taper)
+    ground = quad_mesh((0, 0, 0), (10, 0, 0), (0, 0, -10),
+                       default_material(r=0.5, g=0.5, b=0.5, roughness=1.0), normal=(0, 1, 0))
+    light = quad_mesh((0, 5, 1.5), (1, 0, 0), (0, 0, 1),
+                      default_material(r=1.0, g=1.0, b=1.0, emission=10.0), normal=(0, -1, 0))
+    extra = HostMesh.concat([_bank([default_material(**BARK), default_material(**LEAF)]), ground, light])
+    return TubeSet.from_turtle(segs, leaves, sides, leaf_size, leaf_material=1, extra=extra)
+
+
 def config1_scene(width: int = 1024, height: int = 1024, sides: int = 64, rings: int = 16,
                   max_depth: int = 12) -> SceneSpec:
     """Plain method, large: the 3D stochastic tree (7 iterations, seed 7) with leaf quads.
@@ -358,21 +462,14 @@ def config1_scene(width: int = 1024, height: int = 1024, sides: int = 64, rings:
     tapered rings.  Bark (0.35, 0.22, 0.12) roughness 0.8; leaves (0.1, 0.4,
     0.08) roughness 0.5, transmission 0.3, thin; the light and ground of the
     plain-small scene.  1024^2, adaptive 16..1024 spp stopping at a relative
-    standard error of 1e-2, max depth 12.
+    standard error of 1e-2, max depth 12.  ``tubes`` holds the same scene for
+    the device loft.
     """
-    segs, leaves = stochastic_tree()
-    segs = refine_segments(segs, rings, taper=0.85)
-    tree = loft(segs, sides)
-    tree.materials = np.array([default_material(r=0.35, g=0.22, b=0.12, roughness=0.8)], MATERIAL_DTYPE)
-    leaf = leaf_quads(leaves, size=0.18, material=0)
-    leaf.materials = np.array([default_material(r=0.1, g=0.4, b=0.08, roughness=0.5, transmission=0.3, thin=1.0)],
-                              MATERIAL_DTYPE)
-    ground = quad_mesh((0, 0, 0), (10, 0, 0), (0, 0, -10),
-                       default_material(r=0.5, g=0.5, b=0.5, roughness=1.0), normal=(0, 1, 0))
-    light = quad_mesh((0, 5, 1.5), (1, 0, 0), (0, 0, 1),
-                      default_material(r=1.0, g=1.0, b=1.0, emission=10.0), normal=(0, -1, 0))
-    mesh = HostMesh.concat([tree, leaf, ground, light])
-    lo, hi = HostMesh.concat([tree, leaf]).bounds()
+    tubes = tree_tubes(sides=sides, rings=rings)
+    mesh = tubes.host_mesh()
+    n_tree = 2 * tubes.sides * len(tubes.radii) + 2 * len(tubes.leaves)
+    p = mesh.positions[:n_tree].reshape(-1, 3)
+    lo, hi = p.min(axis=0), p.max(axis=0)
     center = (lo + hi) * 0.5
     extent = float(np.max(hi - lo))
     dist = extent * 0.5 / math.tan(math.radians(20.0)) * 1.2
@@ -380,9 +477,44 @@ def config1_scene(width: int = 1024, height: int = 1024, sides: int = 64, rings:
     params = default_params(background_r=0.0, background_g=0.0, background_b=0.0, max_path_depth=max_depth,
                             russian_roulette_min_depth=3, min_samples=16, max_samples_per_pixel=1024,
                             relative_error_threshold=0.01, adaptive_criterion=1)
-    return SceneSpec(f"plain-large: 3D stochastic L-system tree, {mesh.triangle_count} triangles, 1024x1024, "
+    spec = SceneSpec(f"plain-large: 3D stochastic L-system tree, {mesh.triangle_count} triangles, 1024x1024, "
                      "adaptive 16-1024 spp to relative std-error 1e-2, depth 12", mesh, cam, params, width, height,
                      1024)
+    spec.tubes = tubes
+    return spec
+
+
+def batch_scenes(count: int = 64, seed: int = 2, sides: int = 48, rings: int = 16, max_depth: int = 12,
+                 min_spp: int = 16, max_spp: int = 512, rel_err: float = 0.03):
+    """Batching workload: `count` stochastic trees of the plain-large grammar with
+    iterations drawn uniformly from 4..8, L-system seeds 100, 101, ..., image
+    sizes drawn from 256^2, 512^2, 768^2, 1024^2 and cameras orbiting the tree
+    at a seeded azimuth (every draw from numpy's default generator seeded with
+    `seed`).  Tubes are 48-gons with 16 rings (about 40M triangles over 64
+    scenes).  Shared params: adaptive min_spp..max_spp stopping at a relative
+    standard error of `rel_err` (0.03, i.e. a per-pixel relative MSE of about
+    1e-3), depth 12, black background.  Returns (tubes, cameras, sizes, params).
+    """
+    rng = np.random.default_rng(seed)
+    its = rng.integers(4, 9, count)
+    res = rng.choice(np.array([256, 512, 768, 1024]), count)
+    az = rng.uniform(0.0, 2.0 * math.pi, count)
+    tubes, cams, sizes = [], [], []
+    for k in range(count):
+        t = tree_tubes(iterations=int(its[k]), seed=100 + k, sides=sides, rings=rings)
+        lo, hi = t.bounds()
+        center = (lo + hi) * 0.5
+        extent = float(np.max(hi - lo))
+        dist = extent * 0.5 / math.tan(math.radians(20.0)) * 1.2
+        eye = (center[0] + dist * math.sin(az[k]), center[1] + 0.15 * dist, center[2] + dist * math.cos(az[k]))
+        w = h = int(res[k])
+        tubes.append(t)
+        cams.append(look_at_camera(eye, center, fov_y_deg=40.0, aspect=w / h))
+        sizes.append((w, h))
+    params = default_params(background_r=0.0, background_g=0.0, background_b=0.0, max_path_depth=max_depth,
+                            russian_roulette_min_depth=3, min_samples=min_spp, max_samples_per_pixel=max_spp,
+                            relative_error_threshold=rel_err, adaptive_criterion=1)
+    return tubes, cams, sizes, params
 
 
 def config0_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> SceneSpec:
