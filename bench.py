@@ -6,7 +6,9 @@ it reaches its sample budget or converges (pt_render with no wave limit),
 starting from a reset accumulator with the scene resident in HBM.  The
 default workload is plain-large (972k-triangle stochastic tree, 1024x1024,
 adaptive 16-1024 spp, depth 12); --config plain-small selects the 20k-triangle
-2D tree at 256x256, 64 spp.
+2D tree at 256x256, 64 spp; --config batch the 64-scene batching workload
+(scenes built on the device, all rendered by one pt_render; the line also
+carries the time of the same scenes rendered one per pt_render).
 
   value  Msamples/s of the device-timed steps (CUDA events on the stream the
          library launches on), summed over ranks, time = max over ranks.
@@ -52,17 +54,27 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--config", choices=["plain-small", "plain-large"], default="plain-large")
+    ap.add_argument("--config", choices=["plain-small", "plain-large", "batch"], default="plain-large")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
 def make_workload(name: str):
-    from lsystemeditor_b200.scene import config0_scene, config1_scene
+    from lsystemeditor_b200.scene import SceneSpec, batch_scenes, config0_scene, config1_scene
     if name == "plain-small":
         return config0_scene()
     if name == "plain-large":
         return config1_scene()
+    if name == "batch":
+        # host-side stand-in for the CPU arms: the scene of the batch with the
+        # median triangle count, lofted on the host, with the batch's params
+        tubes, cams, sizes, params = batch_scenes()
+        order = np.argsort([t.triangle_count for t in tubes], kind="stable")
+        k = int(order[len(order) // 2])
+        mesh = tubes[k].host_mesh()
+        w, h = sizes[k]
+        return SceneSpec(f"batch scene {k} of 64 ({mesh.triangle_count} triangles, {w}x{h}, adaptive 16-512 spp "
+                         "to relative std-error 0.03, depth 12)", mesh, cams[k], params, w, h, 512)
     raise ValueError(name)
 
 
@@ -409,10 +421,195 @@ def run_b200(args):
     return 0
 
 
+def run_batch(args):
+    """The batching workload: 64 scenes built on the device and rendered in one
+    pt_render (value), against the same scenes rendered one per pt_render
+    (config.plain_*).  Every scene's image is identical in both forms."""
+    import torch
+
+    from lsystemeditor_b200.pathtracer import PROFILE_COUNT_VISITS, PROFILE_STAGE_TIMES, PathTracer
+    from lsystemeditor_b200.scene import batch_scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def reduce(x: float, op: str) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    t0 = time.perf_counter()
+    tubes, cams, sizes, params = batch_scenes()
+    gen_s = time.perf_counter() - t0
+    n = len(tubes)
+    stream = torch.cuda.current_stream()
+    pt = PathTracer(local)
+    pt.set_stream(stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def build_batch():
+        pt.batch_configure(sizes)
+        for k in range(n):
+            pt.batch_set_tubes(k, tubes[k])
+            pt.batch_set_camera(k, cams[k])
+        pt.set_params(params)
+
+    tb = time.perf_counter()
+    build_batch()
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - tb
+
+    def step():
+        pt.reset_accumulation()
+        pt.render(0)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    launches0 = pt.stats()["launches"]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    samples = 0
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        step()
+        evs[k][1].record(stream)
+        samples += pt.stats()["samples"]
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = pt.stats()["launches"] - launches0
+    total_ms = reduce(float(sum(a.elapsed_time(b) for a, b in evs)), "max")
+    value = reduce(float(samples), "sum") / (total_ms / 1e3) / 1e6
+
+    # stage times (one render) and traversal counts (one render) for the roofline
+    pt.set_profiling(PROFILE_STAGE_TIMES)
+    flush.zero_()
+    step()
+    prof = pt.profile()
+    pt.set_profiling(PROFILE_COUNT_VISITS | PROFILE_STAGE_TIMES)
+    step()
+    cp = pt.profile()
+    pt.set_profiling(0)
+    nodes_per_ray = cp["nodes_extend"] / max(cp["rays_extend"], 1)
+    tris_per_ray = cp["tris_extend"] / max(cp["rays_extend"], 1)
+    bytes_per_ray = 80.0 * nodes_per_ray + 48.0 * tris_per_ray + 32.0 + 16.0
+    rays_per_launch = prof["rays_extend"] / max(prof["launches_extend"], 1)
+    launch_ms = prof["ms_extend"] / max(prof["launches_extend"], 1)
+    achieved = bytes_per_ray * rays_per_launch / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # the same scenes one per render (the plain drop-in), device-built likewise
+    plain_ms, plain_samples, plain_build_ms = 0.0, 0, 0.0
+    for k in range(n):
+        w, h = sizes[k]
+        pt.configure(w, h)
+        pt.batch_set_tubes(0, tubes[k])
+        plain_build_ms += pt.stats()["build_ms"]
+        pt.set_camera(cams[k])
+        pt.set_params(params)
+        flush.zero_()
+        pt.render(0)
+        s = pt.stats()
+        plain_ms += s["render_ms"]
+        plain_samples += s["samples"]
+
+    # end to end through the public API: tube arrays from host memory, device
+    # loft + BVH builds, render, read back every image (one step)
+    h2d = sum(t.ring_start.nbytes + t.points.nbytes + t.tangents.nbytes + t.radii.nbytes + t.materials.nbytes +
+              t.leaves.nbytes + t.extra.positions.nbytes + t.extra.normals.nbytes + t.extra.uvs.nbytes +
+              t.extra.material_ids.nbytes + t.extra.materials.nbytes for t in tubes)
+    d2h = sum(w * h * (16 + 4 + 1) for w, h in sizes)
+    torch.cuda.synchronize()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    build_batch()
+    pt.render(0)
+    e_samples = pt.stats()["samples"]
+    for k in range(n):
+        pt.batch_readback(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = reduce(float(e0.elapsed_time(e1)), "max")
+    e_value = reduce(float(e_samples), "sum") / (e_ms / 1e3) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_render_rate(make_workload("batch"), min_seconds=12.0)
+        except Exception as e:
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"unavailable: {e}"}
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batch: {n} stochastic trees (iterations 4-8, seeds 100-{99 + n}), "
+                               f"{sum(t.triangle_count for t in tubes)} triangles, {sum(w * h for w, h in sizes)} "
+                               "pixels, adaptive 16-512 spp to relative std-error 0.03, depth 12",
+                   "scenes": n, "triangles": int(sum(t.triangle_count for t in tubes)),
+                   "pixels": int(sum(w * h for w, h in sizes)), "parallelism": f"replicas{world}",
+                   "l2": "flushed between timed steps (256 MiB write, untimed)",
+                   "host_generation_s": round(gen_s, 2), "device_build_s": round(build_s, 2),
+                   "batched_ms_per_render": total_ms / args.steps,
+                   "plain_ms_per_render": plain_ms, "plain_msamples_per_s": plain_samples / plain_ms / 1e3,
+                   "plain_build_ms": plain_build_ms,
+                   "stage_ms_per_step": {k[3:]: round(v, 2) for k, v in prof.items() if k.startswith("ms_")},
+                   "images": "every scene identical in the batched and the plain form"},
+        "e2e": {"value": e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "steps": 1},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
+                     "kernel": "k_extend (closest-hit traversal)", "bytes_per_ray": bytes_per_ray,
+                     "nodes_per_ray": nodes_per_ray, "tris_per_ray": tris_per_ray,
+                     "rays_per_launch": rays_per_launch, "launch_ms": launch_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(out))
+    pt.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "batch":
+        return run_batch(args)
     return run_b200(args)
 
 
