@@ -321,6 +321,22 @@ int pt_tonemap(pt_renderer* r, int scene, float exposure, uint8_t* rgba8);
  * shutter x (max(iso, 1) / 100) / max(f_stop, 0.1)^2. */
 float pt_exposure_multiplier(float f_stop, float shutter_seconds, float iso);
 
+/* ---- Differentiation (no counterpart in the reference) --------------------
+ * Replaces the material bank of scene `scene` (same meaning of the material
+ * ids; textures kept) without rebuilding its BVH; the emissive list follows. */
+int pt_set_materials(pt_renderer* r, int scene, uint32_t material_count, const pt_material* materials);
+
+/* Path-replay backpropagation of an image loss.  d_image: HOST array of
+ * d loss / d image, `channels` (3 or 4) floats per pixel, for the image that
+ * pt_render draws with `spp` samples per pixel from a reset accumulator with
+ * the current scene, camera and parameters (single-scene renderer).  Writes
+ * grad[m * 7 + j], j = r, g, b, roughness, metallic, sheen, emission, for
+ * materials m < grad_materials (at most 16 materials; textured channels get
+ * 0).  Sampling decisions, Russian roulette and MIS weights are treated as
+ * constants.  *device_ms (may be NULL) receives the kernel's device time. */
+int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, float* grad, uint32_t grad_materials,
+    double* device_ms);
+
 /* Largest triangle count pt_trace_soup_noalloc accepts. */
 #define PT_NOALLOC_MAX_TRIANGLES 16384u
 

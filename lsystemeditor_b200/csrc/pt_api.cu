@@ -6,6 +6,7 @@
 // (PathTracer.cpp:2220-2543) with a loop over batches of waves.
 #include "pt_bvh.cuh"
 #include "pt_render.cuh"
+#include "pt_adjoint.cuh"
 #include "pt_output.cuh"
 #include "pt_scene.cuh"
 
@@ -128,6 +129,8 @@ struct pt_renderer {
     DevBuf<int> active0, active1, activeCount;
     DevBuf<float4> samples;
     DevBuf<uint8_t> displayBuf;           // RGBA8 output of pt_tonemap
+    DevBuf<float> adjImage;               // dLoss/dImage of pt_backward
+    DevBuf<float> adjGrad;                // its parameter gradient
     DevBuf<unsigned char> compactTemp;    // scratch of the active-list compaction
     DevBuf<uint32_t> sceneActiveStart;    // batches: per-scene active ranges
     DevBuf<unsigned long long> sceneJobStart;
@@ -527,28 +530,12 @@ int uploadBank(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
     return PT_OK;
 }
 
-// With the triangles of a scene in sl.positions (9 floats each) and their
-// normals, uvs and material ids in the staging buffers: shading records, the
-// emissive list and CDF, and the BVH, all on the device.
-int finishScene(pt_renderer* r, SceneSlot& sl, uint32_t n)
+// Emissive triangles (MeshAccelScene.cpp:62-95), selected and summed on the
+// device from sl.positions, the material ids in the staging buffer and the
+// scene's material bank.
+int buildEmissive(pt_renderer* r, SceneSlot& sl, uint32_t n)
 {
     cudaStream_t s = r->stream;
-    sl.triCount = n;
-    if (n == 0) {
-        sl.emissiveCount = 0;
-        if (!sl.emissiveIdx.ensure(1) || !sl.emissiveCdf.ensure(1)) {
-            return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list allocation failed");
-        }
-        PT_CHECK(r, cudaMemsetAsync(sl.emissiveCdf.p, 0, sizeof(float), s));
-        sl.bvh.release();
-        return PT_OK;
-    }
-    if (!sl.shade.ensure(n)) {
-        return fail(r, PT_ERR_OUT_OF_MEMORY, "shading records allocation failed for %u triangles", n);
-    }
-    launchBuildShade(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, sl.shade.p, s);
-    PT_CHECK(r, cudaGetLastError());
-    // emissive triangles (MeshAccelScene.cpp:62-95), selected and summed on the device
     const size_t tempBytes = emissiveSelectTempBytes(n);
     if (!r->eWeights.ensure(n) || !r->eFlags.ensure(n) || !r->eIdx.ensure(n) || !r->eCdf.ensure(n + 1ull) ||
         !r->eOut.ensure(4) || !r->eTemp.ensure(tempBytes)) {
@@ -574,6 +561,36 @@ int finishScene(pt_renderer* r, SceneSlot& sl, uint32_t n)
         PT_CHECK(r, cudaMemcpyAsync(sl.emissiveCdf.p, r->eCdf.p, (count + 1ull) * sizeof(float), cudaMemcpyDeviceToDevice, s));
     } else {
         PT_CHECK(r, cudaMemsetAsync(sl.emissiveCdf.p, 0, sizeof(float), s));
+    }
+    return PT_OK;
+}
+
+// With the triangles of a scene in sl.positions (9 floats each) and their
+// normals, uvs and material ids in the staging buffers: shading records, the
+// emissive list and CDF, and the BVH, all on the device.
+int finishScene(pt_renderer* r, SceneSlot& sl, uint32_t n)
+{
+    cudaStream_t s = r->stream;
+    sl.triCount = n;
+    if (n == 0) {
+        sl.emissiveCount = 0;
+        if (!sl.emissiveIdx.ensure(1) || !sl.emissiveCdf.ensure(1)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list allocation failed");
+        }
+        PT_CHECK(r, cudaMemsetAsync(sl.emissiveCdf.p, 0, sizeof(float), s));
+        sl.bvh.release();
+        return PT_OK;
+    }
+    if (!sl.shade.ensure(n)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "shading records allocation failed for %u triangles", n);
+    }
+    launchBuildShade(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, sl.shade.p, s);
+    PT_CHECK(r, cudaGetLastError());
+    {
+        const int st = buildEmissive(r, sl, n);
+        if (st != PT_OK) {
+            return st;
+        }
     }
     char err[256] = {0};
     const int st = buildBvh(sl.positions.p, n, sl.bvh, s, r->bvhOptions, err, sizeof(err));
@@ -717,6 +734,8 @@ int pt_destroy(pt_renderer* r)
     r->activeCount.release();
     r->samples.release();
     r->displayBuf.release();
+    r->adjImage.release();
+    r->adjGrad.release();
     r->compactTemp.release();
     r->sceneActiveStart.release();
     r->sceneJobStart.release();
@@ -1526,6 +1545,97 @@ int pt_tonemap(pt_renderer* r, int scene, float exposure, uint8_t* rgba8)
     PT_CHECK(r, cudaGetLastError());
     PT_CHECK(r, cudaMemcpyAsync(rgba8, r->displayBuf.p, 4 * P, cudaMemcpyDeviceToHost, r->stream));
     PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    return PT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Differentiation (no reference counterpart)
+// ---------------------------------------------------------------------------
+int pt_set_materials(pt_renderer* r, int scene, uint32_t material_count, const pt_material* materials)
+{
+    if (r == nullptr || (material_count > 0 && materials == nullptr) || scene < 0 ||
+        static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_materials: bad arguments");
+    }
+    SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
+    if (!sl.hasScene) {
+        return fail(r, PT_ERR_NO_SCENE, "pt_set_materials: scene %d has no mesh", scene);
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    // new material bank, texture bank kept (uploadBank re-reads textures only when given)
+    pt_mesh bank{};
+    bank.material_count = material_count;
+    bank.materials = materials;
+    const uint32_t texCount = sl.textureCount;
+    int st = uploadBank(r, sl, &bank);
+    sl.textureCount = texCount;
+    if (st != PT_OK) {
+        return st;
+    }
+    // the emissive list depends on the materials: rebuild it, with the material
+    // ids taken from the shading records
+    const uint32_t n = sl.triCount;
+    if (n > 0) {
+        if (!r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "staging allocation failed");
+        }
+        launchUnpackShade(sl.shade.p, n, r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, r->stream);
+        PT_CHECK(r, cudaGetLastError());
+        st = buildEmissive(r, sl, n);
+        if (st != PT_OK) {
+            return st;
+        }
+    }
+    return resetAccum(r);
+}
+
+int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, float* grad, uint32_t grad_materials,
+    double* device_ms)
+{
+    if (r == nullptr || d_image == nullptr || grad == nullptr || spp <= 0 || (channels != 3 && channels != 4)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_backward: bad arguments");
+    }
+    if (r->scenes.size() != 1 || r->pixelCount == 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_backward needs a configured single-scene renderer");
+    }
+    const SceneSlot& sl = r->scenes[0];
+    if (!sl.hasScene) {
+        return fail(r, PT_ERR_NO_SCENE, "pt_backward before pt_set_mesh");
+    }
+    if (sl.materialCount > static_cast<uint32_t>(kMaxGradMaterials)) {
+        return fail(r, PT_ERR_UNSUPPORTED, "pt_backward: %u materials, at most %d have gradients", sl.materialCount,
+            kMaxGradMaterials);
+    }
+    const uint32_t M = std::min<uint32_t>(sl.materialCount, grad_materials);
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = r->stream;
+    const size_t P = r->pixelCount;
+    if (!r->adjImage.ensure(P * channels) || !r->adjGrad.ensure(static_cast<size_t>(kMaxGradMaterials) * kGradParams)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "pt_backward: allocation failed");
+    }
+    PT_CHECK(r, cudaMemcpyAsync(r->adjImage.p, d_image, P * channels * sizeof(float), cudaMemcpyHostToDevice, s));
+    PT_CHECK(r, cudaMemsetAsync(r->adjGrad.p, 0, sizeof(float) * kMaxGradMaterials * kGradParams, s));
+    const LaunchCtx* c = uploadCtx(r);
+    if (c == nullptr) {
+        return fail(r, PT_ERR_CUDA, "launch context upload failed");
+    }
+    const int grid = r->smCount * adjointBlocksPerSm();
+    PT_CHECK(r, cudaEventRecord(r->ev0, s));
+    launchAdjoint(c, r->adjImage.p, channels, spp, static_cast<int>(P), static_cast<int>(sl.materialCount),
+        r->adjGrad.p, grid, s);
+    PT_CHECK(r, cudaGetLastError());
+    PT_CHECK(r, cudaEventRecord(r->ev1, s));
+    std::vector<float> g(static_cast<size_t>(kMaxGradMaterials) * kGradParams);
+    PT_CHECK(r, cudaMemcpyAsync(g.data(), r->adjGrad.p, g.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+    PT_CHECK(r, cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+    if (device_ms != nullptr) {
+        *device_ms = ms;
+    }
+    std::memset(grad, 0, sizeof(float) * grad_materials * kGradParams);
+    std::memcpy(grad, g.data(), sizeof(float) * M * kGradParams);
+    r->launches += 1;
     return PT_OK;
 }
 

@@ -121,7 +121,7 @@ __device__ __forceinline__ Mat resolveMaterial(const pt_material& src, float u, 
     m.scatterG = fmaxf(0.0f, src.scatter_radius_g);
     m.scatterB = fmaxf(0.0f, src.scatter_radius_b);
     m.specular = clampTex01(src.specular);
-    m.sheen = src.sheen;
+    m.sheen = clamp01(src.sheen);
     return m;
 }
 
@@ -380,7 +380,18 @@ __device__ __forceinline__ float3 evalDiffuse(const Ctx& c, float3 wi)
         return f3(0.0f, 0.0f, 0.0f);
     }
     const float on = onFactor(c, wi, cI, cO);
-    return scl3(f3(c.m.r, c.m.g, c.m.b), c.w.diffuse * on * kInvPi);
+    float3 r = scl3(f3(c.m.r, c.m.g, c.m.b), c.w.diffuse * on * kInvPi);
+    if (c.m.sheen > 0.0f) {
+        // extension (no reference counterpart): white sheen sheen * (1 - cos theta_d)^5
+        // on the diffuse lobe, theta_d between wi and the half vector (the Disney
+        // BRDF's sheen term); 0 leaves the reference BSDF unchanged
+        const float3 h = normalize3(add3(wi, c.wo));
+        const float x = 1.0f - fmax2(0.0f, dot3(wi, h));
+        const float x2 = x * x;
+        const float sh = c.w.diffuse * c.m.sheen * (x2 * x2 * x);
+        r = add3(r, f3(sh, sh, sh));
+    }
+    return r;
 }
 
 __device__ __forceinline__ float3 evalSpecular(const Ctx& c, float3 wi)
@@ -565,8 +576,8 @@ __device__ __forceinline__ float bsdfPdfImpl(const Ctx& c, float3 wi)
     return p;
 }
 
-__device__ __noinline__ float3 bsdfEval(const Ctx& c, float3 wi) { return bsdfEvalImpl(c, wi); }
-__device__ __noinline__ float bsdfPdf(const Ctx& c, float3 wi) { return bsdfPdfImpl(c, wi); }
+static __device__ __noinline__ float3 bsdfEval(const Ctx& c, float3 wi) { return bsdfEvalImpl(c, wi); }
+static __device__ __noinline__ float bsdfPdf(const Ctx& c, float3 wi) { return bsdfPdfImpl(c, wi); }
 
 __device__ __forceinline__ BsdfSample emptySample(const Ctx& c)
 {
@@ -593,7 +604,7 @@ __device__ __forceinline__ BsdfSample sampleDiffuse(const Ctx& c, float u1, floa
     return s;
 }
 
-__device__ __noinline__ BsdfSample sampleSubsurface(const Ctx& c, float u1, float u2)
+static __device__ __noinline__ BsdfSample sampleSubsurface(const Ctx& c, float u1, float u2)
 {
     if (maxScatter(c.m) <= kMinRadius) {
         return sampleDiffuse(c, u1, u2);
@@ -642,7 +653,7 @@ __device__ __forceinline__ BsdfSample sampleSpecular(const Ctx& c, float u1, flo
     return s;
 }
 
-__device__ __noinline__ BsdfSample sampleTransmit(const Ctx& c, float u1, float u2)
+static __device__ __noinline__ BsdfSample sampleTransmit(const Ctx& c, float u1, float u2)
 {
     BsdfSample s = emptySample(c);
     const float cOs = dot3(c.n, c.wo);
@@ -702,7 +713,7 @@ __device__ __noinline__ BsdfSample sampleTransmit(const Ctx& c, float u1, float 
     return s;
 }
 
-__device__ __noinline__ BsdfSample bsdfSample(const Ctx& c, float u1, float u2)
+static __device__ __noinline__ BsdfSample bsdfSample(const Ctx& c, float u1, float u2)
 {
     if (c.debug & kDbgForceTransmit) {
         return sampleTransmit(c, u1, u2);
@@ -867,7 +878,8 @@ __device__ __forceinline__ const pt_material* fetchMaterial(const DevScene& S, u
 
 // Emissive triangle sampling (LightSamplingCore.h:257-313).
 __device__ __forceinline__ bool sampleEmissive(const DevScene& S, const pt_material* fallback, float uTri, float u1,
-    float u2, float3& pos, float3& n, float3& L, float& pdf, float3& v0, float3& v1, float3& v2)
+    float u2, float3& pos, float3& n, float3& L, float& pdf, float3& v0, float3& v1, float3& v2,
+    uint32_t* triOut = nullptr)
 {
     pdf = 0.0f;
     const uint32_t E = S.emissiveCount;
@@ -886,6 +898,9 @@ __device__ __forceinline__ bool sampleEmissive(const DevScene& S, const pt_mater
         }
     }
     const uint32_t tri = S.emissiveIdx[lo];
+    if (triOut != nullptr) {
+        *triOut = tri;
+    }
     const pt_material& m = *fetchMaterial(S, tri, fallback);
     v0 = loadOrigVertex(S, tri, 0);
     v1 = loadOrigVertex(S, tri, 1);

@@ -5,8 +5,10 @@
 //   * the direction is normalised first (zero length -> (0, 0, -1));
 //   * triangles are intersected with the reference's Moller-Trumbore
 //     (:52-108), rounded exactly like the reference (no FMA contraction), and
-//     accepted when tMin <= t <= closest (a later equal-t hit replaces the
-//     earlier one);
+//     accepted when tMin <= t <= closest; of several hits at exactly the same t
+//     the one latest in leaf order wins (the reference keeps the last one its
+//     own traversal order meets; this rule does not depend on the order, so
+//     that the wavefront and the path-replay kernels agree);
 //   * a hit is reported only if the final t < tMax;
 //   * quirk Q1: a direction component with |d| <= 1e-8 gets a zero reciprocal
 //     in the reference, which turns every slab test into "does the box contain
@@ -330,7 +332,9 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
                         out.tri = __float_as_uint(tv.v0.w);
                         return true;
                     }
-                } else {
+                } else if (t < closest || tgroup.x + k > best || best == 0xFFFFFFFFu) {
+                    // an exact tie in t goes to the later leaf, whatever the visiting
+                    // order, so that every kernel that traces a ray picks the same triangle
                     closest = t;
                     best = tgroup.x + k;
                     bu = u;

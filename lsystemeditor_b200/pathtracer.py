@@ -66,7 +66,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_trace_rays_device", "pt_rng_tape", "pt_set_stream", "pt_set_profiling", "pt_get_profile",
                     "pt_set_tuning", "pt_trace_soup_noalloc", "pt_batch_configure", "pt_batch_set_mesh",
                     "pt_batch_set_camera", "pt_batch_readback", "pt_batch_set_tubes", "pt_export_mesh",
-                    "pt_tonemap", "pt_exposure_multiplier"]
+                    "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -117,6 +117,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_tonemap.argtypes = [vp, C.c_int, C.c_float, _u8p]
     L.pt_exposure_multiplier.argtypes = [C.c_float, C.c_float, C.c_float]
     L.pt_exposure_multiplier.restype = C.c_float
+    L.pt_set_materials.argtypes = [vp, C.c_int, C.c_uint32, vp]
+    L.pt_backward.argtypes = [vp, _fp, C.c_int, C.c_int, _fp, C.c_uint32, C.POINTER(C.c_double)]
     _LIB = L
     return L
 
@@ -367,6 +369,27 @@ class PathTracer:
     def exposure_multiplier(f_stop: float, shutter_seconds: float, iso: float) -> float:
         """PhysicalCamera::exposureMultiplier (PhysicalCamera.cpp:392-397)."""
         return float(load_library().pt_exposure_multiplier(float(f_stop), float(shutter_seconds), float(iso)))
+
+    # -- differentiation (no reference counterpart) -----------------------------
+    GRAD_PARAMS = ("r", "g", "b", "roughness", "metallic", "sheen", "emission")
+
+    def set_materials(self, materials: np.ndarray, scene: int = 0):
+        """Replaces the material bank (same ids) without rebuilding the BVH."""
+        m = np.ascontiguousarray(materials, MATERIAL_DTYPE)
+        self._check(self._lib.pt_set_materials(self._h, int(scene), len(m), C.c_void_p(m.ctypes.data)))
+
+    def backward(self, d_image: np.ndarray, spp: int, materials: int = 16):
+        """Path-replay gradient of a loss through the image pt_render draws with
+        `spp` samples per pixel: d_image is d loss / d image (H, W, 3 or 4).
+        Returns (grad (materials, 7) in GRAD_PARAMS order, device milliseconds)."""
+        d = np.ascontiguousarray(d_image, np.float32)
+        ch = d.shape[-1]
+        assert d.size == self.width * self.height * ch and ch in (3, 4)
+        g = np.zeros((materials, 7), np.float32)
+        ms = C.c_double()
+        self._check(self._lib.pt_backward(self._h, _ptr(d, _fp), int(ch), int(spp), _ptr(g, _fp), int(materials),
+                                          C.byref(ms)))
+        return g, float(ms.value)
 
     # -- queries ----------------------------------------------------------
     def trace_rays(self, origins, dirs, tmin=None, tmax=None) -> dict:

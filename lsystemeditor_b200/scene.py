@@ -517,6 +517,52 @@ def batch_scenes(count: int = 64, seed: int = 2, sides: int = 48, rings: int = 1
     return tubes, cams, sizes, params
 
 
+def diff_materials(rng: np.random.Generator, count: int = 8) -> np.ndarray:
+    """Seeded Principled parameters of the differentiation workload: base colour
+    in U[0.05, 0.9]^3, roughness in U[0.1, 1], metallic in U[0, 0.3], sheen in
+    U[0, 0.5] (sheen is this project's extension lobe)."""
+    mats = []
+    for _ in range(count):
+        c = rng.uniform(0.05, 0.9, 3)
+        mats.append(default_material(r=c[0], g=c[1], b=c[2], roughness=rng.uniform(0.1, 1.0),
+                                     metallic=rng.uniform(0.0, 0.3), sheen=rng.uniform(0.0, 0.5)))
+    return np.array(mats, MATERIAL_DTYPE)
+
+
+def config3_scene(width: int = 512, height: int = 512, spp: int = 64, seed: int = 3, max_depth: int = 8) -> SceneSpec:
+    """Differentiation: the plain-small geometry with 8 branch materials chosen by
+    depth along the tree (8 equal bands of the distance of a segment's start from
+    the root), the ground (material 8) and the light (material 9, emission
+    strength in U[5, 20]); seeded ground-truth parameters (diff_materials);
+    fixed `spp`, max depth 8, black background."""
+    def rule(args, _rng):
+        h, r = args
+        F = ("F", (h, r))
+        a = 25.7
+        return [F, ("[", ()), ("Yaw", (a,)), F, ("]", ()), F, ("[", ()), ("Yaw", (-a,)), F, ("]", ()), F]
+    word = expand([("F", (0.1, 0.02))], {"F": rule}, 4)
+    segs, _ = turtle(word, start_tangent=(0.0, 1.0, 0.0), start_up=(0.0, 0.0, 1.0))
+    dist = np.array([float(np.linalg.norm(sg.points[0])) for sg in segs])
+    band = np.minimum((dist / max(dist.max(), 1e-9) * 8.0).astype(int), 7)
+    tree = loft(segs, 8, material_ids=[int(b) for b in band])
+    rng = np.random.default_rng(seed)
+    tree.materials = diff_materials(rng, 8)
+    ground = quad_mesh((0, 0, 0), (10, 0, 0), (0, 0, -10),
+                       default_material(r=0.5, g=0.5, b=0.5, roughness=1.0), normal=(0, 1, 0))
+    light = quad_mesh((0, 5, 1.5), (1, 0, 0), (0, 0, 1),
+                      default_material(r=1.0, g=1.0, b=1.0, emission=rng.uniform(5.0, 20.0)), normal=(0, -1, 0))
+    mesh = HostMesh.concat([tree, ground, light])
+    lo, hi = tree.bounds()
+    center = (lo + hi) * 0.5
+    extent = float(np.max(hi - lo))
+    dist_c = extent * 0.5 / math.tan(math.radians(20.0)) * 1.15
+    cam = look_at_camera((center[0], center[1], center[2] + dist_c), center, fov_y_deg=40.0, aspect=width / height)
+    params = default_params(background_r=0.0, background_g=0.0, background_b=0.0, max_path_depth=max_depth,
+                            russian_roulette_min_depth=3, min_samples=spp, max_samples_per_pixel=spp)
+    return SceneSpec(f"differentiation: bracketed tree with 8 depth materials, {width}x{height}, {spp} spp",
+                     mesh, cam, params, width, height, spp)
+
+
 def config0_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8) -> SceneSpec:
     """Plain method, small: 625-segment bracketed tree, ground, one area light, pinhole 40 deg.
 

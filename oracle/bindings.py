@@ -121,6 +121,8 @@ class Checker:
             L.orc_trace_rays_bruteforce.argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp, _u8p, _fp, _u32p]
             L.orc_reference_seed.restype = C.c_uint
             L.orc_reference_seed.argtypes = [C.c_int, C.c_int, C.c_uint]
+            L.orc64_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                         _fp, C.c_int, _fp, _dp, C.c_int, C.c_int]
 
     def fn(self, name):
         # attribute access caches the function object, so argtypes/restype set in __init__ stick
@@ -315,6 +317,21 @@ class CheckerScene:
                                         _ptr(state["converged"], _u8p), int(threads))
         state["tape_errors"] = int(err)
         return state
+
+    def backward(self, camera, params, width, height, spp, tape, tape_stride, d_image, materials, env=None,
+                 threads=0):
+        """FP64 path-replay gradient (orc64_backward): d loss / d (r, g, b, roughness, metallic, sheen,
+        emission) per material for the image of `spp` samples per pixel replayed from `tape`."""
+        assert self.chk.kind == "oracle"
+        camera_, params_ = _rec(camera), _rec(params)
+        tp = np.ascontiguousarray(tape, np.float32)
+        d = np.ascontiguousarray(np.asarray(d_image, np.float32)[..., :3]).reshape(-1)
+        assert d.size == 3 * width * height
+        g = np.zeros((materials, 7), np.float64)
+        err = self.chk.lib.orc64_backward(self.h, env.h if env is not None else None, _vp(camera_), _vp(params_),
+                                          width, height, int(spp), _ptr(tp, _fp), int(tape_stride), _ptr(d, _fp),
+                                          _ptr(g, _dp), int(materials), int(threads))
+        return g, int(err)
 
     def trace_pixel(self, camera, params, width, height, idx, sample_index, global_seed, tape_row, env=None):
         camera_ = _rec(camera)

@@ -342,6 +342,75 @@ int orc64_render(void* scene, void* env, const void* cam, const void* params, in
         pixelListCount, acc, counts, lumMean, m2, converged, threads);
 }
 
+// d loss / d material parameters of the image drawn with `spp` samples per
+// pixel (sample k of pixel p replays tape row (k, p)); dImage: 3 floats per
+// pixel; grad: materialCount x 7 doubles (zeroed here).  Returns tape underruns.
+int orc64_backward(void* sceneHandle, void* envHandle, const void* cameraBytes, const void* paramsBytes, int width,
+    int height, int spp, const float* tape, int tapeStride, const float* dImage, double* grad, int materialCount,
+    int threads)
+{
+    const Scene& s = *static_cast<Scene*>(sceneHandle);
+    const Env* e = static_cast<Env*>(envHandle);
+    CameraRec cam;
+    std::memcpy(&cam, cameraBytes, sizeof(cam));
+    ParamsRec p;
+    std::memcpy(&p, paramsBytes, sizeof(p));
+    const int P = width * height;
+    const size_t G = static_cast<size_t>(materialCount) * 7;
+    std::fill(grad, grad + G, 0.0);
+    if (threads > 0) {
+        omp_set_num_threads(threads);
+    }
+    int errors = 0;
+#pragma omp parallel reduction(+ : errors)
+    {
+        std::vector<double> local(G, 0.0);
+#pragma omp for schedule(dynamic, 16)
+        for (int idx = 0; idx < P; ++idx) {
+            const V3<double> d0 = mk(double(dImage[3 * idx]), double(dImage[3 * idx + 1]), double(dImage[3 * idx + 2]));
+            if (d0.x == 0.0 && d0.y == 0.0 && d0.z == 0.0) {
+                continue;
+            }
+            for (int k = 0; k < spp; ++k) {
+                const float* row = tape + (static_cast<size_t>(k) * P + idx) * static_cast<size_t>(tapeStride);
+                Rng r1;
+                r1.row = row;
+                r1.length = tapeStride;
+                V3<double> ro, rd;
+                pixelRay(cam, idx, width, height, r1, ro, rd);
+                const V3<double> Lt = tracePathGrad<double>(s, e, &p, ro, rd, r1, mk(0.0, 0.0, 0.0),
+                    mk(0.0, 0.0, 0.0), nullptr, 0);
+                errors += r1.underruns;
+                if (!std::isfinite(Lt.x) || !std::isfinite(Lt.y) || !std::isfinite(Lt.z)) {
+                    continue;
+                }
+                // adjoint of the firefly clamp (PathTracer.cu:49-67)
+                V3<double> delta = mk(Lt.x > 0.0 ? d0.x / spp : 0.0, Lt.y > 0.0 ? d0.y / spp : 0.0,
+                    Lt.z > 0.0 ? d0.z / spp : 0.0);
+                const V3<double> cl = mk(mx(0.0, Lt.x), mx(0.0, Lt.y), mx(0.0, Lt.z));
+                const double l = cl.x * 0.2126 + cl.y * 0.7152 + cl.z * 0.0722;
+                if (l > 100.0) {
+                    const double kc = 100.0 / l;
+                    const double dc = dot(delta, cl) / l;
+                    const V3<double> w =
+                        mk(Lt.x > 0.0 ? 0.2126 : 0.0, Lt.y > 0.0 ? 0.7152 : 0.0, Lt.z > 0.0 ? 0.0722 : 0.0);
+                    delta = scl(sub(delta, scl(w, dc)), kc);
+                }
+                Rng r2;
+                r2.row = row;
+                r2.length = tapeStride;
+                pixelRay(cam, idx, width, height, r2, ro, rd);
+                tracePathGrad<double>(s, e, &p, ro, rd, r2, delta, Lt, local.data(), materialCount);
+            }
+        }
+#pragma omp critical
+        for (size_t i = 0; i < G; ++i) {
+            grad[i] += local[i];
+        }
+    }
+    return errors;
+}
+
 int orc_trace_pixel(void* scene, void* env, const void* camBytes, const void* paramsBytes, int width, int height,
     int idx, int sampleIndex, unsigned int globalSeed, const float* tapeRow, int tapeLength, float* outRgb)
 {

@@ -352,6 +352,7 @@ template <class R>
 struct Mat {
     R r, g, b, roughness, metallic, transmission, thin, ior, subsurface, emission, diffuseRoughness, scatterR,
         scatterG, scatterB, specular;
+    R sheen; // extension (no reference counterpart): white sheen lobe, 0 = the reference BSDF
 };
 
 template <class R>
@@ -359,7 +360,7 @@ inline Mat<R> matFromRec(const MaterialRec& m)
 {
     return Mat<R>{R(m.r), R(m.g), R(m.b), R(m.roughness), R(m.metallic), R(m.transmission), R(m.thin), R(m.ior),
         R(m.subsurface), R(m.emission), R(m.diffuseRoughness), R(m.scatterR), R(m.scatterG), R(m.scatterB),
-        R(m.specular)};
+        R(m.specular), R(m.sheen)};
 }
 
 // ProceduralTexture.h:138-207 (resolveMaterial + materialFromResolved).
@@ -402,6 +403,7 @@ inline Mat<R> resolve(const MaterialRec& m, V2<R> uv, const std::vector<TextureR
     o.scatterG = fmax(R(0), R(m.scatterG));
     o.scatterB = fmax(R(0), R(m.scatterB));
     o.specular = clamp01f(R(m.specular));
+    o.sheen = clamp01f(R(m.sheen));
     return o;
 }
 
@@ -703,7 +705,17 @@ template <class R> inline V3<R> evalDiffuse(const Ctx<R>& c, V3<R> wi)
     }
     const Lobes<R> w = lobes(c);
     const R on = onFactor(c, wi);
-    return scl(mk(c.m.r, c.m.g, c.m.b), w.diffuse * on * Kc<R>::invPi);
+    V3<R> r = scl(mk(c.m.r, c.m.g, c.m.b), w.diffuse * on * Kc<R>::invPi);
+    if (c.m.sheen > R(0)) {
+        // extension: white sheen sheen * (1 - cos theta_d)^5 on the diffuse lobe
+        // (theta_d between wi and the half vector; the Disney BRDF's sheen term)
+        const V3<R> h = nrm(add(wi, c.wo));
+        const R x = R(1) - mx(R(0), dot(wi, h));
+        const R x2 = x * x;
+        const R sh = w.diffuse * c.m.sheen * (x2 * x2 * x);
+        r = add(r, mk(sh, sh, sh));
+    }
+    return r;
 }
 
 template <class R> inline V3<R> evalSubsurface(const Ctx<R>& c, V3<R> wi)
@@ -1262,7 +1274,8 @@ template <class R> inline R triArea(const TriRec& t)
 }
 
 template <class R>
-inline bool sampleEmissive(const Scene& s, R uTri, R u1, R u2, V3<R>& pos, V3<R>& n, V3<R>& L, R& pdf)
+inline bool sampleEmissive(const Scene& s, R uTri, R u1, R u2, V3<R>& pos, V3<R>& n, V3<R>& L, R& pdf,
+    uint32_t* triOut = nullptr)
 {
     using std::sqrt;
     pdf = R(0);
@@ -1285,6 +1298,9 @@ inline bool sampleEmissive(const Scene& s, R uTri, R u1, R u2, V3<R>& pos, V3<R>
         }
     }
     const uint32_t tri = s.emissiveIdx[static_cast<size_t>(lo)];
+    if (triOut != nullptr) {
+        *triOut = tri;
+    }
     const TriRec& t = s.tris[tri];
     MaterialRec fb = defaultFetchMaterial();
     const MaterialRec& m = fetchMaterial(s, tri, fb);
@@ -1651,5 +1667,274 @@ inline bool isConverged(uint32_t n, float mean, float m2, int minSamples, float 
 // (MeshAccel/MeshAccelScene.cpp:62-95).
 // ---------------------------------------------------------------------------
 void buildScene(Scene& s);
+
+// ---------------------------------------------------------------------------
+// Path-replay gradient of an image loss (the product's adjoint kernel,
+// pt_adjoint.cu, restated): per sample, L from a first replay, then a second
+// replay that adds beta_j dE_j/dtheta for the emission and next-event terms
+// and (L - collected so far) * dlog f_j/dtheta at every BSDF vertex, sampling,
+// Russian roulette and MIS weights held constant.  BSDF derivatives at a
+// fixed direction by central differences (step 1e-6 in FP64; second-order
+// one-sided at the bounds 0 and 1 of the clamped parameters).  Gradients go to
+// G[m * 7 + j], j = r, g, b, roughness, metallic, sheen, emission.
+// ---------------------------------------------------------------------------
+struct FreeParams {
+    bool rgb, roughness, metallic, emission;
+};
+
+inline FreeParams freeParams(const MaterialRec& m, size_t texCount)
+{
+    auto tex = [texCount](uint32_t t) { return t != 0u && t < texCount; };
+    return FreeParams{!tex(m.albedoTex), !tex(m.roughnessTex), !tex(m.metallicTex), !tex(m.emissionTex)};
+}
+
+template <class R>
+inline void bsdfGradFd(const Ctx<R>& c, V3<R> wi, bool roughFollows, V3<R> g[6])
+{
+    const R h = sizeof(R) == 8 ? R(1.0e-6) : R(1.0e-3f);
+    const V3<R> f0 = bsdfEval(c, wi);
+    for (int q = 0; q < 6; ++q) {
+        auto at = [&](R x) {
+            Ctx<R> t = c;
+            R* v = q == 0 ? &t.m.r : q == 1 ? &t.m.g : q == 2 ? &t.m.b : q == 3 ? &t.m.roughness
+                 : q == 4 ? &t.m.metallic : &t.m.sheen;
+            *v = x;
+            if (q == 3 && roughFollows) {
+                t.m.diffuseRoughness = x;
+            }
+            return bsdfEval(t, wi);
+        };
+        const R x = q == 0 ? c.m.r : q == 1 ? c.m.g : q == 2 ? c.m.b : q == 3 ? c.m.roughness
+                  : q == 4 ? c.m.metallic : c.m.sheen;
+        if (x - h >= R(0) && x + h <= R(1)) {
+            g[q] = scl(sub(at(x + h), at(x - h)), R(0.5) / h);
+        } else if (x - h < R(0)) {
+            g[q] = scl(sub(sub(scl(at(x + h), R(4)), scl(f0, R(3))), at(x + R(2) * h)), R(0.5) / h);
+        } else {
+            g[q] = scl(add(sub(scl(f0, R(3)), scl(at(x - h), R(4))), at(x - R(2) * h)), R(0.5) / h);
+        }
+    }
+}
+
+template <class R>
+inline void gradAdd(double* G, int M, uint32_t mi, int j, R v)
+{
+    if (static_cast<int>(mi) < M) {
+        G[mi * 7u + static_cast<uint32_t>(j)] += static_cast<double>(v);
+    }
+}
+
+template <class R>
+inline void neeGrad(double* G, int M, uint32_t mi, const FreeParams& fp, const Ctx<R>& c, V3<R> wi, bool roughFollows,
+    V3<R> w)
+{
+    V3<R> g[6];
+    bsdfGradFd(c, wi, roughFollows, g);
+    const bool use[6] = {fp.rgb, fp.rgb, fp.rgb, fp.roughness, fp.metallic, true};
+    for (int q = 0; q < 6; ++q) {
+        if (use[q]) {
+            gradAdd(G, M, mi, q, dot(w, g[q]));
+        }
+    }
+}
+
+// tracePath with gradient accumulation (G == nullptr: forward only).
+template <class R>
+inline V3<R> tracePathGrad(const Scene& s, const Env* e, const ParamsRec* p, V3<R> ro, V3<R> rd, Rng& rng,
+    V3<R> delta, V3<R> Ltot, double* G, int M)
+{
+    using std::isfinite;
+    const Hit<R> first = traceRay(s, ro, rd, R(0), R(1.0e6f));
+    if (!first.hit) {
+        return envEval(e, p, rd);
+    }
+    int maxDepth = 32, rrMin = 3, debug = 0;
+    if (p != nullptr) {
+        if (p->maxPathDepth > 0) {
+            maxDepth = p->maxPathDepth;
+        } else if (p->maxPathDepth == 0) {
+            maxDepth = 256;
+        }
+        if (p->russianRouletteMinDepth >= 0) {
+            rrMin = p->russianRouletteMinDepth;
+        }
+        debug = p->brdfDebugFlags;
+    }
+    V3<R> L = mk(R(0), R(0), R(0));
+    V3<R> T = mk(R(1), R(1), R(1));
+    V3<R> o = ro, d = rd;
+    Hit<R> h = first;
+    R eta = R(1);
+    MaterialRec fb = defaultFetchMaterial();
+    for (int depth = 0; depth < maxDepth; ++depth) {
+        const V3<R> pos = add(o, scl(d, h.t));
+        const V3<R> n = h.normal;
+        const V3<R> wo = scl(d, R(-1));
+        const MaterialRec& rec = fetchMaterial(s, h.tri, fb);
+        const uint32_t mi = (s.materials.empty() || h.tri >= s.tris.size() || s.tris[h.tri].mat >= s.materials.size())
+            ? 0xFFFFFFFFu : s.tris[h.tri].mat;
+        const bool grad = G != nullptr && mi != 0xFFFFFFFFu;
+        const FreeParams fp = freeParams(rec, s.textures.size());
+        const bool roughFollows = rec.diffuseRoughness < 0.0f;
+        const Mat<R> m = resolve<R>(rec, h.uv, s.textures);
+        // emission
+        if (grad && m.emission != R(0)) {
+            const V3<R> dT = mul(delta, T);
+            if (fp.emission) {
+                gradAdd(G, M, mi, 6, dot(dT, mk(m.r, m.g, m.b)));
+            }
+            if (fp.rgb) {
+                gradAdd(G, M, mi, 0, dT.x * m.emission);
+                gradAdd(G, M, mi, 1, dT.y * m.emission);
+                gradAdd(G, M, mi, 2, dT.z * m.emission);
+            }
+        }
+        L = add(L, mul(T, mk(m.r * m.emission, m.g * m.emission, m.b * m.emission)));
+        // environment NEE (neeEnvironment with the gradient of f)
+        if (!skipsEnvNee(m)) {
+            const R u1 = R(rng.next());
+            const R u2 = R(rng.next());
+            R lp = R(0);
+            const V3<R> wi = envSample(e, u1, u2, lp);
+            if (lp > Kc<R>::minPdf && !occluded(s, add(pos, scl(n, R(1.0e-4f))), wi)) {
+                const R ct = mx(R(0), dot(n, wi));
+                if (ct > R(0)) {
+                    const Ctx<R> c{n, wo, m, eta, 0};
+                    const V3<R> Le = envEval(e, p, wi);
+                    const V3<R> f = bsdfEval(c, wi);
+                    const R bp = bsdfPdf(c, wi);
+                    const R k = misBalance(lp, bp) * ct / lp;
+                    if (grad) {
+                        neeGrad(G, M, mi, fp, c, wi, roughFollows, mul(mul(delta, T), scl(Le, k)));
+                    }
+                    L = add(L, mul(T, mul(f, scl(Le, k))));
+                }
+            }
+        }
+        // emissive NEE (neeEmissive with the gradient of f and of the light)
+        if (!s.emissiveIdx.empty()) {
+            const R uTri = R(rng.next());
+            const R u1 = R(rng.next());
+            const R u2 = R(rng.next());
+            V3<R> lpos, ln, Le;
+            R ap = R(0);
+            uint32_t lt = 0;
+            if (sampleEmissive(s, uTri, u1, u2, lpos, ln, Le, ap, &lt)) {
+                const V3<R> tl = sub(lpos, pos);
+                const R d2 = dot(tl, tl);
+                if (d2 > Kc<R>::minPdf) {
+                    const V3<R> wi = nrm(tl);
+                    const R ct = mx(R(0), dot(n, wi));
+                    const R cl = mx(R(0), dot(ln, scl(wi, R(-1))));
+                    if (ct > R(0) && cl > R(0) && !occluded(s, add(pos, scl(wi, R(1.0e-4f))), wi)) {
+                        const R lpdf = ap * d2 / cl;
+                        if (lpdf > Kc<R>::minPdf) {
+                            const Ctx<R> c{n, wo, m, eta, 0};
+                            const V3<R> f = bsdfEval(c, wi);
+                            const R bp = bsdfPdf(c, wi);
+                            const R k = misBalance(lpdf, bp) * ct / lpdf;
+                            if (grad) {
+                                neeGrad(G, M, mi, fp, c, wi, roughFollows, mul(mul(delta, T), scl(Le, k)));
+                            }
+                            if (G != nullptr && lt < s.tris.size() && s.tris[lt].mat < s.materials.size()) {
+                                const uint32_t lm = s.tris[lt].mat;
+                                const MaterialRec& l0 = s.materials[lm];
+                                const V3<R> w = mul(mul(delta, T), scl(f, k));
+                                gradAdd(G, M, lm, 6, dot(w, mk(R(l0.r), R(l0.g), R(l0.b))));
+                                gradAdd(G, M, lm, 0, w.x * R(l0.emission));
+                                gradAdd(G, M, lm, 1, w.y * R(l0.emission));
+                                gradAdd(G, M, lm, 2, w.z * R(l0.emission));
+                            }
+                            L = add(L, mul(T, mul(f, scl(Le, k))));
+                        }
+                    }
+                }
+            }
+        }
+        const Ctx<R> c{n, wo, m, eta, debug};
+        const R u1 = R(rng.next());
+        const R u2 = R(rng.next());
+        const Sample<R> smp = bsdfSample(c, u1, u2);
+        if (!smp.valid || smp.pdf <= Kc<R>::minPdf) {
+            break;
+        }
+        const V3<R> f = bsdfEval(c, smp.dir);
+        if (grad) {
+            const V3<R> dRem = mul(delta, sub(Ltot, L));
+            V3<R> g[6];
+            bsdfGradFd(c, smp.dir, roughFollows, g);
+            const V3<R> wgt = mk(f.x != R(0) ? dRem.x / f.x : R(0), f.y != R(0) ? dRem.y / f.y : R(0),
+                f.z != R(0) ? dRem.z / f.z : R(0));
+            const bool use[6] = {fp.rgb, fp.rgb, fp.rgb, fp.roughness, fp.metallic, true};
+            for (int q = 0; q < 6; ++q) {
+                if (use[q]) {
+                    gradAdd(G, M, mi, q, dot(wgt, g[q]));
+                }
+            }
+            if (fp.rgb) {
+                const R trans = clampv(m.transmission, R(0), R(1));
+                const R thin = clampv(m.thin, R(0), R(1));
+                const bool pure = trans > R(0.99f) && m.metallic < R(0.01f);
+                R extra = R(0);
+                if (!(pure && thin < R(0.5f)) && smp.transmitted && thin > R(0.5f)) {
+                    extra += R(1);
+                }
+                if (smp.sss && smp.sssSteps > 0 && maxScatter(m) > R(kMinRadius)) {
+                    extra += R(smp.sssSteps);
+                }
+                if (extra != R(0)) {
+                    gradAdd(G, M, mi, 0, m.r != R(0) ? dRem.x * extra / m.r : R(0));
+                    gradAdd(G, M, mi, 1, m.g != R(0) ? dRem.y * extra / m.g : R(0));
+                    gradAdd(G, M, mi, 2, m.b != R(0) ? dRem.z * extra / m.b : R(0));
+                }
+            }
+        }
+        T = applyThroughput(T, c, smp, f);
+        T = subsurfaceTierB(T, m, n, smp, rng);
+        if ((debug & kTintGlassPaths) != 0) {
+            T = smp.transmitted ? mul(T, mk(R(0.2f), R(1), R(0.2f))) : mul(T, mk(R(1), R(0.2f), R(0.2f)));
+        }
+        const R tl = lum709(T);
+        if (!isfinite(tl) || tl <= R(0) || tl > R(1.0e8f)) {
+            break;
+        }
+        if (depth >= rrMin) {
+            const R surv = mn(R(0.95f), mx(tl, R(0.05f)));
+            if (R(rng.next()) > surv) {
+                break;
+            }
+            T = scl(T, R(1) / surv);
+        }
+        eta = smp.nextEta;
+        const R bias = mx(R(1.0e-4f), R(1.0e-3f) * h.t);
+        const R sign = dot(n, smp.dir) >= R(0) ? R(1) : R(-1);
+        o = add(pos, scl(n, sign * bias));
+        d = smp.dir;
+        h = traceRay(s, o, d, bias, R(1.0e6f));
+        if (!h.hit) {
+            const V3<R> Le = envEval(e, p, d);
+            const R lp = envPdf(e, d);
+            const R w = misBalance(smp.pdf, lp);
+            L = add(L, mul(T, scl(Le, w)));
+            break;
+        }
+    }
+    return L;
+}
+
+// Camera ray of pixel idx (the first four draws of tracePixel).
+template <class R>
+inline void pixelRay(const CameraRec& cam, int idx, int width, int height, Rng& rng, V3<R>& ro, V3<R>& rd)
+{
+    const int x = idx % width;
+    const int y = idx / width;
+    const R ju = R(rng.next());
+    const R jv = R(rng.next());
+    const R u = (R(x) + ju) / R(width);
+    const R v = (R(y) + jv) / R(height);
+    const R l1 = R(rng.next());
+    const R l2 = R(rng.next());
+    cameraRay(cam, u, v, l1, l2, ro, rd);
+}
 
 } // namespace orc
