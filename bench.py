@@ -8,7 +8,8 @@ default workload is plain-large (972k-triangle stochastic tree, 1024x1024,
 adaptive 16-1024 spp, depth 12); --config plain-small selects the 20k-triangle
 2D tree at 256x256, 64 spp; --config batch the 64-scene batching workload
 (scenes built on the device, all rendered by one pt_render; the line also
-carries the time of the same scenes rendered one per pt_render).
+carries the time of the same scenes rendered one per pt_render); --config
+adjoint the differentiation workload (path-replay gradient, Adam steps).
 
   value  Msamples/s of the device-timed steps (CUDA events on the stream the
          library launches on), summed over ranks, time = max over ranks.
@@ -54,7 +55,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--config", choices=["plain-small", "plain-large", "batch"], default="plain-large")
+    ap.add_argument("--config", choices=["plain-small", "plain-large", "batch", "adjoint"], default="plain-large")
+    ap.add_argument("--opt-steps", type=int, default=200, help="Adam steps of the adjoint workload's optimisation")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -65,6 +67,9 @@ def make_workload(name: str):
         return config0_scene()
     if name == "plain-large":
         return config1_scene()
+    if name == "adjoint":
+        from lsystemeditor_b200.scene import config3_scene
+        return config3_scene()
     if name == "batch":
         # host-side stand-in for the CPU arms: the scene of the batch with the
         # median triangle count, lofted on the host, with the batch's params
@@ -604,12 +609,150 @@ def run_batch(args):
     return 0
 
 
+def run_adjoint(args):
+    """The differentiation workload: 512x512, 64 spp forward and 64 spp path-replay
+    adjoint over 10 materials (8 branch materials, ground, light).  One step =
+    one optimisation step through the public API: forward render, readback, L2
+    loss against a 256-spp target, pt_backward, Adam update, material upload.
+    value = adjoint Msamples/s (device time of pt_backward); config carries the
+    forward and adjoint device times, their ratio, and an Adam run of
+    --opt-steps steps (lr 1e-2) from a separately seeded start."""
+    import torch
+
+    from lsystemeditor_b200.pathtracer import PathTracer
+    from lsystemeditor_b200.scene import config3_scene, diff_materials
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    spec = config3_scene()
+    spp = int(spec.params["max_samples_per_pixel"])
+    W, H = spec.width, spec.height
+    pt = PathTracer(local)
+    stream = torch.cuda.current_stream()
+    pt.set_stream(stream.cuda_stream)
+    pt.configure(W, H, spec.mesh)
+    pt.set_camera(spec.camera)
+    truth = spec.mesh.materials.copy()
+    names = ("r", "g", "b", "roughness", "metallic", "sheen", "emission")
+
+    def theta_of(m):
+        return np.stack([m[n].astype(np.float64) for n in names], -1)
+
+    def with_theta(base, th):
+        m = base.copy()
+        for j, n in enumerate(names):
+            m[n] = th[:, j].astype(np.float32)
+        return m
+
+    # target: 256 spp of the ground truth
+    p_target = spec.params.copy()
+    p_target["min_samples"] = p_target["max_samples_per_pixel"] = 256
+    pt.set_params(p_target)
+    pt.render(0)
+    target = pt.readback()[0][..., :3].astype(np.float64)
+    pt.set_params(spec.params)
+    pt.record_samples(spp)  # the adjoint reads the forward's per-sample radiance
+
+    init = truth.copy()
+    wrong = diff_materials(np.random.default_rng(1003), 8)
+    for n in names[:6]:
+        init[n][:8] = wrong[n]
+    init["emission"][9] = np.float32(np.random.default_rng(1004).uniform(5.0, 20.0))
+    free = np.zeros((len(truth), 7), bool)
+    free[:8, :6] = True
+    free[9, 6] = True
+
+    class Adam:
+        def __init__(self, x, lr):
+            self.x, self.lr, self.m, self.v, self.t = x.copy(), lr, np.zeros_like(x), np.zeros_like(x), 0
+
+        def step(self, g):
+            self.t += 1
+            self.m = 0.9 * self.m + 0.1 * g
+            self.v = 0.999 * self.v + 0.001 * g * g
+            mh = self.m / (1 - 0.9 ** self.t)
+            vh = self.v / (1 - 0.999 ** self.t)
+            self.x = self.x - self.lr * mh / (np.sqrt(vh) + 1e-8)
+            self.x[:, :6] = np.clip(self.x[:, :6], 0.0, 1.0)
+            self.x[:, 6] = np.maximum(self.x[:, 6], 0.0)
+
+    def opt_step(opt, timing=None):
+        pt.set_materials(with_theta(truth, opt.x))
+        pt.reset_accumulation()
+        pt.render(0)
+        fwd_ms = pt.stats()["render_ms"]
+        img = pt.readback()[0][..., :3].astype(np.float64)
+        loss = float(((img - target) ** 2).sum())
+        g, adj_ms = pt.backward((2.0 * (img - target)).astype(np.float32), spp)
+        g = g[:len(truth)].astype(np.float64) * free
+        # the emission strength lives on a 5..20 scale: Adam steps it in units of 10 lr
+        g[:, 6] *= 10.0
+        opt.step(g)
+        if timing is not None:
+            timing.append((fwd_ms, adj_ms))
+        return loss
+
+    opt = Adam(theta_of(init), 1e-2)
+    for _ in range(max(args.warmup, 3)):
+        opt_step(opt)
+    timing = []
+    launches0 = pt.stats()["launches"]
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        opt_step(opt, timing)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - e0) * 1e3 / args.steps
+    clk = clocks.stop()
+    launches = pt.stats()["launches"] - launches0
+    fwd = float(np.mean([a for a, _ in timing]))
+    adj = float(np.mean([b for _, b in timing]))
+    samples = W * H * spp
+    value = samples / (adj / 1e3) / 1e6
+
+    # the optimisation from the start (untimed)
+    opt = Adam(theta_of(init), 1e-2)
+    losses = [opt_step(opt) for _ in range(args.opt_steps)]
+    err0 = float(np.sqrt(np.mean((theta_of(init)[free] - theta_of(truth)[free]) ** 2)))
+    err1 = float(np.sqrt(np.mean((opt.x[free] - theta_of(truth)[free]) ** 2)))
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": adj, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"adjoint: bracketed tree with 8 depth materials, {W}x{H}, {spp} spp forward + "
+                               f"{spp} spp path-replay adjoint, {len(truth)} materials",
+                   "forward_ms": fwd, "adjoint_ms": adj, "adjoint_over_forward": adj / fwd,
+                   "opt_step_wall_ms": wall_ms, "l2": "not flushed (each step re-reads the scene it rendered)",
+                   "optimisation": {"steps": args.opt_steps, "lr": 1e-2,
+                                    "loss_first": losses[0] if losses else None,
+                                    "loss_last": losses[-1] if losses else None,
+                                    "loss_min": min(losses) if losses else None,
+                                    "param_rmse_start": err0, "param_rmse_end": err1}},
+        "e2e": {"value": samples * 2 / (wall_ms / 1e3) / 1e6, "unit": METRIC,
+                "h2d_bytes_per_step": int(W * H * 3 * 4 + len(truth) * 96),
+                "d2h_bytes_per_step": int(W * H * (16 + 4 + 1) + 16 * 7 * 4),
+                "note": "forward + adjoint samples per wall-clock optimisation step through the public API"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    pt.close()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "batch":
         return run_batch(args)
+    if args.config == "adjoint":
+        return run_adjoint(args)
     return run_b200(args)
 
 

@@ -326,6 +326,14 @@ float pt_exposure_multiplier(float f_stop, float shutter_seconds, float iso);
  * ids; textures kept) without rebuilding its BVH; the emissive list follows. */
 int pt_set_materials(pt_renderer* r, int scene, uint32_t material_count, const pt_material* materials);
 
+/* Keeps, from the next render onwards, the radiance of samples 0 .. spp - 1 of
+ * every pixel (16 bytes each, spp x pixels) so that pt_backward reads it
+ * instead of tracing each path a first time.  It is used when the last
+ * pt_render drew exactly spp samples per pixel (min_samples ==
+ * max_samples_per_pixel == spp) with the current scene, camera and
+ * parameters; 0 releases it.  Single-scene renderers. */
+int pt_record_samples(pt_renderer* r, int spp);
+
 /* Path-replay backpropagation of an image loss.  d_image: HOST array of
  * d loss / d image, `channels` (3 or 4) floats per pixel, for the image that
  * pt_render draws with `spp` samples per pixel from a reset accumulator with

@@ -16,7 +16,8 @@
 // f_j the BSDF at the direction sampled at j.  The inner sum is L minus what
 // the path has collected up to and including vertex j, so two replays of the
 // path (one for L, one that accumulates the gradient) need O(1) memory per
-// path.  The Russian-roulette probability and the MIS weights are detached; the
+// path; when the forward render kept every sample's radiance
+// (pt_record_samples), that record replaces the first replay.  The Russian-roulette probability and the MIS weights are detached; the
 // firefly clamp is differentiated exactly.
 //
 // BSDF derivatives at a fixed direction: exact affine differences for the
@@ -100,11 +101,11 @@ __device__ __forceinline__ float3 paramDerivative(float x, float3 g0, Eval g)
     return scl3(add3(sub3(scl3(g0, 3.0f), scl3(g(x - h), 4.0f)), g(x - 2.0f * h)), 0.5f / h);
 }
 
-// d f / d p at direction wi for p = r, g, b, roughness, metallic, sheen (RGB each).
-// roughFollows: the diffuse roughness is the roughness (material value < 0).
-__device__ void bsdfGrad(const Ctx& cx, float3 wi, bool roughFollows, float3 g[6])
+// d f / d p at direction wi for p = r, g, b, roughness, metallic, sheen (RGB each);
+// f0 = f(wi).  roughFollows: the diffuse roughness is the roughness (material
+// value < 0).
+__device__ void bsdfGrad(const Ctx& cx, float3 wi, float3 f0, bool roughFollows, float3 g[6])
 {
-    const float3 f0 = bsdfEval(cx, wi);
     if (cx.w.transmit == 0.0f && cx.w.subsurface == 0.0f) {
         Ctx t = cx;
         t.m.r = t.m.g = t.m.b = 0.0f;
@@ -145,10 +146,10 @@ __device__ void bsdfGrad(const Ctx& cx, float3 wi, bool roughFollows, float3 g[6
 // Gradient of a next-event contribution beta (x) f (x) Le * k with respect to
 // the BSDF parameters of material mi.
 __device__ __forceinline__ void addNeeGrad(GradAcc& acc, int mi, const FreeParams& fp, const Ctx& cx, float3 wi,
-    bool roughFollows, float3 delta, float3 T, float3 Le, float k)
+    float3 f, bool roughFollows, float3 delta, float3 T, float3 Le, float k)
 {
     float3 g[6];
-    bsdfGrad(cx, wi, roughFollows, g);
+    bsdfGrad(cx, wi, f, roughFollows, g);
     const float3 w = mul3(mul3(delta, T), scl3(Le, k));
     const bool use[6] = {fp.rgb, fp.rgb, fp.rgb, fp.roughness, fp.metallic, true};
     for (int q = 0; q < 6; ++q) {
@@ -167,6 +168,7 @@ struct AdjointArgs {
     int materialCount;
     unsigned long long jobs;
     float* grad;           // [materialCount][kGradParams]
+    const float4* record;  // radiance of every sample from the forward render, or null
 };
 
 // One sample of pixel p (sample index k) through the reference estimator.  With
@@ -275,7 +277,7 @@ __device__ float3 replayPath(const LaunchCtx& c, uint32_t p, uint32_t k, float3 
                         if (!traceRay<true, false>(S, so, xnormalize(wi), kShadowBias, kRayTMax, hh, nullptr, nullptr,
                                 sstack, kAdjointBlock)) {
                             if (grad) {
-                                addNeeGrad(*acc, mi, fp, cx, wi, roughFollows, delta, T, Le, kk);
+                                addNeeGrad(*acc, mi, fp, cx, wi, f, roughFollows, delta, T, Le, kk);
                             }
                             L = add3(L, contrib);
                         }
@@ -318,7 +320,7 @@ __device__ float3 replayPath(const LaunchCtx& c, uint32_t p, uint32_t k, float3 
                                 if (!traceRay<true, false>(S, so, sdn, kShadowBias, kRayTMax, hh, nullptr, nullptr,
                                         sstack, kAdjointBlock)) {
                                     if (grad) {
-                                        addNeeGrad(*acc, mi, fp, cx, wi, roughFollows, delta, T, Le, kk);
+                                        addNeeGrad(*acc, mi, fp, cx, wi, f, roughFollows, delta, T, Le, kk);
                                     }
                                     // the light's own emission and colour
                                     const uint32_t lm = __float_as_uint(S.shade[lt].d.w);
@@ -352,7 +354,7 @@ __device__ float3 replayPath(const LaunchCtx& c, uint32_t p, uint32_t k, float3 
             // radiance still to come from this direction: L_total - L
             const float3 dRem = mul3(delta, sub3(Ltot, L));
             float3 g[6];
-            bsdfGrad(cx, smp.dir, roughFollows, g);
+            bsdfGrad(cx, smp.dir, f, roughFollows, g);
             const float3 inv = f3(f.x != 0.0f ? 1.0f / f.x : 0.0f, f.y != 0.0f ? 1.0f / f.y : 0.0f,
                 f.z != 0.0f ? 1.0f / f.z : 0.0f);
             const float3 wgt = mul3(dRem, inv);
@@ -453,10 +455,21 @@ __global__ void __launch_bounds__(kAdjointBlock) k_adjoint(AdjointArgs a)
         if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) {
             continue;
         }
-        const float3 Ltot =
-            replayPath<false>(c, p, k, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), nullptr, 0, sstack);
+        float3 Ltot;
+        if (a.record != nullptr) {
+            const float4 r = a.record[j];  // j = k * pixels + p
+            Ltot = f3(r.x, r.y, r.z);
+        } else {
+            Ltot = replayPath<false>(c, p, k, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), nullptr, 0, sstack);
+        }
         if (!isfinite(Ltot.x) || !isfinite(Ltot.y) || !isfinite(Ltot.z)) {
             continue; // the firefly clamp replaces a non-finite sample by zero
+        }
+        if (Ltot.x == 0.0f && Ltot.y == 0.0f && Ltot.z == 0.0f) {
+            // nothing collected: every emission and next-event term of the path is
+            // zero and so is the radiance behind every vertex (exact up to terms
+            // whose BSDF value is exactly zero towards a visible light)
+            continue;
         }
         // adjoint of the firefly clamp (PathTracer.cu:49-67): negative channels are
         // cut to zero (no gradient); above luminance 100, c -> c * 100 / lum(c),
@@ -516,7 +529,7 @@ int adjointBlocksPerSm()
 }
 
 void launchAdjoint(const LaunchCtx* ctx, const float* dImage, int channels, int spp, int pixels, int materialCount,
-    float* grad, int grid, cudaStream_t s)
+    float* grad, const float4* record, int grid, cudaStream_t s)
 {
     AdjointArgs a;
     a.ctx = ctx;
@@ -527,6 +540,7 @@ void launchAdjoint(const LaunchCtx* ctx, const float* dImage, int channels, int 
     a.materialCount = materialCount;
     a.jobs = static_cast<unsigned long long>(pixels) * static_cast<unsigned long long>(spp);
     a.grad = grad;
+    a.record = record;
     k_adjoint<<<grid, kAdjointBlock, adjointSmemBytes(), s>>>(a);
 }
 

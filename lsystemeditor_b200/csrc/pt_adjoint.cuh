@@ -13,7 +13,9 @@ int adjointBlocksPerSm();
 // grad ([materialCount][kGradParams], zeroed by the caller) += d loss / d params
 // for the image that pt_render draws with `spp` samples per pixel from a reset
 // accumulator; dImage holds d loss / d image, `channels` (3 or 4) floats per pixel.
+// record: each sample's radiance from the forward render ([sample][pixel]), or
+// null to recompute it with a first replay of the path.
 void launchAdjoint(const LaunchCtx* ctx, const float* dImage, int channels, int spp, int pixels, int materialCount,
-    float* grad, int grid, cudaStream_t s);
+    float* grad, const float4* record, int grid, cudaStream_t s);
 
 } // namespace pt

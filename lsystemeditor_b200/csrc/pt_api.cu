@@ -130,6 +130,9 @@ struct pt_renderer {
     DevBuf<float4> samples;
     DevBuf<uint8_t> displayBuf;           // RGBA8 output of pt_tonemap
     DevBuf<float> adjImage;               // dLoss/dImage of pt_backward
+    DevBuf<float4> record;                // per-sample radiance of the last fixed-spp render
+    int recordSpp = 0;                    // samples per pixel kept (0 = off)
+    bool recordValid = false;             // record matches the current scene, camera and params
     DevBuf<float> adjGrad;                // its parameter gradient
     DevBuf<unsigned char> compactTemp;    // scratch of the active-list compaction
     DevBuf<uint32_t> sceneActiveStart;    // batches: per-scene active ranges
@@ -328,6 +331,9 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.acc.samples = r->samples.p;
     c.acc.sampleCapacity = r->samples.n;
     c.activeSel = r->activeSel;
+    const bool rec = r->recordSpp > 0 && r->scenes.size() == 1 && r->record.p != nullptr;
+    c.record = rec ? r->record.p : nullptr;
+    c.recordSpp = rec ? r->recordSpp : 0;
     return c;
 }
 
@@ -385,6 +391,7 @@ int resetAccum(pt_renderer* r)
     r->lastStopRate = 1.0;
     r->wavesDone = 0;
     r->samplesDone = 0;
+    r->recordValid = false;
     return PT_OK;
 }
 
@@ -735,6 +742,7 @@ int pt_destroy(pt_renderer* r)
     r->samples.release();
     r->displayBuf.release();
     r->adjImage.release();
+    r->record.release();
     r->adjGrad.release();
     r->compactTemp.release();
     r->sceneActiveStart.release();
@@ -1068,6 +1076,11 @@ int pt_render(pt_renderer* r, int waves)
             remaining -= B;
         }
     }
+    // the record holds samples 0 .. recordSpp - 1 of every pixel when each pixel
+    // was rendered to exactly that many samples
+    r->recordValid = r->recordSpp > 0 && r->scenes.size() == 1 && r->record.p != nullptr &&
+        r->wavesDone >= r->recordSpp && r->params.min_samples == r->recordSpp &&
+        r->params.max_samples_per_pixel == r->recordSpp;
     PT_CHECK(r, cudaEventRecord(r->ev1, s));
     PT_CHECK(r, cudaEventSynchronize(r->ev1));
     float ms = 0.0f;
@@ -1589,6 +1602,29 @@ int pt_set_materials(pt_renderer* r, int scene, uint32_t material_count, const p
     return resetAccum(r);
 }
 
+int pt_record_samples(pt_renderer* r, int spp)
+{
+    if (r == nullptr || spp < 0) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_record_samples: bad arguments");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    if (spp == 0) {
+        r->record.release();
+        r->recordSpp = 0;
+        r->recordValid = false;
+        return PT_OK;
+    }
+    if (r->scenes.size() != 1 || r->pixelCount == 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_record_samples needs a configured single-scene renderer");
+    }
+    if (!r->record.ensure(static_cast<size_t>(spp) * r->pixelCount)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "pt_record_samples: %d x %zu samples do not fit", spp, r->pixelCount);
+    }
+    r->recordSpp = spp;
+    return resetAccum(r);
+}
+
 int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, float* grad, uint32_t grad_materials,
     double* device_ms)
 {
@@ -1620,9 +1656,10 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
         return fail(r, PT_ERR_CUDA, "launch context upload failed");
     }
     const int grid = r->smCount * adjointBlocksPerSm();
+    const float4* rec = (r->recordValid && r->recordSpp == spp) ? r->record.p : nullptr;
     PT_CHECK(r, cudaEventRecord(r->ev0, s));
     launchAdjoint(c, r->adjImage.p, channels, spp, static_cast<int>(P), static_cast<int>(sl.materialCount),
-        r->adjGrad.p, grid, s);
+        r->adjGrad.p, rec, grid, s);
     PT_CHECK(r, cudaGetLastError());
     PT_CHECK(r, cudaEventRecord(r->ev1, s));
     std::vector<float> g(static_cast<size_t>(kMaxGradMaterials) * kGradParams);

@@ -93,8 +93,18 @@ __device__ __forceinline__ const DevScene& sceneOf(const LaunchCtx& c, uint32_t 
 
 __device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, float3 L)
 {
+    const uint32_t o = c.paths.outIdx[i];
     const float3 s = clampFirefly(L);
-    c.acc.samples[c.paths.outIdx[i]] = make_float4(s.x, s.y, s.z, 1.0f);
+    c.acc.samples[o] = make_float4(s.x, s.y, s.z, 1.0f);
+    if (c.record != nullptr) {
+        // sample index = samples the pixel had at batch start + the job's slot
+        const uint32_t pixel = c.paths.pixel[i];
+        const uint32_t k = c.acc.counts[pixel] + o / static_cast<uint32_t>(c.q.batch->activeCount);
+        if (k < static_cast<uint32_t>(c.recordSpp)) {
+            c.record[static_cast<size_t>(k) * static_cast<size_t>(c.width) * static_cast<size_t>(c.height) + pixel] =
+                make_float4(L.x, L.y, L.z, 0.0f);
+        }
+    }
 }
 
 // Camera path for job j of the current batch (PathTracer.cu:69-96): job

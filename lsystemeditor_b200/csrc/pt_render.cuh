@@ -95,6 +95,10 @@ struct LaunchCtx {
     QueueSet q;
     AccumState acc;
     int activeSel;    // which active[] list is current
+    // optional record of every sample's radiance before the firefly clamp,
+    // [sample index][pixel], for samples 0 .. recordSpp - 1 (the adjoint's input)
+    float4* record;
+    int recordSpp;
 };
 
 // Launchers. The LaunchCtx lives in DEVICE memory (one per renderer) and is

@@ -66,7 +66,8 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_trace_rays_device", "pt_rng_tape", "pt_set_stream", "pt_set_profiling", "pt_get_profile",
                     "pt_set_tuning", "pt_trace_soup_noalloc", "pt_batch_configure", "pt_batch_set_mesh",
                     "pt_batch_set_camera", "pt_batch_readback", "pt_batch_set_tubes", "pt_export_mesh",
-                    "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward"]
+                    "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
+                    "pt_record_samples"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -119,6 +120,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_exposure_multiplier.restype = C.c_float
     L.pt_set_materials.argtypes = [vp, C.c_int, C.c_uint32, vp]
     L.pt_backward.argtypes = [vp, _fp, C.c_int, C.c_int, _fp, C.c_uint32, C.POINTER(C.c_double)]
+    L.pt_record_samples.argtypes = [vp, C.c_int]
     _LIB = L
     return L
 
@@ -377,6 +379,10 @@ class PathTracer:
         """Replaces the material bank (same ids) without rebuilding the BVH."""
         m = np.ascontiguousarray(materials, MATERIAL_DTYPE)
         self._check(self._lib.pt_set_materials(self._h, int(scene), len(m), C.c_void_p(m.ctypes.data)))
+
+    def record_samples(self, spp: int):
+        """Keep every sample's radiance of fixed-spp renders for backward (0 = off)."""
+        self._check(self._lib.pt_record_samples(self._h, int(spp)))
 
     def backward(self, d_image: np.ndarray, spp: int, materials: int = 16):
         """Path-replay gradient of a loss through the image pt_render draws with

@@ -384,6 +384,9 @@ int orc64_backward(void* sceneHandle, void* envHandle, const void* cameraBytes, 
                 if (!std::isfinite(Lt.x) || !std::isfinite(Lt.y) || !std::isfinite(Lt.z)) {
                     continue;
                 }
+                if (Lt.x == 0.0 && Lt.y == 0.0 && Lt.z == 0.0) {
+                    continue; // nothing collected: no gradient (as the product's adjoint)
+                }
                 // adjoint of the firefly clamp (PathTracer.cu:49-67)
                 V3<double> delta = mk(Lt.x > 0.0 ? d0.x / spp : 0.0, Lt.y > 0.0 ? d0.y / spp : 0.0,
                     Lt.z > 0.0 ? d0.z / spp : 0.0);

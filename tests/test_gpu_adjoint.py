@@ -134,3 +134,33 @@ def test_torch_autograd_reduces_loss(tracer):
             theta[:, 0:3].clamp_(0.0, 1.0)
         losses.append(float(loss))
     assert losses[-1] < 0.5 * losses[0], losses
+
+
+def test_recorded_samples_give_the_replayed_gradient(tracer):
+    """pt_record_samples: the adjoint reads each sample's radiance kept by the
+    forward render instead of replaying the path a first time; the gradient is
+    the same (up to the FP32 rounding differences of the two kernels)."""
+    w, h, spp = 48, 40, 6
+    spec, params = _setup(tracer, w, h, spp)
+    mats = spec.mesh.materials
+    target = np.full((h, w, 3), 0.1)
+    img = _render(tracer, mats, spp)
+    d_image = (2.0 * (img - target)).astype(np.float32)
+    g_replay, ms_replay = tracer.backward(d_image, spp)
+    tracer.record_samples(spp)
+    img2 = _render(tracer, mats, spp)
+    assert np.array_equal(img, img2)
+    g_rec, ms_rec = tracer.backward(d_image, spp)
+    M = len(mats)
+    scale = np.abs(g_replay[:M]).max(axis=0)
+    err = np.abs(g_rec[:M] - g_replay[:M]) / np.maximum(scale, 1e-30)
+    assert err.max() < 1e-4, err.max()
+    # a render with other parameters invalidates the record: back to the replay
+    p2 = params.copy()
+    p2["max_path_depth"] = 3
+    tracer.set_params(p2)
+    tracer.render(spp)
+    tracer.set_params(params)
+    g_again, _ = tracer.backward(d_image, spp)
+    assert np.allclose(g_again[:M], g_replay[:M], rtol=0, atol=1e-4 * scale.max())
+    tracer.record_samples(0)
