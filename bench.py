@@ -717,8 +717,15 @@ def run_adjoint(args):
     # the optimisation from the start (untimed)
     opt = Adam(theta_of(init), 1e-2)
     losses = [opt_step(opt) for _ in range(args.opt_steps)]
-    err0 = float(np.sqrt(np.mean((theta_of(init)[free] - theta_of(truth)[free]) ** 2)))
-    err1 = float(np.sqrt(np.mean((opt.x[free] - theta_of(truth)[free]) ** 2)))
+    def errors(x):
+        t = theta_of(truth)
+        out = {}
+        for j, n in enumerate(names[:6]):
+            out[n] = float(np.sqrt(np.mean((x[:8, j] - t[:8, j]) ** 2)))
+        out["emission_abs"] = float(abs(x[9, 6] - t[9, 6]))
+        return out
+    err0 = errors(theta_of(init))
+    err1 = errors(opt.x)
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": adj, "higher_is_better": True, "scaling": "weak",
