@@ -345,6 +345,30 @@ int pt_record_samples(pt_renderer* r, int spp);
 int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, float* grad, uint32_t grad_materials,
     double* device_ms);
 
+/* ---- Preview passes and region render ------------------------------------ */
+/* PathTracer::setPreviewStepsPerLevel (PathTracer.h:89-92): with n > 0 (at
+ * most 128), pt_render first renders n low-resolution preview passes, level i
+ * at 1 / 2^(n - i) of the image (PathTracerPreviewLevels.h:17-49), one sample
+ * per pixel at the pixel centre, depth 4, global seed i + 1; full-resolution
+ * wave w then draws with global seed n + w + 1, as the reference's iteration
+ * count includes the previews.  Until the first full-resolution wave,
+ * pt_tonemap shows the finest preview upsampled.  Single-scene renderers. */
+int pt_set_preview_levels(pt_renderer* r, int levels);
+/* Renders the preview passes not yet rendered since the last reset (pt_render
+ * does it first anyway), so that a display can show them before any wave. */
+int pt_render_previews(pt_renderer* r);
+/* A preview level's float RGBA image (HOST, width x height x 4) and size. */
+int pt_preview_readback(pt_renderer* r, int level, float* rgba, int* width, int* height);
+
+/* setRegionRenderEnabled + setRenderRegion (PathTracer.h:134-138,
+ * PathTracer.cpp:1447-1463): only the pixels of the rectangle (corners ordered
+ * and clamped to the image) take samples; enabling clears the region and keeps
+ * the rest of the image.  A reset (parameter change) clears the whole image and
+ * keeps sampling only the region. */
+int pt_set_region(pt_renderer* r, int enabled, int min_x, int min_y, int max_x, int max_y);
+/* resetRegionAccumulation (PathTracer.h:140): clears the region only. */
+int pt_reset_region(pt_renderer* r);
+
 /* Largest triangle count pt_trace_soup_noalloc accepts. */
 #define PT_NOALLOC_MAX_TRIANGLES 16384u
 

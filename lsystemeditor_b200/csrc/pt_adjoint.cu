@@ -177,17 +177,29 @@ struct AdjointArgs {
 // dot(delta, L) into acc, using Ltot = the first replay's L.  The traversal
 // stack is sstack (this thread's column of the block's shared array) and then
 // local memory, as in the forward kernels.
+// Where a path starts: pixel p of a width x height image, sample index and
+// global seed of its random numbers, subpixel jitter or the pixel centre
+// (tracePixelRadiance, PathTracer.cu:69-105), and the depth limit.
+struct PathStart {
+    uint32_t p;
+    uint32_t width, height;
+    uint32_t sampleIndex;
+    uint32_t globalSeed;
+    bool jitter;
+    int maxDepth;
+};
+
 template <bool Grad>
-__device__ float3 replayPath(const LaunchCtx& c, uint32_t p, uint32_t k, float3 delta, float3 Ltot, GradAcc* acc,
+__device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 delta, float3 Ltot, GradAcc* acc,
     int materialCount, uint2* sstack)
 {
     const DevScene& S = c.scene;
-    const uint32_t width = static_cast<uint32_t>(c.width), height = static_cast<uint32_t>(c.height);
+    const uint32_t p = ps.p, width = ps.width, height = ps.height;
     curandStateXORWOW st;
-    curand_init(pathSeed(c.params, p, width, k, k + 1u), 0ull, 0ull, &st);
+    curand_init(pathSeed(c.params, p, width, ps.sampleIndex, ps.globalSeed), 0ull, 0ull, &st);
     const uint32_t x = p % width, y = p / width;
-    const float ju = curand_uniform(&st);
-    const float jv = curand_uniform(&st);
+    const float ju = ps.jitter ? curand_uniform(&st) : 0.5f;
+    const float jv = ps.jitter ? curand_uniform(&st) : 0.5f;
     const float u = (static_cast<float>(x) + ju) / static_cast<float>(width);
     const float v = (static_cast<float>(y) + jv) / static_cast<float>(height);
     const float l1 = curand_uniform(&st);
@@ -217,7 +229,7 @@ __device__ float3 replayPath(const LaunchCtx& c, uint32_t p, uint32_t k, float3 
             }
             break;
         }
-        if (depth >= c.maxDepth) {
+        if (depth >= ps.maxDepth) {
             break;
         }
         // shading point (k_shade)
@@ -455,12 +467,15 @@ __global__ void __launch_bounds__(kAdjointBlock) k_adjoint(AdjointArgs a)
         if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) {
             continue;
         }
+        // sample k of pixel p as a fresh render draws it: wave k's seed
+        const PathStart start{p, static_cast<uint32_t>(c.width), static_cast<uint32_t>(c.height), k,
+            k + 1u + static_cast<uint32_t>(c.seedOffset), true, c.maxDepth};
         float3 Ltot;
         if (a.record != nullptr) {
             const float4 r = a.record[j];  // j = k * pixels + p
             Ltot = f3(r.x, r.y, r.z);
         } else {
-            Ltot = replayPath<false>(c, p, k, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), nullptr, 0, sstack);
+            Ltot = replayPath<false>(c, start, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), nullptr, 0, sstack);
         }
         if (!isfinite(Ltot.x) || !isfinite(Ltot.y) || !isfinite(Ltot.z)) {
             continue; // the firefly clamp replaces a non-finite sample by zero
@@ -485,7 +500,7 @@ __global__ void __launch_bounds__(kAdjointBlock) k_adjoint(AdjointArgs a)
                 Ltot.z > 0.0f ? 0.0722f : 0.0f);
             delta = scl3(sub3(delta, scl3(w, dc)), kc);
         }
-        replayPath<true>(c, p, k, delta, Ltot, &acc, a.materialCount, sstack);
+        replayPath<true>(c, start, delta, Ltot, &acc, a.materialCount, sstack);
     }
     // block reduction of the (sum, -compensation) pairs, then one atomic per entry
     __shared__ float sHi[kAdjointBlock / 32], sLo[kAdjointBlock / 32];
@@ -519,7 +534,33 @@ __global__ void __launch_bounds__(kAdjointBlock) k_adjoint(AdjointArgs a)
 
 size_t adjointSmemBytes() { return sizeof(uint2) * kSharedStack * kAdjointBlock; }
 
+// Preview pass (sampleKernel with previewPass, PathTracer.cu:132-184): one
+// sample per pixel of a width x height image at the pixel centre, sample index
+// 0 and the given global seed, depth limit kPreviewMaxPathDepth
+// (PathTracerPreviewLevels.h:13), firefly-clamped.
+__global__ void __launch_bounds__(kAdjointBlock) k_preview(const LaunchCtx* __restrict__ cp, int width, int height,
+    uint32_t globalSeed, int maxDepth, float4* out)
+{
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
+    uint2* sstack = smemStack + threadIdx.x;
+    const int n = width * height;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const PathStart start{static_cast<uint32_t>(p), static_cast<uint32_t>(width), static_cast<uint32_t>(height), 0u,
+            globalSeed, false, maxDepth};
+        const float3 L = clampFirefly(
+            replayPath<false>(c, start, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), nullptr, 0, sstack));
+        out[p] = make_float4(L.x, L.y, L.z, 1.0f);
+    }
+}
+
 } // namespace
+
+void launchPreview(const LaunchCtx* ctx, int width, int height, uint32_t globalSeed, int maxDepth, float4* out,
+    int grid, cudaStream_t s)
+{
+    k_preview<<<grid, kAdjointBlock, adjointSmemBytes(), s>>>(ctx, width, height, globalSeed, maxDepth, out);
+}
 
 int adjointBlocksPerSm()
 {

@@ -17,5 +17,9 @@ int adjointBlocksPerSm();
 // null to recompute it with a first replay of the path.
 void launchAdjoint(const LaunchCtx* ctx, const float* dImage, int channels, int spp, int pixels, int materialCount,
     float* grad, const float4* record, int grid, cudaStream_t s);
+// Preview pass of a width x height image (one centred sample per pixel, no
+// accumulation) into out, with the path-replay kernel.
+void launchPreview(const LaunchCtx* ctx, int width, int height, uint32_t globalSeed, int maxDepth, float4* out,
+    int grid, cudaStream_t s);
 
 } // namespace pt

@@ -130,6 +130,13 @@ struct pt_renderer {
     DevBuf<float4> samples;
     DevBuf<uint8_t> displayBuf;           // RGBA8 output of pt_tonemap
     DevBuf<float> adjImage;               // dLoss/dImage of pt_backward
+    // preview passes (PathTracerPreviewLevels.h): level i at 1 / 2^(levels - i)
+    int previewLevels = 0;
+    int previewDone = -1;                 // finest preview level rendered since the last reset
+    DevBuf<float4> previewBuf;            // all levels, coarsest first
+    // region render (PathTracer.h:134-140)
+    bool regionEnabled = false;
+    int regionMinX = 0, regionMinY = 0, regionMaxX = 0, regionMaxY = 0;
     DevBuf<float4> record;                // per-sample radiance of the last fixed-spp render
     int recordSpp = 0;                    // samples per pixel kept (0 = off)
     bool recordValid = false;             // record matches the current scene, camera and params
@@ -334,6 +341,7 @@ LaunchCtx makeCtx(pt_renderer* r)
     const bool rec = r->recordSpp > 0 && r->scenes.size() == 1 && r->record.p != nullptr;
     c.record = rec ? r->record.p : nullptr;
     c.recordSpp = rec ? r->recordSpp : 0;
+    c.seedOffset = r->previewLevels;
     return c;
 }
 
@@ -388,6 +396,13 @@ int resetAccum(pt_renderer* r)
     launchResetAccum(dc, static_cast<int>(r->pixelCount), r->stream);
     PT_CHECK(r, cudaGetLastError());
     r->hostActive = static_cast<int>(r->pixelCount);
+    r->previewDone = -1;
+    if (r->regionEnabled && r->scenes.size() == 1) {
+        // only the region's pixels take samples
+        launchRegion(dc, r->width, r->regionMinX, r->regionMinY, r->regionMaxX, r->regionMaxY, false, r->stream);
+        PT_CHECK(r, cudaGetLastError());
+        r->hostActive = (r->regionMaxX - r->regionMinX + 1) * (r->regionMaxY - r->regionMinY + 1);
+    }
     r->lastStopRate = 1.0;
     r->wavesDone = 0;
     r->samplesDone = 0;
@@ -533,6 +548,52 @@ int uploadBank(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
         }
         PT_CHECK(r, cudaMemcpyAsync(sl.textures.p, mesh->textures, mesh->texture_count * sizeof(pt_texture),
             cudaMemcpyHostToDevice, s));
+    }
+    return PT_OK;
+}
+
+// Preview level i of n (PathTracerPreviewLevels.h:17-49): downscale 2^(n - i),
+// size max(1, axis / downscale).
+void previewDims(int width, int height, int levels, int level, int& w, int& h, int& ds)
+{
+    ds = 1 << (levels - level);
+    w = width / ds >= 1 ? width / ds : 1;
+    h = height / ds >= 1 ? height / ds : 1;
+}
+
+size_t previewOffset(int width, int height, int levels, int level)
+{
+    size_t off = 0;
+    for (int i = 0; i < level; ++i) {
+        int w, h, ds;
+        previewDims(width, height, levels, i, w, h, ds);
+        off += static_cast<size_t>(w) * h;
+    }
+    return off;
+}
+
+// kPreviewMaxPathDepth (PathTracerPreviewLevels.h:13)
+constexpr int kPreviewDepth = 4;
+
+int renderPreviews(pt_renderer* r)
+{
+    const size_t total = previewOffset(r->width, r->height, r->previewLevels, r->previewLevels);
+    if (!r->previewBuf.ensure(total)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "preview buffers allocation failed");
+    }
+    const LaunchCtx* c = uploadCtx(r);
+    if (c == nullptr) {
+        return fail(r, PT_ERR_CUDA, "launch context upload failed");
+    }
+    const int grid = r->smCount * adjointBlocksPerSm();
+    for (int lv = r->previewDone + 1; lv < r->previewLevels; ++lv) {
+        int w, h, ds;
+        previewDims(r->width, r->height, r->previewLevels, lv, w, h, ds);
+        launchPreview(c, w, h, static_cast<uint32_t>(lv + 1), kPreviewDepth,
+            r->previewBuf.p + previewOffset(r->width, r->height, r->previewLevels, lv), grid, r->stream);
+        PT_CHECK(r, cudaGetLastError());
+        r->launches += 1;
+        r->previewDone = lv;
     }
     return PT_OK;
 }
@@ -743,6 +804,7 @@ int pt_destroy(pt_renderer* r)
     r->displayBuf.release();
     r->adjImage.release();
     r->record.release();
+    r->previewBuf.release();
     r->adjGrad.release();
     r->compactTemp.release();
     r->sceneActiveStart.release();
@@ -965,6 +1027,14 @@ int pt_render(pt_renderer* r, int waves)
         const long long jobs0 = static_cast<long long>(std::max(r->hostActive, 1)) * B0;
         const int want = static_cast<int>(std::min<long long>(r->capacityWanted, std::max<long long>(jobs0, 1 << 16)));
         int st = ensurePaths(r, want);
+        if (st != PT_OK) {
+            return st;
+        }
+    }
+    if (r->previewLevels > 0 && r->wavesDone == 0 && r->previewDone < r->previewLevels - 1 && r->scenes.size() == 1) {
+        // the preview passes come first (PathTracer.cpp:2382-2396); iteration i
+        // renders level i with global seed i + 1
+        const int st = renderPreviews(r);
         if (st != PT_OK) {
             return st;
         }
@@ -1291,7 +1361,7 @@ int pt_rng_tape(pt_renderer* r, int first_wave, int waves, int stride, float* ou
     const size_t total = static_cast<size_t>(r->width) * r->height * waves * stride;
     float* d = nullptr;
     PT_CHECK(r, cudaMallocAsync(reinterpret_cast<void**>(&d), total * sizeof(float), r->stream));
-    launchRngTape(r->width, r->height, first_wave, waves, stride, d, r->stream);
+    launchRngTape(r->width, r->height, first_wave, waves, stride, r->previewLevels, d, r->stream);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) {
         e = cudaMemcpyAsync(out, d, total * sizeof(float), cudaMemcpyDeviceToHost, r->stream);
@@ -1553,8 +1623,16 @@ int pt_tonemap(pt_renderer* r, int scene, float exposure, uint8_t* rgba8)
     if (!r->displayBuf.ensure(4 * P)) {
         return fail(r, PT_ERR_OUT_OF_MEMORY, "display buffer allocation failed");
     }
-    launchTonemap(r->acc.p + sl.pixelBase, r->counts.p + sl.pixelBase, r->converged.p + sl.pixelBase,
-        static_cast<int>(P), r->params, exposure, r->displayBuf.p, r->stream);
+    if (scene == 0 && r->scenes.size() == 1 && r->previewLevels > 0 && r->wavesDone == 0 && r->previewDone >= 0) {
+        // no full-resolution wave yet: the finest preview, upsampled (PathTracer.cpp:1546-1552)
+        int w, h, ds;
+        previewDims(r->width, r->height, r->previewLevels, r->previewDone, w, h, ds);
+        launchTonemapPreview(r->previewBuf.p + previewOffset(r->width, r->height, r->previewLevels, r->previewDone),
+            w, h, ds, r->width, r->height, r->params, exposure, r->displayBuf.p, r->stream);
+    } else {
+        launchTonemap(r->acc.p + sl.pixelBase, r->counts.p + sl.pixelBase, r->converged.p + sl.pixelBase,
+            static_cast<int>(P), r->params, exposure, r->displayBuf.p, r->stream);
+    }
     PT_CHECK(r, cudaGetLastError());
     PT_CHECK(r, cudaMemcpyAsync(rgba8, r->displayBuf.p, 4 * P, cudaMemcpyDeviceToHost, r->stream));
     PT_CHECK(r, cudaStreamSynchronize(r->stream));
@@ -1673,6 +1751,109 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
     std::memset(grad, 0, sizeof(float) * grad_materials * kGradParams);
     std::memcpy(grad, g.data(), sizeof(float) * M * kGradParams);
     r->launches += 1;
+    return PT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Preview passes and region render (PathTracer.h:89-92, 134-140)
+// ---------------------------------------------------------------------------
+int pt_set_preview_levels(pt_renderer* r, int levels)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    // clampPreviewStepsPerLevel (PathTracer.cpp:181-190)
+    r->previewLevels = levels < 0 ? 0 : (levels > 128 ? 128 : levels);
+    PT_CHECK(r, cudaSetDevice(r->device));
+    return resetAccum(r);
+}
+
+int pt_render_previews(pt_renderer* r)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    if (r->width <= 0 || r->scenes.size() != 1 || !r->scenes[0].hasScene) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_render_previews needs a configured single scene with a mesh");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    if (r->previewLevels > 0 && r->wavesDone == 0 && r->previewDone < r->previewLevels - 1) {
+        const int st = renderPreviews(r);
+        if (st != PT_OK) {
+            return st;
+        }
+    }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    return PT_OK;
+}
+
+int pt_preview_readback(pt_renderer* r, int level, float* rgba, int* width, int* height)
+{
+    if (r == nullptr || level < 0 || level >= r->previewLevels) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_preview_readback: bad level %d", level);
+    }
+    if (level > r->previewDone) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_preview_readback: level %d not rendered since the last reset", level);
+    }
+    int w, h, ds;
+    previewDims(r->width, r->height, r->previewLevels, level, w, h, ds);
+    if (width != nullptr) {
+        *width = w;
+    }
+    if (height != nullptr) {
+        *height = h;
+    }
+    if (rgba != nullptr) {
+        PT_CHECK(r, cudaSetDevice(r->device));
+        PT_CHECK(r, cudaMemcpyAsync(rgba, r->previewBuf.p + previewOffset(r->width, r->height, r->previewLevels, level),
+            static_cast<size_t>(w) * h * sizeof(float4), cudaMemcpyDeviceToHost, r->stream));
+        PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    }
+    return PT_OK;
+}
+
+int pt_set_region(pt_renderer* r, int enabled, int min_x, int min_y, int max_x, int max_y)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    if (enabled && (r->scenes.size() != 1 || r->width <= 0)) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_set_region needs a configured single-scene renderer");
+    }
+    // PathTracer::setRenderRegion (PathTracer.cpp:1447-1463): ordered and clamped to the image
+    const int mx = std::max(0, r->width - 1), my = std::max(0, r->height - 1);
+    r->regionMinX = std::max(0, std::min(min_x, max_x));
+    r->regionMaxX = std::min(mx, std::max(min_x, max_x));
+    r->regionMinY = std::max(0, std::min(min_y, max_y));
+    r->regionMaxY = std::min(my, std::max(min_y, max_y));
+    r->regionEnabled = enabled != 0;
+    return pt_reset_region(r);
+}
+
+int pt_reset_region(pt_renderer* r)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    if (!r->regionEnabled) {
+        return resetAccum(r);
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    // PathTracer::resetRegionAccumulation: only the region is cleared, the rest
+    // of the image keeps its samples
+    r->activeSel = 0;
+    const LaunchCtx* dc = uploadCtx(r);
+    if (dc == nullptr) {
+        return fail(r, PT_ERR_CUDA, "launch context upload failed");
+    }
+    launchRegion(dc, r->width, r->regionMinX, r->regionMinY, r->regionMaxX, r->regionMaxY, true, r->stream);
+    PT_CHECK(r, cudaGetLastError());
+    r->hostActive = (r->regionMaxX - r->regionMinX + 1) * (r->regionMaxY - r->regionMinY + 1);
+    r->lastStopRate = 1.0;
+    r->wavesDone = 0;
+    r->samplesDone = 0;
+    r->recordValid = false;
+    r->previewDone = -1;
     return PT_OK;
 }
 

@@ -42,7 +42,38 @@ __global__ void k_tonemap(const float4* acc, const uint32_t* counts, const uint8
     }
 }
 
+// The preview shown at full resolution (pathTracerUpsamplePreviewToPbo,
+// PathTracer.cu:883-920): nearest preview pixel x / downscale, clamped.
+__global__ void k_tonemap_preview(const float4* preview, int pw, int ph, int downscale, int width, int height,
+    pt_render_params params, float exposure, uchar4* out)
+{
+    const int n = width * height;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (params.debug_overlay_mode == kDebugOverlayAdaptiveSampling) {
+            out[i] = make_uchar4(255, 0, 0, 255);
+            continue;
+        }
+        const int x = i % width, y = i / width;
+        const int px = min(x / downscale, pw - 1), py = min(y / downscale, ph - 1);
+        const float4 v = preview[py * pw + px];
+        out[i] = make_uchar4(quantise(reinhard(v.x, exposure)), quantise(reinhard(v.y, exposure)),
+            quantise(reinhard(v.z, exposure)), 255);
+    }
+}
+
 } // namespace
+
+void launchTonemapPreview(const float4* preview, int pw, int ph, int downscale, int width, int height,
+    const pt_render_params& params, float exposure, uint8_t* out, cudaStream_t s)
+{
+    const int pixels = width * height;
+    if (pixels <= 0) {
+        return;
+    }
+    const int grid = (pixels + 255) / 256 < 148 * 32 ? (pixels + 255) / 256 : 148 * 32;
+    k_tonemap_preview<<<grid, 256, 0, s>>>(preview, pw, ph, downscale, width, height, params, exposure,
+        reinterpret_cast<uchar4*>(out));
+}
 
 void launchTonemap(const float4* acc, const uint32_t* counts, const uint8_t* converged, int pixels,
     const pt_render_params& params, float exposure, uint8_t* out, cudaStream_t s)

@@ -154,7 +154,7 @@ __device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigne
         local = pixel;
     }
     const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
-    const uint32_t globalSeed = bt.waveBase + slot + 1u;
+    const uint32_t globalSeed = bt.waveBase + slot + 1u + static_cast<uint32_t>(c.seedOffset);
     curandStateXORWOW st;
     curand_init(pathSeed(c.params, local, width, sampleIndex, globalSeed), 0ull, 0ull, &st);
     const uint32_t x = local % width, y = local / width;
@@ -738,7 +738,32 @@ __global__ void __launch_bounds__(256) k_trace_rays(DevScene S, int n, const flo
     }
 }
 
-__global__ void k_rng_tape(int width, int height, int firstWave, int waves, int stride, float* out)
+// Region render (clearRegionAccumulatorKernel, PathTracer.cu:305-344): clears
+// the accumulators of the pixels in [minX, maxX] x [minY, maxY] when `clear`
+// and makes them the active list, row by row (so it stays sorted).
+__global__ void k_region(const LaunchCtx* __restrict__ cp, int width, int minX, int minY, int maxX, int maxY, bool clear)
+{
+    const LaunchCtx& c = *cp;
+    const int rw = maxX - minX + 1, rh = maxY - minY + 1;
+    const int n = rw * rh;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int idx = (minY + t / rw) * width + minX + t % rw;
+        if (clear) {
+            c.acc.acc[idx] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            c.acc.counts[idx] = 0;
+            c.acc.lumMean[idx] = 0.0f;
+            c.acc.m2[idx] = 0.0f;
+            c.acc.converged[idx] = 0;
+        }
+        c.acc.active[0][t] = idx;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c.acc.activeCount[0] = n;
+        c.acc.activeCount[1] = 0;
+    }
+}
+
+__global__ void k_rng_tape(int width, int height, int firstWave, int waves, int stride, int seedOffset, float* out)
 {
     const long long P = static_cast<long long>(width) * height;
     const long long total = P * waves;
@@ -747,7 +772,7 @@ __global__ void k_rng_tape(int width, int height, int firstWave, int waves, int 
         const uint32_t w = static_cast<uint32_t>(k / P);
         const uint32_t p = static_cast<uint32_t>(k % P);
         const uint32_t wave = static_cast<uint32_t>(firstWave) + w;
-        const uint32_t seed = p * 747796405u + wave + (wave + 1u) * 2891336453u;
+        const uint32_t seed = p * 747796405u + wave + (wave + 1u + static_cast<uint32_t>(seedOffset)) * 2891336453u;
         curandStateXORWOW st;
         curand_init(seed, 0ull, 0ull, &st);
         float* row = out + k * stride;
@@ -833,10 +858,16 @@ void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, c
 {
     k_trace_rays<<<gridFor(n), 256, 0, s>>>(S, n, o, d, tmin, tmax, hit, t, tri, normal, uv);
 }
-void launchRngTape(int width, int height, int firstWave, int waves, int stride, float* out, cudaStream_t s)
+void launchRngTape(int width, int height, int firstWave, int waves, int stride, int seedOffset, float* out,
+    cudaStream_t s)
 {
     k_rng_tape<<<gridFor(static_cast<long long>(width) * height * waves), 256, 0, s>>>(width, height, firstWave, waves,
-        stride, out);
+        stride, seedOffset, out);
+}
+void launchRegion(const LaunchCtx* c, int width, int minX, int minY, int maxX, int maxY, bool clear, cudaStream_t s)
+{
+    const long long n = static_cast<long long>(maxX - minX + 1) * (maxY - minY + 1);
+    k_region<<<gridFor(n), 256, 0, s>>>(c, width, minX, minY, maxX, maxY, clear);
 }
 
 } // namespace pt

@@ -99,6 +99,10 @@ struct LaunchCtx {
     // [sample index][pixel], for samples 0 .. recordSpp - 1 (the adjoint's input)
     float4* record;
     int recordSpp;
+    // preview passes rendered before the full-resolution waves: wave w draws with
+    // global seed seedOffset + w + 1 (the reference counts its preview passes as
+    // iterations, PathTracer.cpp:2379)
+    int seedOffset;
 };
 
 // Launchers. The LaunchCtx lives in DEVICE memory (one per renderer) and is
@@ -125,6 +129,10 @@ void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, c
     uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s);
 // Resident blocks per SM of the stage kernels (occupancy calculator).
 void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks);
-void launchRngTape(int width, int height, int firstWave, int waves, int stride, float* out, cudaStream_t s);
+void launchRngTape(int width, int height, int firstWave, int waves, int stride, int seedOffset, float* out,
+    cudaStream_t s);
+// Region render: the pixels of [minX, maxX] x [minY, maxY] become the active
+// list (their accumulators cleared when `clear`).
+void launchRegion(const LaunchCtx* c, int width, int minX, int minY, int maxX, int maxY, bool clear, cudaStream_t s);
 
 } // namespace pt

@@ -67,7 +67,8 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_set_tuning", "pt_trace_soup_noalloc", "pt_batch_configure", "pt_batch_set_mesh",
                     "pt_batch_set_camera", "pt_batch_readback", "pt_batch_set_tubes", "pt_export_mesh",
                     "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
-                    "pt_record_samples"]
+                    "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
+                    "pt_reset_region"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -121,6 +122,11 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_set_materials.argtypes = [vp, C.c_int, C.c_uint32, vp]
     L.pt_backward.argtypes = [vp, _fp, C.c_int, C.c_int, _fp, C.c_uint32, C.POINTER(C.c_double)]
     L.pt_record_samples.argtypes = [vp, C.c_int]
+    L.pt_set_preview_levels.argtypes = [vp, C.c_int]
+    L.pt_render_previews.argtypes = [vp]
+    L.pt_preview_readback.argtypes = [vp, C.c_int, _fp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.pt_set_region.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.pt_reset_region.argtypes = [vp]
     _LIB = L
     return L
 
@@ -371,6 +377,30 @@ class PathTracer:
     def exposure_multiplier(f_stop: float, shutter_seconds: float, iso: float) -> float:
         """PhysicalCamera::exposureMultiplier (PhysicalCamera.cpp:392-397)."""
         return float(load_library().pt_exposure_multiplier(float(f_stop), float(shutter_seconds), float(iso)))
+
+    # -- preview passes and region render (PathTracer.h:89-92, 134-140) --------
+    def set_preview_steps_per_level(self, levels: int):
+        """PathTracer::setPreviewStepsPerLevel: low-resolution preview passes before full resolution."""
+        self._check(self._lib.pt_set_preview_levels(self._h, int(levels)))
+
+    def render_previews(self):
+        """Renders the preview passes (pt_render does it before its first wave anyway)."""
+        self._check(self._lib.pt_render_previews(self._h))
+
+    def preview(self, level: int) -> np.ndarray:
+        w, h = C.c_int(), C.c_int()
+        self._check(self._lib.pt_preview_readback(self._h, int(level), None, C.byref(w), C.byref(h)))
+        out = np.empty((h.value, w.value, 4), np.float32)
+        self._check(self._lib.pt_preview_readback(self._h, int(level), _ptr(out, _fp), C.byref(w), C.byref(h)))
+        return out
+
+    def set_render_region(self, min_x: int, min_y: int, max_x: int, max_y: int, enabled: bool = True):
+        """setRegionRenderEnabled + setRenderRegion: only the rectangle takes samples."""
+        self._check(self._lib.pt_set_region(self._h, int(bool(enabled)), int(min_x), int(min_y), int(max_x),
+                                            int(max_y)))
+
+    def reset_region_accumulation(self):
+        self._check(self._lib.pt_reset_region(self._h))
 
     # -- differentiation (no reference counterpart) -----------------------------
     GRAD_PARAMS = ("r", "g", "b", "roughness", "metallic", "sheen", "emission")

@@ -121,6 +121,8 @@ class Checker:
             L.orc_trace_rays_bruteforce.argtypes = [C.c_void_p, C.c_int, _fp, _fp, _fp, _fp, _u8p, _fp, _u32p]
             L.orc_reference_seed.restype = C.c_uint
             L.orc_reference_seed.argtypes = [C.c_int, C.c_int, C.c_uint]
+            L.orc_render_preview.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, _fp,
+                                             C.c_int, _fp]
             L.orc64_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                          _fp, C.c_int, _fp, _dp, C.c_int, C.c_int]
 
@@ -332,6 +334,16 @@ class CheckerScene:
                                           width, height, int(spp), _ptr(tp, _fp), int(tape_stride), _ptr(d, _fp),
                                           _ptr(g, _dp), int(materials), int(threads))
         return g, int(err)
+
+    def render_preview(self, camera, params, width, height, tape, tape_stride, env=None):
+        """One preview pass (pixel centres, one sample, the caller's params) from a tape [pixel][stride]."""
+        assert self.chk.kind == "oracle"
+        camera_, params_ = _rec(camera), _rec(params)
+        tp = np.ascontiguousarray(tape, np.float32)
+        out = np.zeros((height, width, 4), np.float32)
+        err = self.chk.lib.orc_render_preview(self.h, env.h if env is not None else None, _vp(camera_), _vp(params_),
+                                              width, height, _ptr(tp, _fp), int(tape_stride), _ptr(out, _fp))
+        return out, int(err)
 
     def trace_pixel(self, camera, params, width, height, idx, sample_index, global_seed, tape_row, env=None):
         camera_ = _rec(camera)

@@ -434,6 +434,41 @@ int orc_trace_pixel(void* scene, void* env, const void* camBytes, const void* pa
     return rng.underruns != 0 ? -1 : rng.cursor;
 }
 
+// One preview pass (sampleKernel with previewPass, PathTracer.cu:132-184): per
+// pixel, tape row idx, no jitter draws (pixel centre), lens draws, the path
+// with the given params (the caller sets the preview depth), firefly clamp.
+int orc_render_preview(void* scene, void* env, const void* camBytes, const void* paramsBytes, int width, int height,
+    const float* tape, int tapeStride, float* outRgba)
+{
+    CameraRec cam;
+    std::memcpy(&cam, camBytes, sizeof(cam));
+    ParamsRec p;
+    std::memcpy(&p, paramsBytes, sizeof(p));
+    const Scene& s = *static_cast<Scene*>(scene);
+    const Env* e = static_cast<Env*>(env);
+    int errors = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : errors)
+    for (int idx = 0; idx < width * height; ++idx) {
+        Rng rng;
+        rng.row = tape + static_cast<size_t>(idx) * tapeStride;
+        rng.length = tapeStride;
+        const int x = idx % width, y = idx / width;
+        const float u = (static_cast<float>(x) + 0.5f) / static_cast<float>(width);
+        const float v = (static_cast<float>(y) + 0.5f) / static_cast<float>(height);
+        const float l1 = rng.next();
+        const float l2 = rng.next();
+        V3<float> ro, rd;
+        cameraRay(cam, u, v, l1, l2, ro, rd);
+        const V3<float> c = clampFirefly(tracePath(s, e, &p, ro, rd, rng));
+        outRgba[4 * idx] = c.x;
+        outRgba[4 * idx + 1] = c.y;
+        outRgba[4 * idx + 2] = c.z;
+        outRgba[4 * idx + 3] = 1.0f;
+        errors += rng.underruns;
+    }
+    return errors;
+}
+
 void orc_brdf_eval(const float* normal, const float* wo, const void* material, float eta, int debug, const float* wi,
     float* outRgb)
 {
