@@ -345,6 +345,11 @@ int pt_record_samples(pt_renderer* r, int spp);
 int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, float* grad, uint32_t grad_materials,
     double* device_ms);
 
+/* The environment's importance tables as built on the device
+ * (EnvironmentMap.cpp:76-128): marginal CDF (height + 1 floats) and row CDFs
+ * (height x (width + 1)), HOST outputs, either may be NULL. */
+int pt_environment_tables(pt_renderer* r, float* marginal, float* row);
+
 /* ---- Preview passes and region render ------------------------------------ */
 /* PathTracer::setPreviewStepsPerLevel (PathTracer.h:89-92): with n > 0 (at
  * most 128), pt_render first renders n low-resolution preview passes, level i

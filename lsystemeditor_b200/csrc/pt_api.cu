@@ -116,6 +116,7 @@ struct pt_renderer {
 
     // environment
     DevBuf<float> envPixels, envMarginal, envRow;
+    DevBuf<float> envScratch;             // sin(theta) per row and row totals of the table build
     int envW = 0, envH = 0;
     bool envValid = false;
 
@@ -792,6 +793,7 @@ int pt_destroy(pt_renderer* r)
     r->envPixels.release();
     r->envMarginal.release();
     r->envRow.release();
+    r->envScratch.release();
     r->acc.release();
     r->counts.release();
     r->lumMean.release();
@@ -944,43 +946,24 @@ int pt_set_environment(pt_renderer* r, int width, int height, const float* rgb)
     if (width <= 0 || height <= 0) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_environment: bad size %dx%d", width, height);
     }
-    // importance tables, EnvironmentMap.cpp:76-128 (sequential float sums)
+    // importance tables (EnvironmentMap.cpp:76-128) built on the device with the
+    // reference's sequential single-precision sums; only sin(theta) per row is
+    // evaluated here, with the reference's host expression
     const size_t W = static_cast<size_t>(width), H = static_cast<size_t>(height);
-    std::vector<float> marginal(H + 1, 0.0f), row(H * (W + 1), 0.0f), rowW(H, 0.0f);
+    std::vector<float> sinTheta(H);
     for (size_t y = 0; y < H; ++y) {
         const float v = (static_cast<float>(y) + 0.5f) / static_cast<float>(height);
-        const float st = std::sin(v * 3.14159265f);
-        float sum = 0.0f;
-        const size_t off = y * (W + 1);
-        for (size_t x = 0; x < W; ++x) {
-            const float* px = rgb + (y * W + x) * 3;
-            const float l = std::max(px[0], std::max(px[1], px[2]));
-            sum += std::max(l, 1.0e-6f) * st;
-            row[off + x + 1] = sum;
-        }
-        if (sum > 0.0f) {
-            for (size_t x = 0; x < W; ++x) {
-                row[off + x + 1] /= sum;
-            }
-        }
-        rowW[y] = sum;
+        sinTheta[y] = std::sin(v * 3.14159265f);
     }
-    float total = 0.0f;
-    for (size_t y = 0; y < H; ++y) {
-        total += rowW[y];
-        marginal[y + 1] = total;
-    }
-    if (total > 0.0f) {
-        for (size_t y = 0; y < H; ++y) {
-            marginal[y + 1] /= total;
-        }
-    }
-    if (!r->envPixels.ensure(W * H * 3) || !r->envMarginal.ensure(H + 1) || !r->envRow.ensure(H * (W + 1))) {
+    if (!r->envPixels.ensure(W * H * 3) || !r->envMarginal.ensure(H + 1) || !r->envRow.ensure(H * (W + 1)) ||
+        !r->envScratch.ensure(2 * H)) {
         return fail(r, PT_ERR_OUT_OF_MEMORY, "environment upload failed");
     }
     PT_CHECK(r, cudaMemcpyAsync(r->envPixels.p, rgb, W * H * 3 * sizeof(float), cudaMemcpyHostToDevice, r->stream));
-    PT_CHECK(r, cudaMemcpyAsync(r->envMarginal.p, marginal.data(), marginal.size() * sizeof(float), cudaMemcpyHostToDevice, r->stream));
-    PT_CHECK(r, cudaMemcpyAsync(r->envRow.p, row.data(), row.size() * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PT_CHECK(r, cudaMemcpyAsync(r->envScratch.p, sinTheta.data(), H * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    launchEnvTables(r->envPixels.p, width, height, r->envScratch.p, r->envMarginal.p, r->envRow.p, r->envScratch.p + H,
+        r->stream);
+    PT_CHECK(r, cudaGetLastError());
     PT_CHECK(r, cudaStreamSynchronize(r->stream));
     r->envW = width;
     r->envH = height;
@@ -1854,6 +1837,23 @@ int pt_reset_region(pt_renderer* r)
     r->samplesDone = 0;
     r->recordValid = false;
     r->previewDone = -1;
+    return PT_OK;
+}
+
+int pt_environment_tables(pt_renderer* r, float* marginal, float* row)
+{
+    if (r == nullptr || !r->envValid) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_environment_tables: no environment map");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const size_t W = static_cast<size_t>(r->envW), H = static_cast<size_t>(r->envH);
+    if (marginal != nullptr) {
+        PT_CHECK(r, cudaMemcpyAsync(marginal, r->envMarginal.p, (H + 1) * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+    }
+    if (row != nullptr) {
+        PT_CHECK(r, cudaMemcpyAsync(row, r->envRow.p, H * (W + 1) * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+    }
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
     return PT_OK;
 }
 

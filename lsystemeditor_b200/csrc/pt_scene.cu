@@ -306,7 +306,61 @@ __global__ void k_unpack_shade(const TriShade* shade, uint32_t n, float* nrm, fl
     }
 }
 
+// std::max as the reference uses it: (a < b) ? b : a.
+__device__ __forceinline__ float stdMax(float a, float b) { return a < b ? b : a; }
+
+// Environment importance tables (EnvironmentMap.cpp:76-128), one thread per
+// row: the row's running sum of max(r, g, b) (at least 1e-6) times sin(theta)
+// in single precision, in column order, then divided by the row total.
+__global__ void k_env_rows(const float* rgb, int width, int height, const float* sinTheta, float* row, float* rowW)
+{
+    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < height; y += gridDim.x * blockDim.x) {
+        const float st = sinTheta[y];
+        const size_t off = static_cast<size_t>(y) * (width + 1);
+        const float* px = rgb + static_cast<size_t>(y) * width * 3;
+        float sum = 0.0f;
+        row[off] = 0.0f;
+        for (int x = 0; x < width; ++x) {
+            const float l = stdMax(px[3 * x], stdMax(px[3 * x + 1], px[3 * x + 2]));
+            sum = __fadd_rn(sum, __fmul_rn(stdMax(l, 1.0e-6f), st));
+            row[off + x + 1] = sum;
+        }
+        if (sum > 0.0f) {
+            for (int x = 0; x < width; ++x) {
+                row[off + x + 1] = __fdiv_rn(row[off + x + 1], sum);
+            }
+        }
+        rowW[y] = sum;
+    }
+}
+
+// The marginal over rows, summed in row order by one thread.
+__global__ void k_env_marginal(const float* rowW, int height, float* marginal)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) {
+        return;
+    }
+    float total = 0.0f;
+    marginal[0] = 0.0f;
+    for (int y = 0; y < height; ++y) {
+        total = __fadd_rn(total, rowW[y]);
+        marginal[y + 1] = total;
+    }
+    if (total > 0.0f) {
+        for (int y = 0; y < height; ++y) {
+            marginal[y + 1] = __fdiv_rn(marginal[y + 1], total);
+        }
+    }
+}
+
 } // namespace
+
+void launchEnvTables(const float* rgb, int width, int height, const float* sinTheta, float* marginal, float* row,
+    float* rowW, cudaStream_t s)
+{
+    k_env_rows<<<(height + 127) / 128, 128, 0, s>>>(rgb, width, height, sinTheta, row, rowW);
+    k_env_marginal<<<1, 32, 0, s>>>(rowW, height, marginal);
+}
 
 void launchRingFrames(const TubeSetDev& t, double* frames, cudaStream_t s)
 {

@@ -56,4 +56,11 @@ void launchBuildShade(const float* normals, const float* uvs, const uint32_t* ma
 void launchUnpackShade(const TriShade* shade, uint32_t n, float* normals, float* uvs, uint32_t* materialIds,
     cudaStream_t s);
 
+// Environment-map importance tables on the device (EnvironmentMap.cpp:76-128,
+// same single-precision sums in the same order): row CDFs [H][W + 1] and the
+// marginal [H + 1] from the RGB pixels and the per-row sin(theta) (computed on
+// the host with the reference's expression).  rowW: H floats of scratch.
+void launchEnvTables(const float* rgb, int width, int height, const float* sinTheta, float* marginal, float* row,
+    float* rowW, cudaStream_t s);
+
 } // namespace pt

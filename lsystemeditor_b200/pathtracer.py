@@ -68,7 +68,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_batch_set_camera", "pt_batch_readback", "pt_batch_set_tubes", "pt_export_mesh",
                     "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
-                    "pt_reset_region"]
+                    "pt_reset_region", "pt_environment_tables"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -127,6 +127,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_preview_readback.argtypes = [vp, C.c_int, _fp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.pt_set_region.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.pt_reset_region.argtypes = [vp]
+    L.pt_environment_tables.argtypes = [vp, _fp, _fp]
     _LIB = L
     return L
 
@@ -269,6 +270,13 @@ class PathTracer:
         self._check(self._lib.pt_set_environment(self._h, a.shape[1], a.shape[0], _ptr(a, _fp)))
 
     # -- rendering --------------------------------------------------------
+    def environment_tables(self, width: int, height: int):
+        """The environment map's marginal and row CDFs as built on the device."""
+        marg = np.empty(height + 1, np.float32)
+        row = np.empty((height, width + 1), np.float32)
+        self._check(self._lib.pt_environment_tables(self._h, _ptr(marg, _fp), _ptr(row, _fp)))
+        return marg, row
+
     def reset_accumulation(self):
         self._check(self._lib.pt_reset(self._h))
 

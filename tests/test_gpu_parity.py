@@ -163,3 +163,23 @@ def test_rng_tape_consumption_bound(tracer, oracle):
         assert n >= 0
         used.append(n)
     assert max(used) <= 116 and min(used) >= 4
+
+
+@pytest.mark.parametrize("shape", [(64, 32), (257, 129), (1024, 512)])
+def test_environment_tables_built_on_device_match_reference_build(tracer, oracle, ref, shape):
+    """The importance tables are built on the device with the reference's
+    single-precision sums in the reference's order: bit-identical to the
+    reference compiled for the host (EnvironmentMap.cpp:76-128)."""
+    w, h = shape
+    rng = np.random.default_rng(w)
+    img = rng.uniform(0.0, 2.0, (h, w, 3)).astype(np.float32)
+    img[h // 3, w // 4] = [50.0, 40.0, 30.0]
+    img[:, w // 2] = 0.0
+    tracer.configure(8, 8, random_soup(10, seed=1))
+    tracer.set_environment(img)
+    marg, row = tracer.environment_tables(w, h)
+    for chk in (oracle, ref):
+        m_ref, r_ref = chk.env(img).tables()
+        assert np.array_equal(marg, np.asarray(m_ref).reshape(-1)), chk
+        assert np.array_equal(row.reshape(-1), np.asarray(r_ref).reshape(-1)), chk
+    tracer.set_environment(None)
