@@ -277,8 +277,8 @@ __device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 del
             const float3 wi = envSample(c.env, u1, u2, lp);
             if (lp > kMinPdf) {
                 const float ct = fmax2(0.0f, dot3(n, wi));
-                if (ct > 0.0f) {
-                    const float3 Le = envEval(c.env, c.params, wi);
+                const float3 Le = envEval(c.env, c.params, wi);
+                if (ct > 0.0f && (Le.x != 0.0f || Le.y != 0.0f || Le.z != 0.0f)) {
                     const float3 f = bsdfEval(cx, wi);
                     const float bp = bsdfPdf(cx, wi);
                     const float kk = misBalance(lp, bp) * ct / lp;
@@ -314,20 +314,20 @@ __device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 del
                     const float cl = fmax2(0.0f, dot3(ln, scl3(wi, -1.0f)));
                     if (ct > 0.0f && cl > 0.0f) {
                         const float lpdf = ap * d2 / cl;
-                        if (lpdf > kMinPdf) {
+                        const float3 so = add3(pos, scl3(wi, kShadowBias));
+                        const float3 sdn = xnormalize(wi);
+                        bool occludedBySelf = false;
+                        if (!isDegenerateDir(sdn)) {
+                            float th, tu2, tv2;
+                            occludedBySelf = intersectTriExact(so, sdn, ev0, ev1, ev2, kShadowBias, kRayTMax, th, tu2,
+                                                 tv2) && th < kRayTMax;
+                        }
+                        if (lpdf > kMinPdf && !occludedBySelf) {
                             const float3 f = bsdfEval(cx, wi);
                             const float bp = bsdfPdf(cx, wi);
                             const float kk = misBalance(lpdf, bp) * ct / lpdf;
                             const float3 contrib = mul3(T, mul3(f, scl3(Le, kk)));
-                            const float3 so = add3(pos, scl3(wi, kShadowBias));
-                            const float3 sdn = xnormalize(wi);
-                            bool occludedBySelf = false;
-                            if (!isDegenerateDir(sdn)) {
-                                float th, tu2, tv2;
-                                occludedBySelf = intersectTriExact(so, sdn, ev0, ev1, ev2, kShadowBias, kRayTMax, th,
-                                                     tu2, tv2) && th < kRayTMax;
-                            }
-                            if (!occludedBySelf && (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f)) {
+                            if (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f) {
                                 HitRec hh;
                                 if (!traceRay<true, false>(S, so, sdn, kShadowBias, kRayTMax, hh, nullptr, nullptr,
                                         sstack, kAdjointBlock)) {

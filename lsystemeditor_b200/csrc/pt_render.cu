@@ -369,8 +369,10 @@ __global__ void __launch_bounds__(256, 3) k_shade(const LaunchCtx* __restrict__ 
                 const float3 wi = envSample(c.env, u1, u2, lp);
                 if (lp > kMinPdf) {
                     const float ct = fmax2(0.0f, dot3(n, wi));
-                    if (ct > 0.0f) {
-                        const float3 Le = envEval(c.env, c.params, wi);
+                    const float3 Le = envEval(c.env, c.params, wi);
+                    // A light of exactly zero radiance (a black background) contributes
+                    // exactly zero for any finite BSDF value: the BSDF is not evaluated.
+                    if (ct > 0.0f && (Le.x != 0.0f || Le.y != 0.0f || Le.z != 0.0f)) {
                         const float3 f = bsdfEval(cx, wi);
                         const float bp = bsdfPdf(cx, wi);
                         const float k = misBalance(lp, bp) * ct / lp;
@@ -405,26 +407,27 @@ __global__ void __launch_bounds__(256, 3) k_shade(const LaunchCtx* __restrict__ 
                         const float cl = fmax2(0.0f, dot3(ln, scl3(wi, -1.0f)));
                         if (ct > 0.0f && cl > 0.0f) {
                             const float lp = ap * d2 / cl;
-                            if (lp > kMinPdf) {
+                            // The reference's emissive shadow ray runs to tMax = 1e6
+                            // (LightSamplingCore.h:360-369), so the sampled emitter triangle
+                            // itself occludes it whenever the ray hits that triangle.  An
+                            // any-hit query is true as soon as one triangle is hit, so testing
+                            // the emitter first (same origin, direction and rounding as the
+                            // shadow stage) decides those rays without a traversal -- and
+                            // without evaluating the BSDF for a term that adds nothing.
+                            const float3 so = add3(pos, scl3(wi, kShadowBias));
+                            const float3 sdn = xnormalize(wi);
+                            bool occludedBySelf = false;
+                            if (!isDegenerateDir(sdn)) {
+                                float th, tu2, tv2;
+                                occludedBySelf = intersectTriExact(so, sdn, ev0, ev1, ev2, kShadowBias, kRayTMax, th,
+                                                     tu2, tv2) && th < kRayTMax;
+                            }
+                            if (lp > kMinPdf && !occludedBySelf) {
                                 const float3 f = bsdfEval(cx, wi);
                                 const float bp = bsdfPdf(cx, wi);
                                 const float k = misBalance(lp, bp) * ct / lp;
                                 const float3 contrib = mul3(T, mul3(f, scl3(Le, k)));
-                                // The reference's emissive shadow ray runs to tMax = 1e6
-                                // (LightSamplingCore.h:360-369), so the sampled emitter triangle
-                                // itself occludes it whenever the ray hits that triangle.  An
-                                // any-hit query is true as soon as one triangle is hit, so testing
-                                // the emitter first (same origin, direction and rounding as the
-                                // shadow stage) decides those rays without a traversal.
-                                const float3 so = add3(pos, scl3(wi, kShadowBias));
-                                const float3 sdn = xnormalize(wi);
-                                bool occludedBySelf = false;
-                                if (!isDegenerateDir(sdn)) {
-                                    float th, tu2, tv2;
-                                    occludedBySelf = intersectTriExact(so, sdn, ev0, ev1, ev2, kShadowBias, kRayTMax, th,
-                                                         tu2, tv2) && th < kRayTMax;
-                                }
-                                if (!occludedBySelf && (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f)) {
+                                if (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f) {
                                     c.paths.neeEmis[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
                                     const uint32_t s = warpPush(&c.q.counts[2]);
                                     c.q.shadowPath[s] = i | 0x80000000u;
