@@ -59,12 +59,22 @@ struct DeviceArena {
     }
 };
 
+// Tuning knobs (compile-time; the defaults are the measured best).
+#ifndef PT_BVH_LEAF_SIZE
+#define PT_BVH_LEAF_SIZE 3
+#endif
+#ifndef PT_BVH_TREELET_PASSES
+#define PT_BVH_TREELET_PASSES 1
+#endif
+#ifndef PT_BVH_COST_NODE
+#define PT_BVH_COST_NODE 1.2f
+#endif
 struct BvhBuildOptions {
-    int maxLeafSize = 3;        // triangles per compressed-node leaf (1..3)
-    int treeletPasses = 1;      // treelet SAH reordering passes (0 = plain LBVH)
-    int treeletMinLeaves = 16;  // subtrees smaller than this are left as built
-    float costTriangle = 1.0f;  // SAH cost of one triangle test
-    float costNode = 1.2f;      // SAH cost of one node visit
+    int maxLeafSize = PT_BVH_LEAF_SIZE;          // triangles per compressed-node leaf (1..3)
+    int treeletPasses = PT_BVH_TREELET_PASSES;   // treelet SAH reordering passes (0 = plain LBVH)
+    int treeletMinLeaves = 16;                   // subtrees smaller than this are left as built
+    float costTriangle = 1.0f;                   // SAH cost of one triangle test
+    float costNode = PT_BVH_COST_NODE;           // SAH cost of one node visit
 };
 
 struct BvhBuffers {

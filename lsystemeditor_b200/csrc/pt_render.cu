@@ -219,7 +219,13 @@ __global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ 
 // Counters: [4 + 2p] misses and [5 + 2p] hits of bounce parity p; this kernel
 // zeroes the other parity's pair for the next bounce.
 template <bool Count>
-__global__ void __launch_bounds__(256, 4) k_extend(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
+#ifndef PT_EXTEND_MIN_BLOCKS
+#define PT_EXTEND_MIN_BLOCKS 4
+#endif
+#ifndef PT_SHADE_MIN_BLOCKS
+#define PT_SHADE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
 {
     const LaunchCtx& c = *cp;
     extern __shared__ uint2 smemStack[];
@@ -302,7 +308,7 @@ __global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict_
 }
 
 // Shading of the paths that hit a triangle. One thread per queued path.
-__global__ void __launch_bounds__(256, 3) k_shade(const LaunchCtx* __restrict__ cp, int sel, int iter)
+__global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const LaunchCtx* __restrict__ cp, int sel, int iter)
 {
     const LaunchCtx& c = *cp;
     const unsigned int count = c.q.counts[5 + 2 * (iter & 1)];

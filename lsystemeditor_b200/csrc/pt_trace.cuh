@@ -24,9 +24,16 @@
 
 namespace pt {
 
-constexpr int kTraversalStack = 32;   // entries of the local-memory stack (fallback / Q1 path)
-constexpr int kSharedStack = 20;      // entries per thread of the shared-memory stack
-constexpr int kPostponeLanes = 8;     // postpone triangle tests when fewer lanes want them
+// Tuning knobs (compile-time; the defaults are the measured best).
+#ifndef PT_SHARED_STACK
+#define PT_SHARED_STACK 20
+#endif
+#ifndef PT_POSTPONE_LANES
+#define PT_POSTPONE_LANES 8
+#endif
+constexpr int kTraversalStack = 32;                 // entries of the local-memory stack (fallback / Q1 path)
+constexpr int kSharedStack = PT_SHARED_STACK;       // entries per thread of the shared-memory stack
+constexpr int kPostponeLanes = PT_POSTPONE_LANES;   // postpone triangle tests when fewer lanes want them
 constexpr float kSlabWiden = 1.0000005f;
 
 struct HitRec {
