@@ -108,7 +108,7 @@ typedef struct pt_render_params {
     uint32_t seed_value;
     int32_t adaptive_criterion; /* 0: relative std-dev (reference); 1: relative std-error */
     int32_t samples_per_launch; /* waves traced per launch; 0 = automatic */
-    int32_t reserved;
+    int32_t spectral_wavelengths; /* 0: RGB (reference); 4 or 8: hero-wavelength spectral samples */
 } pt_render_params;
 
 /* Triangle soup in structure-of-arrays form: HostMesh + HostTriangle
@@ -349,6 +349,33 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
  * (EnvironmentMap.cpp:76-128): marginal CDF (height + 1 floats) and row CDFs
  * (height x (width + 1)), HOST outputs, either may be NULL. */
 int pt_environment_tables(pt_renderer* r, float* marginal, float* row);
+
+/* ---- Spectral mode (extension; the reference's integrator is RGB) ---------
+ * With pt_render_params.spectral_wavelengths = 4 or 8, every path carries
+ * that many wavelengths spread evenly over [380, 780] nm from a hero
+ * wavelength drawn per (pixel, sample) (Wilkie et al., EGSR 2014); colours
+ * (materials, textures, background, environment texels, emitters) become
+ * spectra s(lambda) = scale * (1/2 + x / (2 sqrt(1 + x^2))),
+ * x = c0 lambda^2 + c1 lambda + c2 (the function space of the reference's
+ * Spectral/Rgb2Spec.h:58-66, Jakob and Hanika 2019), and each sample is
+ * converted to linear sRGB through CIE 1931 x 2-degree colour matching
+ * weighted by D65 (Spectral/SpectralCore.h:128-139) before accumulation.
+ * Previews and pt_backward stay RGB (pt_backward rejects a spectral render
+ * with PT_ERR_UNSUPPORTED). */
+
+/* The sRGB response per nm, 401 entries (380 .. 780 nm) x 3 floats, HOST
+ * output: a spectrum L gives RGB = integral L(lambda) response(lambda) dlambda;
+ * each channel sums to 1 by the trapezoid rule, so L = 1 gives (1, 1, 1).
+ * Optionally (each output may be NULL) the data it is built from: cie =
+ * x-bar, y-bar, z-bar and D65 at 380 .. 780 nm every 10 nm (41 x 4 floats),
+ * xyz_to_rgb = the XYZ -> linear sRGB matrix (3 x 3, row-major).  Needs no GPU. */
+int pt_spectral_response(float* rgb, float* cie, float* xyz_to_rgb);
+
+/* Spectrum coefficients (c0, c1, c2, scale; lambda in nm) of `count` RGB
+ * colours (radiance rules: negative channels 0, colours brighter than 1 scaled
+ * by their largest channel), HOST arrays, as the renderer uses them.  Needs
+ * no GPU. */
+int pt_spectral_uplift(uint32_t count, const float* rgb, float* coef);
 
 /* ---- Preview passes and region render ------------------------------------ */
 /* PathTracer::setPreviewStepsPerLevel (PathTracer.h:89-92): with n > 0 (at

@@ -9,9 +9,12 @@
 #include "pt_adjoint.cuh"
 #include "pt_output.cuh"
 #include "pt_scene.cuh"
+#include "pt_spectral.cuh"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -62,6 +65,11 @@ struct SceneSlot {
     DevBuf<pt_texture> textures;
     DevBuf<uint32_t> emissiveIdx;
     DevBuf<float> emissiveCdf;
+    // spectral mode: host copies of the banks and their spectrum coefficients
+    std::vector<pt_material> hostMats;
+    std::vector<pt_texture> hostTex;
+    DevBuf<float4> matSpec, texSpec;
+    bool specValid = false;
     BvhBuffers bvh;
     uint32_t triCount = 0;
     uint32_t materialCount = 0;
@@ -81,6 +89,9 @@ struct SceneSlot {
         textures.release();
         emissiveIdx.release();
         emissiveCdf.release();
+        matSpec.release();
+        texSpec.release();
+        specValid = false;
         bvh.release();
         bvh.scratch.release();
         hasScene = false;
@@ -119,6 +130,17 @@ struct pt_renderer {
     DevBuf<float> envScratch;             // sin(theta) per row and row totals of the table build
     int envW = 0, envH = 0;
     bool envValid = false;
+
+    // spectral mode (hero wavelengths)
+    std::vector<float> specRespHost;      // sRGB response table, 401 x 4
+    DevBuf<float4> specResp;
+    DevBuf<float4> envSpec;               // per-texel coefficients of the environment map
+    bool envSpecValid = false;
+    std::map<std::array<uint32_t, 3>, spectral::Coef> specCache; // colour bits -> coefficients
+    float4 specBackground{};
+    int specCapacity = 0;
+    DevBuf<float> pHero;
+    DevBuf<float4> pThrS, pRadS, pNeeEnvS, pNeeEmisS;
 
     // accumulation over the concatenated pixels of all scenes
     int width = 0, height = 0;            // scene 0
@@ -251,6 +273,8 @@ DevScene deviceScene(const SceneSlot* r)
     s.textures = r->textureCount ? r->textures.p : nullptr;
     s.emissiveIdx = r->emissiveIdx.p;
     s.emissiveCdf = r->emissiveCdf.p;
+    s.matSpec = r->specValid ? r->matSpec.p : nullptr;
+    s.texSpec = r->specValid ? r->texSpec.p : nullptr;
     s.nodeCount = r->hasScene ? r->bvh.nodeCount : 0u;
     s.triCount = r->triCount;
     s.materialCount = r->materialCount;
@@ -289,6 +313,7 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.env.width = r->envW;
     c.env.height = r->envH;
     c.env.valid = r->envValid ? 1 : 0;
+    c.env.spec = r->envSpecValid ? r->envSpec.p : nullptr;
     c.cam = r->scenes[0].camera;
     c.params = r->params;
     c.width = r->width;
@@ -314,6 +339,11 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.paths.visEnv = r->pVisEnv.p;
     c.paths.visEmis = r->pVisEmis.p;
     c.paths.scene = r->pScene.p;
+    c.paths.hero = r->pHero.p;
+    c.paths.thrS = r->pThrS.p;
+    c.paths.radS = r->pRadS.p;
+    c.paths.neeEnvS = r->pNeeEnvS.p;
+    c.paths.neeEmisS = r->pNeeEmisS.p;
     c.paths.capacity = r->capacity;
     c.q.extend[0] = r->qExt0.p;
     c.q.extend[1] = r->qExt1.p;
@@ -343,6 +373,9 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.record = rec ? r->record.p : nullptr;
     c.recordSpp = rec ? r->recordSpp : 0;
     c.seedOffset = r->previewLevels;
+    c.spectral = r->params.spectral_wavelengths;
+    c.specResp = r->specResp.p;
+    c.specBackground = r->specBackground;
     return c;
 }
 
@@ -537,6 +570,8 @@ int uploadBank(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
         mats.push_back(defaultMaterial());
     }
     sl.materialCount = static_cast<uint32_t>(mats.size());
+    sl.hostMats = mats;
+    sl.specValid = false;
     if (!sl.materials.ensure(mats.size())) {
         return fail(r, PT_ERR_OUT_OF_MEMORY, "material upload failed");
     }
@@ -549,7 +584,104 @@ int uploadBank(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
         }
         PT_CHECK(r, cudaMemcpyAsync(sl.textures.p, mesh->textures, mesh->texture_count * sizeof(pt_texture),
             cudaMemcpyHostToDevice, s));
+        sl.hostTex.assign(mesh->textures, mesh->textures + mesh->texture_count);
     }
+    return PT_OK;
+}
+
+// --- spectral mode ---------------------------------------------------------------
+
+const std::vector<float>& responseTable(pt_renderer* r)
+{
+    if (r->specRespHost.empty()) {
+        r->specRespHost.resize(4 * spectral::kRespCount);
+        spectral::buildResponseTable(r->specRespHost.data());
+    }
+    return r->specRespHost;
+}
+
+// Radiance-mode coefficients of an RGB colour (cached by the colour's bits).
+spectral::Coef colourCoef(pt_renderer* r, float cr, float cg, float cb)
+{
+    std::array<uint32_t, 3> key;
+    std::memcpy(&key[0], &cr, 4);
+    std::memcpy(&key[1], &cg, 4);
+    std::memcpy(&key[2], &cb, 4);
+    auto it = r->specCache.find(key);
+    if (it != r->specCache.end()) {
+        return it->second;
+    }
+    const spectral::Coef c = spectral::upliftSolve(responseTable(r).data(), cr, cg, cb, true);
+    r->specCache.emplace(key, c);
+    return c;
+}
+
+float4 coefToFloat4(const spectral::Coef& c) { return make_float4(c.c0, c.c1, c.c2, c.scale); }
+
+// Response table, the scenes' and environment's spectrum coefficients and the
+// spectral path state, for a render with nw wavelengths per path.
+int prepareSpectral(pt_renderer* r, int nw)
+{
+    cudaStream_t s = r->stream;
+    const std::vector<float>& resp = responseTable(r);
+    if (r->specResp.p == nullptr || r->specResp.n < static_cast<size_t>(spectral::kRespCount)) {
+        if (!r->specResp.ensure(spectral::kRespCount)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "spectral response table allocation failed");
+        }
+        PT_CHECK(r, cudaMemcpy(r->specResp.p, resp.data(), resp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    for (SceneSlot& sl : r->scenes) {
+        if (sl.specValid) {
+            continue;
+        }
+        std::vector<float4> mc(2 * std::max<size_t>(sl.hostMats.size(), 1));
+        for (size_t m = 0; m < sl.hostMats.size(); ++m) {
+            const pt_material& q = sl.hostMats[m];
+            mc[2 * m] = coefToFloat4(colourCoef(r, q.r, q.g, q.b));
+            mc[2 * m + 1] = coefToFloat4(colourCoef(r, q.scatter_radius_r, q.scatter_radius_g, q.scatter_radius_b));
+        }
+        const size_t nt = std::min<size_t>(sl.textureCount, sl.hostTex.size());
+        std::vector<float4> tc(2 * std::max<size_t>(nt, 1), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+        for (size_t t = 0; t < nt; ++t) {
+            const pt_texture& q = sl.hostTex[t];
+            if (q.kind == 1) {
+                tc[2 * t] = coefToFloat4(colourCoef(r, q.p0[0], q.p0[1], q.p0[2]));
+            } else if (q.kind == 2) {
+                tc[2 * t] = coefToFloat4(colourCoef(r, q.p1[0], q.p1[1], q.p1[2]));
+                tc[2 * t + 1] = coefToFloat4(colourCoef(r, q.p2[0], q.p2[1], q.p2[2]));
+            }
+        }
+        if (!sl.matSpec.ensure(mc.size()) || !sl.texSpec.ensure(tc.size())) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "spectral material tables allocation failed");
+        }
+        // (synchronous copies: the host vectors go out of scope)
+        PT_CHECK(r, cudaMemcpy(sl.matSpec.p, mc.data(), mc.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        PT_CHECK(r, cudaMemcpy(sl.texSpec.p, tc.data(), tc.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        sl.specValid = true;
+    }
+    if (r->envValid && !r->envSpecValid) {
+        const size_t texels = static_cast<size_t>(r->envW) * r->envH;
+        if (!r->envSpec.ensure(texels)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "spectral environment table allocation failed");
+        }
+        spectral::launchUpliftTexels(r->envPixels.p, texels, reinterpret_cast<const float*>(r->specResp.p),
+            r->envSpec.p, s);
+        PT_CHECK(r, cudaGetLastError());
+        r->envSpecValid = true;
+    }
+    const float k = r->params.environment_intensity;
+    r->specBackground =
+        coefToFloat4(colourCoef(r, r->params.background_r * k, r->params.background_g * k, r->params.background_b * k));
+    if (r->specCapacity < r->capacity) {
+        const size_t Q = static_cast<size_t>(r->capacity);
+        const size_t words = static_cast<size_t>(spectral::kMaxWavelengths / 4) * Q;
+        if (!r->pHero.ensure(Q) || !r->pThrS.ensure(words) || !r->pRadS.ensure(words) || !r->pNeeEnvS.ensure(words) ||
+            !r->pNeeEmisS.ensure(words)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "spectral path state allocation failed for %d paths", r->capacity);
+        }
+        r->specCapacity = r->capacity;
+    }
+    (void)nw;
     return PT_OK;
 }
 
@@ -794,6 +926,13 @@ int pt_destroy(pt_renderer* r)
     r->envMarginal.release();
     r->envRow.release();
     r->envScratch.release();
+    r->specResp.release();
+    r->envSpec.release();
+    r->pHero.release();
+    r->pThrS.release();
+    r->pRadS.release();
+    r->pNeeEnvS.release();
+    r->pNeeEmisS.release();
     r->acc.release();
     r->counts.release();
     r->lumMean.release();
@@ -920,6 +1059,10 @@ int pt_set_params(pt_renderer* r, const pt_render_params* params)
     if (r == nullptr || params == nullptr) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_params: null argument");
     }
+    if (params->spectral_wavelengths != 0 && params->spectral_wavelengths != 4 && params->spectral_wavelengths != 8) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_params: spectral_wavelengths must be 0, 4 or 8 (got %d)",
+            params->spectral_wavelengths);
+    }
     r->params = *params;
     return resetAccum(r);
 }
@@ -968,6 +1111,7 @@ int pt_set_environment(pt_renderer* r, int width, int height, const float* rgb)
     r->envW = width;
     r->envH = height;
     r->envValid = true;
+    r->envSpecValid = false;
     return resetAccum(r);
 }
 
@@ -1014,6 +1158,13 @@ int pt_render(pt_renderer* r, int waves)
             return st;
         }
     }
+    const int nw = r->params.spectral_wavelengths;
+    if (nw > 0) {
+        const int st = prepareSpectral(r, nw);
+        if (st != PT_OK) {
+            return st;
+        }
+    }
     if (r->previewLevels > 0 && r->wavesDone == 0 && r->previewDone < r->previewLevels - 1 && r->scenes.size() == 1) {
         // the preview passes come first (PathTracer.cpp:2382-2396); iteration i
         // renders level i with global seed i + 1
@@ -1056,7 +1207,7 @@ int pt_render(pt_renderer* r, int waves)
         }
         {
             StageTimer tm(r, kGenerate);
-            launchGenerate(c, slots, 0, s);
+            launchGenerate(c, slots, 0, nw, s);
         }
         ++launches;
         // Every live path advances one bounce per iteration and a finished path's
@@ -1075,8 +1226,8 @@ int pt_render(pt_renderer* r, int waves)
             }
             {
                 StageTimer tm(r, kShade);
-                launchShadeMiss(c, iter, sel, r->gridShade, s);
-                launchShade(c, sel, iter, r->gridShade, s);
+                launchShadeMiss(c, iter, sel, r->gridShade, nw, s);
+                launchShade(c, sel, iter, r->gridShade, nw, s);
             }
             {
                 StageTimer tm(r, kShadow);
@@ -1084,7 +1235,7 @@ int pt_render(pt_renderer* r, int waves)
             }
             {
                 StageTimer tm(r, kFinalize);
-                launchFinalize(c, sel, r->gridShadow, s);
+                launchFinalize(c, sel, r->gridShadow, nw, s);
             }
             launches += 5;
             r->profile.launches_extend += 1;
@@ -1695,6 +1846,9 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
     if (r->scenes.size() != 1 || r->pixelCount == 0) {
         return fail(r, PT_ERR_NOT_CONFIGURED, "pt_backward needs a configured single-scene renderer");
     }
+    if (r->params.spectral_wavelengths != 0) {
+        return fail(r, PT_ERR_UNSUPPORTED, "pt_backward: the adjoint differentiates the RGB integrator only");
+    }
     const SceneSlot& sl = r->scenes[0];
     if (!sl.hasScene) {
         return fail(r, PT_ERR_NO_SCENE, "pt_backward before pt_set_mesh");
@@ -1740,6 +1894,39 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
 // ---------------------------------------------------------------------------
 // Preview passes and region render (PathTracer.h:89-92, 134-140)
 // ---------------------------------------------------------------------------
+// Spectral mode helpers (host only; no device work).
+int pt_spectral_response(float* rgb, float* cie, float* xyz_to_rgb)
+{
+    if (rgb != nullptr) {
+        std::vector<float> t(4 * spectral::kRespCount);
+        spectral::buildResponseTable(t.data());
+        for (int i = 0; i < spectral::kRespCount; ++i) {
+            rgb[3 * i] = t[4 * i];
+            rgb[3 * i + 1] = t[4 * i + 1];
+            rgb[3 * i + 2] = t[4 * i + 2];
+        }
+    }
+    spectral::spectralSourceTables(cie, xyz_to_rgb);
+    return PT_OK;
+}
+
+int pt_spectral_uplift(uint32_t count, const float* rgb, float* coef)
+{
+    if (count > 0 && (rgb == nullptr || coef == nullptr)) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    std::vector<float> t(4 * spectral::kRespCount);
+    spectral::buildResponseTable(t.data());
+    for (uint32_t i = 0; i < count; ++i) {
+        const spectral::Coef c = spectral::upliftSolve(t.data(), rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], true);
+        coef[4 * i] = c.c0;
+        coef[4 * i + 1] = c.c1;
+        coef[4 * i + 2] = c.c2;
+        coef[4 * i + 3] = c.scale;
+    }
+    return PT_OK;
+}
+
 int pt_set_preview_levels(pt_renderer* r, int levels)
 {
     if (r == nullptr) {

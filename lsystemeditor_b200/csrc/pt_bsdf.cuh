@@ -738,27 +738,42 @@ __device__ __forceinline__ bool skipsEnvNee(const Mat& m)
     return fmax2(0.0f, fmin2(1.0f, m.transmission)) > 0.99f && fmax2(0.0f, fmin2(1.0f, m.metallic)) < 0.01f;
 }
 
-__device__ __forceinline__ float3 applyThroughput(float3 tp, const Ctx& c, const BsdfSample& s, float3 f)
+// Throughput rule of the sampled lobe (BrdfDispatch.h:42-76): the new
+// throughput is tp * f * k, times the base colour when `tint` (thin
+// transmission); false when the sample ends the path.
+__device__ __forceinline__ bool throughputFactor(const Ctx& c, const BsdfSample& s, float& k, bool& tint)
 {
+    tint = false;
     if (!s.valid || s.pdf <= kMinPdf) {
-        return f3(0.0f, 0.0f, 0.0f);
+        return false;
     }
     const float trans = fmax2(0.0f, fmin2(1.0f, c.m.transmission));
     const float thin = fmax2(0.0f, fmin2(1.0f, c.m.thin));
     const bool pure = trans > 0.99f && c.m.metallic < 0.01f;
-    float3 sc;
     if (pure && thin < 0.5f) {
-        sc = scl3(f, 1.0f / s.pdf);
+        k = 1.0f / s.pdf;
     } else if (s.transmitted) {
-        sc = scl3(f, absf(dot3(c.n, s.dir)) / s.pdf);
-        if (thin > 0.5f) {
-            sc = f3(sc.x * c.m.r, sc.y * c.m.g, sc.z * c.m.b);
-        }
+        k = absf(dot3(c.n, s.dir)) / s.pdf;
+        tint = thin > 0.5f;
     } else if (s.sss) {
-        sc = scl3(f, fmax2(0.0f, dot3(c.n, s.dir)) / s.pdf);
+        k = fmax2(0.0f, dot3(c.n, s.dir)) / s.pdf;
     } else {
         const float ct = c.eta > 1.0f + 1.0e-4f ? absf(dot3(c.n, s.dir)) : fmax2(0.0f, dot3(c.n, s.dir));
-        sc = scl3(f, ct / s.pdf);
+        k = ct / s.pdf;
+    }
+    return true;
+}
+
+__device__ __forceinline__ float3 applyThroughput(float3 tp, const Ctx& c, const BsdfSample& s, float3 f)
+{
+    float k;
+    bool tint;
+    if (!throughputFactor(c, s, k, tint)) {
+        return f3(0.0f, 0.0f, 0.0f);
+    }
+    float3 sc = scl3(f, k);
+    if (tint) {
+        sc = f3(sc.x * c.m.r, sc.y * c.m.g, sc.z * c.m.b);
     }
     return f3(tp.x * sc.x, tp.y * sc.y, tp.z * sc.z);
 }

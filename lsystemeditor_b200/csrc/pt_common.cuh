@@ -124,6 +124,11 @@ struct DevScene {
     const pt_texture* textures = nullptr;
     const uint32_t* emissiveIdx = nullptr;
     const float* emissiveCdf = nullptr;
+    // spectral mode: spectrum coefficients (c0, c1, c2, scale) of each
+    // material's base colour [2 m] and scatter radii [2 m + 1], and of each
+    // albedo texture's colours [2 t] (constant / grid colour 1), [2 t + 1] (grid colour 2)
+    const float4* matSpec = nullptr;
+    const float4* texSpec = nullptr;
     uint32_t nodeCount = 0;
     uint32_t triCount = 0;
     uint32_t materialCount = 0;
@@ -135,6 +140,7 @@ struct DevEnv {
     const float* pixels = nullptr; // RGB lat-long
     const float* marginal = nullptr;
     const float* row = nullptr;
+    const float4* spec = nullptr;  // spectral mode: per-texel radiance spectrum coefficients
     int width = 0;
     int height = 0;
     int valid = 0;

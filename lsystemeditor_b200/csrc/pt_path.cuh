@@ -44,5 +44,21 @@ __device__ __forceinline__ float3 clampFirefly(float3 c)
     return f3(__fmul_rn(c.x, k), __fmul_rn(c.y, k), __fmul_rn(c.z, k));
 }
 
+// Spectral samples: a hero-wavelength estimate of a colour can have a
+// negative sRGB channel, which is kept (zeroing it would bias the estimate);
+// the non-finite and luminance rules of clampFirefly apply.
+__device__ __forceinline__ float3 clampFireflySigned(float3 c)
+{
+    if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) {
+        return f3(0.0f, 0.0f, 0.0f);
+    }
+    const float l = __fadd_rn(__fadd_rn(__fmul_rn(c.x, 0.2126f), __fmul_rn(c.y, 0.7152f)), __fmul_rn(c.z, 0.0722f));
+    if (l <= 100.0f) {
+        return c;
+    }
+    const float k = __fdiv_rn(100.0f, l);
+    return f3(__fmul_rn(c.x, k), __fmul_rn(c.y, k), __fmul_rn(c.z, k));
+}
+
 } // namespace
 } // namespace pt

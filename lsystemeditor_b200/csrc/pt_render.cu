@@ -28,6 +28,7 @@
 
 #include "pt_bsdf.cuh"
 #include "pt_path.cuh"
+#include "pt_spectral.cuh"
 #include "pt_trace.cuh"
 
 #include <cooperative_groups.h>
@@ -91,10 +92,314 @@ __device__ __forceinline__ const DevScene& sceneOf(const LaunchCtx& c, uint32_t 
     return c.sceneCount > 1 ? c.scenes[c.paths.scene[i]] : c.scene;
 }
 
-__device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, float3 L)
+// --- per-path colour: RGB (NW = 0, the reference's integrator) or the
+// radiance at NW hero wavelengths (spectral mode) -----------------------------
+template <int NW> struct Col {
+    float v[NW];
+};
+template <> struct Col<0> {
+    float3 c;
+};
+
+template <int NW> __device__ __forceinline__ Col<NW> czero()
 {
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        r.c = f3(0.0f, 0.0f, 0.0f);
+    } else {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            r.v[k] = 0.0f;
+        }
+    }
+    return r;
+}
+template <int NW> __device__ __forceinline__ Col<NW> cadd(const Col<NW>& a, const Col<NW>& b)
+{
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        r.c = add3(a.c, b.c);
+    } else {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            r.v[k] = a.v[k] + b.v[k];
+        }
+    }
+    return r;
+}
+template <int NW> __device__ __forceinline__ Col<NW> cmul(const Col<NW>& a, const Col<NW>& b)
+{
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        r.c = mul3(a.c, b.c);
+    } else {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            r.v[k] = a.v[k] * b.v[k];
+        }
+    }
+    return r;
+}
+template <int NW> __device__ __forceinline__ Col<NW> cscl(const Col<NW>& a, float s)
+{
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        r.c = scl3(a.c, s);
+    } else {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            r.v[k] = a.v[k] * s;
+        }
+    }
+    return r;
+}
+template <int NW> __device__ __forceinline__ bool cnonzero(const Col<NW>& a)
+{
+    if constexpr (NW == 0) {
+        return a.c.x != 0.0f || a.c.y != 0.0f || a.c.z != 0.0f;
+    } else {
+        bool nz = false;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            nz = nz || a.v[k] != 0.0f;
+        }
+        return nz;
+    }
+}
+
+// Wavelengths of a path (spectral mode).
+template <int NW> struct Waves {
+    float lam[NW > 0 ? NW : 1];
+};
+template <int NW> __device__ __forceinline__ Waves<NW> pathWaves(const LaunchCtx& c, uint32_t i)
+{
+    Waves<NW> w;
+    if constexpr (NW > 0) {
+        const float u = c.paths.hero[i];
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            w.lam[k] = spectral::heroLambda(u, k, NW);
+        }
+    } else {
+        w.lam[0] = 0.0f;
+    }
+    return w;
+}
+
+// The spectrum of coefficient record q at the path's wavelengths.
+template <int NW> __device__ __forceinline__ Col<NW> coefCol(float4 q, const Waves<NW>& w)
+{
+    Col<NW> r;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        r.v[k] = spectral::evalCoef(q, w.lam[k]);
+    }
+    return r;
+}
+
+// Colour of a float4 path field (xyz in RGB mode; the spectral words otherwise).
+template <int NW> __device__ __forceinline__ Col<NW> loadCol(float4 rgb, const float4* spec, int cap, uint32_t i)
+{
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        r.c = f3(rgb.x, rgb.y, rgb.z);
+    } else {
+        (void)rgb;
+#pragma unroll
+        for (int j = 0; j < NW / 4; ++j) {
+            const float4 q = spec[static_cast<size_t>(j) * cap + i];
+            r.v[4 * j] = q.x;
+            r.v[4 * j + 1] = q.y;
+            r.v[4 * j + 2] = q.z;
+            r.v[4 * j + 3] = q.w;
+        }
+    }
+    return r;
+}
+// Stores a colour with `w` in the RGB field's fourth word (the RGB field
+// keeps only w in spectral mode).
+template <int NW> __device__ __forceinline__ void storeCol(float4* rgb, float4* spec, int cap, uint32_t i, const Col<NW>& v,
+    float w)
+{
+    if constexpr (NW == 0) {
+        rgb[i] = make_float4(v.c.x, v.c.y, v.c.z, w);
+    } else {
+        if (rgb != nullptr) {
+            rgb[i] = make_float4(0.0f, 0.0f, 0.0f, w);
+        }
+#pragma unroll
+        for (int j = 0; j < NW / 4; ++j) {
+            spec[static_cast<size_t>(j) * cap + i] =
+                make_float4(v.v[4 * j], v.v[4 * j + 1], v.v[4 * j + 2], v.v[4 * j + 3]);
+        }
+    }
+}
+template <int NW> __device__ __forceinline__ Col<NW> pendingEnv(const LaunchCtx& c, uint32_t i)
+{
+    if constexpr (NW == 0) {
+        return loadCol<0>(c.paths.neeEnv[i], nullptr, 0, i);
+    } else {
+        return loadCol<NW>(make_float4(0.0f, 0.0f, 0.0f, 0.0f), c.paths.neeEnvS, c.paths.capacity, i);
+    }
+}
+template <int NW> __device__ __forceinline__ Col<NW> pendingEmis(const LaunchCtx& c, uint32_t i)
+{
+    if constexpr (NW == 0) {
+        return loadCol<0>(c.paths.neeEmis[i], nullptr, 0, i);
+    } else {
+        return loadCol<NW>(make_float4(0.0f, 0.0f, 0.0f, 0.0f), c.paths.neeEmisS, c.paths.capacity, i);
+    }
+}
+
+// Environment / background radiance in direction d (LightSamplingCore.h:56-77).
+template <int NW> __device__ __forceinline__ Col<NW> envCol(const LaunchCtx& c, float3 d, const Waves<NW>& w)
+{
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        r.c = envEval(c.env, c.params, d);
+    } else {
+        float4 q = c.specBackground;
+        if (c.env.valid) {
+            float u, v;
+            dirToLatLong(d, u, v);
+            const int x = min(max(static_cast<int>(u * static_cast<float>(c.env.width)), 0), c.env.width - 1);
+            const int y = min(max(static_cast<int>(v * static_cast<float>(c.env.height)), 0), c.env.height - 1);
+            q = c.env.spec[static_cast<size_t>(y) * c.env.width + x];
+        }
+        r = coefCol<NW>(q, w);
+    }
+    return r;
+}
+
+// Spectrum coefficients of the base colour and scatter radii of the material
+// at a hit, following resolveMaterial's albedo-texture rules.
+__device__ __forceinline__ void matCoefs(const DevScene& S, uint32_t mi, const pt_material& src, float u, float v,
+    float4& base, float4& scatter)
+{
+    if (S.matSpec == nullptr || S.materials == nullptr || mi >= S.materialCount) {
+        base = make_float4(0.0f, 0.0f, 0.0f, 1.6f); // the fallback material's grey 0.8
+        scatter = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else {
+        base = S.matSpec[2 * mi];
+        scatter = S.matSpec[2 * mi + 1];
+    }
+    const uint32_t ti = src.albedo_tex;
+    if (ti != 0u && S.textures != nullptr && ti < S.textureCount) {
+        const pt_texture& t = S.textures[ti];
+        if (t.kind == 1) {
+            base = S.texSpec[2 * ti];
+        } else if (t.kind == 2) {
+            const float fx = fractf(u * t.p0[0]);
+            const float fy = fractf(v * t.p0[1]);
+            base = S.texSpec[2 * ti + ((fx < t.p0[2] || fy < t.p0[2]) ? 1 : 0)];
+        } else {
+            base = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
+}
+
+// BSDF value (RGB), or at each wavelength.  The spectral value at lambda is
+// the RGB BSDF of the material with every colour channel set to the colour's
+// spectrum at lambda.  All lobes but a scattering subsurface lobe are affine in
+// the base colour, f(rho) = f(0) + rho (f(1) - f(0)), so one RGB evaluation
+// with base (0, 1, 1) gives every wavelength; with a scattering subsurface
+// lobe (radius per wavelength) each wavelength is evaluated on its own.
+template <int NW>
+__device__ __forceinline__ Col<NW> evalCol(const Ctx& cx, float3 wi, const Col<NW>& rho, float4 scatter, const Waves<NW>& w)
+{
+    Col<NW> f;
+    if constexpr (NW == 0) {
+        (void)rho;
+        (void)scatter;
+        (void)w;
+        f.c = bsdfEval(cx, wi);
+    } else {
+        if (cx.w.subsurface != 0.0f && maxScatter(cx.m) > kMinRadius) {
+#pragma unroll 1
+            for (int k = 0; k < NW; ++k) {
+                Ctx ck = cx;
+                ck.m.r = ck.m.g = ck.m.b = rho.v[k];
+                const float rk = spectral::evalCoef(scatter, w.lam[k]);
+                ck.m.scatterR = ck.m.scatterG = ck.m.scatterB = rk;
+                f.v[k] = bsdfEval(ck, wi).x;
+            }
+        } else {
+            Ctx ca = cx;
+            ca.m.r = 0.0f;
+            ca.m.g = 1.0f;
+            ca.m.b = 1.0f;
+            const float3 e = bsdfEval(ca, wi);
+            const float b = e.y - e.x;
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                f.v[k] = e.x + b * rho.v[k];
+            }
+        }
+    }
+    return f;
+}
+
+template <int NW>
+__device__ __forceinline__ Col<NW> throughCol(const Col<NW>& T, const Ctx& cx, const BsdfSample& smp, const Col<NW>& f,
+    const Col<NW>& rho)
+{
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        (void)rho;
+        r.c = applyThroughput(T.c, cx, smp, f.c);
+    } else {
+        float k;
+        bool tint;
+        if (!throughputFactor(cx, smp, k, tint)) {
+            return czero<NW>();
+        }
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            float sc = f.v[j] * k;
+            if (tint) {
+                sc = sc * rho.v[j];
+            }
+            r.v[j] = T.v[j] * sc;
+        }
+    }
+    return r;
+}
+
+// Russian-roulette weight of a throughput: Rec. 709 luminance (RGB), the mean
+// over the wavelengths (spectral).
+template <int NW> __device__ __forceinline__ float pathWeight(const Col<NW>& T)
+{
+    if constexpr (NW == 0) {
+        return lum709(T.c);
+    } else {
+        float s = 0.0f;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            s += T.v[k];
+        }
+        return s * (1.0f / static_cast<float>(NW));
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, const Col<NW>& Lc, const Waves<NW>& w)
+{
+    float3 L;
+    if constexpr (NW == 0) {
+        (void)w;
+        L = Lc.c;
+    } else {
+        // hero-wavelength estimate of linear sRGB: each wavelength is uniform
+        // over the range, so sum_k L_k resp(lambda_k) (range / NW)
+        float3 a = f3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            a = add3(a, scl3(spectral::responseAt(c.specResp, w.lam[k]), Lc.v[k]));
+        }
+        L = scl3(a, spectral::kLambdaRange / static_cast<float>(NW));
+    }
     const uint32_t o = c.paths.outIdx[i];
-    const float3 s = clampFirefly(L);
+    const float3 s = NW == 0 ? clampFirefly(L) : clampFireflySigned(L);
     c.acc.samples[o] = make_float4(s.x, s.y, s.z, 1.0f);
     if (c.record != nullptr) {
         // sample index = samples the pixel had at batch start + the job's slot
@@ -110,7 +415,7 @@ __device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, floa
 // Camera path for job j of the current batch (PathTracer.cu:69-96): job
 // j = slot * activeCount + listIndex draws sample `counts[pixel] + slot` of
 // pixel active[listIndex] with the reference seed for wave waveBase + slot.
-__device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigned long long j)
+template <int NW> __device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigned long long j)
 {
     const BatchInfo& bt = *c.q.batch;
     const int activeCount = bt.activeCount;
@@ -156,7 +461,8 @@ __device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigne
     const uint32_t sampleIndex = c.acc.counts[pixel] + slot;
     const uint32_t globalSeed = bt.waveBase + slot + 1u + static_cast<uint32_t>(c.seedOffset);
     curandStateXORWOW st;
-    curand_init(pathSeed(c.params, local, width, sampleIndex, globalSeed), 0ull, 0ull, &st);
+    const uint32_t seed = pathSeed(c.params, local, width, sampleIndex, globalSeed);
+    curand_init(seed, 0ull, 0ull, &st);
     const uint32_t x = local % width, y = local / width;
     const float ju = curand_uniform(&st);
     const float jv = curand_uniform(&st);
@@ -173,12 +479,21 @@ __device__ __forceinline__ void initPath(const LaunchCtx& c, uint32_t i, unsigne
     c.paths.dir[i] = make_float4(rd.x, rd.y, rd.z, 0.0f);
     c.paths.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
     c.paths.rad[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
+    if constexpr (NW > 0) {
+        c.paths.hero[i] = spectral::heroU(seed);
+#pragma unroll
+        for (int q = 0; q < NW / 4; ++q) {
+            c.paths.thrS[static_cast<size_t>(q) * c.paths.capacity + i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+            c.paths.radS[static_cast<size_t>(q) * c.paths.capacity + i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
     c.paths.visEnv[i] = 0;
     c.paths.visEmis[i] = 0;
 }
 
 // A terminated path's slot takes the batch's next job, if any, and joins the
 // next extend queue: launches stay full until the batch drains.
+template <int NW>
 __device__ __forceinline__ void recyclePath(const LaunchCtx& c, uint32_t i, unsigned int* nextCount, uint32_t* nextQueue)
 {
     cg::coalesced_group g = cg::coalesced_threads();
@@ -189,13 +504,14 @@ __device__ __forceinline__ void recyclePath(const LaunchCtx& c, uint32_t i, unsi
     base = g.shfl(base, 0);
     const unsigned long long j = base + g.thread_rank();
     if (j < c.q.batch->jobs) {
-        initPath(c, i, j);
+        initPath<NW>(c, i, j);
         const uint32_t s = warpPush(nextCount);
         nextQueue[s] = i;
     }
 }
 
 // First `count` jobs of a batch into slots 0..count-1 (extend queue = identity).
+template <int NW>
 __global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ cp, int count, int extendSel)
 {
     const LaunchCtx& c = *cp;
@@ -210,7 +526,7 @@ __global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ 
         c.q.counts[10] = 0u;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        initPath(c, static_cast<uint32_t>(i), static_cast<unsigned long long>(i));
+        initPath<NW>(c, static_cast<uint32_t>(i), static_cast<unsigned long long>(i));
     }
 }
 
@@ -271,6 +587,7 @@ __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const Laun
 
 // Paths whose ray left the scene: previous bounce's NEE, then the
 // environment / background term (PathIntegratorRandCore.h:215-216, 338-346).
+template <int NW>
 __global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict__ cp, int iter, int sel)
 {
     const LaunchCtx& c = *cp;
@@ -279,35 +596,35 @@ __global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict_
     uint32_t* nextQueue = c.q.extend[sel ^ 1];
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = c.q.missQueue[k];
+        const Waves<NW> wv = pathWaves<NW>(c, i);
         const float4 d4 = c.paths.dir[i];
         const float3 d = f3(d4.x, d4.y, d4.z);
         const float4 r4 = c.paths.rad[i];
         const int depth = __float_as_int(r4.w);
-        float3 L;
+        Col<NW> L;
         if (depth == 0) {
-            L = envEval(c.env, c.params, d);
+            L = envCol<NW>(c, d, wv);
         } else {
-            L = f3(r4.x, r4.y, r4.z);
+            L = loadCol<NW>(r4, c.paths.radS, c.paths.capacity, i);
             if (c.paths.visEnv[i]) {
-                const float4 e = c.paths.neeEnv[i];
-                L = add3(L, f3(e.x, e.y, e.z));
+                L = cadd(L, pendingEnv<NW>(c, i));
             }
             if (c.paths.visEmis[i]) {
-                const float4 e = c.paths.neeEmis[i];
-                L = add3(L, f3(e.x, e.y, e.z));
+                L = cadd(L, pendingEmis<NW>(c, i));
             }
-            const float4 t4 = c.paths.thr[i];
-            const float3 Le = envEval(c.env, c.params, d);
+            const Col<NW> T = loadCol<NW>(c.paths.thr[i], c.paths.thrS, c.paths.capacity, i);
+            const Col<NW> Le = envCol<NW>(c, d, wv);
             const float lp = envPdf(c.env, d);
             const float w = misBalance(d4.w, lp);
-            L = add3(L, mul3(f3(t4.x, t4.y, t4.z), scl3(Le, w)));
+            L = cadd(L, cmul(T, cscl(Le, w)));
         }
-        writeSample(c, i, L);
-        recyclePath(c, i, nextCount, nextQueue);
+        writeSample<NW>(c, i, L, wv);
+        recyclePath<NW>(c, i, nextCount, nextQueue);
     }
 }
 
 // Shading of the paths that hit a triangle. One thread per queued path.
+template <int NW>
 __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const LaunchCtx* __restrict__ cp, int sel, int iter)
 {
     const LaunchCtx& c = *cp;
@@ -316,21 +633,21 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
     unsigned int* nextCount = &c.q.counts[sel ^ 1];
     uint32_t* nextQueue = c.q.extend[sel ^ 1];
     const int debugFlags = c.params.brdf_debug_flags;
+    const int cap = c.paths.capacity;
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = queue[k];
         const DevScene& S = sceneOf(c, i);
+        const Waves<NW> wv = pathWaves<NW>(c, i);
         const float4 r4 = c.paths.rad[i];
-        float3 L = f3(r4.x, r4.y, r4.z);
+        Col<NW> L = loadCol<NW>(r4, c.paths.radS, cap, i);
         const int depth = __float_as_int(r4.w);
         // NEE contributions of the previous bounce, in the reference's order
         // (the flags are clear for a path that starts at this bounce).
         if (c.paths.visEnv[i]) {
-            const float4 e = c.paths.neeEnv[i];
-            L = add3(L, f3(e.x, e.y, e.z));
+            L = cadd(L, pendingEnv<NW>(c, i));
         }
         if (c.paths.visEmis[i]) {
-            const float4 e = c.paths.neeEmis[i];
-            L = add3(L, f3(e.x, e.y, e.z));
+            L = cadd(L, pendingEmis<NW>(c, i));
         }
         const float4 h4 = c.paths.hit[i];
         const uint32_t tri = __float_as_uint(h4.w);
@@ -344,7 +661,7 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
         } else {
             const float4 o4 = c.paths.orig[i];
             const float4 t4 = c.paths.thr[i];
-            float3 T = f3(t4.x, t4.y, t4.z);
+            Col<NW> T = loadCol<NW>(t4, c.paths.thrS, cap, i);
             float eta = t4.w;
             const float t = h4.x;
             const float3 pos = xadd(f3(o4.x, o4.y, o4.z), xscl(d, t));
@@ -363,8 +680,21 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
             cx.wo = scl3(d, -1.0f);
             cx.eta = eta;
             cx.debug = 0;
+            // base colour at the path's wavelengths (spectral mode)
+            Col<NW> rho;
+            float4 scatterCoef = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            Col<NW> emis;
+            if constexpr (NW == 0) {
+                rho.c = f3(cx.m.r, cx.m.g, cx.m.b);
+                emis.c = f3(cx.m.r * cx.m.emission, cx.m.g * cx.m.emission, cx.m.b * cx.m.emission);
+            } else {
+                float4 baseCoef;
+                matCoefs(S, mi, srcMat, tu, tv, baseCoef, scatterCoef);
+                rho = coefCol<NW>(baseCoef, wv);
+                emis = cscl(rho, cx.m.emission);
+            }
             // emission (PathIntegratorRandCore.h:248)
-            L = add3(L, mul3(T, f3(cx.m.r * cx.m.emission, cx.m.g * cx.m.emission, cx.m.b * cx.m.emission)));
+            L = cadd(L, cmul(T, emis));
             curandStateXORWOW st;
             rngLoad(c.paths, i, st);
             // environment NEE (PathIntegratorRandCore.h:65-108)
@@ -375,18 +705,18 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
                 const float3 wi = envSample(c.env, u1, u2, lp);
                 if (lp > kMinPdf) {
                     const float ct = fmax2(0.0f, dot3(n, wi));
-                    const float3 Le = envEval(c.env, c.params, wi);
+                    const Col<NW> Le = envCol<NW>(c, wi, wv);
                     // A light of exactly zero radiance (a black background) contributes
                     // exactly zero for any finite BSDF value: the BSDF is not evaluated.
-                    if (ct > 0.0f && (Le.x != 0.0f || Le.y != 0.0f || Le.z != 0.0f)) {
-                        const float3 f = bsdfEval(cx, wi);
+                    if (ct > 0.0f && cnonzero(Le)) {
+                        const Col<NW> f = evalCol<NW>(cx, wi, rho, scatterCoef, wv);
                         const float bp = bsdfPdf(cx, wi);
-                        const float k = misBalance(lp, bp) * ct / lp;
-                        const float3 contrib = mul3(T, mul3(f, scl3(Le, k)));
+                        const float kw = misBalance(lp, bp) * ct / lp;
+                        const Col<NW> contrib = cmul(T, cmul(f, cscl(Le, kw)));
                         // A contribution of exactly zero adds nothing whether or not the light
                         // is occluded, so its shadow ray is not traced (black backgrounds).
-                        if (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f) {
-                            c.paths.neeEnv[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                        if (cnonzero(contrib)) {
+                            storeCol<NW>(c.paths.neeEnv, c.paths.neeEnvS, cap, i, contrib, 0.0f);
                             const uint32_t s = warpPush(&c.q.counts[2]);
                             const float3 so = add3(pos, scl3(n, kShadowBias));
                             c.q.shadowPath[s] = i;
@@ -402,9 +732,10 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
                 const float uTri = curand_uniform(&st);
                 const float u1 = curand_uniform(&st);
                 const float u2 = curand_uniform(&st);
-                float3 lpos, ln, Le, ev0, ev1, ev2;
+                float3 lpos, ln, LeRgb, ev0, ev1, ev2;
                 float ap;
-                if (sampleEmissive(S, &kFallbackMaterial, uTri, u1, u2, lpos, ln, Le, ap, ev0, ev1, ev2)) {
+                uint32_t etri = 0u;
+                if (sampleEmissive(S, &kFallbackMaterial, uTri, u1, u2, lpos, ln, LeRgb, ap, ev0, ev1, ev2, &etri)) {
                     const float3 tl = sub3(lpos, pos);
                     const float d2 = dot3(tl, tl);
                     if (d2 > kMinPdf) {
@@ -429,12 +760,24 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
                                                      tu2, tv2) && th < kRayTMax;
                             }
                             if (lp > kMinPdf && !occludedBySelf) {
-                                const float3 f = bsdfEval(cx, wi);
+                                Col<NW> Le;
+                                if constexpr (NW == 0) {
+                                    Le.c = LeRgb;
+                                } else {
+                                    // the emitter's own material colour (no texture), as sampleEmissive
+                                    const uint32_t emi = __float_as_uint(S.shade[etri].d.w);
+                                    const bool ok = S.matSpec != nullptr && S.materials != nullptr &&
+                                        emi < S.materialCount;
+                                    const float4 q = ok ? S.matSpec[2 * emi] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                                    const float em = ok ? S.materials[emi].emission : 0.0f;
+                                    Le = cscl(coefCol<NW>(q, wv), em);
+                                }
+                                const Col<NW> f = evalCol<NW>(cx, wi, rho, scatterCoef, wv);
                                 const float bp = bsdfPdf(cx, wi);
-                                const float k = misBalance(lp, bp) * ct / lp;
-                                const float3 contrib = mul3(T, mul3(f, scl3(Le, k)));
-                                if (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f) {
-                                    c.paths.neeEmis[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                                const float kw = misBalance(lp, bp) * ct / lp;
+                                const Col<NW> contrib = cmul(T, cmul(f, cscl(Le, kw)));
+                                if (cnonzero(contrib)) {
+                                    storeCol<NW>(c.paths.neeEmis, c.paths.neeEmisS, cap, i, contrib, 0.0f);
                                     const uint32_t s = warpPush(&c.q.counts[2]);
                                     c.q.shadowPath[s] = i | 0x80000000u;
                                     c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
@@ -454,8 +797,8 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
             if (!smp.valid || smp.pdf <= kMinPdf) {
                 done = true;
             } else {
-                const float3 f = bsdfEval(cx, smp.dir);
-                T = applyThroughput(T, cx, smp, f);
+                const Col<NW> f = evalCol<NW>(cx, smp.dir, rho, scatterCoef, wv);
+                T = throughCol<NW>(T, cx, smp, f, rho);
                 if (smp.sss && smp.sssSteps > 0) {
                     // subsurface tier B (PathIntegratorRandCore.h:169-204)
                     const float maxR = maxScatter(cx.m);
@@ -466,18 +809,21 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
                             const float u3 = curand_uniform(&st);
                             const float mfp = maxR * (-logf(fmax2(1.0e-8f, u3)));
                             const float surv = expf(-mfp / maxR);
-                            T = mul3(T, scl3(f3(cx.m.r, cx.m.g, cx.m.b), surv));
+                            T = cmul(T, cscl(rho, surv));
                         }
                         const float ed = sqrtf(dot3(smp.exitOffset, smp.exitOffset));
                         if (ed > 0.0f) {
-                            T = scl3(T, expf(-ed / maxR));
+                            T = cscl(T, expf(-ed / maxR));
                         }
                     }
                 }
-                if (debugFlags & kDbgTintGlass) {
-                    T = smp.transmitted ? mul3(T, f3(0.2f, 1.0f, 0.2f)) : mul3(T, f3(1.0f, 0.2f, 0.2f));
+                if constexpr (NW == 0) {
+                    // debug tint of glass paths (RGB display aid; not applied to spectra)
+                    if (debugFlags & kDbgTintGlass) {
+                        T.c = smp.transmitted ? mul3(T.c, f3(0.2f, 1.0f, 0.2f)) : mul3(T.c, f3(1.0f, 0.2f, 0.2f));
+                    }
                 }
-                const float tl = lum709(T);
+                const float tl = pathWeight<NW>(T);
                 if (!isfinite(tl) || tl <= 0.0f || tl > 1.0e8f) {
                     done = true;
                 } else {
@@ -487,7 +833,7 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
                         if (curand_uniform(&st) > surv) {
                             survive = false;
                         } else {
-                            T = scl3(T, 1.0f / surv);
+                            T = cscl(T, 1.0f / surv);
                         }
                     }
                     if (!survive) {
@@ -499,26 +845,27 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
                         const float3 no = xadd(pos, xscl(n, __fmul_rn(sign, bias)));
                         c.paths.orig[i] = make_float4(no.x, no.y, no.z, bias);
                         c.paths.dir[i] = make_float4(smp.dir.x, smp.dir.y, smp.dir.z, smp.pdf);
-                        c.paths.thr[i] = make_float4(T.x, T.y, T.z, eta);
+                        storeCol<NW>(c.paths.thr, c.paths.thrS, cap, i, T, eta);
                         cont = true;
                     }
                 }
             }
             rngStore(c.paths, i, st);
         }
+        (void)done;
         c.paths.visEnv[i] = 0;
         c.paths.visEmis[i] = 0;
         if (cont) {
-            c.paths.rad[i] = make_float4(L.x, L.y, L.z, __int_as_float(depth + 1));
+            storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth + 1));
             const uint32_t s = warpPush(nextCount);
             nextQueue[s] = i;
         } else if (pendEnv || pendEmis) {
-            c.paths.rad[i] = make_float4(L.x, L.y, L.z, __int_as_float(depth));
+            storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth));
             const uint32_t s = warpPush(&c.q.counts[3]);
             c.q.finish[s] = i;
         } else {
-            writeSample(c, i, L);
-            recyclePath(c, i, nextCount, nextQueue);
+            writeSample<NW>(c, i, L, wv);
+            recyclePath<NW>(c, i, nextCount, nextQueue);
         }
     }
 }
@@ -563,6 +910,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__
 }
 
 // Paths that terminated while their NEE shadow rays were in flight.
+template <int NW>
 __global__ void __launch_bounds__(256) k_finalize(const LaunchCtx* __restrict__ cp, int sel)
 {
     const LaunchCtx& c = *cp;
@@ -571,18 +919,16 @@ __global__ void __launch_bounds__(256) k_finalize(const LaunchCtx* __restrict__ 
     uint32_t* nextQueue = c.q.extend[sel ^ 1];
     for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t i = c.q.finish[k];
-        const float4 r4 = c.paths.rad[i];
-        float3 L = f3(r4.x, r4.y, r4.z);
+        const Waves<NW> wv = pathWaves<NW>(c, i);
+        Col<NW> L = loadCol<NW>(c.paths.rad[i], c.paths.radS, c.paths.capacity, i);
         if (c.paths.visEnv[i]) {
-            const float4 e = c.paths.neeEnv[i];
-            L = add3(L, f3(e.x, e.y, e.z));
+            L = cadd(L, pendingEnv<NW>(c, i));
         }
         if (c.paths.visEmis[i]) {
-            const float4 e = c.paths.neeEmis[i];
-            L = add3(L, f3(e.x, e.y, e.z));
+            L = cadd(L, pendingEmis<NW>(c, i));
         }
-        writeSample(c, i, L);
-        recyclePath(c, i, nextCount, nextQueue);
+        writeSample<NW>(c, i, L, wv);
+        recyclePath<NW>(c, i, nextCount, nextQueue);
     }
 }
 
@@ -802,9 +1148,15 @@ inline int gridFor(long long n, int block = 256, int cap = 148 * 16)
 
 } // namespace
 
-void launchGenerate(const LaunchCtx* d, int count, int extendSel, cudaStream_t s)
+void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s)
 {
-    k_generate<<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
+    if (nw == 8) {
+        k_generate<8><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
+    } else if (nw == 4) {
+        k_generate<4><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
+    } else {
+        k_generate<0><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
+    }
 }
 void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid, bool count, cudaStream_t s)
 {
@@ -815,13 +1167,25 @@ void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid
         k_extend<false><<<grid, 256, smem, s>>>(c, sel, identity, iter);
     }
 }
-void launchShadeMiss(const LaunchCtx* c, int iter, int sel, int grid, cudaStream_t s)
+void launchShadeMiss(const LaunchCtx* c, int iter, int sel, int grid, int nw, cudaStream_t s)
 {
-    k_shade_miss<<<grid, 256, 0, s>>>(c, iter, sel);
+    if (nw == 8) {
+        k_shade_miss<8><<<grid, 256, 0, s>>>(c, iter, sel);
+    } else if (nw == 4) {
+        k_shade_miss<4><<<grid, 256, 0, s>>>(c, iter, sel);
+    } else {
+        k_shade_miss<0><<<grid, 256, 0, s>>>(c, iter, sel);
+    }
 }
-void launchShade(const LaunchCtx* c, int sel, int iter, int grid, cudaStream_t s)
+void launchShade(const LaunchCtx* c, int sel, int iter, int grid, int nw, cudaStream_t s)
 {
-    k_shade<<<grid, 256, 0, s>>>(c, sel, iter);
+    if (nw == 8) {
+        k_shade<8><<<grid, 256, 0, s>>>(c, sel, iter);
+    } else if (nw == 4) {
+        k_shade<4><<<grid, 256, 0, s>>>(c, sel, iter);
+    } else {
+        k_shade<0><<<grid, 256, 0, s>>>(c, sel, iter);
+    }
 }
 void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, cudaStream_t s)
 {
@@ -837,10 +1201,19 @@ void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
     extendBlocks = shadeBlocks = shadowBlocks = 1;
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extendBlocks, k_extend<false>, 256, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadeBlocks, k_shade, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadeBlocks, k_shade<0>, 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadowBlocks, k_shadow<false>, 256, smem);
 }
-void launchFinalize(const LaunchCtx* c, int sel, int grid, cudaStream_t s) { k_finalize<<<grid, 256, 0, s>>>(c, sel); }
+void launchFinalize(const LaunchCtx* c, int sel, int grid, int nw, cudaStream_t s)
+{
+    if (nw == 8) {
+        k_finalize<8><<<grid, 256, 0, s>>>(c, sel);
+    } else if (nw == 4) {
+        k_finalize<4><<<grid, 256, 0, s>>>(c, sel);
+    } else {
+        k_finalize<0><<<grid, 256, 0, s>>>(c, sel);
+    }
+}
 void launchAccumulate(const LaunchCtx* c, int activeCount, int batch, cudaStream_t s)
 {
     k_accumulate<<<gridFor(activeCount), 256, 0, s>>>(c, activeCount, batch);

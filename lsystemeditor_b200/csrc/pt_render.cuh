@@ -21,6 +21,15 @@ struct PathSoA {
     uint8_t* visEnv = nullptr;   // 1 = that contribution is unoccluded
     uint8_t* visEmis = nullptr;
     uint16_t* scene = nullptr;   // scene of the path (written only when more than one scene is rendered)
+    // spectral mode (NW wavelengths per path): the path's hero draw, and NW / 4
+    // float4 per path of throughput, radiance and pending NEE contributions,
+    // word j of path i at [j * capacity + i] (the RGB fields above then carry
+    // only the medium IOR in thr.w and the depth in rad.w)
+    float* hero = nullptr;
+    float4* thrS = nullptr;
+    float4* radS = nullptr;
+    float4* neeEnvS = nullptr;
+    float4* neeEmisS = nullptr;
     int capacity = 0;
 };
 
@@ -103,18 +112,25 @@ struct LaunchCtx {
     // global seed seedOffset + w + 1 (the reference counts its preview passes as
     // iterations, PathTracer.cpp:2379)
     int seedOffset;
+    // spectral mode: wavelengths per path (0 = RGB, the reference's integrator),
+    // the sRGB response table (401 entries, 1 nm apart from 380 nm) and the
+    // spectrum coefficients of the background colour times the environment intensity
+    int spectral;
+    const float4* specResp;
+    float4 specBackground;
 };
 
 // Launchers. The LaunchCtx lives in DEVICE memory (one per renderer) and is
 // passed by pointer: a large by-value kernel parameter whose members are
 // taken by reference would be copied to local memory by every thread.
 // `grid` is a persistent-style grid; kernels loop over device-side counts.
-void launchGenerate(const LaunchCtx* d, int count, int extendSel, cudaStream_t s);
+// `nw` (generate, shade-miss, shade, finalize): wavelengths per path, 0 = RGB.
+void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s);
 void launchExtend(const LaunchCtx* d, int sel, bool identity, int iter, int grid, bool count, cudaStream_t s);
-void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, cudaStream_t s);
-void launchShade(const LaunchCtx* d, int sel, int iter, int grid, cudaStream_t s);
+void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, int nw, cudaStream_t s);
+void launchShade(const LaunchCtx* d, int sel, int iter, int grid, int nw, cudaStream_t s);
 void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, cudaStream_t s);
-void launchFinalize(const LaunchCtx* d, int sel, int grid, cudaStream_t s);
+void launchFinalize(const LaunchCtx* d, int sel, int grid, int nw, cudaStream_t s);
 void launchAccumulate(const LaunchCtx* d, int activeCount, int batch, cudaStream_t s);
 // Stable compaction of the active list (pixels neither converged nor at the
 // sample cap), so that the list stays sorted by pixel and thereby by scene.

@@ -68,7 +68,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_batch_set_camera", "pt_batch_readback", "pt_batch_set_tubes", "pt_export_mesh",
                     "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
-                    "pt_reset_region", "pt_environment_tables"]
+                    "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -128,6 +128,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_set_region.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L.pt_reset_region.argtypes = [vp]
     L.pt_environment_tables.argtypes = [vp, _fp, _fp]
+    L.pt_spectral_response.argtypes = [_fp, _fp, _fp]
+    L.pt_spectral_uplift.argtypes = [C.c_uint32, _fp, _fp]
     _LIB = L
     return L
 
@@ -385,6 +387,37 @@ class PathTracer:
     def exposure_multiplier(f_stop: float, shutter_seconds: float, iso: float) -> float:
         """PhysicalCamera::exposureMultiplier (PhysicalCamera.cpp:392-397)."""
         return float(load_library().pt_exposure_multiplier(float(f_stop), float(shutter_seconds), float(iso)))
+
+    # -- spectral mode (params["spectral_wavelengths"] = 4 or 8) --------------
+    @staticmethod
+    def spectral_response() -> np.ndarray:
+        """sRGB response per nm, 380 .. 780 nm (401 x 3); each channel sums to 1 (trapezoid rule)."""
+        out = np.empty((401, 3), np.float32)
+        rc = load_library().pt_spectral_response(_ptr(out, _fp), None, None)
+        if rc != PT_OK:
+            raise PathTracerError(rc, "pt_spectral_response failed")
+        return out
+
+    @staticmethod
+    def spectral_source_tables() -> Tuple[np.ndarray, np.ndarray]:
+        """(x-bar, y-bar, z-bar, D65) at 380 .. 780 nm every 10 nm (41 x 4) and the XYZ -> sRGB matrix."""
+        cie = np.empty((41, 4), np.float32)
+        m = np.empty((3, 3), np.float32)
+        rc = load_library().pt_spectral_response(None, _ptr(cie, _fp), _ptr(m, _fp))
+        if rc != PT_OK:
+            raise PathTracerError(rc, "pt_spectral_response failed")
+        return cie, m
+
+    @staticmethod
+    def spectral_uplift(rgb) -> np.ndarray:
+        """Spectrum coefficients (c0, c1, c2, scale), lambda in nm, of RGB colours (n x 3) as the renderer uses
+        them: scale * (1/2 + x / (2 sqrt(1 + x^2))), x = c0 lambda^2 + c1 lambda + c2."""
+        a = np.ascontiguousarray(np.asarray(rgb, np.float32).reshape(-1, 3))
+        out = np.empty((len(a), 4), np.float32)
+        rc = load_library().pt_spectral_uplift(len(a), _ptr(a, _fp), _ptr(out, _fp))
+        if rc != PT_OK:
+            raise PathTracerError(rc, "pt_spectral_uplift failed")
+        return out
 
     # -- preview passes and region render (PathTracer.h:89-92, 134-140) --------
     def set_preview_steps_per_level(self, levels: int):

@@ -67,7 +67,7 @@ PARAMS_DTYPE = np.dtype([
     ("seed_value", "<u4"),
     ("adaptive_criterion", "<i4"),   # 0: relative std-dev (reference), 1: relative std-error
     ("samples_per_launch", "<i4"),   # 0: automatic batch of waves per launch
-    ("reserved", "<i4"),
+    ("spectral_wavelengths", "<i4"), # 0: RGB (reference); 4 or 8 hero wavelengths
 ])
 assert PARAMS_DTYPE.itemsize == 64
 

@@ -125,6 +125,14 @@ class Checker:
                                              C.c_int, _fp]
             L.orc64_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                          _fp, C.c_int, _fp, _dp, C.c_int, C.c_int]
+            spec = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint, _fp, C.c_int,
+                    C.c_int, _fp, _fp, C.c_int, _fp, C.c_int, _fp, _fp]
+            L.orc_render_spectral.argtypes = spec + [_fp, _u32p, _fp, _fp, _u8p, C.c_int]
+            L.orc64_render_spectral.argtypes = spec + [_dp, _u32p, _dp, _dp, _u8p, C.c_int]
+            L.orc_spec_eval.restype = C.c_float
+            L.orc_spec_eval.argtypes = [_fp, C.c_float]
+            L.orc_hero_lambda.restype = C.c_float
+            L.orc_hero_lambda.argtypes = [C.c_uint, C.c_int, C.c_int]
 
     def fn(self, name):
         # attribute access caches the function object, so argtypes/restype set in __init__ stick
@@ -132,6 +140,39 @@ class Checker:
 
     def max_threads(self) -> int:
         return int(self.fn("max_threads")())
+
+    # -- the reference's spectral helpers (reference build only) -------------
+    def ref_spectral_cie(self, lambdas) -> np.ndarray:
+        """x-bar, y-bar, z-bar, D65 of Spectral/SpectralCore.h at each wavelength (n x 4)."""
+        lam = np.ascontiguousarray(lambdas, np.float32)
+        out = np.empty((len(lam), 4), np.float32)
+        self.lib.ref_spectral_cie.argtypes = [_fp, C.c_int, _fp]
+        self.lib.ref_spectral_cie(_ptr(lam, _fp), len(lam), _ptr(out, _fp))
+        return out
+
+    def ref_spectral_xyz_to_srgb(self, xyz) -> np.ndarray:
+        a = np.ascontiguousarray(np.asarray(xyz, np.float32).reshape(-1, 3))
+        out = np.empty_like(a)
+        self.lib.ref_spectral_xyz_to_srgb.argtypes = [_fp, C.c_int, _fp]
+        self.lib.ref_spectral_xyz_to_srgb(_ptr(a, _fp), len(a), _ptr(out, _fp))
+        return out
+
+    def ref_spectral_sigmoid(self, coef, lambdas) -> np.ndarray:
+        c = np.ascontiguousarray(np.asarray(coef, np.float32).reshape(-1, 3))
+        lam = np.ascontiguousarray(lambdas, np.float32)
+        out = np.empty(len(lam), np.float32)
+        self.lib.ref_spectral_sigmoid.argtypes = [_fp, _fp, C.c_int, _fp]
+        self.lib.ref_spectral_sigmoid(_ptr(c, _fp), _ptr(lam, _fp), len(lam), _ptr(out, _fp))
+        return out
+
+    def spec_eval(self, coef, lam: float) -> float:
+        """Spectrum of a coefficient record (c0, c1, c2, scale) at lam nm, FP32 (oracle only)."""
+        c = np.ascontiguousarray(coef, np.float32)
+        return float(self.lib.orc_spec_eval(_ptr(c, _fp), C.c_float(lam)))
+
+    def hero_lambda(self, seed: int, k: int, nw: int) -> float:
+        """Wavelength k of nw of the path with this seed (oracle only)."""
+        return float(self.lib.orc_hero_lambda(C.c_uint(seed), int(k), int(nw)))
 
     # -- scene ------------------------------------------------------------
     def scene(self, mesh) -> "CheckerScene":
@@ -317,6 +358,39 @@ class CheckerScene:
             err = self.chk.fn("render")(*args, _ptr(state["acc"], _fp), _ptr(state["counts"], _u32p),
                                         _ptr(state["lum_mean"], _fp), _ptr(state["m2"], _fp),
                                         _ptr(state["converged"], _u8p), int(threads))
+        state["tape_errors"] = int(err)
+        return state
+
+    def render_spectral(self, camera, params, width, height, waves, spectral, seed_base=1, tape=None, tape_stride=0,
+                        env=None, state=None, threads=0, fp64=False):
+        """Hero-wavelength render (orc_render_spectral).  `spectral` holds the inputs the product derives from
+        the scene: nw, resp (401 x 3), mat (materials x 8), tex (textures x 8), env (texels x 4 or None),
+        bg (4)."""
+        assert self.chk.kind == "oracle"
+        camera_, params_ = _rec(camera), _rec(params)
+        P = width * height
+        ft = np.float64 if fp64 else np.float32
+        if state is None:
+            state = dict(acc=np.zeros((P, 4), ft), counts=np.zeros(P, np.uint32), lum_mean=np.zeros(P, ft),
+                         m2=np.zeros(P, ft), converged=np.zeros(P, np.uint8))
+        tp = None if tape is None else np.ascontiguousarray(tape, np.float32)
+        f32 = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)  # noqa: E731
+        resp, mat, tex = f32(spectral["resp"]), f32(spectral["mat"]), f32(spectral.get("tex"))
+        envc, bg = f32(spectral.get("env")), f32(spectral["bg"])
+        keep = (resp, mat, tex, envc, bg)
+        args = (self.h, env.h if env is not None else None, _vp(camera_), _vp(params_), width, height, waves,
+                C.c_uint(seed_base), _ptr(tp, _fp), int(tape_stride), int(spectral["nw"]), _ptr(resp, _fp),
+                _ptr(mat, _fp), 0 if mat is None else len(mat.reshape(-1, 8)), _ptr(tex, _fp),
+                0 if tex is None else len(tex.reshape(-1, 8)), _ptr(envc, _fp), _ptr(bg, _fp))
+        if fp64:
+            err = self.chk.lib.orc64_render_spectral(*args, _ptr(state["acc"], _dp), _ptr(state["counts"], _u32p),
+                                                     _ptr(state["lum_mean"], _dp), _ptr(state["m2"], _dp),
+                                                     _ptr(state["converged"], _u8p), int(threads))
+        else:
+            err = self.chk.lib.orc_render_spectral(*args, _ptr(state["acc"], _fp), _ptr(state["counts"], _u32p),
+                                                   _ptr(state["lum_mean"], _fp), _ptr(state["m2"], _fp),
+                                                   _ptr(state["converged"], _u8p), int(threads))
+        del keep
         state["tape_errors"] = int(err)
         return state
 

@@ -179,6 +179,89 @@ int renderImpl(void* sceneHandle, void* envHandle, const void* cameraBytes, cons
     return errors;
 }
 
+// renderImpl in spectral mode: each sample is a hero-wavelength sample whose
+// wavelengths come from the reference seed of (pixel, sample index, wave).
+template <class R>
+int renderSpectralImpl(void* sceneHandle, void* envHandle, const void* cameraBytes, const void* paramsBytes, int width,
+    int height, int waves, unsigned int seedBase, const float* tape, int tapeStride, const SpecSetup& sp, R* acc,
+    uint32_t* counts, R* lumMean, R* m2, uint8_t* converged, int threads)
+{
+    const Scene& s = *static_cast<Scene*>(sceneHandle);
+    const Env* e = static_cast<Env*>(envHandle);
+    CameraRec cam;
+    std::memcpy(&cam, cameraBytes, sizeof(cam));
+    ParamsRec p;
+    std::memcpy(&p, paramsBytes, sizeof(p));
+    const int P = width * height;
+    if (threads > 0) {
+        omp_set_num_threads(threads);
+    }
+    int errors = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : errors)
+    for (int idx = 0; idx < P; ++idx) {
+        for (int w = 0; w < waves; ++w) {
+            if (converged[idx] != 0) {
+                break;
+            }
+            const uint32_t gs = seedBase + static_cast<uint32_t>(w);
+            const uint32_t n = counts[idx];
+            const uint32_t seed = referenceSeed(idx, static_cast<int>(n), gs);
+            Rng rng;
+            if (tape != nullptr) {
+                rng.row = tape + (static_cast<size_t>(w) * P + idx) * static_cast<size_t>(tapeStride);
+                rng.length = tapeStride;
+            } else {
+                rng.seedPcg(seed, 0x9e3779b97f4a7c15ULL);
+            }
+            const V3<R> smp = tracePixelSpectral<R>(s, e, cam, p, sp, seed, idx, width, height, rng);
+            errors += rng.underruns;
+            const R sl = smp.x * R(0.2126f) + smp.y * R(0.7152f) + smp.z * R(0.0722f);
+            const R pm = lumMean[idx];
+            const R delta = sl - pm;
+            const R nm = pm + delta / R(n + 1);
+            m2[idx] = m2[idx] + delta * (sl - nm);
+            lumMean[idx] = nm;
+            R* a = acc + 4 * static_cast<size_t>(idx);
+            const R invN = R(1) / R(n + 1);
+            a[0] = (a[0] * R(n) + smp.x) * invN;
+            a[1] = (a[1] * R(n) + smp.y) * invN;
+            a[2] = (a[2] * R(n) + smp.z) * invN;
+            a[3] = R(1);
+            const uint32_t nc = n + 1;
+            counts[idx] = nc;
+            if (p.maxSamplesPerPixel > 0 && nc >= static_cast<uint32_t>(p.maxSamplesPerPixel)) {
+                converged[idx] = 1;
+                continue;
+            }
+            if ((nc % 4u) != 0) {
+                continue;
+            }
+            if (isConverged(nc, static_cast<float>(nm), static_cast<float>(m2[idx]), p.minSamples,
+                    p.relativeErrorThreshold)) {
+                converged[idx] = 1;
+            }
+        }
+    }
+    return errors;
+}
+
+SpecSetup makeSpecSetup(int nw, const float* resp, const float* matCoef, int matCount, const float* texCoef,
+    int texCount, const float* envCoef, const float* bgCoef)
+{
+    SpecSetup sp;
+    sp.nw = nw;
+    sp.resp = resp;
+    sp.mat = matCoef;
+    sp.matCount = static_cast<size_t>(matCount);
+    sp.tex = texCoef;
+    sp.texCount = static_cast<size_t>(texCount);
+    sp.env = envCoef;
+    for (int k = 0; k < 4; ++k) {
+        sp.bg[k] = bgCoef[k];
+    }
+    return sp;
+}
+
 Ctx<float> makeCtx(const float* normal, const float* wo, const void* material, float eta, int debug)
 {
     MaterialRec m;
@@ -341,6 +424,36 @@ int orc64_render(void* scene, void* env, const void* cam, const void* params, in
     return renderImpl<double>(scene, env, cam, params, width, height, waves, seedBase, tape, tapeStride, pixelList,
         pixelListCount, acc, counts, lumMean, m2, converged, threads);
 }
+
+// Spectral-mode render (FP32 and FP64): nw wavelengths per sample; resp 401 x 3;
+// matCoef: per material base and scatter records (8 floats); texCoef: per
+// texture two colour records (8 floats); envCoef: per texel (4 floats) or null;
+// bgCoef: background x intensity (4 floats).  Returns tape underruns.
+int orc_render_spectral(void* scene, void* env, const void* cam, const void* params, int width, int height, int waves,
+    unsigned int seedBase, const float* tape, int tapeStride, int nw, const float* resp, const float* matCoef,
+    int matCount, const float* texCoef, int texCount, const float* envCoef, const float* bgCoef, float* acc,
+    uint32_t* counts, float* lumMean, float* m2, uint8_t* converged, int threads)
+{
+    const SpecSetup sp = makeSpecSetup(nw, resp, matCoef, matCount, texCoef, texCount, envCoef, bgCoef);
+    return renderSpectralImpl<float>(scene, env, cam, params, width, height, waves, seedBase, tape, tapeStride, sp,
+        acc, counts, lumMean, m2, converged, threads);
+}
+
+int orc64_render_spectral(void* scene, void* env, const void* cam, const void* params, int width, int height,
+    int waves, unsigned int seedBase, const float* tape, int tapeStride, int nw, const float* resp,
+    const float* matCoef, int matCount, const float* texCoef, int texCount, const float* envCoef, const float* bgCoef,
+    double* acc, uint32_t* counts, double* lumMean, double* m2, uint8_t* converged, int threads)
+{
+    const SpecSetup sp = makeSpecSetup(nw, resp, matCoef, matCount, texCoef, texCount, envCoef, bgCoef);
+    return renderSpectralImpl<double>(scene, env, cam, params, width, height, waves, seedBase, tape, tapeStride, sp,
+        acc, counts, lumMean, m2, converged, threads);
+}
+
+// The spectrum of coefficient record c at lambda (FP32, the product's operation order).
+float orc_spec_eval(const float* c, float lambda) { return specEval<float>(c, lambda); }
+
+// Hero draw and wavelength k of nw for a path seed.
+float orc_hero_lambda(unsigned int seed, int k, int nw) { return heroLambda(heroU(seed), k, nw); }
 
 // d loss / d material parameters of the image drawn with `spp` samples per
 // pixel (sample k of pixel p replays tape row (k, p)); dImage: 3 floats per

@@ -1646,6 +1646,358 @@ inline V3<R> tracePixel(const Scene& s, const Env* e, const CameraRec& cam, cons
     return clampFirefly(tracePath(s, e, &p, ro, rd, rng));
 }
 
+// ---------------------------------------------------------------------------
+// Hero-wavelength spectral mode: an extension with no reference counterpart on
+// the render path (the reference's Spectral/ helpers are not called by its
+// integrator).  Restated here from the product's definition:
+//   * spectrum of a colour: scale * (1/2 + x / (2 sqrt(1 + x^2))),
+//     x = c0 l^2 + c1 l + c2 (the function of Spectral/Rgb2Spec.h:58-66);
+//   * NW wavelengths 380 + 400 frac(u + k / NW), u from a hash of the path seed;
+//   * the BSDF at lambda is the RGB BSDF of the material with every colour
+//     channel set to the colour's spectrum at lambda; sampling, pdfs, MIS and
+//     the random-number draws are those of the RGB material;
+//   * Russian roulette weighs the mean throughput over the wavelengths;
+//   * a sample's sRGB = sum_k L_k response(lambda_k) 400 / NW, then the
+//     firefly clamp without zeroing negative channels.
+// The coefficient records and the response table are inputs (they come from
+// the product's host functions, which other tests check on their own).
+// ---------------------------------------------------------------------------
+constexpr int kSpecMax = 8;
+
+struct SpecSetup {
+    int nw = 0;
+    const float* resp = nullptr;  // 401 x 3, 1 nm apart from 380 nm
+    const float* mat = nullptr;   // per material: base colour, scatter radii (4 floats each)
+    size_t matCount = 0;
+    const float* tex = nullptr;   // per texture: colour A, colour B (4 floats each)
+    size_t texCount = 0;
+    const float* env = nullptr;   // per environment texel (4 floats), or null
+    float bg[4] = {0.0f, 0.0f, 0.0f, 0.0f}; // background x intensity
+};
+
+template <class R> inline R specEval(const float* c, R lambda)
+{
+    using std::sqrt;
+    const R x = R(c[0]) * lambda * lambda + R(c[1]) * lambda + R(c[2]);
+    const R y = R(1) / sqrt(x * x + R(1));
+    return (R(0.5f) * x * y + R(0.5f)) * R(c[3]);
+}
+
+inline float heroU(uint32_t seed)
+{
+    uint32_t x = seed ^ 0x9E3779B9u;
+    x ^= x >> 16;
+    x *= 0x7FEB352Du;
+    x ^= x >> 15;
+    x *= 0x846CA68Bu;
+    x ^= x >> 16;
+    return static_cast<float>(x >> 8) * (1.0f / 16777216.0f);
+}
+
+inline float heroLambda(float u, int k, int nw)
+{
+    float t = u + static_cast<float>(k) / static_cast<float>(nw);
+    if (t >= 1.0f) {
+        t = t - 1.0f;
+    }
+    return 380.0f + 400.0f * t;
+}
+
+template <class R> inline V3<R> specResponse(const float* resp, R lambda)
+{
+    const R x = lambda - R(380);
+    const int i = clampv(static_cast<int>(x), 0, 399);
+    const R w = x - R(i);
+    const R v = R(1) - w;
+    const float* a = resp + 3 * i;
+    const float* b = resp + 3 * (i + 1);
+    return mk(R(a[0]) * v + R(b[0]) * w, R(a[1]) * v + R(b[1]) * w, R(a[2]) * v + R(b[2]) * w);
+}
+
+template <class R> inline const float* specEnvCoef(const Env* e, const SpecSetup& sp, V3<R> d)
+{
+    if (!envValid(e) || sp.env == nullptr) {
+        return sp.bg;
+    }
+    const V3<R> uv = dirToLatLong(d);
+    const int x = clampv(static_cast<int>(uv.x * R(e->width)), 0, e->width - 1);
+    const int y = clampv(static_cast<int>(uv.y * R(e->height)), 0, e->height - 1);
+    return sp.env + 4 * (static_cast<size_t>(y) * e->width + x);
+}
+
+// Coefficient records of the material at a hit (base colour after the albedo
+// texture rules of resolve(), scatter radii).
+template <class R>
+inline void specMatCoefs(const Scene& s, const SpecSetup& sp, uint32_t tri, V2<R> uv, const float*& base,
+    const float*& scatter)
+{
+    static const float kGrey[4] = {0.0f, 0.0f, 0.0f, 1.6f}; // the fallback material's 0.8
+    static const float kZero[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    base = kGrey;
+    scatter = kZero;
+    if (s.materials.empty() || tri >= s.tris.size()) {
+        return;
+    }
+    const uint32_t mi = s.tris[tri].mat;
+    if (mi >= s.materials.size() || mi >= sp.matCount) {
+        return;
+    }
+    base = sp.mat + 8 * static_cast<size_t>(mi);
+    scatter = base + 4;
+    const MaterialRec& m = s.materials[mi];
+    const uint32_t n = static_cast<uint32_t>(s.textures.size());
+    if (m.albedoTex != 0u && n != 0u && m.albedoTex < n && m.albedoTex < sp.texCount) {
+        const TextureRec& t = s.textures[m.albedoTex];
+        const float* tc = sp.tex + 8 * static_cast<size_t>(m.albedoTex);
+        if (t.kind == 1) {
+            base = tc;
+        } else if (t.kind == 2) {
+            const R fx = fract(uv.x * R(t.p0[0]));
+            const R fy = fract(uv.y * R(t.p0[1]));
+            base = (fx < R(t.p0[2]) || fy < R(t.p0[2])) ? tc + 4 : tc;
+        } else {
+            base = kZero;
+        }
+    }
+}
+
+// The material of a hit at wavelength k: every colour channel set to its spectrum there.
+template <class R> inline Mat<R> greyAt(const Mat<R>& m, R rho, R radius)
+{
+    Mat<R> g = m;
+    g.r = g.g = g.b = rho;
+    g.scatterR = g.scatterG = g.scatterB = radius;
+    return g;
+}
+
+template <class R>
+inline void tracePathSpectral(const Scene& s, const Env* e, const ParamsRec* p, const SpecSetup& sp, const R* lam,
+    V3<R> ro, V3<R> rd, Rng& rng, R* L)
+{
+    using std::exp; using std::isfinite; using std::log;
+    const int NW = sp.nw;
+    for (int k = 0; k < NW; ++k) {
+        L[k] = R(0);
+    }
+    const Hit<R> first = traceRay(s, ro, rd, R(0), R(1.0e6f));
+    if (!first.hit) {
+        const float* q = specEnvCoef(e, sp, rd);
+        for (int k = 0; k < NW; ++k) {
+            L[k] = specEval(q, lam[k]);
+        }
+        return;
+    }
+    int maxDepth = 32, rrMin = 3, debug = 0;
+    if (p->maxPathDepth > 0) {
+        maxDepth = p->maxPathDepth;
+    } else if (p->maxPathDepth == 0) {
+        maxDepth = 256;
+    }
+    if (p->russianRouletteMinDepth >= 0) {
+        rrMin = p->russianRouletteMinDepth;
+    }
+    debug = p->brdfDebugFlags;
+    R T[kSpecMax];
+    for (int k = 0; k < NW; ++k) {
+        T[k] = R(1);
+    }
+    V3<R> o = ro, d = rd;
+    Hit<R> h = first;
+    R eta = R(1);
+    MaterialRec fb = defaultFetchMaterial();
+    for (int depth = 0; depth < maxDepth; ++depth) {
+        const V3<R> pos = add(o, scl(d, h.t));
+        const V3<R> n = h.normal;
+        const V3<R> wo = scl(d, R(-1));
+        const Mat<R> m = resolve<R>(fetchMaterial(s, h.tri, fb), h.uv, s.textures);
+        const float* baseC;
+        const float* scatC;
+        specMatCoefs<R>(s, sp, h.tri, h.uv, baseC, scatC);
+        R rho[kSpecMax], rad[kSpecMax];
+        for (int k = 0; k < NW; ++k) {
+            rho[k] = specEval(baseC, lam[k]);
+            rad[k] = specEval(scatC, lam[k]);
+            L[k] = L[k] + T[k] * (rho[k] * m.emission);
+        }
+        auto bsdfAt = [&](int k, V3<R> wi) -> R {
+            const Ctx<R> ck{n, wo, greyAt(m, rho[k], rad[k]), eta, 0};
+            return bsdfEval(ck, wi).x;
+        };
+        // environment NEE (the geometry of neeEnvironment)
+        R add1[kSpecMax], add2[kSpecMax];
+        bool has1 = false, has2 = false;
+        if (!skipsEnvNee(m)) {
+            const R u1 = R(rng.next());
+            const R u2 = R(rng.next());
+            R lp = R(0);
+            const V3<R> wi = envSample(e, u1, u2, lp);
+            if (lp > Kc<R>::minPdf && !occluded(s, add(pos, scl(n, R(1.0e-4f))), wi)) {
+                const R ct = mx(R(0), dot(n, wi));
+                if (ct > R(0)) {
+                    const float* q = specEnvCoef(e, sp, wi);
+                    const R bp = bsdfPdf(Ctx<R>{n, wo, m, eta, 0}, wi);
+                    const R kw = misBalance(lp, bp) * ct / lp;
+                    for (int k = 0; k < NW; ++k) {
+                        add1[k] = T[k] * (bsdfAt(k, wi) * (specEval(q, lam[k]) * kw));
+                    }
+                    has1 = true;
+                }
+            }
+        }
+        // emissive NEE (the geometry of neeEmissive)
+        if (!s.emissiveIdx.empty()) {
+            const R uTri = R(rng.next());
+            const R u1 = R(rng.next());
+            const R u2 = R(rng.next());
+            V3<R> lpos, ln, Lrgb;
+            R ap = R(0);
+            uint32_t etri = 0;
+            if (sampleEmissive(s, uTri, u1, u2, lpos, ln, Lrgb, ap, &etri)) {
+                const V3<R> tl = sub(lpos, pos);
+                const R d2 = dot(tl, tl);
+                if (d2 > Kc<R>::minPdf) {
+                    const V3<R> wi = nrm(tl);
+                    const R ct = mx(R(0), dot(n, wi));
+                    const R cl = mx(R(0), dot(ln, scl(wi, R(-1))));
+                    const R lp = ap * d2 / cl;
+                    if (ct > R(0) && cl > R(0) && !occluded(s, add(pos, scl(wi, R(1.0e-4f))), wi) &&
+                        lp > Kc<R>::minPdf) {
+                        static const float kZero[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                        const uint32_t emi = s.tris[etri].mat;
+                        const bool ok = emi < s.materials.size() && emi < sp.matCount;
+                        const float* q = ok ? sp.mat + 8 * static_cast<size_t>(emi) : kZero;
+                        const R em = ok ? R(s.materials[emi].emission) : R(0);
+                        const R bp = bsdfPdf(Ctx<R>{n, wo, m, eta, 0}, wi);
+                        const R kw = misBalance(lp, bp) * ct / lp;
+                        for (int k = 0; k < NW; ++k) {
+                            add2[k] = T[k] * (bsdfAt(k, wi) * ((specEval(q, lam[k]) * em) * kw));
+                        }
+                        has2 = true;
+                    }
+                }
+            }
+        }
+        for (int k = 0; k < NW; ++k) {
+            if (has1) {
+                L[k] = L[k] + add1[k];
+            }
+            if (has2) {
+                L[k] = L[k] + add2[k];
+            }
+        }
+        const Ctx<R> c{n, wo, m, eta, debug};
+        const R u1 = R(rng.next());
+        const R u2 = R(rng.next());
+        const Sample<R> smp = bsdfSample(c, u1, u2);
+        if (!smp.valid || smp.pdf <= Kc<R>::minPdf) {
+            break;
+        }
+        for (int k = 0; k < NW; ++k) {
+            const Mat<R> gk = greyAt(m, rho[k], rad[k]);
+            const Ctx<R> ck{n, wo, gk, eta, 0};
+            const R fk = bsdfEval(ck, smp.dir).x;
+            T[k] = applyThroughput(mk(T[k], T[k], T[k]), ck, smp, mk(fk, fk, fk)).x;
+        }
+        if (smp.sss && smp.sssSteps > 0) {
+            // subsurfaceTierB with the base colour at each wavelength
+            const R maxR = maxScatter(m);
+            if (maxR > R(kMinRadius)) {
+                for (int step = 0; step < smp.sssSteps; ++step) {
+                    (void)rng.next();
+                    (void)rng.next();
+                    const R c3 = R(rng.next());
+                    const R mfp = maxR * (-log(mx(R(1.0e-8f), c3)));
+                    const R surv = exp(-mfp / maxR);
+                    for (int k = 0; k < NW; ++k) {
+                        T[k] = T[k] * (rho[k] * surv);
+                    }
+                }
+                const R ed = len(smp.exitOffset);
+                if (ed > R(0)) {
+                    for (int k = 0; k < NW; ++k) {
+                        T[k] = T[k] * exp(-ed / maxR);
+                    }
+                }
+            }
+        }
+        R tl = R(0);
+        for (int k = 0; k < NW; ++k) {
+            tl = tl + T[k];
+        }
+        tl = tl * (R(1) / R(NW));
+        if (!isfinite(tl) || tl <= R(0) || tl > R(1.0e8f)) {
+            break;
+        }
+        if (depth >= rrMin) {
+            const R surv = mn(R(0.95f), mx(tl, R(0.05f)));
+            if (R(rng.next()) > surv) {
+                break;
+            }
+            for (int k = 0; k < NW; ++k) {
+                T[k] = T[k] * (R(1) / surv);
+            }
+        }
+        eta = smp.nextEta;
+        const R bias = mx(R(1.0e-4f), R(1.0e-3f) * h.t);
+        const R sign = dot(n, smp.dir) >= R(0) ? R(1) : R(-1);
+        o = add(pos, scl(n, sign * bias));
+        d = smp.dir;
+        h = traceRay(s, o, d, bias, R(1.0e6f));
+        if (!h.hit) {
+            const float* q = specEnvCoef(e, sp, d);
+            const R lp = envPdf(e, d);
+            const R w = misBalance(smp.pdf, lp);
+            for (int k = 0; k < NW; ++k) {
+                L[k] = L[k] + T[k] * (specEval(q, lam[k]) * w);
+            }
+            break;
+        }
+    }
+}
+
+// sRGB of a spectral sample, then the firefly clamp without zeroing negative channels.
+template <class R> inline V3<R> spectralSampleRgb(const SpecSetup& sp, const R* lam, const R* L)
+{
+    using std::isfinite;
+    V3<R> a = mk(R(0), R(0), R(0));
+    for (int k = 0; k < sp.nw; ++k) {
+        a = add(a, scl(specResponse(sp.resp, lam[k]), L[k]));
+    }
+    V3<R> c = scl(a, R(400.0f) / R(sp.nw));
+    if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) {
+        return mk(R(0), R(0), R(0));
+    }
+    const R l = c.x * R(0.2126f) + c.y * R(0.7152f) + c.z * R(0.0722f);
+    if (l <= R(100)) {
+        return c;
+    }
+    const R kk = R(100) / l;
+    return mk(c.x * kk, c.y * kk, c.z * kk);
+}
+
+template <class R>
+inline V3<R> tracePixelSpectral(const Scene& s, const Env* e, const CameraRec& cam, const ParamsRec& p,
+    const SpecSetup& sp, uint32_t seed, int idx, int width, int height, Rng& rng)
+{
+    const int x = idx % width;
+    const int y = idx / width;
+    const R ju = R(rng.next());
+    const R jv = R(rng.next());
+    const R u = (R(x) + ju) / R(width);
+    const R v = (R(y) + jv) / R(height);
+    const R l1 = R(rng.next());
+    const R l2 = R(rng.next());
+    V3<R> ro, rd;
+    cameraRay(cam, u, v, l1, l2, ro, rd);
+    const float hu = heroU(seed);
+    R lam[kSpecMax], L[kSpecMax];
+    for (int k = 0; k < sp.nw; ++k) {
+        lam[k] = R(heroLambda(hu, k, sp.nw));
+    }
+    tracePathSpectral(s, e, &p, sp, lam, ro, rd, rng, L);
+    return spectralSampleRgb(sp, lam, L);
+}
+
 // PathTracerAdaptiveSampling.h:16-40.
 inline bool isConverged(uint32_t n, float mean, float m2, int minSamples, float thr)
 {

@@ -169,6 +169,36 @@ Vec3 refTracePixel(
 
 extern "C" {
 
+// The reference's spectral helpers (Spectral/SpectralCore.h:42-139,
+// Spectral/Rgb2Spec.h:58-66; not called by its RGB integrator): per
+// wavelength x-bar, y-bar, z-bar and D65 (4 floats).
+void ref_spectral_cie(const float* lambdas, int n, float* out)
+{
+    for (int i = 0; i < n; ++i) {
+        out[4 * i] = SpectralDetail::cieXAtWavelength(lambdas[i]);
+        out[4 * i + 1] = SpectralDetail::cieYAtWavelength(lambdas[i]);
+        out[4 * i + 2] = SpectralDetail::cieZAtWavelength(lambdas[i]);
+        out[4 * i + 3] = SpectralDetail::d65IlluminantAtWavelength(lambdas[i]);
+    }
+}
+
+// spectralLinearSrgbFromXyz of n XYZ triples.
+void ref_spectral_xyz_to_srgb(const float* xyz, int n, float* rgb)
+{
+    for (int i = 0; i < n; ++i) {
+        SpectralDetail::spectralLinearSrgbFromXyz(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], rgb[3 * i], rgb[3 * i + 1],
+            rgb[3 * i + 2]);
+    }
+}
+
+// rgb2specEvalCoefficients of n coefficient triples at n wavelengths.
+void ref_spectral_sigmoid(const float* coef, const float* lambdas, int n, float* out)
+{
+    for (int i = 0; i < n; ++i) {
+        out[i] = rgb2specEvalCoefficients(coef + 3 * i, lambdas[i]);
+    }
+}
+
 int ref_sizeof_material() { return static_cast<int>(sizeof(MaterialGpu)); }
 int ref_sizeof_texture() { return static_cast<int>(sizeof(TextureDescGpu)); }
 int ref_sizeof_camera() { return static_cast<int>(sizeof(CameraGpu)); }

@@ -86,7 +86,29 @@ def compute(chk: Checker):
     return out
 
 
+def spectral_inputs():
+    """Seeded inputs of the spectral fixtures."""
+    rng = np.random.default_rng(31)
+    lam10 = np.arange(380, 781, 10, dtype=np.float32)
+    xyz = rng.uniform(0.0, 1.2, size=(32, 3)).astype(np.float32)
+    # coefficient triples in nanometre units of the kind the uplift produces
+    c0 = rng.uniform(-1e-3, 1e-3, 256)
+    peak = rng.uniform(400.0, 700.0, 256)
+    c1 = -2.0 * c0 * peak
+    c2 = c0 * peak * peak + rng.uniform(-20.0, 20.0, 256)
+    coef = np.stack([c0, c1, c2], 1).astype(np.float32)
+    lam = rng.uniform(380.0, 780.0, 256).astype(np.float32)
+    return lam10, xyz, coef, lam
+
+
+def compute_spectral(ref):
+    """The reference's spectral helpers (reference build only)."""
+    lam10, xyz, coef, lam = spectral_inputs()
+    return dict(spec_cie=ref.ref_spectral_cie(lam10), spec_srgb=ref.ref_spectral_xyz_to_srgb(xyz),
+                spec_sigmoid=ref.ref_spectral_sigmoid(coef, lam))
+
+
 if __name__ == "__main__":
     ref = Checker("ref")
-    np.savez_compressed(OUT, **compute(ref))
+    np.savez_compressed(OUT, **compute(ref), **compute_spectral(ref))
     print("wrote", OUT, os.path.getsize(OUT), "bytes")

@@ -84,3 +84,44 @@ def rel_rmse(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     a = a.reshape(-1, a.shape[-1]).astype(np.float64)
     b = b.reshape(-1, b.shape[-1]).astype(np.float64)
     return np.sqrt(((a - b) ** 2).mean(0)) / np.maximum(np.sqrt((b ** 2).mean(0)), 1e-30)
+
+
+def spectral_inputs(mesh: HostMesh, params, nw: int, env: np.ndarray = None) -> dict:
+    """The spectral records the renderer derives from a scene (through its host functions), as the oracle's
+    spectral render takes them: response table, per-material base / scatter coefficients, per-texture colour
+    coefficients, per-texel environment coefficients, background x intensity."""
+    from lsystemeditor_b200.pathtracer import PathTracer
+    up = PathTracer.spectral_uplift
+    m = mesh.materials if len(mesh.materials) else np.array([default_material()], MATERIAL_DTYPE)
+    base = np.stack([m["r"], m["g"], m["b"]], 1)
+    scat = np.stack([m["scatter_radius_r"], m["scatter_radius_g"], m["scatter_radius_b"]], 1)
+    mat = np.concatenate([up(base), up(scat)], 1).astype(np.float32)
+    tex = np.zeros((max(len(mesh.textures), 1), 8), np.float32)
+    for i, t in enumerate(mesh.textures):
+        if t["kind"] == 1:
+            tex[i, :4] = up(t["p0"][:3])[0]
+        elif t["kind"] == 2:
+            tex[i, :4] = up(t["p1"][:3])[0]
+            tex[i, 4:] = up(t["p2"][:3])[0]
+    p = np.asarray(params).reshape(())
+    k = np.float32(p["environment_intensity"])
+    bg = up(np.array([p["background_r"] * k, p["background_g"] * k, p["background_b"] * k], np.float32))[0]
+    envc = None if env is None else up(np.asarray(env, np.float32).reshape(-1, 3))
+    return dict(nw=int(nw), resp=PathTracer.spectral_response(), mat=mat, tex=tex, env=envc, bg=bg)
+
+
+def spectral_zoo_scene(n_per_mat: int = 300, seed: int = 3) -> HostMesh:
+    """zoo_scene with coloured textures (a constant colour and a two-colour grid) and a tinted light."""
+    mesh = zoo_scene(n_per_mat, seed)
+    tex = np.zeros(4, TEXTURE_DTYPE)
+    tex[:3] = mesh.textures[:3]
+    tex[1]["p1"] = [0.8, 0.15, 0.1, 0.0]
+    tex[1]["p2"] = [0.1, 0.3, 0.85, 0.0]
+    tex[3]["kind"] = 1
+    tex[3]["p0"] = [0.2, 0.7, 0.25, 0.0]
+    mesh.textures = tex
+    mesh.materials[6]["albedo_tex"] = 3
+    mesh.materials[len(mesh.materials) - 1]["r"] = 1.0
+    mesh.materials[len(mesh.materials) - 1]["g"] = 0.85
+    mesh.materials[len(mesh.materials) - 1]["b"] = 0.6
+    return mesh

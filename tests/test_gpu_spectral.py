@@ -1,0 +1,133 @@
+"""Hero-wavelength spectral mode on the GPU (params spectral_wavelengths = 4 or 8).
+
+* Images match the oracle's spectral restatement on the same random numbers
+  (relative RMSE per channel <= 1e-3): coloured materials and textures, glass,
+  thin transmission, subsurface with per-wavelength radii, emitters, a
+  background colour and an environment map.
+* Every result states its error against the FP64 oracle.
+* A grey scene converges to its RGB render (the wavelength draw takes no
+  random numbers, so the paths are the same).
+* A batch renders each scene as its plain spectral render does, bit for bit.
+* Invalid wavelength counts and a spectral pt_backward are rejected.
+"""
+import numpy as np
+import pytest
+
+from lsystemeditor_b200.pathtracer import PathTracer, PathTracerError
+from lsystemeditor_b200.records import default_params
+from tests.helpers import rel_rmse, sky, spectral_inputs, spectral_zoo_scene, zoo_camera
+
+pytestmark = pytest.mark.gpu
+
+IMAGE_REL_RMSE = 1e-3
+
+
+def _spectral_pair(tracer, oracle, mesh, camera, params, w, h, waves, stride, env=None, fp64=False):
+    tracer.configure(w, h, mesh)
+    tracer.set_camera(camera)
+    tracer.set_params(params)
+    tracer.set_environment(env)
+    tape = tracer.rng_tape(0, waves, stride)
+    tracer.reset_accumulation()
+    tracer.render(waves)
+    rgba, counts, conv = tracer.readback()
+    sc = oracle.scene(mesh)
+    oenv = oracle.env(env) if env is not None else None
+    sp = spectral_inputs(mesh, params, int(params["spectral_wavelengths"]), env)
+    st = sc.render_spectral(camera, params, w, h, waves, sp, seed_base=1, tape=tape, tape_stride=stride, env=oenv)
+    assert st["tape_errors"] == 0, "tape too short for the paths traced"
+    st64 = None
+    if fp64:
+        st64 = sc.render_spectral(camera, params, w, h, waves, sp, seed_base=1, tape=tape, tape_stride=stride,
+                                  env=oenv, fp64=True)
+    return rgba.reshape(-1, 4), counts.reshape(-1), st, st64
+
+
+@pytest.mark.parametrize("nw", [4, 8])
+def test_spectral_parity_zoo(tracer, oracle, nw):
+    mesh = spectral_zoo_scene()
+    w, h, waves = 48, 40, 8
+    params = default_params(background_r=0.05, background_g=0.07, background_b=0.12, max_path_depth=8,
+                            min_samples=waves, max_samples_per_pixel=waves, spectral_wavelengths=nw)
+    rgba, counts, st, st64 = _spectral_pair(tracer, oracle, mesh, zoo_camera(w, h), params, w, h, waves, 200,
+                                            fp64=True)
+    assert np.all(counts == waves) and np.array_equal(counts, st["counts"])
+    err = rel_rmse(rgba[:, :3], st["acc"][:, :3])
+    assert np.all(err <= IMAGE_REL_RMSE), f"relative RMSE {err}"
+    err64 = rel_rmse(rgba[:, :3], st64["acc"][:, :3])
+    print(f"spectral nw={nw}: relative RMSE vs FP32 oracle {err}, vs FP64 oracle {err64}")
+    assert np.all(err64 <= 1e-2), f"relative RMSE vs FP64 oracle {err64}"
+    # the spectral render is a different image from the RGB one (colours interreflect per wavelength)
+    assert np.abs(rgba[:, :3]).sum() > 0
+
+
+def test_spectral_parity_environment_map(tracer, oracle):
+    mesh = spectral_zoo_scene(n_per_mat=150, seed=9)
+    w, h, waves = 40, 32, 6
+    params = default_params(max_path_depth=6, min_samples=waves, max_samples_per_pixel=waves,
+                            environment_intensity=1.3, spectral_wavelengths=4)
+    rgba, counts, st, _ = _spectral_pair(tracer, oracle, mesh, zoo_camera(w, h), params, w, h, waves, 160,
+                                         env=sky())
+    err = rel_rmse(rgba[:, :3], st["acc"][:, :3])
+    assert np.all(err <= IMAGE_REL_RMSE), f"relative RMSE {err}"
+
+
+def test_spectral_grey_scene_converges_to_rgb(tracer):
+    from tests.test_spectral import _grey_scene
+    from lsystemeditor_b200.records import look_at_camera
+    w, h, spp = 48, 40, 256
+    mesh = _grey_scene()
+    cam = look_at_camera((0.0, 1.0, 8.0), (0.0, 0.0, 0.0), fov_y_deg=45.0, aspect=w / h)
+    base = dict(background_r=0.3, background_g=0.3, background_b=0.3, max_path_depth=5, min_samples=spp,
+                max_samples_per_pixel=spp)
+    tracer.configure(w, h, mesh)
+    tracer.set_camera(cam)
+    tracer.set_environment(None)
+    tracer.set_params(default_params(**base))
+    tracer.render(0)
+    rgb = tracer.readback()[0][..., :3].astype(np.float64)
+    tracer.set_params(default_params(spectral_wavelengths=8, **base))
+    tracer.render(0)
+    spec = tracer.readback()[0][..., :3].astype(np.float64)
+    ratio = spec.mean((0, 1)) / rgb.mean((0, 1))
+    assert np.all(np.abs(ratio - 1.0) <= 5e-3), ratio
+    assert np.all(rel_rmse(spec.reshape(-1, 3), rgb.reshape(-1, 3)) <= 0.05)
+
+
+def test_spectral_batch_matches_plain():
+    mesh_a = spectral_zoo_scene(n_per_mat=80, seed=11)
+    mesh_b = spectral_zoo_scene(n_per_mat=120, seed=12)
+    sizes = [(40, 32), (24, 24)]
+    params = default_params(background_r=0.1, background_g=0.12, background_b=0.2, max_path_depth=6,
+                            min_samples=4, max_samples_per_pixel=4, spectral_wavelengths=8)
+    plain = []
+    with PathTracer(0) as t:
+        for mesh, (w, h) in zip([mesh_a, mesh_b], sizes):
+            t.configure(w, h, mesh)
+            t.set_camera(zoo_camera(w, h))
+            t.set_params(params)
+            t.render(0)
+            plain.append(t.readback()[0])
+    with PathTracer(0) as t:
+        t.batch_configure(sizes)
+        for k, (mesh, (w, h)) in enumerate(zip([mesh_a, mesh_b], sizes)):
+            t.batch_set_mesh(k, mesh)
+            t.batch_set_camera(k, zoo_camera(w, h))
+        t.set_params(params)
+        t.render(0)
+        for k in range(2):
+            assert np.array_equal(t.batch_readback(k)[0], plain[k]), f"scene {k} differs from its plain render"
+
+
+def test_spectral_rejects_bad_counts_and_backward(tracer):
+    mesh = spectral_zoo_scene(n_per_mat=20, seed=2)
+    tracer.configure(16, 16, mesh)
+    tracer.set_camera(zoo_camera(16, 16))
+    with pytest.raises(PathTracerError):
+        tracer.set_params(default_params(spectral_wavelengths=3))
+    tracer.set_params(default_params(min_samples=2, max_samples_per_pixel=2, spectral_wavelengths=4))
+    tracer.record_samples(2)
+    tracer.render(0)
+    with pytest.raises(PathTracerError):
+        tracer.backward(np.ones((16, 16, 3), np.float32), 2, 8)
+    tracer.record_samples(0)
