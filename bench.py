@@ -58,6 +58,9 @@ def parse_args():
     ap.add_argument("--config", choices=["plain-small", "plain-large", "batch", "adjoint"], default="plain-large")
     ap.add_argument("--opt-steps", type=int, default=200, help="Adam steps of the adjoint workload's optimisation")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],
+                    help="hero wavelengths per path: auto = the workload's own (plain-small 4, plain-large 8, "
+                         "batch and adjoint RGB), 0 = RGB like the reference's integrator")
     return ap.parse_args()
 
 
@@ -203,13 +206,28 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(spec, args.config),
+        "config": {**workload_config(spec, args.config), "colour": colour_note(0) + "; the B200 arm renders "
+                   + colour_note(wavelengths(args))},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": descr["cores"], "kind": kind,
                          "sample": descr["sample"]},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
     return 0
+
+
+WORKLOAD_WAVELENGTHS = {"plain-small": 4, "plain-large": 8, "batch": 0, "adjoint": 0}
+
+
+def wavelengths(args) -> int:
+    return WORKLOAD_WAVELENGTHS[args.config] if args.spectral == "auto" else int(args.spectral)
+
+
+def colour_note(nw: int) -> str:
+    if nw == 0:
+        return "RGB (the reference's integrator)"
+    return (f"hero-wavelength spectral, {nw} wavelengths per path over 380-780 nm, CIE 1931 x D65 -> linear sRGB "
+            "per sample")
 
 
 def workload_config(spec, name):
@@ -259,6 +277,8 @@ def run_b200(args):
         return float(t.item())
 
     spec = make_workload(args.config)
+    nw = wavelengths(args)
+    spec.params["spectral_wavelengths"] = nw
     stream = torch.cuda.current_stream()
     pt = PathTracer(local)
     pt.set_stream(stream.cuda_stream)
@@ -402,6 +422,7 @@ def run_b200(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**workload_config(spec, args.config), "parallelism": f"replicas{world}",
+                   "colour": colour_note(nw), "spectral_wavelengths": nw,
                    "bvh_nodes": int(st["bvh_nodes"]),
                    "mrays_per_s": (cp["rays_extend"] + cp["rays_shadow"]) / (total_ms / args.steps / 1e3) / 1e6,
                    "stage_ms_per_step": {k: round(v, 4) for k, v in stages.items()},
@@ -417,6 +438,8 @@ def run_b200(args):
         "clocks": clk,
     }
     if cpu is not None:
+        if nw > 0:
+            cpu["sample"] += "; renders RGB (the reference has no spectral integrator)"
         out["cpu_baseline"] = cpu
     if rank == 0:
         print(json.dumps(out))

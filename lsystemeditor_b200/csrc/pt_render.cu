@@ -167,32 +167,40 @@ template <int NW> __device__ __forceinline__ bool cnonzero(const Col<NW>& a)
     }
 }
 
-// Wavelengths of a path (spectral mode).
+// Wavelengths of a path (spectral mode): the hero draw, wavelength k derived
+// on use (a few instructions, cheaper than keeping NW registers live).
 template <int NW> struct Waves {
-    float lam[NW > 0 ? NW : 1];
+    float u;
+    __device__ __forceinline__ float lam(int k) const { return spectral::heroLambda(u, k, NW); }
 };
 template <int NW> __device__ __forceinline__ Waves<NW> pathWaves(const LaunchCtx& c, uint32_t i)
 {
     Waves<NW> w;
     if constexpr (NW > 0) {
-        const float u = c.paths.hero[i];
-#pragma unroll
-        for (int k = 0; k < NW; ++k) {
-            w.lam[k] = spectral::heroLambda(u, k, NW);
-        }
+        w.u = c.paths.hero[i];
     } else {
-        w.lam[0] = 0.0f;
+        w.u = 0.0f;
     }
     return w;
 }
 
-// The spectrum of coefficient record q at the path's wavelengths.
+// The spectrum of coefficient record q at the path's wavelengths.  A grey
+// record (c = 0) is the constant scale / 2 and a zero scale is 0, exactly what
+// evalCoef gives for them, without its square root and division.
 template <int NW> __device__ __forceinline__ Col<NW> coefCol(float4 q, const Waves<NW>& w)
 {
     Col<NW> r;
+    if (q.x == 0.0f && q.y == 0.0f && q.z == 0.0f) {
+        const float v = __fmul_rn(0.5f, q.w);
 #pragma unroll
-    for (int k = 0; k < NW; ++k) {
-        r.v[k] = spectral::evalCoef(q, w.lam[k]);
+        for (int k = 0; k < NW; ++k) {
+            r.v[k] = v;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            r.v[k] = spectral::evalCoef(q, w.lam(k));
+        }
     }
     return r;
 }
@@ -302,10 +310,13 @@ __device__ __forceinline__ void matCoefs(const DevScene& S, uint32_t mi, const p
 // the RGB BSDF of the material with every colour channel set to the colour's
 // spectrum at lambda.  All lobes but a scattering subsurface lobe are affine in
 // the base colour, f(rho) = f(0) + rho (f(1) - f(0)), so one RGB evaluation
-// with base (0, 1, 1) gives every wavelength; with a scattering subsurface
-// lobe (radius per wavelength) each wavelength is evaluated on its own.
+// with base (0, 1, 1) gives every wavelength: in spectral mode the shade
+// kernel keeps the material's base at (0, 1, 1) (sampling and pdfs do not read
+// it).  With a scattering subsurface lobe (radius per wavelength) each
+// wavelength is evaluated on its own, cx's colour fields modified in place and
+// restored.
 template <int NW>
-__device__ __forceinline__ Col<NW> evalCol(const Ctx& cx, float3 wi, const Col<NW>& rho, float4 scatter, const Waves<NW>& w)
+__device__ __forceinline__ Col<NW> evalCol(Ctx& cx, float3 wi, const Col<NW>& rho, float4 scatter, const Waves<NW>& w)
 {
     Col<NW> f;
     if constexpr (NW == 0) {
@@ -315,20 +326,21 @@ __device__ __forceinline__ Col<NW> evalCol(const Ctx& cx, float3 wi, const Col<N
         f.c = bsdfEval(cx, wi);
     } else {
         if (cx.w.subsurface != 0.0f && maxScatter(cx.m) > kMinRadius) {
+            const float sr = cx.m.scatterR, sg = cx.m.scatterG, sb = cx.m.scatterB;
 #pragma unroll 1
             for (int k = 0; k < NW; ++k) {
-                Ctx ck = cx;
-                ck.m.r = ck.m.g = ck.m.b = rho.v[k];
-                const float rk = spectral::evalCoef(scatter, w.lam[k]);
-                ck.m.scatterR = ck.m.scatterG = ck.m.scatterB = rk;
-                f.v[k] = bsdfEval(ck, wi).x;
+                cx.m.r = cx.m.g = cx.m.b = rho.v[k];
+                const float rk = spectral::evalCoef(scatter, w.lam(k));
+                cx.m.scatterR = cx.m.scatterG = cx.m.scatterB = rk;
+                f.v[k] = bsdfEval(cx, wi).x;
             }
+            cx.m.r = 0.0f;
+            cx.m.g = cx.m.b = 1.0f;
+            cx.m.scatterR = sr;
+            cx.m.scatterG = sg;
+            cx.m.scatterB = sb;
         } else {
-            Ctx ca = cx;
-            ca.m.r = 0.0f;
-            ca.m.g = 1.0f;
-            ca.m.b = 1.0f;
-            const float3 e = bsdfEval(ca, wi);
+            const float3 e = bsdfEval(cx, wi);
             const float b = e.y - e.x;
 #pragma unroll
             for (int k = 0; k < NW; ++k) {
@@ -394,7 +406,7 @@ __device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, cons
         float3 a = f3(0.0f, 0.0f, 0.0f);
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
-            a = add3(a, scl3(spectral::responseAt(c.specResp, w.lam[k]), Lc.v[k]));
+            a = add3(a, scl3(spectral::responseAt(c.specResp, w.lam(k)), Lc.v[k]));
         }
         L = scl3(a, spectral::kLambdaRange / static_cast<float>(NW));
     }
@@ -541,6 +553,9 @@ template <bool Count>
 #ifndef PT_SHADE_MIN_BLOCKS
 #define PT_SHADE_MIN_BLOCKS 3
 #endif
+#ifndef PT_SHADE_SPEC_MIN_BLOCKS
+#define PT_SHADE_SPEC_MIN_BLOCKS 3
+#endif
 __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
 {
     const LaunchCtx& c = *cp;
@@ -625,7 +640,8 @@ __global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict_
 
 // Shading of the paths that hit a triangle. One thread per queued path.
 template <int NW>
-__global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const LaunchCtx* __restrict__ cp, int sel, int iter)
+__global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_SPEC_MIN_BLOCKS)
+    k_shade(const LaunchCtx* __restrict__ cp, int sel, int iter)
 {
     const LaunchCtx& c = *cp;
     const unsigned int count = c.q.counts[5 + 2 * (iter & 1)];
@@ -639,15 +655,21 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
         const DevScene& S = sceneOf(c, i);
         const Waves<NW> wv = pathWaves<NW>(c, i);
         const float4 r4 = c.paths.rad[i];
-        Col<NW> L = loadCol<NW>(r4, c.paths.radS, cap, i);
         const int depth = __float_as_int(r4.w);
-        // NEE contributions of the previous bounce, in the reference's order
-        // (the flags are clear for a path that starts at this bounce).
-        if (c.paths.visEnv[i]) {
-            L = cadd(L, pendingEnv<NW>(c, i));
-        }
-        if (c.paths.visEmis[i]) {
-            L = cadd(L, pendingEmis<NW>(c, i));
+        // RGB: the radiance stays in registers through the bounce.  Spectral: it
+        // is updated in memory (NEE of the previous bounce and the emission, in
+        // one read-modify-write below) and reloaded only by a path that ends.
+        Col<NW> L = czero<NW>();
+        if constexpr (NW == 0) {
+            L = loadCol<NW>(r4, c.paths.radS, cap, i);
+            // NEE contributions of the previous bounce, in the reference's order
+            // (the flags are clear for a path that starts at this bounce).
+            if (c.paths.visEnv[i]) {
+                L = cadd(L, pendingEnv<NW>(c, i));
+            }
+            if (c.paths.visEmis[i]) {
+                L = cadd(L, pendingEmis<NW>(c, i));
+            }
         }
         const float4 h4 = c.paths.hit[i];
         const uint32_t tri = __float_as_uint(h4.w);
@@ -683,18 +705,32 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
             // base colour at the path's wavelengths (spectral mode)
             Col<NW> rho;
             float4 scatterCoef = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            Col<NW> emis;
             if constexpr (NW == 0) {
                 rho.c = f3(cx.m.r, cx.m.g, cx.m.b);
-                emis.c = f3(cx.m.r * cx.m.emission, cx.m.g * cx.m.emission, cx.m.b * cx.m.emission);
+                // emission (PathIntegratorRandCore.h:248)
+                L = cadd(L, cmul(T, Col<0>{f3(cx.m.r * cx.m.emission, cx.m.g * cx.m.emission,
+                                               cx.m.b * cx.m.emission)}));
             } else {
                 float4 baseCoef;
                 matCoefs(S, mi, srcMat, tu, tv, baseCoef, scatterCoef);
                 rho = coefCol<NW>(baseCoef, wv);
-                emis = cscl(rho, cx.m.emission);
+                cx.m.r = 0.0f; // evalCol's affine form (the RGB base is not read again)
+                cx.m.g = 1.0f;
+                cx.m.b = 1.0f;
+                Col<NW> Lm = loadCol<NW>(r4, c.paths.radS, cap, i);
+                if (c.paths.visEnv[i]) {
+                    Lm = cadd(Lm, pendingEnv<NW>(c, i));
+                }
+                if (c.paths.visEmis[i]) {
+                    Lm = cadd(Lm, pendingEmis<NW>(c, i));
+                }
+                // emission (PathIntegratorRandCore.h:248)
+#pragma unroll
+                for (int q = 0; q < NW; ++q) {
+                    Lm.v[q] = Lm.v[q] + T.v[q] * (rho.v[q] * cx.m.emission);
+                }
+                storeCol<NW>(nullptr, c.paths.radS, cap, i, Lm, 0.0f);
             }
-            // emission (PathIntegratorRandCore.h:248)
-            L = cadd(L, cmul(T, emis));
             curandStateXORWOW st;
             rngLoad(c.paths, i, st);
             // environment NEE (PathIntegratorRandCore.h:65-108)
@@ -853,19 +889,48 @@ __global__ void __launch_bounds__(256, PT_SHADE_MIN_BLOCKS) k_shade(const Launch
             rngStore(c.paths, i, st);
         }
         (void)done;
-        c.paths.visEnv[i] = 0;
-        c.paths.visEmis[i] = 0;
-        if (cont) {
-            storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth + 1));
-            const uint32_t s = warpPush(nextCount);
-            nextQueue[s] = i;
-        } else if (pendEnv || pendEmis) {
-            storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth));
-            const uint32_t s = warpPush(&c.q.counts[3]);
-            c.q.finish[s] = i;
+        if constexpr (NW == 0) {
+            c.paths.visEnv[i] = 0;
+            c.paths.visEmis[i] = 0;
+            if (cont) {
+                storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth + 1));
+                const uint32_t s = warpPush(nextCount);
+                nextQueue[s] = i;
+            } else if (pendEnv || pendEmis) {
+                storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth));
+                const uint32_t s = warpPush(&c.q.counts[3]);
+                c.q.finish[s] = i;
+            } else {
+                writeSample<NW>(c, i, L, wv);
+                recyclePath<NW>(c, i, nextCount, nextQueue);
+            }
         } else {
-            writeSample<NW>(c, i, L, wv);
-            recyclePath<NW>(c, i, nextCount, nextQueue);
+            if (cont || pendEnv || pendEmis) {
+                // the radiance is in radS already
+                c.paths.rad[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(cont ? depth + 1 : depth));
+                if (cont) {
+                    const uint32_t s = warpPush(nextCount);
+                    nextQueue[s] = i;
+                } else {
+                    const uint32_t s = warpPush(&c.q.counts[3]);
+                    c.q.finish[s] = i;
+                }
+            } else {
+                L = loadCol<NW>(r4, c.paths.radS, cap, i);
+                if (depth >= c.maxDepth) {
+                    // (no read-modify-write happened: add the previous bounce's NEE here)
+                    if (c.paths.visEnv[i]) {
+                        L = cadd(L, pendingEnv<NW>(c, i));
+                    }
+                    if (c.paths.visEmis[i]) {
+                        L = cadd(L, pendingEmis<NW>(c, i));
+                    }
+                }
+                writeSample<NW>(c, i, L, wv);
+                recyclePath<NW>(c, i, nextCount, nextQueue);
+            }
+            c.paths.visEnv[i] = 0;
+            c.paths.visEmis[i] = 0;
         }
     }
 }

@@ -248,10 +248,10 @@ __host__ __device__ inline float heroU(uint32_t seed)
     return static_cast<float>(x >> 8) * (1.0f / 16777216.0f);
 }
 
-// Wavelength k of NW: 380 + 400 frac(u + k / NW).
+// Wavelength k of NW: 380 + 400 frac(u + k / NW) (k / NW is exact for NW = 4, 8).
 __device__ __forceinline__ float heroLambda(float u, int k, int nw)
 {
-    float t = __fadd_rn(u, __fdiv_rn(static_cast<float>(k), static_cast<float>(nw)));
+    float t = __fadd_rn(u, static_cast<float>(k) / static_cast<float>(nw));
     if (t >= 1.0f) {
         t = __fsub_rn(t, 1.0f);
     }
