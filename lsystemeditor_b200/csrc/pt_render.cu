@@ -402,13 +402,17 @@ __device__ __forceinline__ void writeSample(const LaunchCtx& c, uint32_t i, cons
         L = Lc.c;
     } else {
         // hero-wavelength estimate of linear sRGB: each wavelength is uniform
-        // over the range, so sum_k L_k resp(lambda_k) (range / NW)
-        float3 a = f3(0.0f, 0.0f, 0.0f);
+        // over the range, so sum_k L_k resp(lambda_k) (range / NW); a zero
+        // spectrum (a path that left a black scene) gives exactly 0
+        L = f3(0.0f, 0.0f, 0.0f);
+        if (cnonzero(Lc)) {
+            float3 a = f3(0.0f, 0.0f, 0.0f);
 #pragma unroll
-        for (int k = 0; k < NW; ++k) {
-            a = add3(a, scl3(spectral::responseAt(c.specResp, w.lam(k)), Lc.v[k]));
+            for (int k = 0; k < NW; ++k) {
+                a = add3(a, scl3(spectral::responseAt(c.specResp, w.lam(k)), Lc.v[k]));
+            }
+            L = scl3(a, spectral::kLambdaRange / static_cast<float>(NW));
         }
-        L = scl3(a, spectral::kLambdaRange / static_cast<float>(NW));
     }
     const uint32_t o = c.paths.outIdx[i];
     const float3 s = NW == 0 ? clampFirefly(L) : clampFireflySigned(L);
@@ -492,12 +496,9 @@ template <int NW> __device__ __forceinline__ void initPath(const LaunchCtx& c, u
     c.paths.thr[i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
     c.paths.rad[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
     if constexpr (NW > 0) {
+        // (the spectral throughput and radiance of a path at depth 0 are 1 and
+        // 0: they are not stored, the shade kernels know them)
         c.paths.hero[i] = spectral::heroU(seed);
-#pragma unroll
-        for (int q = 0; q < NW / 4; ++q) {
-            c.paths.thrS[static_cast<size_t>(q) * c.paths.capacity + i] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-            c.paths.radS[static_cast<size_t>(q) * c.paths.capacity + i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
     }
     c.paths.visEnv[i] = 0;
     c.paths.visEmis[i] = 0;
@@ -683,7 +684,19 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
         } else {
             const float4 o4 = c.paths.orig[i];
             const float4 t4 = c.paths.thr[i];
-            Col<NW> T = loadCol<NW>(t4, c.paths.thrS, cap, i);
+            Col<NW> T;
+            if constexpr (NW == 0) {
+                T = loadCol<NW>(t4, c.paths.thrS, cap, i);
+            } else {
+                if (depth == 0) {
+#pragma unroll
+                    for (int q = 0; q < NW; ++q) {
+                        T.v[q] = 1.0f;
+                    }
+                } else {
+                    T = loadCol<NW>(t4, c.paths.thrS, cap, i);
+                }
+            }
             float eta = t4.w;
             const float t = h4.x;
             const float3 pos = xadd(f3(o4.x, o4.y, o4.z), xscl(d, t));
@@ -717,7 +730,7 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                 cx.m.r = 0.0f; // evalCol's affine form (the RGB base is not read again)
                 cx.m.g = 1.0f;
                 cx.m.b = 1.0f;
-                Col<NW> Lm = loadCol<NW>(r4, c.paths.radS, cap, i);
+                Col<NW> Lm = depth == 0 ? czero<NW>() : loadCol<NW>(r4, c.paths.radS, cap, i);
                 if (c.paths.visEnv[i]) {
                     Lm = cadd(Lm, pendingEnv<NW>(c, i));
                 }

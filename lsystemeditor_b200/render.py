@@ -36,6 +36,8 @@ def main(argv=None) -> int:
     ap.add_argument("--frames", type=int, default=1)
     ap.add_argument("--capacity", type=int, default=0, help="path slots in flight (0 = library default)")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],
+                    help="hero wavelengths per path (auto: plain-small 4, plain-large 8; 0 = RGB)")
     ap.add_argument("--save", default="")
     ap.add_argument("--stage-times", action="store_true",
                     help="time every stage launch with CUDA events and print the per-stage totals and ray counts")
@@ -46,6 +48,8 @@ def main(argv=None) -> int:
     from .pathtracer import PROFILE_STAGE_TIMES, PathTracer
     spec = make_spec(a.workload, a.width, a.height)
     params = spec.params.copy()
+    params["spectral_wavelengths"] = {"plain-small": 4, "plain-large": 8}[a.workload] if a.spectral == "auto" \
+        else int(a.spectral)
     if a.spp > 0:
         params["min_samples"] = a.spp
         params["max_samples_per_pixel"] = a.spp
@@ -58,7 +62,10 @@ def main(argv=None) -> int:
         pt.set_params(params)
         if a.stage_times:
             pt.set_profiling(PROFILE_STAGE_TIMES)
+        nw = int(params["spectral_wavelengths"])
+        colour = f"{nw} wavelengths" if nw else "RGB"
         print(f"{spec.name}: {spec.mesh.triangle_count} triangles, {spec.width}x{spec.height}, "
+              f"{colour}, "
               f"scene ready in {time.perf_counter() - t0:.2f} s", flush=True)
         launched = pt.stats()["launches"]
         for f in range(a.frames):
