@@ -125,6 +125,15 @@ typedef struct pt_mesh {
     const pt_texture* textures;
 } pt_mesh;
 
+/* Placement of one object in an instanced scene (no reference counterpart:
+ * the reference flattens its ProceduralInstance list into one mesh,
+ * Application/src/MeshBuilder/MeshSceneContent.h:16-20). */
+typedef struct pt_instance {
+    float object_to_world[12]; /* 3 x 4 row-major: linear part | translation */
+    uint32_t object;           /* index into the objects of pt_set_instances  */
+    uint32_t pad[3];
+} pt_instance;
+
 /* Statistics of the accumulation (PathTracer.h:94-99 plus timings). */
 typedef struct pt_stats {
     int64_t waves;              /* currentSampleCount: full-resolution waves taken */
@@ -349,6 +358,46 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
  * (EnvironmentMap.cpp:76-128): marginal CDF (height + 1 floats) and row CDFs
  * (height x (width + 1)), HOST outputs, either may be NULL. */
 int pt_environment_tables(pt_renderer* r, float* marginal, float* row);
+
+/* ---- Instanced scenes and the distant light (extensions) -----------------
+ * pt_set_instances: `object_count` meshes (HOST arrays; the material and
+ * texture banks of objects[0] serve all objects) placed by `instance_count`
+ * instances.  Every object gets its own BVH and the instances a top-level BVH,
+ * all built on the device; rays are traversed in two levels (object-space rays
+ * for the objects).  Emissive triangles inside objects are reached by BSDF
+ * sampling only.  pt_export_mesh and pt_backward reject instanced scenes. */
+int pt_set_instances(pt_renderer* r, int scene, uint32_t object_count, const pt_mesh* objects,
+    uint32_t instance_count, const pt_instance* instances);
+
+/* Batch view: scene `scene` renders the geometry and materials of scene
+ * `source` (set before or after) with its own camera and image, so several
+ * views of one scene share their BVHs in one render.  Setting a mesh on
+ * `scene` ends the sharing. */
+int pt_batch_share_scene(pt_renderer* r, int scene, int source);
+
+/* Distant light: constant radiance inside a cone of half-angle `half_angle`
+ * (radians, 0 < half_angle < 1.5) around `direction` (towards the light).
+ * Radiance: `radiance` (RGB) when temperature_k <= 0, else a blackbody of that
+ * temperature whose linear sRGB has Rec. 709 luminance `luminance` (and whose
+ * spectrum is Planck's law in spectral mode).  It is sampled together with
+ * the environment: the next-event sample of the sky takes one extra random
+ * number, drawn just before the environment sample's two, to pick the light
+ * (probability 1/2, or 1 when the sky is black) or the environment, and is
+ * MIS-weighted against BSDF sampling by the
+ * mixture's density; escaping rays see environment plus light.  NULL or
+ * enabled = 0 removes it (the reference's estimator then runs unchanged).
+ * Preview passes show the environment only; pt_backward rejects a scene lit
+ * by it. */
+typedef struct pt_distant_light {
+    float direction[3];
+    float half_angle;
+    float radiance[3];
+    float temperature_k;
+    float luminance;
+    int32_t enabled;
+} pt_distant_light;
+
+int pt_set_distant_light(pt_renderer* r, const pt_distant_light* light);
 
 /* ---- Spectral mode (extension; the reference's integrator is RGB) ---------
  * With pt_render_params.spectral_wavelengths = 4 or 8, every path carries

@@ -189,7 +189,7 @@ struct PathStart {
     int maxDepth;
 };
 
-template <bool Grad>
+template <bool Grad, bool Inst = false>
 __device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 delta, float3 Ltot, GradAcc* acc,
     int materialCount, uint2* sstack)
 {
@@ -216,7 +216,7 @@ __device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 del
         // closest hit (k_extend)
         HitRec h;
         const bool hit =
-            traceRay<false, false>(S, ro, xnormalize(rd), tMin, kRayTMax, h, nullptr, nullptr, sstack, kAdjointBlock);
+            traceRay<false, false, Inst>(S, ro, xnormalize(rd), tMin, kRayTMax, h, nullptr, nullptr, sstack, kAdjointBlock);
         if (!hit) {
             // k_shade_miss: the pending next-event terms are already in L
             if (depth == 0) {
@@ -238,7 +238,7 @@ __device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 del
         const TriShade sh = S.shade[h.tri];
         float3 n;
         float tu, tv;
-        hitShading(sh, dn, h.u, h.v, n, tu, tv);
+        hitShadingAt(S, sh, h.inst, dn, h.u, h.v, n, tu, tv);
         const uint32_t mi = __float_as_uint(sh.d.w);
         const bool known = S.materials != nullptr && mi < S.materialCount;
         const pt_material& srcMat = known ? S.materials[mi] : kFallbackMaterial;
@@ -286,7 +286,7 @@ __device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 del
                     if (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f) {
                         const float3 so = add3(pos, scl3(n, kShadowBias));
                         HitRec hh;
-                        if (!traceRay<true, false>(S, so, xnormalize(wi), kShadowBias, kRayTMax, hh, nullptr, nullptr,
+                        if (!traceRay<true, false, Inst>(S, so, xnormalize(wi), kShadowBias, kRayTMax, hh, nullptr, nullptr,
                                 sstack, kAdjointBlock)) {
                             if (grad) {
                                 addNeeGrad(*acc, mi, fp, cx, wi, f, roughFollows, delta, T, Le, kk);
@@ -329,7 +329,7 @@ __device__ float3 replayPath(const LaunchCtx& c, const PathStart& ps, float3 del
                             const float3 contrib = mul3(T, mul3(f, scl3(Le, kk)));
                             if (contrib.x != 0.0f || contrib.y != 0.0f || contrib.z != 0.0f) {
                                 HitRec hh;
-                                if (!traceRay<true, false>(S, so, sdn, kShadowBias, kRayTMax, hh, nullptr, nullptr,
+                                if (!traceRay<true, false, Inst>(S, so, sdn, kShadowBias, kRayTMax, hh, nullptr, nullptr,
                                         sstack, kAdjointBlock)) {
                                     if (grad) {
                                         addNeeGrad(*acc, mi, fp, cx, wi, f, roughFollows, delta, T, Le, kk);
@@ -538,6 +538,7 @@ size_t adjointSmemBytes() { return sizeof(uint2) * kSharedStack * kAdjointBlock;
 // sample per pixel of a width x height image at the pixel centre, sample index
 // 0 and the given global seed, depth limit kPreviewMaxPathDepth
 // (PathTracerPreviewLevels.h:13), firefly-clamped.
+template <bool Inst>
 __global__ void __launch_bounds__(kAdjointBlock) k_preview(const LaunchCtx* __restrict__ cp, int width, int height,
     uint32_t globalSeed, int maxDepth, float4* out)
 {
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(kAdjointBlock) k_preview(const LaunchCtx* __re
         const PathStart start{static_cast<uint32_t>(p), static_cast<uint32_t>(width), static_cast<uint32_t>(height), 0u,
             globalSeed, false, maxDepth};
         const float3 L = clampFirefly(
-            replayPath<false>(c, start, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), nullptr, 0, sstack));
+            replayPath<false, Inst>(c, start, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), nullptr, 0, sstack));
         out[p] = make_float4(L.x, L.y, L.z, 1.0f);
     }
 }
@@ -557,9 +558,13 @@ __global__ void __launch_bounds__(kAdjointBlock) k_preview(const LaunchCtx* __re
 } // namespace
 
 void launchPreview(const LaunchCtx* ctx, int width, int height, uint32_t globalSeed, int maxDepth, float4* out,
-    int grid, cudaStream_t s)
+    int grid, bool inst, cudaStream_t s)
 {
-    k_preview<<<grid, kAdjointBlock, adjointSmemBytes(), s>>>(ctx, width, height, globalSeed, maxDepth, out);
+    if (inst) {
+        k_preview<true><<<grid, kAdjointBlock, adjointSmemBytes(), s>>>(ctx, width, height, globalSeed, maxDepth, out);
+    } else {
+        k_preview<false><<<grid, kAdjointBlock, adjointSmemBytes(), s>>>(ctx, width, height, globalSeed, maxDepth, out);
+    }
 }
 
 int adjointBlocksPerSm()

@@ -20,6 +20,6 @@ void launchAdjoint(const LaunchCtx* ctx, const float* dImage, int channels, int 
 // Preview pass of a width x height image (one centred sample per pixel, no
 // accumulation) into out, with the path-replay kernel.
 void launchPreview(const LaunchCtx* ctx, int width, int height, uint32_t globalSeed, int maxDepth, float4* out,
-    int grid, cudaStream_t s);
+    int grid, bool inst, cudaStream_t s);
 
 } // namespace pt

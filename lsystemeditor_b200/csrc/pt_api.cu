@@ -71,6 +71,14 @@ struct SceneSlot {
     DevBuf<float4> matSpec, texSpec;
     bool specValid = false;
     BvhBuffers bvh;
+    // instanced scene: one BVH per object, the top-level BVH over the instances
+    std::vector<BvhBuffers> objBvh;
+    BvhBuffers tlas;
+    DevBuf<float> tlasBoxes;
+    DevBuf<DevInstance> instances;
+    DevBuf<DevBlas> blases;
+    uint32_t instanceCount = 0;
+    int shareFrom = -1;           // batch view of another slot's geometry (-1: own geometry)
     uint32_t triCount = 0;
     uint32_t materialCount = 0;
     uint32_t textureCount = 0;
@@ -80,6 +88,21 @@ struct SceneSlot {
     int height = 0;
     uint32_t pixelBase = 0;
     pt_camera camera{};
+
+    void releaseInstances()
+    {
+        for (BvhBuffers& b : objBvh) {
+            b.release();
+            b.scratch.release();
+        }
+        objBvh.clear();
+        tlas.release();
+        tlas.scratch.release();
+        tlasBoxes.release();
+        instances.release();
+        blases.release();
+        instanceCount = 0;
+    }
 
     void release()
     {
@@ -92,6 +115,7 @@ struct SceneSlot {
         matSpec.release();
         texSpec.release();
         specValid = false;
+        releaseInstances();
         bvh.release();
         bvh.scratch.release();
         hasScene = false;
@@ -139,6 +163,7 @@ struct pt_renderer {
     std::map<std::array<uint32_t, 3>, spectral::Coef> specCache; // colour bits -> coefficients
     float4 specBackground{};
     int specCapacity = 0;
+    DevSun sun{};                         // distant light (enabled = 0: none)
     DevBuf<float> pHero;
     DevBuf<float4> pThrS, pRadS, pNeeEnvS, pNeeEmisS;
 
@@ -178,6 +203,7 @@ struct pt_renderer {
     DevBuf<uint4> pRngA;
     DevBuf<uint2> pRngB;
     DevBuf<float4> pOrig, pDir, pThr, pRad, pHit, pNeeEnv, pNeeEmis;
+    DevBuf<uint32_t> pHitInst;
     DevBuf<uint8_t> pVisEnv, pVisEmis;
     DevBuf<uint16_t> pScene;
     DevBuf<uint32_t> qExt0, qExt1, qFinish, qShadowPath, qMiss, qHit;
@@ -262,6 +288,15 @@ pt_material defaultMaterial()
     return m;
 }
 
+uint32_t sceneNodeCount(const SceneSlot& sl)
+{
+    uint32_t n = sl.instanceCount > 0 ? sl.tlas.nodeCount : sl.bvh.nodeCount;
+    for (const BvhBuffers& b : sl.objBvh) {
+        n += b.nodeCount;
+    }
+    return n;
+}
+
 DevScene deviceScene(const SceneSlot* r)
 {
     DevScene s;
@@ -275,6 +310,13 @@ DevScene deviceScene(const SceneSlot* r)
     s.emissiveCdf = r->emissiveCdf.p;
     s.matSpec = r->specValid ? r->matSpec.p : nullptr;
     s.texSpec = r->specValid ? r->texSpec.p : nullptr;
+    if (r->instanceCount > 0) {
+        s.tlasNodes = r->tlas.nodes;
+        s.tlasLeaves = r->tlas.tris;
+        s.instances = r->instances.p;
+        s.blases = r->blases.p;
+        s.instanceCount = r->hasScene ? r->instanceCount : 0u;
+    }
     s.nodeCount = r->hasScene ? r->bvh.nodeCount : 0u;
     s.triCount = r->triCount;
     s.materialCount = r->materialCount;
@@ -290,7 +332,7 @@ int ensurePaths(pt_renderer* r, int capacity)
     }
     const size_t Q = static_cast<size_t>(capacity);
     bool ok = r->pPixel.ensure(Q) && r->pOut.ensure(Q) && r->pRngA.ensure(Q) && r->pRngB.ensure(Q) &&
-        r->pOrig.ensure(Q) && r->pDir.ensure(Q) && r->pThr.ensure(Q) && r->pRad.ensure(Q) && r->pHit.ensure(Q) &&
+        r->pOrig.ensure(Q) && r->pDir.ensure(Q) && r->pThr.ensure(Q) && r->pRad.ensure(Q) && r->pHit.ensure(Q) && r->pHitInst.ensure(Q) &&
         r->pNeeEnv.ensure(Q) && r->pNeeEmis.ensure(Q) && r->pVisEnv.ensure(Q) && r->pVisEmis.ensure(Q) && r->pScene.ensure(Q) &&
         r->qExt0.ensure(Q) && r->qExt1.ensure(Q) && r->qFinish.ensure(Q) && r->qShadowPath.ensure(2 * Q) &&
         r->qMiss.ensure(Q) && r->qHit.ensure(Q) &&
@@ -334,6 +376,7 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.paths.thr = r->pThr.p;
     c.paths.rad = r->pRad.p;
     c.paths.hit = r->pHit.p;
+    c.paths.hitInst = r->pHitInst.p;
     c.paths.neeEnv = r->pNeeEnv.p;
     c.paths.neeEmis = r->pNeeEmis.p;
     c.paths.visEnv = r->pVisEnv.p;
@@ -376,6 +419,14 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.spectral = r->params.spectral_wavelengths;
     c.specResp = r->specResp.p;
     c.specBackground = r->specBackground;
+    c.sun = r->sun;
+    if (c.sun.enabled) {
+        // a black sky leaves every next-event sample to the light
+        const float k = r->params.environment_intensity;
+        const bool skyLit = r->envValid || r->params.background_r * k != 0.0f || r->params.background_g * k != 0.0f ||
+            r->params.background_b * k != 0.0f;
+        c.sun.select = skyLit ? 0.5f : 1.0f;
+    }
     return c;
 }
 
@@ -395,7 +446,7 @@ const LaunchCtx* uploadCtx(pt_renderer* r)
         r->hostViews.resize(n);
         for (size_t k = 0; k < n; ++k) {
             const SceneSlot& sl = r->scenes[k];
-            r->hostScenes[k] = deviceScene(&sl);
+            r->hostScenes[k] = deviceScene(sl.shareFrom >= 0 ? &r->scenes[static_cast<size_t>(sl.shareFrom)] : &sl);
             SceneView v{};
             v.cam = sl.camera;
             v.width = sl.width;
@@ -618,6 +669,68 @@ spectral::Coef colourCoef(pt_renderer* r, float cr, float cg, float cb)
 
 float4 coefToFloat4(const spectral::Coef& c) { return make_float4(c.c0, c.c1, c.c2, c.scale); }
 
+// The distant light's device record: frame, cone constants (double precision),
+// and its radiance: RGB as given, or a blackbody of the given temperature whose
+// sRGB (through the response table) has the given Rec. 709 luminance.
+int setDistantLight(pt_renderer* r, const pt_distant_light* l)
+{
+    r->sun = DevSun{};
+    if (l == nullptr || l->enabled == 0) {
+        return PT_OK;
+    }
+    const double dx = l->direction[0], dy = l->direction[1], dz = l->direction[2];
+    const double len = std::sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(len > 0.0) || !std::isfinite(len) || !(l->half_angle > 0.0f) || !(l->half_angle < 1.5f)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_distant_light: bad direction or half-angle");
+    }
+    const double d[3] = {dx / len, dy / len, dz / len};
+    // frame: the same construction as the BSDF's basis()
+    const double up[3] = {std::fabs(d[1]) < 0.999 ? 0.0 : 1.0, std::fabs(d[1]) < 0.999 ? 1.0 : 0.0, 0.0};
+    double t[3] = {up[1] * d[2] - up[2] * d[1], up[2] * d[0] - up[0] * d[2], up[0] * d[1] - up[1] * d[0]};
+    const double tl = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    for (double& x : t) {
+        x /= tl;
+    }
+    const double b[3] = {d[1] * t[2] - d[2] * t[1], d[2] * t[0] - d[0] * t[2], d[0] * t[1] - d[1] * t[0]};
+    DevSun& S = r->sun;
+    S.dir = make_float3(static_cast<float>(d[0]), static_cast<float>(d[1]), static_cast<float>(d[2]));
+    S.t = make_float3(static_cast<float>(t[0]), static_cast<float>(t[1]), static_cast<float>(t[2]));
+    S.b = make_float3(static_cast<float>(b[0]), static_cast<float>(b[1]), static_cast<float>(b[2]));
+    const double ha = l->half_angle;
+    const double omc = 2.0 * std::sin(0.5 * ha) * std::sin(0.5 * ha);
+    S.omc = static_cast<float>(omc);
+    S.sin2 = static_cast<float>(std::sin(ha) * std::sin(ha));
+    S.pdf = static_cast<float>(1.0 / (2.0 * 3.14159265358979323846 * omc));
+    S.temperature = l->temperature_k;
+    if (l->temperature_k > 0.0f) {
+        const std::vector<float>& resp = responseTable(r);
+        double rgb[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < spectral::kRespCount; ++i) {
+            const double lu = (380.0 + i) * 1.0e-3;
+            const double B = 1.0 / (lu * lu * lu * lu * lu * std::expm1(14387.769 / (lu * l->temperature_k)));
+            const double w = (i == 0 || i == spectral::kRespCount - 1) ? 0.5 : 1.0;
+            for (int c = 0; c < 3; ++c) {
+                rgb[c] += w * B * resp[4 * i + c];
+            }
+        }
+        const double K = 0.2126 * rgb[0] + 0.7152 * rgb[1] + 0.0722 * rgb[2];
+        if (!(K > 0.0)) {
+            return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_distant_light: temperature %g K gives no light",
+                static_cast<double>(l->temperature_k));
+        }
+        const double scale = l->luminance / K;
+        S.scale = static_cast<float>(scale);
+        S.rgb = make_float3(static_cast<float>(rgb[0] * scale), static_cast<float>(rgb[1] * scale),
+            static_cast<float>(rgb[2] * scale));
+    } else {
+        S.rgb = make_float3(l->radiance[0], l->radiance[1], l->radiance[2]);
+        S.coef = coefToFloat4(colourCoef(r, l->radiance[0], l->radiance[1], l->radiance[2]));
+    }
+    S.select = 1.0f;
+    S.enabled = 1;
+    return PT_OK;
+}
+
 // Response table, the scenes' and environment's spectrum coefficients and the
 // spectral path state, for a render with nw wavelengths per path.
 int prepareSpectral(pt_renderer* r, int nw)
@@ -631,7 +744,7 @@ int prepareSpectral(pt_renderer* r, int nw)
         PT_CHECK(r, cudaMemcpy(r->specResp.p, resp.data(), resp.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     for (SceneSlot& sl : r->scenes) {
-        if (sl.specValid) {
+        if (sl.specValid || sl.shareFrom >= 0) {
             continue;
         }
         std::vector<float4> mc(2 * std::max<size_t>(sl.hostMats.size(), 1));
@@ -723,7 +836,8 @@ int renderPreviews(pt_renderer* r)
         int w, h, ds;
         previewDims(r->width, r->height, r->previewLevels, lv, w, h, ds);
         launchPreview(c, w, h, static_cast<uint32_t>(lv + 1), kPreviewDepth,
-            r->previewBuf.p + previewOffset(r->width, r->height, r->previewLevels, lv), grid, r->stream);
+            r->previewBuf.p + previewOffset(r->width, r->height, r->previewLevels, lv), grid,
+            r->scenes[0].instanceCount > 0, r->stream);
         PT_CHECK(r, cudaGetLastError());
         r->launches += 1;
         r->previewDone = lv;
@@ -817,6 +931,8 @@ int setSceneMesh(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
     cudaStream_t s = r->stream;
     PT_CHECK(r, cudaEventRecord(r->ev0, s));
     sl.hasScene = false;
+    sl.shareFrom = -1;
+    sl.releaseInstances();
     sl.triCount = n;
     {
         const int st = uploadBank(r, sl, mesh);
@@ -847,7 +963,185 @@ int setSceneMesh(pt_renderer* r, SceneSlot& sl, const pt_mesh* mesh)
     sl.hasScene = true;
     uint32_t nodes = 0;
     for (const SceneSlot& x : r->scenes) {
-        nodes += x.hasScene ? x.bvh.nodeCount : 0u;
+        nodes += x.hasScene ? sceneNodeCount(x) : 0u;
+    }
+    r->stats.bvh_nodes = static_cast<int32_t>(nodes);
+    return resetAccum(r);
+}
+
+// Instanced scene (no reference counterpart: the reference flattens its
+// ProceduralInstance list into one mesh).  Objects are uploaded one after the
+// other (positions and shading records concatenated, each object's shading
+// records at its triBase), each gets its own BVH, and the instances' world
+// boxes (the object's vertex bounds through the transform) get a top-level BVH
+// built by the same builder from one box-shaped record per instance
+// (v0 = lo, v1 = hi, v2 = lo).
+int setSceneInstances(pt_renderer* r, SceneSlot& sl, uint32_t objectCount, const pt_mesh* objects,
+    uint32_t instanceCount, const pt_instance* inst)
+{
+    if (objectCount == 0 || objects == nullptr || instanceCount == 0 || inst == nullptr) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_instances: no objects or no instances");
+    }
+    uint64_t total = 0;
+    std::vector<uint32_t> triBase(objectCount);
+    std::vector<double> objLo(3 * objectCount, 0.0), objHi(3 * objectCount, 0.0);
+    for (uint32_t o = 0; o < objectCount; ++o) {
+        const pt_mesh& m = objects[o];
+        if (m.triangle_count > 0 && (m.positions == nullptr || m.normals == nullptr || m.uvs == nullptr ||
+                                        m.material_ids == nullptr)) {
+            return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_instances: object %u misses per-triangle arrays", o);
+        }
+        triBase[o] = static_cast<uint32_t>(total);
+        total += m.triangle_count;
+        for (int a = 0; a < 3; ++a) {
+            objLo[3 * o + a] = 1e300;
+            objHi[3 * o + a] = -1e300;
+        }
+        for (size_t k = 0; k < 3ull * m.triangle_count; ++k) {
+            for (int a = 0; a < 3; ++a) {
+                const double v = m.positions[3 * k + a];
+                objLo[3 * o + a] = std::min(objLo[3 * o + a], v);
+                objHi[3 * o + a] = std::max(objHi[3 * o + a], v);
+            }
+        }
+    }
+    if (total == 0 || total > 0x7FFFFFFFull) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_instances: %llu object triangles",
+            static_cast<unsigned long long>(total));
+    }
+    // instance records and world boxes
+    std::vector<DevInstance> dinst(instanceCount);
+    std::vector<float> boxes(9ull * instanceCount);
+    for (uint32_t i = 0; i < instanceCount; ++i) {
+        const pt_instance& I = inst[i];
+        if (I.object >= objectCount) {
+            return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_instances: instance %u names object %u of %u", i, I.object,
+                objectCount);
+        }
+        double M[3][4];
+        for (int a = 0; a < 3; ++a) {
+            for (int b = 0; b < 4; ++b) {
+                M[a][b] = I.object_to_world[4 * a + b];
+            }
+        }
+        const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
+            M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) + M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        if (!(std::fabs(det) > 1e-12) || !std::isfinite(det)) {
+            return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_instances: instance %u has a singular transform", i);
+        }
+        double Inv[3][3];
+        Inv[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det;
+        Inv[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+        Inv[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det;
+        Inv[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+        Inv[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det;
+        Inv[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+        Inv[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det;
+        Inv[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+        Inv[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+        DevInstance& D = dinst[i];
+        for (int a = 0; a < 3; ++a) {
+            const double tw = -(Inv[a][0] * M[0][3] + Inv[a][1] * M[1][3] + Inv[a][2] * M[2][3]);
+            D.w2o[a] = make_float4(static_cast<float>(Inv[a][0]), static_cast<float>(Inv[a][1]),
+                static_cast<float>(Inv[a][2]), static_cast<float>(tw));
+            D.o2w[a] = make_float4(static_cast<float>(M[a][0]), static_cast<float>(M[a][1]), static_cast<float>(M[a][2]),
+                static_cast<float>(M[a][3]));
+        }
+        D.meta = make_uint4(I.object, 0u, 0u, 0u);
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int c = 0; c < 8; ++c) {
+            const double p[3] = {(c & 1) ? objHi[3 * I.object] : objLo[3 * I.object],
+                (c & 2) ? objHi[3 * I.object + 1] : objLo[3 * I.object + 1],
+                (c & 4) ? objHi[3 * I.object + 2] : objLo[3 * I.object + 2]};
+            for (int a = 0; a < 3; ++a) {
+                const double w = M[a][0] * p[0] + M[a][1] * p[1] + M[a][2] * p[2] + M[a][3];
+                lo[a] = std::min(lo[a], w);
+                hi[a] = std::max(hi[a], w);
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            // widened by a relative margin so that float rounding of the object
+            // space ray cannot step outside
+            const double pad = 1e-5 * (hi[a] - lo[a]) + 1e-6 * std::max(std::fabs(lo[a]), std::fabs(hi[a])) + 1e-7;
+            boxes[9 * i + a] = static_cast<float>(lo[a] - pad);
+            boxes[9 * i + 3 + a] = static_cast<float>(hi[a] + pad);
+            boxes[9 * i + 6 + a] = static_cast<float>(lo[a] - pad);
+        }
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    cudaStream_t s = r->stream;
+    PT_CHECK(r, cudaEventRecord(r->ev0, s));
+    sl.hasScene = false;
+    sl.shareFrom = -1;
+    sl.releaseInstances();
+    sl.bvh.release();
+    int st = uploadBank(r, sl, &objects[0]);
+    if (st != PT_OK) {
+        return st;
+    }
+    const uint32_t n = static_cast<uint32_t>(total);
+    sl.triCount = n;
+    if (!sl.positions.ensure(9ull * n) || !sl.shade.ensure(n) || !r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "pt_set_instances: allocation failed for %u object triangles", n);
+    }
+    for (uint32_t o = 0; o < objectCount; ++o) {
+        const pt_mesh& m = objects[o];
+        const size_t e = m.triangle_count, b = triBase[o];
+        if (e == 0) {
+            continue;
+        }
+        PT_CHECK(r, cudaMemcpyAsync(sl.positions.p + 9 * b, m.positions, 9 * e * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9 * b, m.normals, 9 * e * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stage.p + 9ull * n + 6 * b, m.uvs, 6 * e * sizeof(float), cudaMemcpyHostToDevice, s));
+        PT_CHECK(r, cudaMemcpyAsync(r->stageIds.p + b, m.material_ids, e * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    }
+    launchBuildShade(r->stage.p, r->stage.p + 9ull * n, r->stageIds.p, n, sl.shade.p, s);
+    PT_CHECK(r, cudaGetLastError());
+    // emitters inside objects are reached by BSDF sampling only
+    sl.emissiveCount = 0;
+    if (!sl.emissiveIdx.ensure(1) || !sl.emissiveCdf.ensure(1)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "emissive list allocation failed");
+    }
+    PT_CHECK(r, cudaMemsetAsync(sl.emissiveCdf.p, 0, sizeof(float), s));
+    sl.objBvh.resize(objectCount);
+    std::vector<DevBlas> dblas(objectCount);
+    char err[256] = {0};
+    for (uint32_t o = 0; o < objectCount; ++o) {
+        const uint32_t e = objects[o].triangle_count;
+        dblas[o] = DevBlas{nullptr, nullptr, triBase[o], 0u};
+        if (e == 0) {
+            continue;
+        }
+        st = buildBvh(sl.positions.p + 9ull * triBase[o], e, sl.objBvh[o], s, r->bvhOptions, err, sizeof(err));
+        if (st != PT_OK) {
+            return fail(r, st, "object %u BVH build: %s", o, err);
+        }
+        dblas[o].nodes = sl.objBvh[o].nodes;
+        dblas[o].tris = sl.objBvh[o].tris;
+        dblas[o].nodeCount = sl.objBvh[o].nodeCount;
+    }
+    if (!sl.tlasBoxes.ensure(9ull * instanceCount) || !sl.instances.ensure(instanceCount) ||
+        !sl.blases.ensure(objectCount)) {
+        return fail(r, PT_ERR_OUT_OF_MEMORY, "instance tables allocation failed");
+    }
+    // (synchronous copies: the host vectors go out of scope)
+    PT_CHECK(r, cudaMemcpy(sl.tlasBoxes.p, boxes.data(), boxes.size() * sizeof(float), cudaMemcpyHostToDevice));
+    PT_CHECK(r, cudaMemcpy(sl.instances.p, dinst.data(), dinst.size() * sizeof(DevInstance), cudaMemcpyHostToDevice));
+    PT_CHECK(r, cudaMemcpy(sl.blases.p, dblas.data(), dblas.size() * sizeof(DevBlas), cudaMemcpyHostToDevice));
+    st = buildBvh(sl.tlasBoxes.p, instanceCount, sl.tlas, s, r->bvhOptions, err, sizeof(err));
+    if (st != PT_OK) {
+        return fail(r, st, "top-level BVH build: %s", err);
+    }
+    sl.instanceCount = instanceCount;
+    PT_CHECK(r, cudaEventRecord(r->ev1, s));
+    PT_CHECK(r, cudaEventSynchronize(r->ev1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+    r->stats.build_ms = ms;
+    sl.hasScene = true;
+    uint32_t nodes = 0;
+    for (const SceneSlot& x : r->scenes) {
+        nodes += x.hasScene ? sceneNodeCount(x) : 0u;
     }
     r->stats.bvh_nodes = static_cast<int32_t>(nodes);
     return resetAccum(r);
@@ -959,6 +1253,7 @@ int pt_destroy(pt_renderer* r)
     r->pThr.release();
     r->pRad.release();
     r->pHit.release();
+    r->pHitInst.release();
     r->pNeeEnv.release();
     r->pNeeEmis.release();
     r->pVisEnv.release();
@@ -1142,7 +1437,9 @@ int pt_render(pt_renderer* r, int waves)
         return fail(r, PT_ERR_NOT_CONFIGURED, "pt_render before pt_configure");
     }
     for (size_t k = 0; k < r->scenes.size(); ++k) {
-        if (!r->scenes[k].hasScene) {
+        const SceneSlot& sl = r->scenes[k];
+        const bool has = sl.shareFrom >= 0 ? r->scenes[static_cast<size_t>(sl.shareFrom)].hasScene : sl.hasScene;
+        if (!has) {
             return fail(r, PT_ERR_NO_SCENE, "pt_render before the mesh of scene %zu was set", k);
         }
     }
@@ -1157,6 +1454,10 @@ int pt_render(pt_renderer* r, int waves)
         if (st != PT_OK) {
             return st;
         }
+    }
+    bool inst = false;
+    for (const SceneSlot& sl : r->scenes) {
+        inst = inst || sl.instanceCount > 0;
     }
     const int nw = r->params.spectral_wavelengths;
     if (nw > 0) {
@@ -1222,7 +1523,7 @@ int pt_render(pt_renderer* r, int waves)
             const int iter = static_cast<int>(it & 0x7fffffff);
             {
                 StageTimer tm(r, kExtend);
-                launchExtend(c, sel, it == 0, iter, r->gridExtend, countVisits, s);
+                launchExtend(c, sel, it == 0, iter, r->gridExtend, countVisits, inst, s);
             }
             {
                 StageTimer tm(r, kShade);
@@ -1231,7 +1532,7 @@ int pt_render(pt_renderer* r, int waves)
             }
             {
                 StageTimer tm(r, kShadow);
-                launchShadow(c, iter, r->gridShadow, countVisits, s);
+                launchShadow(c, iter, r->gridShadow, countVisits, inst, s);
             }
             {
                 StageTimer tm(r, kFinalize);
@@ -1531,6 +1832,32 @@ int pt_batch_configure(pt_renderer* r, int scene_count, const int* widths, const
     return configureLayout(r, widths, heights);
 }
 
+int pt_batch_share_scene(pt_renderer* r, int scene, int source)
+{
+    if (r == nullptr || scene < 0 || source < 0 || scene == source || static_cast<size_t>(scene) >= r->scenes.size() ||
+        static_cast<size_t>(source) >= r->scenes.size() || r->scenes[static_cast<size_t>(source)].shareFrom >= 0) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_share_scene: bad scene %d or source %d", scene, source);
+    }
+    SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
+    for (const SceneSlot& x : r->scenes) {
+        if (x.shareFrom == scene) {
+            return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_batch_share_scene: scene %d is itself shared", scene);
+        }
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    const int w = sl.width, h = sl.height;
+    const uint32_t base = sl.pixelBase;
+    const pt_camera cam = sl.camera;
+    sl.release();
+    sl.width = w;
+    sl.height = h;
+    sl.pixelBase = base;
+    sl.camera = cam;
+    sl.shareFrom = source;
+    return resetAccum(r);
+}
+
 int pt_batch_set_mesh(pt_renderer* r, int scene, const pt_mesh* mesh)
 {
     if (r == nullptr || mesh == nullptr || scene < 0 || static_cast<size_t>(scene) >= r->scenes.size()) {
@@ -1615,6 +1942,8 @@ int pt_batch_set_tubes(pt_renderer* r, int scene, const pt_tubes* tubes, const p
     SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
     PT_CHECK(r, cudaEventRecord(r->ev0, s));
     sl.hasScene = false;
+    sl.shareFrom = -1;
+    sl.releaseInstances();
     int st = uploadBank(r, sl, extra);
     if (st != PT_OK) {
         return st;
@@ -1688,7 +2017,7 @@ int pt_batch_set_tubes(pt_renderer* r, int scene, const pt_tubes* tubes, const p
     sl.hasScene = true;
     uint32_t nodes = 0;
     for (const SceneSlot& x : r->scenes) {
-        nodes += x.hasScene ? x.bvh.nodeCount : 0u;
+        nodes += x.hasScene ? sceneNodeCount(x) : 0u;
     }
     r->stats.bvh_nodes = static_cast<int32_t>(nodes);
     return resetAccum(r);
@@ -1703,6 +2032,9 @@ int pt_export_mesh(pt_renderer* r, int scene, uint32_t* triangle_count, float* p
     const SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
     if (!sl.hasScene) {
         return fail(r, PT_ERR_NO_SCENE, "pt_export_mesh: scene %d has no mesh", scene);
+    }
+    if (sl.instanceCount > 0) {
+        return fail(r, PT_ERR_UNSUPPORTED, "pt_export_mesh: scene %d is instanced", scene);
     }
     PT_CHECK(r, cudaSetDevice(r->device));
     cudaStream_t s = r->stream;
@@ -1798,8 +2130,8 @@ int pt_set_materials(pt_renderer* r, int scene, uint32_t material_count, const p
         return st;
     }
     // the emissive list depends on the materials: rebuild it, with the material
-    // ids taken from the shading records
-    const uint32_t n = sl.triCount;
+    // ids taken from the shading records (instanced scenes have none)
+    const uint32_t n = sl.instanceCount > 0 ? 0u : sl.triCount;
     if (n > 0) {
         if (!r->stage.ensure(15ull * n) || !r->stageIds.ensure(n)) {
             return fail(r, PT_ERR_OUT_OF_MEMORY, "staging allocation failed");
@@ -1849,6 +2181,9 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
     if (r->params.spectral_wavelengths != 0) {
         return fail(r, PT_ERR_UNSUPPORTED, "pt_backward: the adjoint differentiates the RGB integrator only");
     }
+    if (r->scenes[0].instanceCount > 0 || r->sun.enabled) {
+        return fail(r, PT_ERR_UNSUPPORTED, "pt_backward: instanced scenes and the distant light are not differentiated");
+    }
     const SceneSlot& sl = r->scenes[0];
     if (!sl.hasScene) {
         return fail(r, PT_ERR_NO_SCENE, "pt_backward before pt_set_mesh");
@@ -1894,6 +2229,30 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
 // ---------------------------------------------------------------------------
 // Preview passes and region render (PathTracer.h:89-92, 134-140)
 // ---------------------------------------------------------------------------
+int pt_set_instances(pt_renderer* r, int scene, uint32_t object_count, const pt_mesh* objects,
+    uint32_t instance_count, const pt_instance* instances)
+{
+    if (r == nullptr || scene < 0 || static_cast<size_t>(scene) >= r->scenes.size()) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_instances: bad scene %d", scene);
+    }
+    return setSceneInstances(r, r->scenes[static_cast<size_t>(scene)], object_count, objects, instance_count,
+        instances);
+}
+
+int pt_set_distant_light(pt_renderer* r, const pt_distant_light* light)
+{
+    if (r == nullptr) {
+        return PT_ERR_INVALID_ARGUMENT;
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const int st = setDistantLight(r, light);
+    if (st != PT_OK) {
+        r->sun = DevSun{};
+        return st;
+    }
+    return resetAccum(r);
+}
+
 // Spectral mode helpers (host only; no device work).
 int pt_spectral_response(float* rgb, float* cie, float* xyz_to_rgb)
 {

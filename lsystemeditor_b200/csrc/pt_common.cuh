@@ -115,6 +115,22 @@ struct alignas(16) TriShade {
     float4 a, b, c, d;
 };
 
+// Instanced scenes (no reference counterpart; the reference flattens its
+// instances into one mesh, MeshSceneContent.h:16-20): an instance places one
+// object (a bottom-level BVH) with an affine transform.
+struct alignas(16) DevInstance {
+    float4 w2o[3]; // world -> object rows (linear part, translation in w)
+    float4 o2w[3]; // object -> world rows
+    uint4 meta;    // x = object index
+};
+
+struct DevBlas {
+    const CwNode* nodes;
+    const TriVerts* tris;  // leaf order, v0.w = the object's own triangle index
+    uint32_t triBase;      // first shading record of the object in the scene's shade array
+    uint32_t nodeCount;
+};
+
 struct DevScene {
     const CwNode* nodes = nullptr;
     const TriVerts* tris = nullptr;      // leaf order
@@ -129,6 +145,15 @@ struct DevScene {
     // albedo texture's colours [2 t] (constant / grid colour 1), [2 t + 1] (grid colour 2)
     const float4* matSpec = nullptr;
     const float4* texSpec = nullptr;
+    // instanced scene (instanceCount > 0): a top-level BVH over the instances'
+    // world boxes (its leaf records hold the instance index in v0.w), the
+    // instances and their objects; nodes / tris above are then unused and the
+    // shading records of all objects are concatenated in `shade`
+    const CwNode* tlasNodes = nullptr;
+    const TriVerts* tlasLeaves = nullptr;
+    const DevInstance* instances = nullptr;
+    const DevBlas* blases = nullptr;
+    uint32_t instanceCount = 0;
     uint32_t nodeCount = 0;
     uint32_t triCount = 0;
     uint32_t materialCount = 0;

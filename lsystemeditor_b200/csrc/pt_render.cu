@@ -279,6 +279,65 @@ template <int NW> __device__ __forceinline__ Col<NW> envCol(const LaunchCtx& c, 
     return r;
 }
 
+// --- distant light ---------------------------------------------------------------
+// Is direction d (any length) inside the light's cone?  Tested through the
+// sine (|d x dir|^2 <= sin^2 * |d|^2), which keeps its precision for the small
+// half-angles of a sun.
+__device__ __forceinline__ bool inSun(const DevSun& s, float3 d)
+{
+    const float3 x = cross3(d, s.dir);
+    return dot3(d, s.dir) > 0.0f && dot3(x, x) <= s.sin2 * dot3(d, d);
+}
+// Uniform direction in the cone (u1 -> 1 - cos theta over [0, omc], u2 -> phi).
+__device__ __forceinline__ float3 sunSample(const DevSun& s, float u1, float u2)
+{
+    const float h = u1 * s.omc;
+    const float ct = 1.0f - h;
+    const float st = sqrtf(fmax2(0.0f, h * (2.0f - h)));
+    float sp, cp;
+    sincosf(2.0f * kPi * u2, &sp, &cp);
+    return normalize3(add3(add3(scl3(s.t, st * cp), scl3(s.b, st * sp)), scl3(s.dir, ct)));
+}
+// Density of the sky's next-event sample (the light with probability select,
+// else the environment) in direction d.
+__device__ __forceinline__ float skyPdf(const LaunchCtx& c, float3 d)
+{
+    const float ls = inSun(c.sun, d) ? c.sun.pdf : 0.0f;
+    return c.sun.select * ls + (1.0f - c.sun.select) * envPdf(c.env, d);
+}
+// Relative blackbody spectral radiance (Planck's law, lambda in micrometres).
+__device__ __forceinline__ float planckRel(float lambdaNm, float temperature)
+{
+    const float lu = lambdaNm * 1.0e-3f;
+    const float l2 = lu * lu;
+    return 1.0f / (l2 * l2 * lu * expm1f(14387.769f / (lu * temperature)));
+}
+template <int NW> __device__ __forceinline__ Col<NW> sunCol(const LaunchCtx& c, const Waves<NW>& w)
+{
+    Col<NW> r;
+    if constexpr (NW == 0) {
+        (void)w;
+        r.c = c.sun.rgb;
+    } else if (c.sun.temperature > 0.0f) {
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            r.v[k] = c.sun.scale * planckRel(w.lam(k), c.sun.temperature);
+        }
+    } else {
+        r = coefCol<NW>(c.sun.coef, w);
+    }
+    return r;
+}
+// Sky radiance (environment plus the light where d is inside its cone).
+template <int NW> __device__ __forceinline__ Col<NW> skyCol(const LaunchCtx& c, float3 d, const Waves<NW>& w)
+{
+    Col<NW> L = envCol<NW>(c, d, w);
+    if (c.sun.enabled && inSun(c.sun, d)) {
+        L = cadd(L, sunCol<NW>(c, w));
+    }
+    return L;
+}
+
 // Spectrum coefficients of the base colour and scatter radii of the material
 // at a hit, following resolveMaterial's albedo-texture rules.
 __device__ __forceinline__ void matCoefs(const DevScene& S, uint32_t mi, const pt_material& src, float u, float v,
@@ -547,7 +606,7 @@ __global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ 
 // the hit queue of this bounce so that the two shade kernels run coherent work.
 // Counters: [4 + 2p] misses and [5 + 2p] hits of bounce parity p; this kernel
 // zeroes the other parity's pair for the next bounce.
-template <bool Count>
+template <bool Count, bool Inst>
 #ifndef PT_EXTEND_MIN_BLOCKS
 #define PT_EXTEND_MIN_BLOCKS 4
 #endif
@@ -588,10 +647,14 @@ __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const Laun
         const float4 d4 = c.paths.dir[i];
         const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
         HitRec h;
-        const bool hit = traceRay<false, Count>(sceneOf(c, i), f3(o4.x, o4.y, o4.z), dn, o4.w, kRayTMax, h, c.q.overflow,
+        const DevScene& S = sceneOf(c, i);
+        const bool hit = traceRay<false, Count, Inst>(S, f3(o4.x, o4.y, o4.z), dn, o4.w, kRayTMax, h, c.q.overflow,
             c.q.visits, smemStack + threadIdx.x, blockDim.x);
         if (hit) {
             c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+            if (Inst && S.instanceCount > 0) {
+                c.paths.hitInst[i] = h.inst;
+            }
             const uint32_t s = warpPush(&c.q.counts[5 + 2 * par]);
             c.q.hitQueue[s] = i;
         } else {
@@ -618,8 +681,9 @@ __global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict_
         const float4 r4 = c.paths.rad[i];
         const int depth = __float_as_int(r4.w);
         Col<NW> L;
+        const bool sunOn = c.sun.enabled != 0;
         if (depth == 0) {
-            L = envCol<NW>(c, d, wv);
+            L = sunOn ? skyCol<NW>(c, d, wv) : envCol<NW>(c, d, wv);
         } else {
             L = loadCol<NW>(r4, c.paths.radS, c.paths.capacity, i);
             if (c.paths.visEnv[i]) {
@@ -629,8 +693,8 @@ __global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict_
                 L = cadd(L, pendingEmis<NW>(c, i));
             }
             const Col<NW> T = loadCol<NW>(c.paths.thr[i], c.paths.thrS, c.paths.capacity, i);
-            const Col<NW> Le = envCol<NW>(c, d, wv);
-            const float lp = envPdf(c.env, d);
+            const Col<NW> Le = sunOn ? skyCol<NW>(c, d, wv) : envCol<NW>(c, d, wv);
+            const float lp = sunOn ? skyPdf(c, d) : envPdf(c.env, d);
             const float w = misBalance(d4.w, lp);
             L = cadd(L, cmul(T, cscl(Le, w)));
         }
@@ -704,7 +768,11 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
             const TriShade sh = S.shade[tri];
             float3 n;
             float tu, tv;
-            hitShading(sh, dn, h4.y, h4.z, n, tu, tv);
+            if (S.instanceCount == 0) {
+                hitShading(sh, dn, h4.y, h4.z, n, tu, tv);
+            } else {
+                hitShadingAt(S, sh, c.paths.hitInst[i], dn, h4.y, h4.z, n, tu, tv);
+            }
             const uint32_t mi = __float_as_uint(sh.d.w);
             const pt_material& srcMat =
                 (S.materials != nullptr && mi < S.materialCount) ? S.materials[mi] : kFallbackMaterial;
@@ -746,15 +814,27 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
             }
             curandStateXORWOW st;
             rngLoad(c.paths, i, st);
-            // environment NEE (PathIntegratorRandCore.h:65-108)
+            // environment NEE (PathIntegratorRandCore.h:65-108); with a distant
+            // light, one more draw first picks the light or the environment
             if (!skipsEnvNee(cx.m)) {
+                const bool sunOn = c.sun.enabled != 0;
+                const float uSel = sunOn ? curand_uniform(&st) : 0.0f;
                 const float u1 = curand_uniform(&st);
                 const float u2 = curand_uniform(&st);
                 float lp = 0.0f;
-                const float3 wi = envSample(c.env, u1, u2, lp);
+                float3 wi;
+                if (!sunOn) {
+                    wi = envSample(c.env, u1, u2, lp);
+                } else if (uSel < c.sun.select) {
+                    wi = sunSample(c.sun, u1, u2);
+                    lp = skyPdf(c, wi);
+                } else {
+                    wi = envSample(c.env, u1, u2, lp);
+                    lp = lp > kMinPdf ? skyPdf(c, wi) : 0.0f;
+                }
                 if (lp > kMinPdf) {
                     const float ct = fmax2(0.0f, dot3(n, wi));
-                    const Col<NW> Le = envCol<NW>(c, wi, wv);
+                    const Col<NW> Le = sunOn ? skyCol<NW>(c, wi, wv) : envCol<NW>(c, wi, wv);
                     // A light of exactly zero radiance (a black background) contributes
                     // exactly zero for any finite BSDF value: the BSDF is not evaluated.
                     if (ct > 0.0f && cnonzero(Le)) {
@@ -949,7 +1029,7 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
 }
 
 // Occlusion of the queued shadow rays (LightSamplingCore.h:187-197, 360-369).
-template <bool Count>
+template <bool Count, bool Inst>
 __global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__ cp, int iter)
 {
     const LaunchCtx& c = *cp;
@@ -974,7 +1054,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__
         const float4 d4 = c.q.shadowDir[k];
         const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
         HitRec h;
-        const bool occluded = traceRay<true, Count>(sceneOf(c, e & 0x7FFFFFFFu), f3(o4.x, o4.y, o4.z), dn, kShadowBias, kRayTMax, h,
+        const bool occluded = traceRay<true, Count, Inst>(sceneOf(c, e & 0x7FFFFFFFu), f3(o4.x, o4.y, o4.z), dn, kShadowBias, kRayTMax, h,
             c.q.overflow, c.q.visits + 2, smemStack + threadIdx.x, blockDim.x);
         if (!occluded) {
             const uint32_t i = e & 0x7FFFFFFFu;
@@ -1146,12 +1226,12 @@ __global__ void __launch_bounds__(256) k_trace_rays(DevScene S, int n, const flo
         const float3 ro = f3(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
         const float3 dn = xnormalize(f3(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
         HitRec h;
-        const bool ok = traceRay<false>(S, ro, dn, tmin[i], tmax[i], h);
+        const bool ok = traceRay<false, false, true>(S, ro, dn, tmin[i], tmax[i], h);
         hit[i] = ok ? 1 : 0;
         float3 nn = f3(0.0f, 0.0f, 0.0f);
         float tu = 0.0f, tv = 0.0f;
         if (ok) {
-            hitShading(S.shade[h.tri], dn, h.u, h.v, nn, tu, tv);
+            hitShadingAt(S, S.shade[h.tri], h.inst, dn, h.u, h.v, nn, tu, tv);
         }
         if (t) {
             t[i] = ok ? h.t : 0.0f;
@@ -1236,13 +1316,19 @@ void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaSt
         k_generate<0><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
     }
 }
-void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid, bool count, cudaStream_t s)
+void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid, bool count, bool inst, cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
-    if (count) {
-        k_extend<true><<<grid, 256, smem, s>>>(c, sel, identity, iter);
+    if (inst) {
+        if (count) {
+            k_extend<true, true><<<grid, 256, smem, s>>>(c, sel, identity, iter);
+        } else {
+            k_extend<false, true><<<grid, 256, smem, s>>>(c, sel, identity, iter);
+        }
+    } else if (count) {
+        k_extend<true, false><<<grid, 256, smem, s>>>(c, sel, identity, iter);
     } else {
-        k_extend<false><<<grid, 256, smem, s>>>(c, sel, identity, iter);
+        k_extend<false, false><<<grid, 256, smem, s>>>(c, sel, identity, iter);
     }
 }
 void launchShadeMiss(const LaunchCtx* c, int iter, int sel, int grid, int nw, cudaStream_t s)
@@ -1265,22 +1351,28 @@ void launchShade(const LaunchCtx* c, int sel, int iter, int grid, int nw, cudaSt
         k_shade<0><<<grid, 256, 0, s>>>(c, sel, iter);
     }
 }
-void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, cudaStream_t s)
+void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, bool inst, cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
-    if (count) {
-        k_shadow<true><<<grid, 256, smem, s>>>(c, iter);
+    if (inst) {
+        if (count) {
+            k_shadow<true, true><<<grid, 256, smem, s>>>(c, iter);
+        } else {
+            k_shadow<false, true><<<grid, 256, smem, s>>>(c, iter);
+        }
+    } else if (count) {
+        k_shadow<true, false><<<grid, 256, smem, s>>>(c, iter);
     } else {
-        k_shadow<false><<<grid, 256, smem, s>>>(c, iter);
+        k_shadow<false, false><<<grid, 256, smem, s>>>(c, iter);
     }
 }
 void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
 {
     extendBlocks = shadeBlocks = shadowBlocks = 1;
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extendBlocks, k_extend<false>, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extendBlocks, k_extend<false, false>, 256, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadeBlocks, k_shade<0>, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadowBlocks, k_shadow<false>, 256, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadowBlocks, k_shadow<false, false>, 256, smem);
 }
 void launchFinalize(const LaunchCtx* c, int sel, int grid, int nw, cudaStream_t s)
 {

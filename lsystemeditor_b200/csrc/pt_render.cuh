@@ -16,6 +16,7 @@ struct PathSoA {
     float4* thr = nullptr;       // throughput, medium IOR
     float4* rad = nullptr;       // radiance, depth (int bits)
     float4* hit = nullptr;       // t, u, v, triangle (uint bits, 0xFFFFFFFF = miss)
+    uint32_t* hitInst = nullptr; // instance of the hit (instanced scenes only)
     float4* neeEnv = nullptr;    // pending environment-NEE contribution
     float4* neeEmis = nullptr;   // pending emissive-NEE contribution
     uint8_t* visEnv = nullptr;   // 1 = that contribution is unoccluded
@@ -82,6 +83,24 @@ struct SceneView {
     uint32_t pad;
 };
 
+// Distant light (no reference counterpart): a cone of directions around
+// `dir` of constant radiance, sampled together
+// with the environment: the sky's next-event sample picks the light with
+// probability `select`, else the environment, and is weighted against BSDF
+// sampling by the mixture's density.
+struct DevSun {
+    float3 dir, t, b;   // unit direction towards the light and a frame around it
+    float omc;          // 1 - cos(half-angle), from double precision
+    float sin2;         // sin^2(half-angle)
+    float pdf;          // 1 / (2 pi omc): uniform over the cone
+    float select;
+    float3 rgb;         // RGB radiance
+    float temperature;  // spectral mode: > 0 -> scale * Planck(lambda, temperature)
+    float scale;
+    float4 coef;        // spectral mode, temperature <= 0: spectrum of rgb
+    int enabled;
+};
+
 struct LaunchCtx {
     DevScene scene;           // scene 0
     DevEnv env;
@@ -118,6 +137,7 @@ struct LaunchCtx {
     int spectral;
     const float4* specResp;
     float4 specBackground;
+    DevSun sun;
 };
 
 // Launchers. The LaunchCtx lives in DEVICE memory (one per renderer) and is
@@ -126,10 +146,11 @@ struct LaunchCtx {
 // `grid` is a persistent-style grid; kernels loop over device-side counts.
 // `nw` (generate, shade-miss, shade, finalize): wavelengths per path, 0 = RGB.
 void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s);
-void launchExtend(const LaunchCtx* d, int sel, bool identity, int iter, int grid, bool count, cudaStream_t s);
+// inst: compile-time instanced-scene traversal (any scene of the context instanced).
+void launchExtend(const LaunchCtx* d, int sel, bool identity, int iter, int grid, bool count, bool inst, cudaStream_t s);
 void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, int nw, cudaStream_t s);
 void launchShade(const LaunchCtx* d, int sel, int iter, int grid, int nw, cudaStream_t s);
-void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, cudaStream_t s);
+void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, bool inst, cudaStream_t s);
 void launchFinalize(const LaunchCtx* d, int sel, int grid, int nw, cudaStream_t s);
 void launchAccumulate(const LaunchCtx* d, int activeCount, int batch, cudaStream_t s);
 // Stable compaction of the active list (pixels neither converged nor at the

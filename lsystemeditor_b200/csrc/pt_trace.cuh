@@ -40,7 +40,8 @@ struct HitRec {
     float t;
     float u;
     float v;
-    uint32_t tri; // original triangle index, 0xFFFFFFFF = miss
+    uint32_t tri;  // original triangle index (instanced scene: shading-record index), 0xFFFFFFFF = miss
+    uint32_t inst; // instance of the hit in an instanced scene, else 0xFFFFFFFF
 };
 
 // Moller-Trumbore, MeshAccelIntersectCore.h:52-93, exact rounding.
@@ -88,6 +89,48 @@ __device__ __forceinline__ void hitShading(const TriShade& s, float3 dn, float b
     n = xnormalize(m);
     tu = __fadd_rn(__fadd_rn(__fmul_rn(s.a.w, bw), __fmul_rn(s.c.w, bu)), __fmul_rn(s.d.y, bv));
     tv = __fadd_rn(__fadd_rn(__fmul_rn(s.b.w, bw), __fmul_rn(s.d.x, bu)), __fmul_rn(s.d.z, bv));
+}
+
+// Affine transforms of an instance (rows r[0..2]: linear part, translation in w).
+__device__ __forceinline__ float3 xformPoint(const float4* r, float3 p)
+{
+    return f3(fmaf(r[0].x, p.x, fmaf(r[0].y, p.y, fmaf(r[0].z, p.z, r[0].w))),
+        fmaf(r[1].x, p.x, fmaf(r[1].y, p.y, fmaf(r[1].z, p.z, r[1].w))),
+        fmaf(r[2].x, p.x, fmaf(r[2].y, p.y, fmaf(r[2].z, p.z, r[2].w))));
+}
+__device__ __forceinline__ float3 xformVector(const float4* r, float3 v)
+{
+    return f3(fmaf(r[0].x, v.x, fmaf(r[0].y, v.y, r[0].z * v.z)), fmaf(r[1].x, v.x, fmaf(r[1].y, v.y, r[1].z * v.z)),
+        fmaf(r[2].x, v.x, fmaf(r[2].y, v.y, r[2].z * v.z)));
+}
+// Normal to world space: the transpose of the world -> object linear part.
+__device__ __forceinline__ float3 xformNormal(const float4* w2o, float3 n)
+{
+    return f3(fmaf(w2o[0].x, n.x, fmaf(w2o[1].x, n.y, w2o[2].x * n.z)),
+        fmaf(w2o[0].y, n.x, fmaf(w2o[1].y, n.y, w2o[2].y * n.z)),
+        fmaf(w2o[0].z, n.x, fmaf(w2o[1].z, n.y, w2o[2].z * n.z)));
+}
+
+// Shading normal (facing the world ray dn) and uv of a hit in any scene: for
+// an instanced scene the interpolated object-space normal is carried to world
+// space before the flip.
+__device__ __forceinline__ void hitShadingAt(const DevScene& S, const TriShade& sh, uint32_t inst, float3 dn, float bu,
+    float bv, float3& n, float& tu, float& tv)
+{
+    if (inst == 0xFFFFFFFFu || S.instanceCount == 0) {
+        hitShading(sh, dn, bu, bv, n, tu, tv);
+        return;
+    }
+    const float bw = __fsub_rn(__fsub_rn(1.0f, bu), bv);
+    const float3 n0 = f3(sh.a.x, sh.a.y, sh.a.z), n1 = f3(sh.b.x, sh.b.y, sh.b.z), n2 = f3(sh.c.x, sh.c.y, sh.c.z);
+    const float3 mo = xadd(xadd(xscl(n0, bw), xscl(n1, bu)), xscl(n2, bv));
+    float3 m = xnormalize(xformNormal(S.instances[inst].w2o, mo));
+    if (xdot(m, dn) > 0.0f) {
+        m = xscl(m, -1.0f);
+    }
+    n = m;
+    tu = __fadd_rn(__fadd_rn(__fmul_rn(sh.a.w, bw), __fmul_rn(sh.c.w, bu)), __fmul_rn(sh.d.y, bv));
+    tv = __fadd_rn(__fadd_rn(__fmul_rn(sh.b.w, bw), __fmul_rn(sh.d.x, bu)), __fmul_rn(sh.d.z, bv));
 }
 
 __device__ __forceinline__ bool isDegenerateDir(float3 dn)
@@ -156,6 +199,7 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
     HitRec& out)
 {
     out.tri = 0xFFFFFFFFu;
+    out.inst = 0xFFFFFFFFu;
     if (tMin > 0.0f || S.nodeCount == 0) {
         return false;
     }
@@ -247,18 +291,204 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
     return false;
 }
 
+// Two-level traversal of an instanced scene: the top-level BVH's leaves are
+// instances; on reaching one, the ray goes to the object's space
+// (o' = W2O o, d' = W2O d, unnormalised, so t is the same parameter) and the
+// object's BVH is traversed on the same stack above the top level's entries;
+// when those are used up the world ray is restored.  Exact-t ties go to the
+// larger (instance, leaf) pair.
+template <bool AnyHit, bool Count>
+__device__ __noinline__ bool traceInstanced(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, HitRec& out,
+    unsigned int* overflowCounter, unsigned long long* visits, uint2* sstack, int sstride)
+{
+    out.tri = 0xFFFFFFFFu;
+    out.inst = 0xFFFFFFFFu;
+    float3 ro = o, idir;
+    uint32_t oct = 0, octinv = 7;
+    auto setRay = [&](float3 a, float3 d) {
+        ro = a;
+        const float dx = fabsf(d.x) < 1.0e-20f ? copysignf(1.0e-20f, d.x) : d.x;
+        const float dy = fabsf(d.y) < 1.0e-20f ? copysignf(1.0e-20f, d.y) : d.y;
+        const float dz = fabsf(d.z) < 1.0e-20f ? copysignf(1.0e-20f, d.z) : d.z;
+        idir = f3(__frcp_rn(dx), __frcp_rn(dy), __frcp_rn(dz));
+        oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+        octinv = 7u - oct;
+    };
+    setRay(o, dn);
+    float3 rd = dn;
+    const CwNode* nodes = S.tlasNodes;
+    const TriVerts* leaves = S.tlasLeaves;
+    int level = 0, base = 0;
+    uint32_t curInst = 0, curTriBase = 0;
+    uint2 stack[kTraversalStack];
+    int sp = 0;
+    uint2 ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
+    uint2 tgroup = make_uint2(0u, 0u);
+    float closest = tMax;
+    unsigned long long bestKey = ~0ull;
+    uint32_t bestTri = 0xFFFFFFFFu, bestInst = 0xFFFFFFFFu;
+    float bu = 0.0f, bv = 0.0f;
+    bool overflow = false;
+    uint32_t nodeVisits = 0, triVisits = 0;
+    auto push = [&](uint2 g) -> bool {
+        if (sstack != nullptr && sp < kSharedStack) {
+            sstack[sp * sstride] = g;
+        } else if (sp < (sstack != nullptr ? kSharedStack : 0) + kTraversalStack) {
+            stack[sp - (sstack != nullptr ? kSharedStack : 0)] = g;
+        } else {
+            return false;
+        }
+        ++sp;
+        return true;
+    };
+    while (true) {
+        if (ngroup.y > 0x00FFFFFFu) {
+            const uint32_t bit = 31u - __clz(ngroup.y);
+            ngroup.y &= ~(1u << bit);
+            const uint32_t slot = (bit - 24u) ^ octinv;
+            const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
+            if (ngroup.y > 0x00FFFFFFu && !push(ngroup)) {
+                overflow = true;
+            }
+            uint32_t childBase, triBase, imask;
+            const uint32_t hits = intersectChildren(nodes, child, ro, idir, octinv, tMin, closest, childBase, triBase,
+                imask);
+            if (Count) {
+                ++nodeVisits;
+            }
+            ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
+            tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
+        } else {
+            tgroup = ngroup;
+            ngroup = make_uint2(0u, 0u);
+        }
+        while (tgroup.y != 0u) {
+            if (level == 0) {
+                // an instance: descend into its object
+                const int k = __ffs(tgroup.y) - 1;
+                tgroup.y &= tgroup.y - 1u;
+                const uint32_t inst = __float_as_uint(__ldg(&leaves[tgroup.x + k].v0.w));
+                bool saved = true;
+                if (ngroup.y > 0x00FFFFFFu) {
+                    saved = push(ngroup);
+                }
+                if (saved && tgroup.y != 0u) {
+                    saved = push(tgroup);
+                }
+                if (!saved) {
+                    overflow = true; // the rest of this top-level group is dropped
+                }
+                const DevInstance& I = S.instances[inst];
+                const DevBlas B = S.blases[I.meta.x];
+                curInst = inst;
+                curTriBase = B.triBase;
+                nodes = B.nodes;
+                leaves = B.tris;
+                rd = xformVector(I.w2o, dn);
+                setRay(xformPoint(I.w2o, o), rd);
+                level = 1;
+                base = sp;
+                ngroup = make_uint2(0u, B.nodeCount > 0 ? (0x80000000u | (1u << oct)) : 0u);
+                tgroup = make_uint2(0u, 0u);
+                break;
+            }
+            if (ngroup.y > 0x00FFFFFFu && __popc(__activemask()) < kPostponeLanes && push(tgroup)) {
+                break;
+            }
+            const int k = __ffs(tgroup.y) - 1;
+            tgroup.y &= tgroup.y - 1u;
+            const TriVerts tv = leaves[tgroup.x + k];
+            float t, u, v;
+            if (Count) {
+                ++triVisits;
+            }
+            if (intersectTriExact(ro, rd, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                    f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
+                const unsigned long long key =
+                    (static_cast<unsigned long long>(curInst) << 32) | static_cast<unsigned long long>(tgroup.x + k);
+                if (AnyHit) {
+                    if (t < tMax) {
+                        if (Count) {
+                            atomicAdd(&visits[0], static_cast<unsigned long long>(nodeVisits));
+                            atomicAdd(&visits[1], static_cast<unsigned long long>(triVisits));
+                        }
+                        out.t = t;
+                        out.u = u;
+                        out.v = v;
+                        out.tri = curTriBase + __float_as_uint(tv.v0.w);
+                        out.inst = curInst;
+                        return true;
+                    }
+                } else if (t < closest || key > bestKey || bestKey == ~0ull) {
+                    closest = t;
+                    bestKey = key;
+                    bestTri = curTriBase + __float_as_uint(tv.v0.w);
+                    bestInst = curInst;
+                    bu = u;
+                    bv = v;
+                }
+            }
+        }
+        if (ngroup.y <= 0x00FFFFFFu) {
+            if (level == 1 && sp == base) {
+                // the object is done: back to the top level in world space
+                level = 0;
+                nodes = S.tlasNodes;
+                leaves = S.tlasLeaves;
+                rd = dn;
+                setRay(o, dn);
+            }
+            if (ngroup.y <= 0x00FFFFFFu) {
+                if (sp == 0) {
+                    break;
+                }
+                --sp;
+                if (sstack != nullptr && sp < kSharedStack) {
+                    ngroup = sstack[sp * sstride];
+                } else {
+                    ngroup = stack[sp - (sstack != nullptr ? kSharedStack : 0)];
+                }
+            }
+        }
+    }
+    if (overflow && overflowCounter != nullptr) {
+        atomicAdd(overflowCounter, 1u);
+    }
+    if (Count) {
+        atomicAdd(&visits[0], static_cast<unsigned long long>(nodeVisits));
+        atomicAdd(&visits[1], static_cast<unsigned long long>(triVisits));
+    }
+    if (!AnyHit && bestTri != 0xFFFFFFFFu && closest < tMax) {
+        out.t = closest;
+        out.u = bu;
+        out.v = bv;
+        out.tri = bestTri;
+        out.inst = bestInst;
+        return true;
+    }
+    return false;
+}
+
 // Closest hit (AnyHit = false) or occlusion (AnyHit = true) for a normalised
 // direction dn. Returns true on a hit; out.tri is the ORIGINAL triangle index.
 // Count = true adds the nodes and triangles visited to visits[0] / visits[1].
 // The traversal stack lives in shared memory when `sstack` is given (this
 // thread's column of a [kSharedStack][blockDim] array, so that consecutive
 // threads hit consecutive banks), spilling to a local array beyond that.
-template <bool AnyHit, bool Count = false>
+// Inst = true compiles the instanced-scene branch in (kernels launched for
+// scenes without instances use Inst = false and keep their register budget).
+template <bool AnyHit, bool Count = false, bool Inst = false>
 __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, HitRec& out,
     unsigned int* overflowCounter = nullptr, unsigned long long* visits = nullptr, uint2* sstack = nullptr,
     int sstride = 0)
 {
     out.tri = 0xFFFFFFFFu;
+    out.inst = 0xFFFFFFFFu;
+    if constexpr (Inst) {
+        if (S.instanceCount > 0) {
+            return traceInstanced<AnyHit, Count>(S, o, dn, tMin, tMax, out, overflowCounter, visits, sstack, sstride);
+        }
+    }
     if (S.nodeCount == 0) {
         return false;
     }

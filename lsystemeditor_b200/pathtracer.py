@@ -53,6 +53,15 @@ PROFILE_STAGE_TIMES = 1
 PROFILE_COUNT_VISITS = 2
 
 
+class PtInstance(C.Structure):
+    _fields_ = [("object_to_world", C.c_float * 12), ("object", C.c_uint32), ("pad", C.c_uint32 * 3)]
+
+
+class PtDistantLight(C.Structure):
+    _fields_ = [("direction", C.c_float * 3), ("half_angle", C.c_float), ("radiance", C.c_float * 3),
+                ("temperature_k", C.c_float), ("luminance", C.c_float), ("enabled", C.c_int32)]
+
+
 class PtStats(C.Structure):
     _fields_ = [("waves", C.c_int64), ("active_pixels", C.c_int64), ("samples", C.c_int64), ("rays", C.c_int64),
                 ("launches", C.c_int64), ("render_ms", C.c_double), ("build_ms", C.c_double),
@@ -68,7 +77,8 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_batch_set_camera", "pt_batch_readback", "pt_batch_set_tubes", "pt_export_mesh",
                     "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
-                    "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift"]
+                    "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift",
+                    "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -130,6 +140,9 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_environment_tables.argtypes = [vp, _fp, _fp]
     L.pt_spectral_response.argtypes = [_fp, _fp, _fp]
     L.pt_spectral_uplift.argtypes = [C.c_uint32, _fp, _fp]
+    L.pt_set_instances.argtypes = [vp, C.c_int, C.c_uint32, C.POINTER(PtMesh), C.c_uint32, C.POINTER(PtInstance)]
+    L.pt_set_distant_light.argtypes = [vp, C.POINTER(PtDistantLight)]
+    L.pt_batch_share_scene.argtypes = [vp, C.c_int, C.c_int]
     _LIB = L
     return L
 
@@ -208,6 +221,36 @@ class PathTracer:
         self._mesh_keepalive = m
 
     rebuild_mesh_scene = set_mesh
+
+    def set_instances(self, objects, instances, scene: int = 0):
+        """Instanced scene: `objects` (list of HostMesh; objects[0]'s material and texture banks serve all) placed
+        by `instances`, a list of (object_to_world 3x4, object index).  One BVH per object, a top-level BVH over
+        the instances, both built on the device."""
+        keep = [self._pt_mesh(m) for m in objects]
+        arr = (PtMesh * len(keep))(*[s for _, s in keep])
+        inst = (PtInstance * len(instances))()
+        for k, (mat, obj) in enumerate(instances):
+            m = np.asarray(mat, np.float32).reshape(3, 4)
+            inst[k].object_to_world = (C.c_float * 12)(*m.reshape(-1).tolist())
+            inst[k].object = int(obj)
+        self._check(self._lib.pt_set_instances(self._h, int(scene), len(keep), arr, len(instances), inst))
+        self._mesh_keepalive = [m for m, _ in keep]
+
+    def set_distant_light(self, direction=None, half_angle: float = 0.0, radiance=(0.0, 0.0, 0.0),
+                          temperature_k: float = 0.0, luminance: float = 1.0):
+        """Distant light in a cone of `half_angle` radians around `direction` (towards the light): RGB
+        `radiance`, or a blackbody of `temperature_k` with Rec. 709 luminance `luminance`.  None removes it."""
+        if direction is None:
+            self._check(self._lib.pt_set_distant_light(self._h, None))
+            return
+        l = PtDistantLight()
+        l.direction = (C.c_float * 3)(*[float(x) for x in direction])
+        l.half_angle = float(half_angle)
+        l.radiance = (C.c_float * 3)(*[float(x) for x in radiance])
+        l.temperature_k = float(temperature_k)
+        l.luminance = float(luminance)
+        l.enabled = 1
+        self._check(self._lib.pt_set_distant_light(self._h, C.byref(l)))
 
     def set_camera(self, camera: np.ndarray):
         cam = np.ascontiguousarray(camera, CAMERA_DTYPE)
@@ -332,6 +375,10 @@ class PathTracer:
     def batch_set_mesh(self, scene: int, mesh: HostMesh):
         m, s = self._pt_mesh(mesh)
         self._check(self._lib.pt_batch_set_mesh(self._h, int(scene), C.byref(s)))
+
+    def batch_share_scene(self, scene: int, source: int):
+        """Scene `scene` renders scene `source`'s geometry with its own camera and image (one BVH, several views)."""
+        self._check(self._lib.pt_batch_share_scene(self._h, int(scene), int(source)))
 
     def batch_set_camera(self, scene: int, camera: np.ndarray):
         cam = np.ascontiguousarray(camera, CAMERA_DTYPE)

@@ -588,3 +588,103 @@ def config0_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth:
                             russian_roulette_min_depth=3, min_samples=spp, max_samples_per_pixel=spp)
     return SceneSpec("plain-small: 2D bracketed OL-system, 625 segments, 256x256, 64 spp, depth 8",
                      mesh, cam, params, width, height, spp)
+
+
+@dataclasses.dataclass
+class InstancedScene:
+    """Objects placed by instances (pt_set_instances).  ``objects[0]``'s material
+    and texture banks serve every object.  ``flatten`` bakes the instances into
+    one mesh, which is what the reference does with its ProceduralInstance list
+    (MeshSceneContent.h:16-20): the instanced render is checked against it."""
+    objects: List[HostMesh]
+    instances: List[Tuple[np.ndarray, int]]   # (3x4 object-to-world, object index)
+
+    @property
+    def triangle_count(self) -> int:
+        return int(sum(self.objects[o].triangle_count for _, o in self.instances))
+
+    @property
+    def unique_triangles(self) -> int:
+        return int(sum(m.triangle_count for m in self.objects))
+
+    def flatten(self) -> HostMesh:
+        parts = []
+        for mat, o in self.instances:
+            m = self.objects[o]
+            M = np.asarray(mat, np.float64).reshape(3, 4)
+            A, t = M[:, :3], M[:, 3]
+            N = np.linalg.inv(A).T
+            pos = (m.positions.reshape(-1, 3).astype(np.float64) @ A.T + t).astype(np.float32)
+            nrm = (m.normals.reshape(-1, 3).astype(np.float64) @ N.T).astype(np.float32)
+            parts.append(HostMesh(pos.reshape(-1, 3, 3), nrm.reshape(-1, 3, 3), m.uvs, m.material_ids,
+                                  np.zeros((0,), MATERIAL_DTYPE), np.zeros((0,), TEXTURE_DTYPE)))
+        flat = HostMesh.concat(parts)
+        flat.materials = self.objects[0].materials
+        flat.textures = self.objects[0].textures
+        return flat
+
+
+def placement(x: float, z: float, yaw: float, scale: float, y: float = 0.0) -> np.ndarray:
+    """3x4 object-to-world matrix: uniform scale, rotation about +Y by yaw (radians), translation."""
+    c, s = math.cos(yaw), math.sin(yaw)
+    return np.array([[scale * c, 0.0, scale * s, x], [0.0, scale, 0.0, y], [-scale * s, 0.0, scale * c, z]],
+                    np.float32)
+
+
+SUN_TEMPERATURE = 5800.0
+SUN_HALF_ANGLE = math.radians(0.53) * 0.5
+
+
+def forest_scene(width: int = 1920, height: int = 1080, trees: int = 12, instances: int = 500, seed: int = 200,
+                 extent: float = 200.0, sides: int = 40, rings: int = 16, views: int = 4, max_depth: int = 16,
+                 min_spp: int = 32, max_spp: int = 2048, rel_err: float = 0.01, iterations=(6, 8)):
+    """Large instanced forest: `trees` distinct stochastic trees of the plain-large
+    grammar (iterations drawn from 6..8, L-system seeds seed .. seed + trees - 1),
+    `instances` placements at seeded positions on an extent x extent ground with
+    random yaw and scale 0.7..1.3, the ground as one more object.  Light: a
+    sun-like distant light (0.53 degree cone, 5800 K blackbody, elevation 35
+    degrees) plus a uniform sky.  Cameras: `views` views orbiting the centre at
+    a seeded azimuth (the batched form renders them in one launch).  Adaptive
+    min_spp..max_spp to a relative standard error of rel_err, depth 16.  The
+    small forms used by the tests shrink `iterations`, `extent` and the counts.
+
+    Returns (InstancedScene, cameras, params, sun) with sun = dict(direction,
+    half_angle, temperature_k, luminance)."""
+    rng = np.random.default_rng(seed)
+    its = rng.integers(iterations[0], iterations[1] + 1, trees)
+    bark = default_material(**BARK)
+    leaf = default_material(**LEAF)
+    ground_mat = default_material(r=0.2, g=0.28, b=0.12, roughness=1.0)
+    objects = []
+    for k in range(trees):
+        segs, leaves = stochastic_tree(iterations=int(its[k]), seed=seed + k)
+        segs = refine_segments(segs, rings, taper=0.85)
+        ts = TubeSet.from_turtle(segs, leaves, sides, 0.18, leaf_material=1, extra=_bank([bark, leaf, ground_mat]))
+        objects.append(ts.host_mesh())
+    half = 0.5 * extent
+    ground = quad_mesh((0, 0, 0), (half, 0, 0), (0, 0, -half), ground_mat, normal=(0, 1, 0))
+    ground.material_ids[:] = 2
+    ground.materials = np.zeros((0,), MATERIAL_DTYPE)
+    objects.append(ground)
+    inst = []
+    pos = rng.uniform(-0.45 * extent, 0.45 * extent, size=(instances, 2))
+    yaw = rng.uniform(0.0, 2.0 * math.pi, instances)
+    scl = rng.uniform(0.7, 1.3, instances)
+    which = rng.integers(0, trees, instances)
+    for k in range(instances):
+        inst.append((placement(float(pos[k, 0]), float(pos[k, 1]), float(yaw[k]), float(scl[k])), int(which[k])))
+    inst.append((placement(0.0, 0.0, 0.0, 1.0), trees))
+    scene = InstancedScene(objects, inst)
+    az = rng.uniform(0.0, 2.0 * math.pi, views)
+    cams = []
+    for k in range(views):
+        r = 0.55 * extent
+        eye = (r * math.sin(az[k]), 6.0, r * math.cos(az[k]))
+        cams.append(look_at_camera(eye, (0.0, 4.0, 0.0), fov_y_deg=40.0, aspect=width / height))
+    params = default_params(background_r=0.45, background_g=0.55, background_b=0.75, max_path_depth=max_depth,
+                            russian_roulette_min_depth=3, min_samples=min_spp, max_samples_per_pixel=max_spp,
+                            relative_error_threshold=rel_err, adaptive_criterion=1)
+    el = math.radians(35.0)
+    sun = dict(direction=(math.cos(el) * 0.6, math.sin(el), math.cos(el) * 0.8), half_angle=SUN_HALF_ANGLE,
+               temperature_k=SUN_TEMPERATURE, luminance=3.0 / (2.0 * math.pi * (1.0 - math.cos(SUN_HALF_ANGLE))))
+    return scene, cams, params, sun

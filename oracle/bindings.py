@@ -131,6 +131,7 @@ class Checker:
             L.orc64_render_spectral.argtypes = spec + [_dp, _u32p, _dp, _dp, _u8p, C.c_int]
             L.orc_spec_eval.restype = C.c_float
             L.orc_spec_eval.argtypes = [_fp, C.c_float]
+            L.orc_scene_set_sun.argtypes = [C.c_void_p, C.c_int, _fp, C.c_float, _fp, C.c_float, C.c_float, _fp, _fp]
             L.orc_hero_lambda.restype = C.c_float
             L.orc_hero_lambda.argtypes = [C.c_uint, C.c_int, C.c_int]
 
@@ -360,6 +361,21 @@ class CheckerScene:
                                         _ptr(state["converged"], _u8p), int(threads))
         state["tape_errors"] = int(err)
         return state
+
+    def set_sun(self, direction=None, half_angle=0.0, radiance=(0.0, 0.0, 0.0), temperature_k=0.0, luminance=1.0,
+                resp=None, coef=None):
+        """Distant light of this scene (orc_scene_set_sun; None removes it).  resp: the 401 x 3 response table
+        (blackbody radiance); coef: spectrum coefficients of `radiance` (spectral renders, temperature <= 0)."""
+        assert self.chk.kind == "oracle"
+        if direction is None:
+            self.chk.lib.orc_scene_set_sun(self.h, 0, None, 0.0, None, 0.0, 0.0, None, None)
+            return
+        d = np.ascontiguousarray(direction, np.float32)
+        rad = np.ascontiguousarray(radiance, np.float32)
+        rs = None if resp is None else np.ascontiguousarray(resp, np.float32)
+        cf = None if coef is None else np.ascontiguousarray(coef, np.float32)
+        self.chk.lib.orc_scene_set_sun(self.h, 1, _ptr(d, _fp), C.c_float(half_angle), _ptr(rad, _fp),
+                                       C.c_float(temperature_k), C.c_float(luminance), _ptr(rs, _fp), _ptr(cf, _fp))
 
     def render_spectral(self, camera, params, width, height, waves, spectral, seed_base=1, tape=None, tape_stride=0,
                         env=None, state=None, threads=0, fp64=False):

@@ -449,6 +449,66 @@ int orc64_render_spectral(void* scene, void* env, const void* cam, const void* p
         acc, counts, lumMean, m2, converged, threads);
 }
 
+// Distant light of a scene (restated from the product's definition): frame,
+// cone constants in double, radiance RGB as given or a blackbody of the given
+// temperature scaled to Rec. 709 luminance `luminance` through the response
+// table resp (401 x 3, 1 nm from 380 nm); spectral coefficients of the RGB
+// radiance `coef` (4 floats) for temperature <= 0.  enabled = 0 removes it.
+void orc_scene_set_sun(void* h, int enabled, const float* dir, float halfAngle, const float* rgb, float temperature,
+    float luminance, const float* resp, const float* coef)
+{
+    Scene& s = *static_cast<Scene*>(h);
+    s.sun = SunSetup{};
+    if (!enabled) {
+        return;
+    }
+    SunSetup& l = s.sun;
+    const double len = std::sqrt(double(dir[0]) * dir[0] + double(dir[1]) * dir[1] + double(dir[2]) * dir[2]);
+    const double d[3] = {dir[0] / len, dir[1] / len, dir[2] / len};
+    const double up[3] = {std::fabs(d[1]) < 0.999 ? 0.0 : 1.0, std::fabs(d[1]) < 0.999 ? 1.0 : 0.0, 0.0};
+    double t[3] = {up[1] * d[2] - up[2] * d[1], up[2] * d[0] - up[0] * d[2], up[0] * d[1] - up[1] * d[0]};
+    const double tl = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    for (double& x : t) {
+        x /= tl;
+    }
+    const double b[3] = {d[1] * t[2] - d[2] * t[1], d[2] * t[0] - d[0] * t[2], d[0] * t[1] - d[1] * t[0]};
+    for (int k = 0; k < 3; ++k) {
+        l.dir[k] = static_cast<float>(d[k]);
+        l.t[k] = static_cast<float>(t[k]);
+        l.b[k] = static_cast<float>(b[k]);
+    }
+    const double omc = 2.0 * std::sin(0.5 * halfAngle) * std::sin(0.5 * halfAngle);
+    l.omc = static_cast<float>(omc);
+    l.sin2 = static_cast<float>(std::sin(double(halfAngle)) * std::sin(double(halfAngle)));
+    l.pdf = static_cast<float>(1.0 / (2.0 * 3.14159265358979323846 * omc));
+    l.temperature = temperature;
+    if (temperature > 0.0f) {
+        double c[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < 401; ++i) {
+            const double lu = (380.0 + i) * 1.0e-3;
+            const double B = 1.0 / (lu * lu * lu * lu * lu * std::expm1(14387.769 / (lu * temperature)));
+            const double w = (i == 0 || i == 400) ? 0.5 : 1.0;
+            for (int k = 0; k < 3; ++k) {
+                c[k] += w * B * resp[3 * i + k];
+            }
+        }
+        const double K = 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2];
+        const double scale = luminance / K;
+        l.scale = static_cast<float>(scale);
+        for (int k = 0; k < 3; ++k) {
+            l.rgb[k] = static_cast<float>(c[k] * scale);
+        }
+    } else {
+        for (int k = 0; k < 3; ++k) {
+            l.rgb[k] = rgb[k];
+        }
+        for (int k = 0; k < 4; ++k) {
+            l.coef[k] = coef != nullptr ? coef[k] : 0.0f;
+        }
+    }
+    l.enabled = true;
+}
+
 // The spectrum of coefficient record c at lambda (FP32, the product's operation order).
 float orc_spec_eval(const float* c, float lambda) { return specEval<float>(c, lambda); }
 

@@ -127,7 +127,22 @@ struct BvhNode {
     uint32_t left, right, triStart, triCount;
 };
 
+// Distant light (an extension with no reference counterpart), restated from
+// the product's definition: constant radiance in a cone around `dir`; the
+// sky's next-event sample picks it with probability select (1/2, or 1 when the
+// sky is black) after one extra draw, else the environment; MIS against BSDF
+// sampling uses the mixture density; escaping rays see environment + light.
+struct SunSetup {
+    bool enabled = false;
+    float dir[3] = {0, 0, 0}, t[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+    float omc = 0.0f, sin2 = 0.0f, pdf = 0.0f;
+    float rgb[3] = {0, 0, 0};
+    float temperature = 0.0f, scale = 0.0f;
+    float coef[4] = {0, 0, 0, 0};
+};
+
 struct Scene {
+    SunSetup sun;
     std::vector<TriRec> tris;
     std::vector<MaterialRec> materials;
     std::vector<TextureRec> textures;
@@ -1237,6 +1252,48 @@ template <class R> inline R envPdf(const Env* e, V3<R> d)
     return envPdfTable(e, x, y, uv.y);
 }
 
+template <class R> inline bool sunIn(const SunSetup& l, V3<R> d)
+{
+    const V3<R> sd = mk(R(l.dir[0]), R(l.dir[1]), R(l.dir[2]));
+    const V3<R> x = cross(d, sd);
+    return dot(d, sd) > R(0) && dot(x, x) <= R(l.sin2) * dot(d, d);
+}
+
+template <class R> inline V3<R> sunSampleDir(const SunSetup& l, R u1, R u2)
+{
+    using std::cos; using std::sin; using std::sqrt;
+    const R h = u1 * R(l.omc);
+    const R ct = R(1) - h;
+    const R st = sqrt(mx(R(0), h * (R(2) - h)));
+    const R ph = R(2) * Kc<R>::pi * u2;
+    const V3<R> t = mk(R(l.t[0]), R(l.t[1]), R(l.t[2])), b = mk(R(l.b[0]), R(l.b[1]), R(l.b[2]));
+    const V3<R> d = mk(R(l.dir[0]), R(l.dir[1]), R(l.dir[2]));
+    return nrm(add(add(scl(t, st * cos(ph)), scl(b, st * sin(ph))), scl(d, ct)));
+}
+
+inline float sunSelect(const Env* e, const ParamsRec* p)
+{
+    const float k = p->environmentIntensity;
+    const bool lit = envValid(e) || p->backgroundR * k != 0.0f || p->backgroundG * k != 0.0f || p->backgroundB * k != 0.0f;
+    return lit ? 0.5f : 1.0f;
+}
+
+template <class R> inline R skyPdfAt(const Scene& s, const Env* e, const ParamsRec* p, V3<R> d)
+{
+    const R sel = R(sunSelect(e, p));
+    const R ls = sunIn(s.sun, d) ? R(s.sun.pdf) : R(0);
+    return sel * ls + (R(1) - sel) * envPdf(e, d);
+}
+
+template <class R> inline V3<R> skyEval(const Scene& s, const Env* e, const ParamsRec* p, V3<R> d)
+{
+    V3<R> L = envEval(e, p, d);
+    if (s.sun.enabled && sunIn(s.sun, d)) {
+        L = add(L, mk(R(s.sun.rgb[0]), R(s.sun.rgb[1]), R(s.sun.rgb[2])));
+    }
+    return L;
+}
+
 template <class R> inline bool occluded(const Scene& s, V3<R> origin, V3<R> wi)
 {
     return traceRay(s, origin, wi, R(1.0e-4f), R(1.0e6f)).hit;
@@ -1440,10 +1497,21 @@ inline V3<R> neeEnvironment(const Scene& s, const Env* e, const ParamsRec* p, V3
     if (skipsEnvNee(m)) {
         return mk(R(0), R(0), R(0));
     }
+    const bool sunOn = s.sun.enabled;
+    const R uSel = sunOn ? R(rng.next()) : R(0);
     const R u1 = R(rng.next());
     const R u2 = R(rng.next());
     R lp = R(0);
-    const V3<R> wi = envSample(e, u1, u2, lp);
+    V3<R> wi;
+    if (!sunOn) {
+        wi = envSample(e, u1, u2, lp);
+    } else if (uSel < R(sunSelect(e, p))) {
+        wi = sunSampleDir(s.sun, u1, u2);
+        lp = skyPdfAt(s, e, p, wi);
+    } else {
+        wi = envSample(e, u1, u2, lp);
+        lp = lp > Kc<R>::minPdf ? skyPdfAt(s, e, p, wi) : R(0);
+    }
     if (lp <= Kc<R>::minPdf) {
         return mk(R(0), R(0), R(0));
     }
@@ -1455,7 +1523,7 @@ inline V3<R> neeEnvironment(const Scene& s, const Env* e, const ParamsRec* p, V3
         return mk(R(0), R(0), R(0));
     }
     const Ctx<R> c{n, wo, m, eta, 0};
-    const V3<R> L = envEval(e, p, wi);
+    const V3<R> L = sunOn ? skyEval(s, e, p, wi) : envEval(e, p, wi);
     const V3<R> f = bsdfEval(c, wi);
     const R bp = bsdfPdf(c, wi);
     const R w = misBalance(lp, bp);
@@ -1538,7 +1606,7 @@ inline V3<R> tracePath(const Scene& s, const Env* e, const ParamsRec* p, V3<R> r
     using std::isfinite;
     const Hit<R> first = traceRay(s, ro, rd, R(0), R(1.0e6f));
     if (!first.hit) {
-        return envEval(e, p, rd);
+        return s.sun.enabled ? skyEval(s, e, p, rd) : envEval(e, p, rd);
     }
     int maxDepth = 32, rrMin = 3, debug = 0;
     if (p != nullptr) {
@@ -1597,8 +1665,8 @@ inline V3<R> tracePath(const Scene& s, const Env* e, const ParamsRec* p, V3<R> r
         d = smp.dir;
         h = traceRay(s, o, d, bias, R(1.0e6f));
         if (!h.hit) {
-            const V3<R> Le = envEval(e, p, d);
-            const R lp = envPdf(e, d);
+            const V3<R> Le = s.sun.enabled ? skyEval(s, e, p, d) : envEval(e, p, d);
+            const R lp = s.sun.enabled ? skyPdfAt(s, e, p, d) : envPdf(e, d);
             const R w = misBalance(smp.pdf, lp);
             L = add(L, mul(T, scl(Le, w)));
             break;
@@ -1714,6 +1782,19 @@ template <class R> inline V3<R> specResponse(const float* resp, R lambda)
     return mk(R(a[0]) * v + R(b[0]) * w, R(a[1]) * v + R(b[1]) * w, R(a[2]) * v + R(b[2]) * w);
 }
 
+// Spectral radiance of the distant light at lambda (Planck's law in
+// micrometres times the scale, or the spectrum of its RGB radiance).
+template <class R> inline R specSun(const SunSetup& l, R lambda)
+{
+    using std::expm1;
+    if (l.temperature > 0.0f) {
+        const R lu = lambda * R(1.0e-3f);
+        const R l2 = lu * lu;
+        return R(l.scale) / (l2 * l2 * lu * expm1(R(14387.769f) / (lu * R(l.temperature))));
+    }
+    return specEval(l.coef, lambda);
+}
+
 template <class R> inline const float* specEnvCoef(const Env* e, const SpecSetup& sp, V3<R> d)
 {
     if (!envValid(e) || sp.env == nullptr) {
@@ -1779,11 +1860,16 @@ inline void tracePathSpectral(const Scene& s, const Env* e, const ParamsRec* p, 
     for (int k = 0; k < NW; ++k) {
         L[k] = R(0);
     }
+    const bool sunOn = s.sun.enabled;
     const Hit<R> first = traceRay(s, ro, rd, R(0), R(1.0e6f));
     if (!first.hit) {
         const float* q = specEnvCoef(e, sp, rd);
+        const bool inS = sunOn && sunIn(s.sun, rd);
         for (int k = 0; k < NW; ++k) {
             L[k] = specEval(q, lam[k]);
+            if (inS) {
+                L[k] = L[k] + specSun(s.sun, lam[k]);
+            }
         }
         return;
     }
@@ -1827,18 +1913,33 @@ inline void tracePathSpectral(const Scene& s, const Env* e, const ParamsRec* p, 
         R add1[kSpecMax], add2[kSpecMax];
         bool has1 = false, has2 = false;
         if (!skipsEnvNee(m)) {
+            const R uSel = sunOn ? R(rng.next()) : R(0);
             const R u1 = R(rng.next());
             const R u2 = R(rng.next());
             R lp = R(0);
-            const V3<R> wi = envSample(e, u1, u2, lp);
+            V3<R> wi;
+            if (!sunOn) {
+                wi = envSample(e, u1, u2, lp);
+            } else if (uSel < R(sunSelect(e, p))) {
+                wi = sunSampleDir(s.sun, u1, u2);
+                lp = skyPdfAt(s, e, p, wi);
+            } else {
+                wi = envSample(e, u1, u2, lp);
+                lp = lp > Kc<R>::minPdf ? skyPdfAt(s, e, p, wi) : R(0);
+            }
             if (lp > Kc<R>::minPdf && !occluded(s, add(pos, scl(n, R(1.0e-4f))), wi)) {
                 const R ct = mx(R(0), dot(n, wi));
                 if (ct > R(0)) {
                     const float* q = specEnvCoef(e, sp, wi);
+                    const bool inS = sunOn && sunIn(s.sun, wi);
                     const R bp = bsdfPdf(Ctx<R>{n, wo, m, eta, 0}, wi);
                     const R kw = misBalance(lp, bp) * ct / lp;
                     for (int k = 0; k < NW; ++k) {
-                        add1[k] = T[k] * (bsdfAt(k, wi) * (specEval(q, lam[k]) * kw));
+                        R Le = specEval(q, lam[k]);
+                        if (inS) {
+                            Le = Le + specSun(s.sun, lam[k]);
+                        }
+                        add1[k] = T[k] * (bsdfAt(k, wi) * (Le * kw));
                     }
                     has1 = true;
                 }
@@ -1945,10 +2046,15 @@ inline void tracePathSpectral(const Scene& s, const Env* e, const ParamsRec* p, 
         h = traceRay(s, o, d, bias, R(1.0e6f));
         if (!h.hit) {
             const float* q = specEnvCoef(e, sp, d);
-            const R lp = envPdf(e, d);
+            const R lp = sunOn ? skyPdfAt(s, e, p, d) : envPdf(e, d);
             const R w = misBalance(smp.pdf, lp);
+            const bool inS = sunOn && sunIn(s.sun, d);
             for (int k = 0; k < NW; ++k) {
-                L[k] = L[k] + T[k] * (specEval(q, lam[k]) * w);
+                R Le = specEval(q, lam[k]);
+                if (inS) {
+                    Le = Le + specSun(s.sun, lam[k]);
+                }
+                L[k] = L[k] + T[k] * (Le * w);
             }
             break;
         }
