@@ -9,7 +9,10 @@ adaptive 16-1024 spp, depth 12); --config plain-small selects the 20k-triangle
 2D tree at 256x256, 64 spp; --config batch the 64-scene batching workload
 (scenes built on the device, all rendered by one pt_render; the line also
 carries the time of the same scenes rendered one per pt_render); --config
-adjoint the differentiation workload (path-replay gradient, Adam steps).
+adjoint the differentiation workload (path-replay gradient, Adam steps);
+--config forest the instanced forest (263M instanced triangles, sun + sky, 4
+views of 1920x1080 per launch; a step takes about a minute, so run it with
+--steps 1).
 
   value  Msamples/s of the device-timed steps (CUDA events on the stream the
          library launches on), summed over ranks, time = max over ranks.
@@ -55,7 +58,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--config", choices=["plain-small", "plain-large", "batch", "adjoint"], default="plain-large")
+    ap.add_argument("--config", choices=["plain-small", "plain-large", "batch", "adjoint", "forest"],
+                    default="plain-large")
     ap.add_argument("--opt-steps", type=int, default=200, help="Adam steps of the adjoint workload's optimisation")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],
@@ -216,7 +220,7 @@ def run_reference(args):
     return 0
 
 
-WORKLOAD_WAVELENGTHS = {"plain-small": 4, "plain-large": 8, "batch": 0, "adjoint": 0}
+WORKLOAD_WAVELENGTHS = {"plain-small": 4, "plain-large": 8, "batch": 0, "adjoint": 0, "forest": 8}
 
 
 def wavelengths(args) -> int:
@@ -775,10 +779,203 @@ def run_adjoint(args):
     return 0
 
 
+def run_forest(args):
+    """The instanced forest: 500 instances of 12 trees (6.0M unique, 263M
+    instanced triangles), a 5800 K sun in a 0.53 degree cone plus a uniform
+    sky, 1920x1080, adaptive 32-2048 spp, depth 16, 8 hero wavelengths.  One
+    step renders the batched form, 4 camera views sharing the scene's BVHs in
+    one pt_render (value); the plain form (one view per render) is reported
+    beside it."""
+    import torch
+    import torch.distributed as dist
+
+    from lsystemeditor_b200.pathtracer import PROFILE_COUNT_VISITS, PROFILE_STAGE_TIMES, PathTracer
+    from lsystemeditor_b200.scene import forest_scene
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def reduce(x: float, op) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    W, H, V = 1920, 1080, 4
+    scene, cams, params, sun = forest_scene(width=W, height=H, views=V)
+    nw = wavelengths(args)
+    params["spectral_wavelengths"] = nw
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def setup(pt, objects):
+        pt.batch_configure([(W, H)] * V)
+        pt.set_instances(objects, scene.instances, scene=0)
+        for k in range(1, V):
+            pt.batch_share_scene(k, 0)
+        for k in range(V):
+            pt.batch_set_camera(k, cams[k])
+        pt.set_params(params)
+        pt.set_distant_light(**sun)
+
+    pt = PathTracer(local)
+    pt.set_stream(stream.cuda_stream)
+    setup(pt, scene.objects)
+
+    def step():
+        pt.reset_accumulation()
+        pt.render(0)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    launches0 = pt.stats()["launches"]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    samples = 0
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        step()
+        evs[k][1].record(stream)
+        samples += pt.stats()["samples"]
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = pt.stats()["launches"] - launches0
+    total_ms = reduce(float(sum(a.elapsed_time(b) for a, b in evs)), dist.ReduceOp.MAX if world > 1 else None)
+    value = reduce(float(samples), dist.ReduceOp.SUM if world > 1 else None) / (total_ms / 1e3) / 1e6
+
+    # ---- plain form (view 0 alone), stage times and traversal counts -------
+    plain = PathTracer(local)
+    plain.set_stream(stream.cuda_stream)
+    plain.configure(W, H)
+    plain.set_instances(scene.objects, scene.instances)
+    plain.set_camera(cams[0])
+    plain.set_params(params)
+    plain.set_distant_light(**sun)
+    plain.reset_accumulation()
+    plain.render(0)
+    plain.set_profiling(PROFILE_STAGE_TIMES)
+    flush.zero_()
+    plain.reset_accumulation()
+    plain.render(0)
+    ps, prof = plain.stats(), plain.profile()
+    plain_value = ps["samples"] / (ps["render_ms"] / 1e3) / 1e6
+    stages = {k[3:]: round(v, 3) for k, v in prof.items() if k.startswith("ms_")}
+    plain.set_profiling(PROFILE_COUNT_VISITS | PROFILE_STAGE_TIMES)
+    plain.reset_accumulation()
+    plain.render(0)
+    cp = plain.profile()
+    plain.close()
+    nodes_per_ray = cp["nodes_extend"] / max(cp["rays_extend"], 1)
+    tris_per_ray = cp["tris_extend"] / max(cp["rays_extend"], 1)
+    bytes_per_ray = 80.0 * nodes_per_ray + 48.0 * tris_per_ray + 32.0 + 16.0
+    rays_per_launch = prof["rays_extend"] / max(prof["launches_extend"], 1)
+    launch_ms = prof["ms_extend"] / max(prof["launches_extend"], 1)
+    achieved = bytes_per_ray * rays_per_launch / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # ---- end to end: objects from pinned host memory, 4 views, readback ----
+    keep = []
+
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(a.dtype).reshape(a.shape)
+        v[...] = a
+        keep.append(t)
+        return v
+
+    pobjs = []
+    h2d = 0
+    for mesh in scene.objects:
+        m = mesh.contiguous()
+        pm = type(m)(*[pinned(getattr(m, f)) for f in ("positions", "normals", "uvs", "material_ids", "materials",
+                                                         "textures")])
+        h2d += sum(getattr(m, f).nbytes for f in ("positions", "normals", "uvs", "material_ids", "materials",
+                                                   "textures"))
+        pobjs.append(pm)
+    h2d += 64 * len(scene.instances) + V * 80 + 64 + 40
+    d2h = V * W * H * (16 + 4 + 1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    setup(pt, pobjs)
+    pt.render(0)
+    e_samples = pt.stats()["samples"]
+    for k in range(V):
+        pt.batch_readback(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = reduce(float(e0.elapsed_time(e1)), dist.ReduceOp.MAX if world > 1 else None)
+    e_value = reduce(float(e_samples), dist.ReduceOp.SUM if world > 1 else None) / (e_ms / 1e3) / 1e6
+    st = pt.stats()
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"forest: {len(scene.instances) - 1} instances of {len(scene.objects) - 1} stochastic "
+                               f"trees + ground, {scene.unique_triangles} unique / {scene.triangle_count} instanced "
+                               f"triangles, sun 5800 K in a 0.53 degree cone + uniform sky, {V} views of {W}x{H}, "
+                               "adaptive 32-2048 spp to relative std-error 1e-2, depth 16",
+                   "views_per_launch": V, "colour": colour_note(nw), "spectral_wavelengths": nw,
+                   "plain_msamples_per_s": plain_value, "plain_ms_per_view": ps["render_ms"],
+                   "stage_ms_per_view": stages, "bvh_nodes": int(st["bvh_nodes"]),
+                   "l2": "flushed before every timed render (256 MiB write, untimed)",
+                   "parallelism": f"replicas{world}"},
+        "e2e": {"value": e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": (achieved / hbm_peak) if achieved else None, "traffic": None,
+                     "kernel": "k_extend<instanced> (two-level closest-hit traversal, plain view)",
+                     "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray, "tris_per_ray": tris_per_ray,
+                     "rays_per_launch": rays_per_launch, "launch_ms": launch_ms,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "cpu_baseline": {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
+                         "sample": "not run: the reference flattens the instances into one 263M-triangle mesh and "
+                                   "builds its BVH on one host thread, which alone exceeds a bench run"},
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    pt.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
+        if args.config == "forest":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference flattens the forest's 263M "
+                                  "instanced triangles and builds their BVH on one host thread; not runnable in a "
+                                  "bench's budget"}))
+            return 0
         return run_reference(args)
+    if args.config == "forest":
+        return run_forest(args)
     if args.config == "batch":
         return run_batch(args)
     if args.config == "adjoint":

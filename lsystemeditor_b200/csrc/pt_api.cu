@@ -1128,7 +1128,10 @@ int setSceneInstances(pt_renderer* r, SceneSlot& sl, uint32_t objectCount, const
     PT_CHECK(r, cudaMemcpy(sl.tlasBoxes.p, boxes.data(), boxes.size() * sizeof(float), cudaMemcpyHostToDevice));
     PT_CHECK(r, cudaMemcpy(sl.instances.p, dinst.data(), dinst.size() * sizeof(DevInstance), cudaMemcpyHostToDevice));
     PT_CHECK(r, cudaMemcpy(sl.blases.p, dblas.data(), dblas.size() * sizeof(DevBlas), cudaMemcpyHostToDevice));
-    st = buildBvh(sl.tlasBoxes.p, instanceCount, sl.tlas, s, r->bvhOptions, err, sizeof(err));
+    // one instance per top-level leaf: every instance box is tested before its object is entered
+    BvhBuildOptions topOptions = r->bvhOptions;
+    topOptions.maxLeafSize = 1;
+    st = buildBvh(sl.tlasBoxes.p, instanceCount, sl.tlas, s, topOptions, err, sizeof(err));
     if (st != PT_OK) {
         return fail(r, st, "top-level BVH build: %s", err);
     }

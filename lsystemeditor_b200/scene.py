@@ -661,8 +661,7 @@ def forest_scene(width: int = 1920, height: int = 1080, trees: int = 12, instanc
         segs = refine_segments(segs, rings, taper=0.85)
         ts = TubeSet.from_turtle(segs, leaves, sides, 0.18, leaf_material=1, extra=_bank([bark, leaf, ground_mat]))
         objects.append(ts.host_mesh())
-    half = 0.5 * extent
-    ground = quad_mesh((0, 0, 0), (half, 0, 0), (0, 0, -half), ground_mat, normal=(0, 1, 0))
+    ground = quad_mesh((0, 0, 0), (extent, 0, 0), (0, 0, -extent), ground_mat, normal=(0, 1, 0))
     ground.material_ids[:] = 2
     ground.materials = np.zeros((0,), MATERIAL_DTYPE)
     objects.append(ground)
@@ -678,7 +677,7 @@ def forest_scene(width: int = 1920, height: int = 1080, trees: int = 12, instanc
     az = rng.uniform(0.0, 2.0 * math.pi, views)
     cams = []
     for k in range(views):
-        r = 0.55 * extent
+        r = 0.47 * extent
         eye = (r * math.sin(az[k]), 6.0, r * math.cos(az[k]))
         cams.append(look_at_camera(eye, (0.0, 4.0, 0.0), fov_y_deg=40.0, aspect=width / height))
     params = default_params(background_r=0.45, background_g=0.55, background_b=0.75, max_path_depth=max_depth,
