@@ -62,6 +62,7 @@ def parse_args():
                     default="plain-large")
     ap.add_argument("--opt-steps", type=int, default=200, help="Adam steps of the adjoint workload's optimisation")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="batch workload: keep the default scheduling knobs")
     ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],
                     help="hero wavelengths per path: auto = the workload's own (plain-small 4, plain-large 8, "
                          "batch and adjoint RGB), 0 = RGB like the reference's integrator")
@@ -504,6 +505,9 @@ def run_batch(args):
     build_batch()
     torch.cuda.synchronize()
     build_s = time.perf_counter() - tb
+    # scheduling knobs chosen by the autotuner on short probes (untimed; the
+    # image does not depend on them)
+    tune = pt.autotune(waves=4) if not args.no_autotune else None
 
     def step():
         pt.reset_accumulation()
@@ -606,6 +610,7 @@ def run_batch(args):
                                f"{sum(t.triangle_count for t in tubes)} triangles, {sum(w * h for w, h in sizes)} "
                                "pixels, adaptive 16-512 spp to relative std-error 0.03, depth 12",
                    "scenes": n, "triangles": int(sum(t.triangle_count for t in tubes)),
+                   "autotune": tune, "frame_loop": "CUDA graphs of 4 bounce iterations",
                    "pixels": int(sum(w * h for w, h in sizes)), "parallelism": f"replicas{world}",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "host_generation_s": round(gen_s, 2), "device_build_s": round(build_s, 2),

@@ -399,6 +399,26 @@ typedef struct pt_distant_light {
 
 int pt_set_distant_light(pt_renderer* r, const pt_distant_light* light);
 
+/* ---- Autotuner (no reference counterpart) ---------------------------------
+ * Chooses the scheduling knobs for the current scene(s), camera(s) and
+ * parameters: path capacity (paths in flight, 2^20 .. 2^23), blocks per SM of
+ * the stage kernels (occupancy calculator, 2, 3, 4) and waves per launch
+ * (pt_render_params.samples_per_launch: automatic, 4, 16, 64), one knob at a
+ * time from the current configuration, each candidate timed on the device
+ * over `waves` waves from a reset accumulator.  The fastest is kept (also in
+ * the params) and the accumulation is reset.  The knobs change only how the
+ * work is scheduled: every candidate renders the same image. */
+typedef struct pt_tuning {
+    int32_t path_capacity;
+    int32_t blocks_per_sm;       /* 0 = occupancy calculator */
+    int32_t samples_per_launch;  /* 0 = automatic */
+    int32_t trials;
+    double ms_default;           /* probe time of the configuration it started from */
+    double ms_best;
+} pt_tuning;
+
+int pt_autotune(pt_renderer* r, int waves, pt_tuning* out);
+
 /* ---- Spectral mode (extension; the reference's integrator is RGB) ---------
  * With pt_render_params.spectral_wavelengths = 4 or 8, every path carries
  * that many wavelengths spread evenly over [380, 780] nm from a hero

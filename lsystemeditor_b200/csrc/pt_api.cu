@@ -213,6 +213,11 @@ struct pt_renderer {
     DevBuf<unsigned long long> qVisits;   // [0..1] extend nodes/tris, [2..3] shadow nodes/tris
     DevBuf<unsigned int> qOverflow;
     int gridExtend = 0, gridShade = 0, gridShadow = 0;
+    // CUDA graphs of four bounce iterations (the first block of a batch, later
+    // blocks) and the launch configuration they were captured for
+    cudaGraphExec_t bounceGraph[2] = {nullptr, nullptr};
+    unsigned long long bounceKey[6] = {0, 0, 0, 0, 0, 0};
+    bool useGraphs = true;
     int capacityWanted = 1 << 23;     // paths in flight per launch (one chunk for most frames)
     int blocksPerSmOverride = 0;
 
@@ -1150,6 +1155,67 @@ int setSceneInstances(pt_renderer* r, SceneSlot& sl, uint32_t objectCount, const
     return resetAccum(r);
 }
 
+void releaseBounceGraphs(pt_renderer* r)
+{
+    for (cudaGraphExec_t& g : r->bounceGraph) {
+        if (g != nullptr) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    }
+}
+
+// The graphs of four bounce iterations for this launch configuration
+// (captured on first use; false: run without graphs, e.g. when the caller's
+// stream is itself being captured).
+bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
+{
+    const unsigned long long key[6] = {reinterpret_cast<unsigned long long>(c), static_cast<unsigned long long>(r->gridExtend),
+        static_cast<unsigned long long>(r->gridShade), static_cast<unsigned long long>(r->gridShadow),
+        static_cast<unsigned long long>(inst ? 1 : 0) | (static_cast<unsigned long long>(nw) << 1),
+        reinterpret_cast<unsigned long long>(r->stream)};
+    if (r->bounceGraph[0] != nullptr && std::equal(key, key + 6, r->bounceKey)) {
+        return true;
+    }
+    releaseBounceGraphs(r);
+    cudaStream_t s = r->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        return false;
+    }
+    for (int g = 0; g < 2; ++g) {
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            releaseBounceGraphs(r);
+            r->useGraphs = false;
+            return false;
+        }
+        int sel = 0;
+        for (int it = 0; it < 4; ++it) {
+            launchExtend(c, sel, g == 0 && it == 0, it, r->gridExtend, false, inst, s);
+            launchShadeMiss(c, it, sel, r->gridShade, nw, s);
+            launchShade(c, sel, it, r->gridShade, nw, s);
+            launchShadow(c, it, r->gridShadow, false, inst, s);
+            launchFinalize(c, sel, r->gridShadow, nw, s);
+            sel ^= 1;
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (e != cudaSuccess || graph == nullptr ||
+            cudaGraphInstantiate(&r->bounceGraph[g], graph, 0) != cudaSuccess) {
+            if (graph != nullptr) {
+                cudaGraphDestroy(graph);
+            }
+            cudaGetLastError();
+            releaseBounceGraphs(r);
+            r->useGraphs = false;
+            return false;
+        }
+        cudaGraphDestroy(graph);
+    }
+    std::copy(key, key + 6, r->bounceKey);
+    return true;
+}
+
 } // namespace
 
 
@@ -1276,6 +1342,7 @@ int pt_destroy(pt_renderer* r)
     r->qOverflow.release();
     r->dctx.release();
     r->dbatch.release();
+    releaseBounceGraphs(r);
     for (cudaEvent_t e : r->eventPool) {
         cudaEventDestroy(e);
     }
@@ -1519,7 +1586,25 @@ int pt_render(pt_renderer* r, int waves)
         const long long maxIters =
             (jobs * (maxDepthEff + 1) + slots - 1) / std::max(slots, 1) + maxDepthEff + 8;
         int sel = 0;
-        for (long long it = 0;; ++it) {
+        const bool graphs = r->useGraphs && r->profileFlags == 0 && ensureBounceGraphs(r, c, inst, nw);
+        for (long long it = 0; graphs; it += 4) {
+            // the same four iterations as below, replayed from a graph: sel is 0
+            // again after four, and the kernels use only the parity of `iter`
+            if (it > maxIters) {
+                return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
+            }
+            PT_CHECK(r, cudaGraphLaunch(r->bounceGraph[it == 0 ? 0 : 1], s));
+            launches += 20;
+            r->profile.launches_extend += 4;
+            r->profile.launches_shadow += 4;
+            unsigned int live = 0;
+            PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+            PT_CHECK(r, cudaStreamSynchronize(s));
+            if (live == 0) {
+                break;
+            }
+        }
+        for (long long it = 0; !graphs; ++it) {
             if (it > maxIters) {
                 return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
             }
@@ -1775,6 +1860,7 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_tuning: bad arguments");
     }
     r->capacityWanted = path_capacity > 0 ? path_capacity : (1 << 23);
+    r->blocksPerSmOverride = blocks_per_sm;
     if (blocks_per_sm > 0) {
         r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
     } else {
@@ -1785,6 +1871,86 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
         r->gridShadow = r->smCount * std::max(bsh, 1);
     }
     return PT_OK;
+}
+
+int pt_autotune(pt_renderer* r, int waves, pt_tuning* out)
+{
+    if (r == nullptr || waves <= 0 || out == nullptr) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_autotune: bad arguments");
+    }
+    if (r->width <= 0) {
+        return fail(r, PT_ERR_NOT_CONFIGURED, "pt_autotune before pt_configure");
+    }
+    *out = pt_tuning{};
+    struct Knobs {
+        int capacity, blocks, perLaunch;
+    };
+    Knobs cur{r->capacityWanted, r->blocksPerSmOverride, r->params.samples_per_launch};
+    int trials = 0;
+    auto trial = [&](const Knobs& k, double& ms) -> int {
+        int st = pt_set_tuning(r, k.capacity, k.blocks);
+        if (st != PT_OK) {
+            return st;
+        }
+        r->params.samples_per_launch = k.perLaunch;
+        st = resetAccum(r);
+        if (st != PT_OK) {
+            return st;
+        }
+        st = pt_render(r, waves);
+        ms = r->stats.render_ms;
+        ++trials;
+        return st;
+    };
+    double ms = 0.0;
+    int st = trial(cur, ms); // warm-up: allocations, graphs
+    if (st == PT_OK) {
+        st = trial(cur, ms);
+    }
+    if (st != PT_OK) {
+        return st;
+    }
+    out->ms_default = ms;
+    Knobs best = cur;
+    double bestMs = ms;
+    const int capacities[4] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
+    const int blocks[4] = {0, 2, 3, 4};
+    const int perLaunch[4] = {0, 4, 16, 64};
+    for (int knob = 0; knob < 3; ++knob) {
+        const Knobs base = best;
+        for (int i = 0; i < 4; ++i) {
+            Knobs k = base;
+            if (knob == 0) {
+                k.capacity = capacities[i];
+            } else if (knob == 1) {
+                k.blocks = blocks[i];
+            } else {
+                k.perLaunch = perLaunch[i];
+            }
+            if (k.capacity == base.capacity && k.blocks == base.blocks && k.perLaunch == base.perLaunch) {
+                continue;
+            }
+            st = trial(k, ms);
+            if (st != PT_OK) {
+                return st;
+            }
+            if (ms < bestMs) {
+                bestMs = ms;
+                best = k;
+            }
+        }
+    }
+    st = pt_set_tuning(r, best.capacity, best.blocks);
+    if (st != PT_OK) {
+        return st;
+    }
+    r->params.samples_per_launch = best.perLaunch;
+    out->path_capacity = best.capacity;
+    out->blocks_per_sm = best.blocks;
+    out->samples_per_launch = best.perLaunch;
+    out->trials = trials;
+    out->ms_best = bestMs;
+    return resetAccum(r);
 }
 
 int pt_rng_tape(pt_renderer* r, int first_wave, int waves, int stride, float* out)

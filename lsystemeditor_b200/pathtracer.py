@@ -62,6 +62,11 @@ class PtDistantLight(C.Structure):
                 ("temperature_k", C.c_float), ("luminance", C.c_float), ("enabled", C.c_int32)]
 
 
+class PtTuning(C.Structure):
+    _fields_ = [("path_capacity", C.c_int32), ("blocks_per_sm", C.c_int32), ("samples_per_launch", C.c_int32),
+                ("trials", C.c_int32), ("ms_default", C.c_double), ("ms_best", C.c_double)]
+
+
 class PtStats(C.Structure):
     _fields_ = [("waves", C.c_int64), ("active_pixels", C.c_int64), ("samples", C.c_int64), ("rays", C.c_int64),
                 ("launches", C.c_int64), ("render_ms", C.c_double), ("build_ms", C.c_double),
@@ -78,7 +83,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
                     "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift",
-                    "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene"]
+                    "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -143,6 +148,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_set_instances.argtypes = [vp, C.c_int, C.c_uint32, C.POINTER(PtMesh), C.c_uint32, C.POINTER(PtInstance)]
     L.pt_set_distant_light.argtypes = [vp, C.POINTER(PtDistantLight)]
     L.pt_batch_share_scene.argtypes = [vp, C.c_int, C.c_int]
+    L.pt_autotune.argtypes = [vp, C.c_int, C.POINTER(PtTuning)]
     _LIB = L
     return L
 
@@ -533,6 +539,14 @@ class PathTracer:
         """PathTracer::pickSurface (PathTracer.cpp:1991-2013): tMin 0.001, tMax 1e30."""
         r = self.trace_rays(np.asarray(origin)[None], np.asarray(direction)[None], 0.001, 1.0e30)
         return {k: v[0] for k, v in r.items()}
+
+    def autotune(self, waves: int = 8) -> dict:
+        """pt_autotune: path capacity, blocks per SM and waves per launch chosen by timing `waves`-wave renders of
+        the current setup (the image does not depend on them); the accumulation is reset afterwards."""
+        t = PtTuning()
+        self._check(self._lib.pt_autotune(self._h, int(waves), C.byref(t)))
+        self._params["samples_per_launch"] = t.samples_per_launch
+        return {f: getattr(t, f) for f, _ in PtTuning._fields_}
 
     # -- runtime plumbing ---------------------------------------------------
     def set_stream(self, stream_handle: Optional[int]):
