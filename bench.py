@@ -359,6 +359,10 @@ def run_b200(args):
     except OSError:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    # the traversal's working set (nodes + leaf triangles) fits in L2 for the
+    # plain scenes: its own roof is the L2-resident read bandwidth, measured here
+    l2_peak = pt.measure_l2(32 << 20, 64)
+    working_set = 80.0 * pt.stats()["bvh_nodes"] + 48.0 * spec.mesh.triangle_count
     # DRAM bytes per k_extend ray from an ncu capture (profiles/), scaled to a launch
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_extend.json")
@@ -438,7 +442,10 @@ def run_b200(args):
                      "kernel": "k_extend (closest-hit traversal)",
                      "bytes_per_ray": bytes_per_ray, "nodes_per_ray": nodes_per_ray, "tris_per_ray": tris_per_ray,
                      "rays_per_launch": rays_per_launch, "launch_ms": launch_ms,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"},
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
+                     "l2": {"working_set_mb": working_set / 1e6, "peak_gbs": l2_peak,
+                            "frac": (achieved / l2_peak) if achieved and l2_peak else None,
+                            "peak_source": "pt_measure_l2: 32 MiB L2-resident 128-bit reads, measured in this run"}},
         "gpu_launches": int(launches),
         "clocks": clk,
     }

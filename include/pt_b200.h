@@ -419,6 +419,13 @@ typedef struct pt_tuning {
 
 int pt_autotune(pt_renderer* r, int waves, pt_tuning* out);
 
+/* L2-resident read bandwidth of this GPU (no reference counterpart; the roof
+ * of kernels whose working set fits in L2): 128-bit loads that bypass L1 over
+ * a `bytes` buffer (keep it well under the L2 size), `reps` passes after one
+ * warming pass, timed with events on the renderer's stream.  *gb_per_s
+ * receives bytes read / time. */
+int pt_measure_l2(pt_renderer* r, uint64_t bytes, int reps, double* gb_per_s);
+
 /* ---- Spectral mode (extension; the reference's integrator is RGB) ---------
  * With pt_render_params.spectral_wavelengths = 4 or 8, every path carries
  * that many wavelengths spread evenly over [380, 780] nm from a hero

@@ -11,6 +11,11 @@
 #include "pt_scene.cuh"
 #include "pt_spectral.cuh"
 
+namespace pt {
+// pt_l2probe.cu
+int measureL2ReadBandwidth(size_t bytes, int reps, int smCount, cudaStream_t s, double& gbPerS);
+} // namespace pt
+
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -1869,6 +1874,19 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
         r->gridExtend = r->smCount * std::max(be, 1);
         r->gridShade = r->smCount * std::max(bs, 1);
         r->gridShadow = r->smCount * std::max(bsh, 1);
+    }
+    return PT_OK;
+}
+
+int pt_measure_l2(pt_renderer* r, uint64_t bytes, int reps, double* gb_per_s)
+{
+    if (r == nullptr || gb_per_s == nullptr || bytes < 16 || reps <= 0) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_measure_l2: bad arguments");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    const int st = measureL2ReadBandwidth(static_cast<size_t>(bytes), reps, r->smCount, r->stream, *gb_per_s);
+    if (st != PT_OK) {
+        return fail(r, st, "pt_measure_l2: the measurement failed");
     }
     return PT_OK;
 }

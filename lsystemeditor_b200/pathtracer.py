@@ -83,7 +83,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
                     "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift",
-                    "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune"]
+                    "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune", "pt_measure_l2"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -149,6 +149,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_set_distant_light.argtypes = [vp, C.POINTER(PtDistantLight)]
     L.pt_batch_share_scene.argtypes = [vp, C.c_int, C.c_int]
     L.pt_autotune.argtypes = [vp, C.c_int, C.POINTER(PtTuning)]
+    L.pt_measure_l2.argtypes = [vp, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
     _LIB = L
     return L
 
@@ -547,6 +548,12 @@ class PathTracer:
         self._check(self._lib.pt_autotune(self._h, int(waves), C.byref(t)))
         self._params["samples_per_launch"] = t.samples_per_launch
         return {f: getattr(t, f) for f, _ in PtTuning._fields_}
+
+    def measure_l2(self, nbytes: int = 32 << 20, reps: int = 64) -> float:
+        """pt_measure_l2: L2-resident read bandwidth in GB/s."""
+        v = C.c_double()
+        self._check(self._lib.pt_measure_l2(self._h, int(nbytes), int(reps), C.byref(v)))
+        return float(v.value)
 
     # -- runtime plumbing ---------------------------------------------------
     def set_stream(self, stream_handle: Optional[int]):
