@@ -218,6 +218,8 @@ struct pt_renderer {
     DevBuf<unsigned long long> qVisits;   // [0..1] extend nodes/tris, [2..3] shadow nodes/tris
     DevBuf<unsigned int> qOverflow;
     int gridExtend = 0, gridShade = 0, gridShadow = 0;
+    int gridExtendLane = 0;          // grid of the per-lane closest-hit kernel
+    bool extendLane = false;         // per-lane ray replacement in this render's closest-hit stage
     // CUDA graphs of four bounce iterations (the first block of a batch, later
     // blocks) and the launch configuration they were captured for
     cudaGraphExec_t bounceGraph[2] = {nullptr, nullptr};
@@ -1170,6 +1172,16 @@ void releaseBounceGraphs(pt_renderer* r)
     }
 }
 
+#ifndef PT_EXTEND_LANE_MIN_NODES
+#define PT_EXTEND_LANE_MIN_NODES 32768
+#endif
+
+// Grid of the closest-hit stage: the per-lane kernel has its own occupancy.
+int extendGrid(const pt_renderer* r, bool count, bool inst)
+{
+    return (r->extendLane && !count && !inst) ? r->gridExtendLane : r->gridExtend;
+}
+
 // The graphs of four bounce iterations for this launch configuration
 // (captured on first use; false: run without graphs, e.g. when the caller's
 // stream is itself being captured).
@@ -1177,7 +1189,9 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
 {
     const unsigned long long key[6] = {reinterpret_cast<unsigned long long>(c), static_cast<unsigned long long>(r->gridExtend),
         static_cast<unsigned long long>(r->gridShade), static_cast<unsigned long long>(r->gridShadow),
-        static_cast<unsigned long long>(inst ? 1 : 0) | (static_cast<unsigned long long>(nw) << 1),
+        static_cast<unsigned long long>(inst ? 1 : 0) | (static_cast<unsigned long long>(nw) << 1) |
+            (static_cast<unsigned long long>(r->extendLane ? 1 : 0) << 8) |
+            (static_cast<unsigned long long>(r->gridExtendLane) << 9),
         reinterpret_cast<unsigned long long>(r->stream)};
     if (r->bounceGraph[0] != nullptr && std::equal(key, key + 6, r->bounceKey)) {
         return true;
@@ -1196,7 +1210,7 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
         }
         int sel = 0;
         for (int it = 0; it < 4; ++it) {
-            launchExtend(c, sel, g == 0 && it == 0, it, r->gridExtend, false, inst, s);
+            launchExtend(c, sel, g == 0 && it == 0, it, extendGrid(r, false, inst), false, inst, r->extendLane, s);
             launchShadeMiss(c, it, sel, r->gridShade, nw, s);
             launchShade(c, sel, it, r->gridShade, nw, s);
             launchShadow(c, it, r->gridShadow, false, inst, s);
@@ -1256,6 +1270,7 @@ int pt_create(pt_renderer** out, int device)
     r->gridExtend = r->smCount * std::max(be, 1);
     r->gridShade = r->smCount * std::max(bs, 1);
     r->gridShadow = r->smCount * std::max(bsh, 1);
+    r->gridExtendLane = r->smCount * extendLaneOccupancy();
     *out = r;
     return PT_OK;
 }
@@ -1531,9 +1546,14 @@ int pt_render(pt_renderer* r, int waves)
         }
     }
     bool inst = false;
+    uint32_t maxNodes = 0;
     for (const SceneSlot& sl : r->scenes) {
         inst = inst || sl.instanceCount > 0;
+        maxNodes = std::max(maxNodes, sl.bvh.nodeCount);
     }
+    // Per-lane ray replacement pays where traversals are long (large trees);
+    // on small scenes the extra routing launch costs more than it saves.
+    r->extendLane = !inst && maxNodes >= static_cast<uint32_t>(PT_EXTEND_LANE_MIN_NODES);
     const int nw = r->params.spectral_wavelengths;
     if (nw > 0) {
         const int st = prepareSpectral(r, nw);
@@ -1599,7 +1619,7 @@ int pt_render(pt_renderer* r, int waves)
                 return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
             }
             PT_CHECK(r, cudaGraphLaunch(r->bounceGraph[it == 0 ? 0 : 1], s));
-            launches += 20;
+            launches += 4 * (4 + extendKernels(false, inst, r->extendLane));
             r->profile.launches_extend += 4;
             r->profile.launches_shadow += 4;
             unsigned int live = 0;
@@ -1616,7 +1636,7 @@ int pt_render(pt_renderer* r, int waves)
             const int iter = static_cast<int>(it & 0x7fffffff);
             {
                 StageTimer tm(r, kExtend);
-                launchExtend(c, sel, it == 0, iter, r->gridExtend, countVisits, inst, s);
+                launchExtend(c, sel, it == 0, iter, extendGrid(r, countVisits, inst), countVisits, inst, r->extendLane, s);
             }
             {
                 StageTimer tm(r, kShade);
@@ -1631,7 +1651,7 @@ int pt_render(pt_renderer* r, int waves)
                 StageTimer tm(r, kFinalize);
                 launchFinalize(c, sel, r->gridShadow, nw, s);
             }
-            launches += 5;
+            launches += 4 + extendKernels(countVisits, inst, r->extendLane);
             r->profile.launches_extend += 1;
             r->profile.launches_shadow += 1;
             sel ^= 1;
@@ -1868,12 +1888,14 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
     r->blocksPerSmOverride = blocks_per_sm;
     if (blocks_per_sm > 0) {
         r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
+        r->gridExtendLane = r->smCount * std::min(blocks_per_sm, extendLaneOccupancy());
     } else {
         int be = 1, bs = 1, bsh = 1;
         stageOccupancy(be, bs, bsh);
         r->gridExtend = r->smCount * std::max(be, 1);
         r->gridShade = r->smCount * std::max(bs, 1);
         r->gridShadow = r->smCount * std::max(bsh, 1);
+        r->gridExtendLane = r->smCount * extendLaneOccupancy();
     }
     return PT_OK;
 }

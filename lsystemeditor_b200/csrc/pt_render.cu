@@ -664,6 +664,191 @@ __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const Laun
     }
 }
 
+#ifndef PT_EXTEND_LANE_THREADS
+#define PT_EXTEND_LANE_THREADS 256
+#endif
+#ifndef PT_EXTEND_LANE_MIN_BLOCKS
+#define PT_EXTEND_LANE_MIN_BLOCKS 3
+#endif
+
+// Closest hit with per-lane ray replacement (Aila & Laine 2009, "dynamic
+// fetch"): a lane whose ray is finished takes the next queue entry at once,
+// while the other lanes of its warp go on traversing, so a warp is not held
+// by its longest ray.  One loop iteration is one step of traceRay's
+// traversal (a node's children, then the triangles of that node), with the
+// same postponing, stacks and tie rule, so the hits are traceRay's.  Rays
+// finish in no particular order; the result of queue entry k goes back into
+// entry k (path index, bit 31 set for a miss) and k_route splits the queue
+// into the miss and hit queues in queue order afterwards.  Flat scenes only
+// (no instances, no visit counting).
+__global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLOCKS)
+    k_extend_lane(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
+{
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
+    const unsigned int count = c.q.counts[sel];
+    const int par = iter & 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&c.q.rays[0], static_cast<unsigned long long>(count));
+        c.q.counts[sel ^ 1] = 0u;
+        c.q.counts[2] = 0u;
+        c.q.counts[3] = 0u;
+        c.q.counts[4 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[5 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[8 + (par ^ 1)] = 0u;
+    }
+    uint32_t* queue = c.q.extend[sel];
+    unsigned int* fetch = &c.q.counts[8 + par];
+    uint2* sstack = smemStack + threadIdx.x;
+    const int sstride = blockDim.x;
+    uint2 stack[kTraversalStack];
+
+    bool active = false;
+    unsigned int k = 0;
+    uint32_t i = 0;
+    const DevScene* S = nullptr;
+    float3 o = f3(0.0f, 0.0f, 0.0f), dn = o, idir = o;
+    float tMin = 0.0f;
+    uint32_t octinv = 0;
+    uint2 ngroup = make_uint2(0u, 0u), tgroup = make_uint2(0u, 0u);
+    int sp = 0;
+    float closest = kRayTMax;
+    uint32_t best = 0xFFFFFFFFu;
+    float bu = 0.0f, bv = 0.0f;
+    bool overflow = false;
+
+    auto push = [&](uint2 g) -> bool {
+        if (sp < kSharedStack) {
+            sstack[sp * sstride] = g;
+        } else if (sp < kSharedStack + kTraversalStack) {
+            stack[sp - kSharedStack] = g;
+        } else {
+            return false;
+        }
+        ++sp;
+        return true;
+    };
+    for (;;) {
+        if (!active) {
+            // lanes without a ray take the next queue entries together (one atomic)
+            cg::coalesced_group g = cg::coalesced_threads();
+            unsigned int base = 0;
+            if (g.thread_rank() == 0) {
+                base = atomicAdd(fetch, g.size());
+            }
+            k = g.shfl(base, 0) + g.thread_rank();
+            if (k >= count) {
+                break; // the queue is drained
+            }
+            i = identity ? k : queue[k];
+            S = &sceneOf(c, i);
+            const float4 o4 = c.paths.orig[i];
+            const float4 d4 = c.paths.dir[i];
+            o = f3(o4.x, o4.y, o4.z);
+            tMin = o4.w;
+            dn = xnormalize(f3(d4.x, d4.y, d4.z));
+            if (S->nodeCount == 0 || isDegenerateDir(dn)) {
+                // empty scene, or quirk Q1: decided here without the wide traversal
+                HitRec h;
+                bool hit = false;
+                h.tri = 0xFFFFFFFFu;
+                if (S->nodeCount != 0) {
+                    hit = traceQ1(*S, o, dn, tMin, kRayTMax, false, h);
+                }
+                if (hit) {
+                    c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+                }
+                queue[k] = hit ? i : (i | 0x80000000u);
+                continue;
+            }
+            idir = f3(__frcp_rn(dn.x), __frcp_rn(dn.y), __frcp_rn(dn.z));
+            const uint32_t oct = (dn.x < 0.0f ? 4u : 0u) | (dn.y < 0.0f ? 2u : 0u) | (dn.z < 0.0f ? 1u : 0u);
+            octinv = 7u - oct;
+            ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
+            tgroup = make_uint2(0u, 0u);
+            sp = 0;
+            closest = kRayTMax;
+            best = 0xFFFFFFFFu;
+            bu = bv = 0.0f;
+            active = true;
+        }
+        // one traversal step (traceRay's loop body)
+        if (ngroup.y > 0x00FFFFFFu) {
+            const uint32_t bit = 31u - __clz(ngroup.y);
+            ngroup.y &= ~(1u << bit);
+            const uint32_t slot = (bit - 24u) ^ octinv;
+            const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
+            if (ngroup.y > 0x00FFFFFFu && !push(ngroup)) {
+                overflow = true;
+            }
+            uint32_t childBase, triBase, imask;
+            const uint32_t hits =
+                intersectChildren(S->nodes, child, o, idir, octinv, tMin, closest, childBase, triBase, imask);
+            ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
+            tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
+        } else {
+            tgroup = ngroup;
+            ngroup = make_uint2(0u, 0u);
+        }
+        while (tgroup.y != 0u) {
+            if (ngroup.y > 0x00FFFFFFu && __popc(__activemask()) < kPostponeLanes && push(tgroup)) {
+                break;
+            }
+            const int kt = __ffs(tgroup.y) - 1;
+            tgroup.y &= tgroup.y - 1u;
+            const TriVerts tv = S->tris[tgroup.x + kt];
+            float t, u, v;
+            if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                    f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
+                if (t < closest || tgroup.x + kt > best || best == 0xFFFFFFFFu) {
+                    closest = t;
+                    best = tgroup.x + kt;
+                    bu = u;
+                    bv = v;
+                }
+            }
+        }
+        if (ngroup.y <= 0x00FFFFFFu) {
+            if (sp == 0) {
+                // the ray is finished
+                const bool hit = best != 0xFFFFFFFFu && closest < kRayTMax;
+                if (hit) {
+                    c.paths.hit[i] = make_float4(closest, bu, bv, __ldg(&S->tris[best].v0.w));
+                }
+                queue[k] = hit ? i : (i | 0x80000000u);
+                if (overflow && c.q.overflow != nullptr) {
+                    atomicAdd(c.q.overflow, 1u); // rays whose stack overflowed, as traceRay counts them
+                }
+                overflow = false;
+                active = false;
+                continue;
+            }
+            --sp;
+            ngroup = sp < kSharedStack ? sstack[sp * sstride] : stack[sp - kSharedStack];
+        }
+    }
+}
+
+// Splits the queue that k_extend_lane marked into the miss and hit queues of
+// this bounce, in queue order (consecutive lanes, consecutive entries).
+__global__ void __launch_bounds__(256) k_route(const LaunchCtx* __restrict__ cp, int sel, int iter)
+{
+    const LaunchCtx& c = *cp;
+    const unsigned int count = c.q.counts[sel];
+    const int par = iter & 1;
+    const uint32_t* queue = c.q.extend[sel];
+    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t e = queue[k];
+        if (e & 0x80000000u) {
+            const uint32_t s = warpPush(&c.q.counts[4 + 2 * par]);
+            c.q.missQueue[s] = e & 0x7FFFFFFFu;
+        } else {
+            const uint32_t s = warpPush(&c.q.counts[5 + 2 * par]);
+            c.q.hitQueue[s] = e;
+        }
+    }
+}
+
 // Paths whose ray left the scene: previous bounce's NEE, then the
 // environment / background term (PathIntegratorRandCore.h:215-216, 338-346).
 template <int NW>
@@ -1316,7 +1501,8 @@ void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaSt
         k_generate<0><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
     }
 }
-void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid, bool count, bool inst, cudaStream_t s)
+void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid, bool count, bool inst, bool lane,
+    cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
     if (inst) {
@@ -1327,9 +1513,24 @@ void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid
         }
     } else if (count) {
         k_extend<true, false><<<grid, 256, smem, s>>>(c, sel, identity, iter);
+    } else if (lane) {
+        k_extend_lane<<<grid, PT_EXTEND_LANE_THREADS, sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS, s>>>(c, sel,
+            identity, iter);
+        k_route<<<grid, 256, 0, s>>>(c, sel, iter);
     } else {
         k_extend<false, false><<<grid, 256, smem, s>>>(c, sel, identity, iter);
     }
+}
+int extendKernels(bool count, bool inst, bool lane)
+{
+    return (!inst && !count && lane) ? 2 : 1;
+}
+int extendLaneOccupancy()
+{
+    int blocks = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_extend_lane, PT_EXTEND_LANE_THREADS,
+        sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS);
+    return blocks > 0 ? blocks : 1;
 }
 void launchShadeMiss(const LaunchCtx* c, int iter, int sel, int grid, int nw, cudaStream_t s)
 {

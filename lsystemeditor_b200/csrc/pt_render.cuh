@@ -147,7 +147,14 @@ struct LaunchCtx {
 // `nw` (generate, shade-miss, shade, finalize): wavelengths per path, 0 = RGB.
 void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s);
 // inst: compile-time instanced-scene traversal (any scene of the context instanced).
-void launchExtend(const LaunchCtx* d, int sel, bool identity, int iter, int grid, bool count, bool inst, cudaStream_t s);
+// Closest-hit stage.  lane: per-lane ray replacement (k_extend_lane + k_route;
+// flat scenes, no visit counting), else one warp-fetch k_extend.
+void launchExtend(const LaunchCtx* d, int sel, bool identity, int iter, int grid, bool count, bool inst, bool lane,
+    cudaStream_t s);
+// Kernels one launchExtend call launches (closest hit, and the routing pass after it).
+int extendKernels(bool count, bool inst, bool lane);
+// Resident blocks per SM of the per-lane closest-hit kernel.
+int extendLaneOccupancy();
 void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, int nw, cudaStream_t s);
 void launchShade(const LaunchCtx* d, int sel, int iter, int grid, int nw, cudaStream_t s);
 void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, bool inst, cudaStream_t s);
