@@ -830,29 +830,83 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
 }
 
 // Splits the queue that k_extend_lane marked into the miss and hit queues of
-// this bounce, in queue order (consecutive lanes, consecutive entries).
+// this bounce, in queue order.  A block takes a tile of 8 x 256 consecutive
+// entries, counts its hits and misses per warp and row (ballots), reserves
+// both output ranges with one atomic each, and writes every entry to its rank
+// within the tile: two atomics per 2048 entries instead of two per warp.
+constexpr int kRouteRows = 8;
 __global__ void __launch_bounds__(256) k_route(const LaunchCtx* __restrict__ cp, int sel, int iter)
 {
     const LaunchCtx& c = *cp;
     const unsigned int count = c.q.counts[sel];
     const int par = iter & 1;
     const uint32_t* queue = c.q.extend[sel];
-    for (unsigned int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-        const uint32_t e = queue[k];
-        if (e & 0x80000000u) {
-            const uint32_t s = warpPush(&c.q.counts[4 + 2 * par]);
-            c.q.missQueue[s] = e & 0x7FFFFFFFu;
-        } else {
-            const uint32_t s = warpPush(&c.q.counts[5 + 2 * par]);
-            c.q.hitQueue[s] = e;
+    __shared__ unsigned int sHit[kRouteRows * 8], sMiss[kRouteRows * 8]; // exclusive offsets per (row, warp)
+    __shared__ unsigned int sBase[2];
+    const unsigned int lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned int below = (1u << lane) - 1u;
+    const unsigned int tile = 256u * kRouteRows;
+    for (unsigned int t0 = blockIdx.x * tile; t0 < count; t0 += gridDim.x * tile) {
+        uint32_t e[kRouteRows];
+        unsigned int hitMask[kRouteRows], missMask[kRouteRows];
+#pragma unroll
+        for (int r = 0; r < kRouteRows; ++r) {
+            const unsigned int k = t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
+            const bool valid = k < count;
+            e[r] = valid ? queue[k] : 0u;
+            const bool miss = valid && (e[r] & 0x80000000u) != 0u;
+            hitMask[r] = __ballot_sync(0xffffffffu, valid && !miss);
+            missMask[r] = __ballot_sync(0xffffffffu, miss);
+            if (lane == 0) {
+                sHit[r * 8 + warp] = __popc(hitMask[r]);
+                sMiss[r * 8 + warp] = __popc(missMask[r]);
+            }
         }
+        __syncthreads();
+        if (warp == 0) {
+            // exclusive scan of the 64 (row, warp) counts in queue order, two per lane
+            const unsigned int h0 = sHit[2 * lane], h1 = sHit[2 * lane + 1];
+            const unsigned int m0 = sMiss[2 * lane], m1 = sMiss[2 * lane + 1];
+            unsigned int h = h0 + h1, m = m0 + m1;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned int ho = __shfl_up_sync(0xffffffffu, h, d);
+                const unsigned int mo = __shfl_up_sync(0xffffffffu, m, d);
+                if (lane >= static_cast<unsigned int>(d)) {
+                    h += ho;
+                    m += mo;
+                }
+            }
+            const unsigned int hTot = __shfl_sync(0xffffffffu, h, 31), mTot = __shfl_sync(0xffffffffu, m, 31);
+            sHit[2 * lane] = h - h0 - h1;
+            sHit[2 * lane + 1] = h - h1;
+            sMiss[2 * lane] = m - m0 - m1;
+            sMiss[2 * lane + 1] = m - m1;
+            if (lane == 0) {
+                sBase[0] = hTot ? atomicAdd(&c.q.counts[5 + 2 * par], hTot) : 0u;
+                sBase[1] = mTot ? atomicAdd(&c.q.counts[4 + 2 * par], mTot) : 0u;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kRouteRows; ++r) {
+            if ((hitMask[r] >> lane) & 1u) {
+                c.q.hitQueue[sBase[0] + sHit[r * 8 + warp] + __popc(hitMask[r] & below)] = e[r];
+            } else if ((missMask[r] >> lane) & 1u) {
+                c.q.missQueue[sBase[1] + sMiss[r * 8 + warp] + __popc(missMask[r] & below)] = e[r] & 0x7FFFFFFFu;
+            }
+        }
+        __syncthreads(); // the shared offsets are rewritten by the next tile
     }
 }
 
 // Paths whose ray left the scene: previous bounce's NEE, then the
 // environment / background term (PathIntegratorRandCore.h:215-216, 338-346).
+#ifndef PT_SHADE_MISS_MIN_BLOCKS
+#define PT_SHADE_MISS_MIN_BLOCKS 1
+#endif
 template <int NW>
-__global__ void __launch_bounds__(256) k_shade_miss(const LaunchCtx* __restrict__ cp, int iter, int sel)
+__global__ void __launch_bounds__(256, PT_SHADE_MISS_MIN_BLOCKS) k_shade_miss(const LaunchCtx* __restrict__ cp, int iter, int sel)
 {
     const LaunchCtx& c = *cp;
     const unsigned int count = c.q.counts[4 + 2 * (iter & 1)];
@@ -1534,6 +1588,12 @@ int extendLaneOccupancy()
 }
 void launchShadeMiss(const LaunchCtx* c, int iter, int sel, int grid, int nw, cudaStream_t s)
 {
+    if (PT_SHADE_MISS_MIN_BLOCKS > 1) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        grid = sms * PT_SHADE_MISS_MIN_BLOCKS;
+    }
     if (nw == 8) {
         k_shade_miss<8><<<grid, 256, 0, s>>>(c, iter, sel);
     } else if (nw == 4) {
