@@ -211,6 +211,7 @@ struct pt_renderer {
     DevBuf<uint32_t> pHitInst;
     DevBuf<uint8_t> pVisEnv, pVisEmis;
     DevBuf<uint16_t> pScene;
+    DevBuf<uint8_t> pNextFlag;            // slot-ordered mode: paths marked for the next bounce
     DevBuf<uint32_t> qExt0, qExt1, qFinish, qShadowPath, qMiss, qHit;
     DevBuf<float4> qShadowO, qShadowD;
     DevBuf<unsigned int> qCounts;
@@ -219,7 +220,9 @@ struct pt_renderer {
     DevBuf<unsigned int> qOverflow;
     int gridExtend = 0, gridShade = 0, gridShadow = 0;
     int gridExtendLane = 0;          // grid of the per-lane closest-hit kernel
+    int gridShadeMiss = 0;           // grid of the miss shader (its own occupancy)
     bool extendLane = false;         // per-lane ray replacement in this render's closest-hit stage
+    int extendMode = PT_EXTEND_MODE_AUTO;
     // CUDA graphs of four bounce iterations (the first block of a batch, later
     // blocks) and the launch configuration they were captured for
     cudaGraphExec_t bounceGraph[2] = {nullptr, nullptr};
@@ -349,13 +352,25 @@ int ensurePaths(pt_renderer* r, int capacity)
         r->qExt0.ensure(Q) && r->qExt1.ensure(Q) && r->qFinish.ensure(Q) && r->qShadowPath.ensure(2 * Q) &&
         r->qMiss.ensure(Q) && r->qHit.ensure(Q) &&
         r->qShadowO.ensure(2 * Q) && r->qShadowD.ensure(2 * Q) && r->qCounts.ensure(16) && r->qRays.ensure(2) &&
-        r->qVisits.ensure(4) && r->qOverflow.ensure(1) && r->dbatch.ensure(1);
+        r->qVisits.ensure(4) && r->qOverflow.ensure(1) && r->dbatch.ensure(1) && r->pNextFlag.ensure(Q);
     if (!ok) {
         return fail(r, PT_ERR_OUT_OF_MEMORY, "path state allocation failed for %d paths", capacity);
+    }
+    if (cudaMemset(r->pNextFlag.p, 0, Q) != cudaSuccess) {
+        return fail(r, PT_ERR_CUDA, "path state initialisation failed");
     }
     r->capacity = capacity;
     return PT_OK;
 }
+
+#ifndef PT_SLOT_ORDER
+#define PT_SLOT_ORDER 1
+#endif
+
+// Slot-ordered next queue (k_next_queue): with the per-lane closest-hit kernel,
+// whose queue order does not matter to it, the shade kernels read consecutive
+// slots' path state.
+bool slotOrdered(const pt_renderer* r) { return PT_SLOT_ORDER && r->extendLane; }
 
 LaunchCtx makeCtx(pt_renderer* r)
 {
@@ -402,6 +417,7 @@ LaunchCtx makeCtx(pt_renderer* r)
     c.paths.capacity = r->capacity;
     c.q.extend[0] = r->qExt0.p;
     c.q.extend[1] = r->qExt1.p;
+    c.q.nextFlag = slotOrdered(r) ? r->pNextFlag.p : nullptr;
     c.q.finish = r->qFinish.p;
     c.q.missQueue = r->qMiss.p;
     c.q.hitQueue = r->qHit.p;
@@ -1191,7 +1207,8 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
         static_cast<unsigned long long>(r->gridShade), static_cast<unsigned long long>(r->gridShadow),
         static_cast<unsigned long long>(inst ? 1 : 0) | (static_cast<unsigned long long>(nw) << 1) |
             (static_cast<unsigned long long>(r->extendLane ? 1 : 0) << 8) |
-            (static_cast<unsigned long long>(r->gridExtendLane) << 9),
+            (static_cast<unsigned long long>(r->gridExtendLane) << 9) |
+            (static_cast<unsigned long long>(r->gridShadeMiss) << 36),
         reinterpret_cast<unsigned long long>(r->stream)};
     if (r->bounceGraph[0] != nullptr && std::equal(key, key + 6, r->bounceKey)) {
         return true;
@@ -1211,10 +1228,13 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
         int sel = 0;
         for (int it = 0; it < 4; ++it) {
             launchExtend(c, sel, g == 0 && it == 0, it, extendGrid(r, false, inst), false, inst, r->extendLane, s);
-            launchShadeMiss(c, it, sel, r->gridShade, nw, s);
+            launchShadeMiss(c, it, sel, r->gridShadeMiss, nw, s);
             launchShade(c, sel, it, r->gridShade, nw, s);
             launchShadow(c, it, r->gridShadow, false, inst, s);
             launchFinalize(c, sel, r->gridShadow, nw, s);
+            if (slotOrdered(r)) {
+                launchNextQueue(c, sel, r->gridShadow, s);
+            }
             sel ^= 1;
         }
         cudaGraph_t graph = nullptr;
@@ -1271,6 +1291,7 @@ int pt_create(pt_renderer** out, int device)
     r->gridShade = r->smCount * std::max(bs, 1);
     r->gridShadow = r->smCount * std::max(bsh, 1);
     r->gridExtendLane = r->smCount * extendLaneOccupancy();
+    r->gridShadeMiss = r->smCount * shadeMissOccupancy();
     *out = r;
     return PT_OK;
 }
@@ -1348,6 +1369,7 @@ int pt_destroy(pt_renderer* r)
     r->pVisEnv.release();
     r->pVisEmis.release();
     r->pScene.release();
+    r->pNextFlag.release();
     r->qExt0.release();
     r->qExt1.release();
     r->qFinish.release();
@@ -1553,7 +1575,9 @@ int pt_render(pt_renderer* r, int waves)
     }
     // Per-lane ray replacement pays where traversals are long (large trees);
     // on small scenes the extra routing launch costs more than it saves.
-    r->extendLane = !inst && maxNodes >= static_cast<uint32_t>(PT_EXTEND_LANE_MIN_NODES);
+    r->extendLane = !inst && (r->extendMode == PT_EXTEND_MODE_LANE ||
+                                 (r->extendMode == PT_EXTEND_MODE_AUTO &&
+                                     maxNodes >= static_cast<uint32_t>(PT_EXTEND_LANE_MIN_NODES)));
     const int nw = r->params.spectral_wavelengths;
     if (nw > 0) {
         const int st = prepareSpectral(r, nw);
@@ -1592,6 +1616,11 @@ int pt_render(pt_renderer* r, int waves)
         r->hbatch.nextJob = static_cast<unsigned long long>(slots);
         r->hbatch.activeCount = active;
         r->hbatch.waveBase = static_cast<uint32_t>(r->wavesDone);
+        r->hbatch.slotCount = slots;
+        if (slotOrdered(r)) {
+            // (marks are cleared by k_next_queue; this also clears those of a render that failed)
+            PT_CHECK(r, cudaMemsetAsync(r->pNextFlag.p, 0, static_cast<size_t>(slots), s));
+        }
         PT_CHECK(r, cudaMemcpyAsync(r->dbatch.p, &r->hbatch, sizeof(BatchInfo), cudaMemcpyHostToDevice, s));
         const LaunchCtx* c = uploadCtx(r);
         if (c == nullptr) {
@@ -1619,7 +1648,7 @@ int pt_render(pt_renderer* r, int waves)
                 return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
             }
             PT_CHECK(r, cudaGraphLaunch(r->bounceGraph[it == 0 ? 0 : 1], s));
-            launches += 4 * (4 + extendKernels(false, inst, r->extendLane));
+            launches += 4 * (4 + extendKernels(false, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0));
             r->profile.launches_extend += 4;
             r->profile.launches_shadow += 4;
             unsigned int live = 0;
@@ -1640,7 +1669,7 @@ int pt_render(pt_renderer* r, int waves)
             }
             {
                 StageTimer tm(r, kShade);
-                launchShadeMiss(c, iter, sel, r->gridShade, nw, s);
+                launchShadeMiss(c, iter, sel, r->gridShadeMiss, nw, s);
                 launchShade(c, sel, iter, r->gridShade, nw, s);
             }
             {
@@ -1650,8 +1679,11 @@ int pt_render(pt_renderer* r, int waves)
             {
                 StageTimer tm(r, kFinalize);
                 launchFinalize(c, sel, r->gridShadow, nw, s);
+                if (slotOrdered(r)) {
+                    launchNextQueue(c, sel, r->gridShadow, s);
+                }
             }
-            launches += 4 + extendKernels(countVisits, inst, r->extendLane);
+            launches += 4 + extendKernels(countVisits, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0);
             r->profile.launches_extend += 1;
             r->profile.launches_shadow += 1;
             sel ^= 1;
@@ -1879,6 +1911,15 @@ int pt_get_profile(const pt_renderer* r, pt_profile* out)
     return PT_OK;
 }
 
+int pt_set_extend_mode(pt_renderer* r, int mode)
+{
+    if (r == nullptr || mode < PT_EXTEND_MODE_AUTO || mode > PT_EXTEND_MODE_LANE) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_extend_mode: mode must be 0 (auto), 1 (warp) or 2 (lane)");
+    }
+    r->extendMode = mode;
+    return PT_OK;
+}
+
 int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
 {
     if (r == nullptr || path_capacity < 0 || blocks_per_sm < 0 || path_capacity > (1 << 26)) {
@@ -1889,6 +1930,7 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
     if (blocks_per_sm > 0) {
         r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
         r->gridExtendLane = r->smCount * std::min(blocks_per_sm, extendLaneOccupancy());
+        r->gridShadeMiss = r->smCount * std::min(blocks_per_sm, shadeMissOccupancy());
     } else {
         int be = 1, bs = 1, bsh = 1;
         stageOccupancy(be, bs, bsh);
@@ -1896,6 +1938,7 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
         r->gridShade = r->smCount * std::max(bs, 1);
         r->gridShadow = r->smCount * std::max(bsh, 1);
         r->gridExtendLane = r->smCount * extendLaneOccupancy();
+        r->gridShadeMiss = r->smCount * shadeMissOccupancy();
     }
     return PT_OK;
 }

@@ -563,6 +563,18 @@ template <int NW> __device__ __forceinline__ void initPath(const LaunchCtx& c, u
     c.paths.visEmis[i] = 0;
 }
 
+// Path i joins the next bounce's extend queue: marked for k_next_queue in
+// slot-ordered mode, else pushed (one atomic per warp).
+__device__ __forceinline__ void queueNext(const LaunchCtx& c, uint32_t i, unsigned int* nextCount, uint32_t* nextQueue)
+{
+    if (c.q.nextFlag != nullptr) {
+        c.q.nextFlag[i] = 1;
+    } else {
+        const uint32_t s = warpPush(nextCount);
+        nextQueue[s] = i;
+    }
+}
+
 // A terminated path's slot takes the batch's next job, if any, and joins the
 // next extend queue: launches stay full until the batch drains.
 template <int NW>
@@ -577,8 +589,7 @@ __device__ __forceinline__ void recyclePath(const LaunchCtx& c, uint32_t i, unsi
     const unsigned long long j = base + g.thread_rank();
     if (j < c.q.batch->jobs) {
         initPath<NW>(c, i, j);
-        const uint32_t s = warpPush(nextCount);
-        nextQueue[s] = i;
+        queueNext(c, i, nextCount, nextQueue);
     }
 }
 
@@ -900,10 +911,69 @@ __global__ void __launch_bounds__(256) k_route(const LaunchCtx* __restrict__ cp,
     }
 }
 
+// Slot-ordered mode: lists the slots the shade kernels marked as the next
+// bounce's extend queue, in increasing slot order within tiles of 2048 (the
+// tiles in the order they reserve their ranges), and clears the marks.  The
+// extend and shade kernels then read the path state of consecutive slots.
+__global__ void __launch_bounds__(256) k_next_queue(const LaunchCtx* __restrict__ cp, int sel)
+{
+    const LaunchCtx& c = *cp;
+    const unsigned int n = static_cast<unsigned int>(c.q.batch->slotCount);
+    uint8_t* flag = c.q.nextFlag;
+    uint32_t* out = c.q.extend[sel ^ 1];
+    __shared__ unsigned int sOff[kRouteRows * 8];
+    __shared__ unsigned int sBase;
+    const unsigned int lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned int below = (1u << lane) - 1u;
+    const unsigned int tile = 256u * kRouteRows;
+    for (unsigned int t0 = blockIdx.x * tile; t0 < n; t0 += gridDim.x * tile) {
+        unsigned int mask[kRouteRows];
+#pragma unroll
+        for (int r = 0; r < kRouteRows; ++r) {
+            const unsigned int k = t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
+            const bool on = k < n && flag[k] != 0;
+            if (on) {
+                flag[k] = 0;
+            }
+            mask[r] = __ballot_sync(0xffffffffu, on);
+            if (lane == 0) {
+                sOff[r * 8 + warp] = __popc(mask[r]);
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const unsigned int a0 = sOff[2 * lane], a1 = sOff[2 * lane + 1];
+            unsigned int a = a0 + a1;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned int o = __shfl_up_sync(0xffffffffu, a, d);
+                if (lane >= static_cast<unsigned int>(d)) {
+                    a += o;
+                }
+            }
+            const unsigned int tot = __shfl_sync(0xffffffffu, a, 31);
+            sOff[2 * lane] = a - a0 - a1;
+            sOff[2 * lane + 1] = a - a1;
+            if (lane == 0) {
+                sBase = tot ? atomicAdd(&c.q.counts[sel ^ 1], tot) : 0u;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kRouteRows; ++r) {
+            if ((mask[r] >> lane) & 1u) {
+                out[sBase + sOff[r * 8 + warp] + __popc(mask[r] & below)] =
+                    t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Paths whose ray left the scene: previous bounce's NEE, then the
 // environment / background term (PathIntegratorRandCore.h:215-216, 338-346).
 #ifndef PT_SHADE_MISS_MIN_BLOCKS
-#define PT_SHADE_MISS_MIN_BLOCKS 1
+#define PT_SHADE_MISS_MIN_BLOCKS 4
 #endif
 template <int NW>
 __global__ void __launch_bounds__(256, PT_SHADE_MISS_MIN_BLOCKS) k_shade_miss(const LaunchCtx* __restrict__ cp, int iter, int sel)
@@ -1226,8 +1296,7 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
             c.paths.visEmis[i] = 0;
             if (cont) {
                 storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth + 1));
-                const uint32_t s = warpPush(nextCount);
-                nextQueue[s] = i;
+                queueNext(c, i, nextCount, nextQueue);
             } else if (pendEnv || pendEmis) {
                 storeCol<NW>(c.paths.rad, c.paths.radS, cap, i, L, __int_as_float(depth));
                 const uint32_t s = warpPush(&c.q.counts[3]);
@@ -1241,8 +1310,7 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                 // the radiance is in radS already
                 c.paths.rad[i] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(cont ? depth + 1 : depth));
                 if (cont) {
-                    const uint32_t s = warpPush(nextCount);
-                    nextQueue[s] = i;
+                    queueNext(c, i, nextCount, nextQueue);
                 } else {
                     const uint32_t s = warpPush(&c.q.counts[3]);
                     c.q.finish[s] = i;
@@ -1579,6 +1647,16 @@ int extendKernels(bool count, bool inst, bool lane)
 {
     return (!inst && !count && lane) ? 2 : 1;
 }
+void launchNextQueue(const LaunchCtx* c, int sel, int grid, cudaStream_t s)
+{
+    k_next_queue<<<grid, 256, 0, s>>>(c, sel);
+}
+int shadeMissOccupancy()
+{
+    int blocks = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_shade_miss<8>, 256, 0);
+    return blocks > 0 ? blocks : 1;
+}
 int extendLaneOccupancy()
 {
     int blocks = 1;
@@ -1588,12 +1666,6 @@ int extendLaneOccupancy()
 }
 void launchShadeMiss(const LaunchCtx* c, int iter, int sel, int grid, int nw, cudaStream_t s)
 {
-    if (PT_SHADE_MISS_MIN_BLOCKS > 1) {
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        grid = sms * PT_SHADE_MISS_MIN_BLOCKS;
-    }
     if (nw == 8) {
         k_shade_miss<8><<<grid, 256, 0, s>>>(c, iter, sel);
     } else if (nw == 4) {

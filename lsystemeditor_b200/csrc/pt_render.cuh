@@ -41,10 +41,14 @@ struct BatchInfo {
     unsigned long long nextJob;  // first job not yet handed to a path slot
     int activeCount;
     uint32_t waveBase;
+    int slotCount;               // path slots in use in this batch
 };
 
 struct QueueSet {
     uint32_t* extend[2] = {nullptr, nullptr}; // path indices, ping-pong
+    // slot-ordered mode (non-null): the shade kernels mark the paths of the next
+    // bounce here and k_next_queue lists them in slot order
+    uint8_t* nextFlag = nullptr;
     uint32_t* finish = nullptr;               // paths that ended with shadow rays in flight
     uint32_t* missQueue = nullptr;            // paths whose last ray left the scene
     uint32_t* hitQueue = nullptr;             // paths whose last ray hit a triangle
@@ -153,8 +157,11 @@ void launchExtend(const LaunchCtx* d, int sel, bool identity, int iter, int grid
     cudaStream_t s);
 // Kernels one launchExtend call launches (closest hit, and the routing pass after it).
 int extendKernels(bool count, bool inst, bool lane);
-// Resident blocks per SM of the per-lane closest-hit kernel.
+// Resident blocks per SM of the per-lane closest-hit kernel and of the miss shader.
 int extendLaneOccupancy();
+int shadeMissOccupancy();
+// Slot-ordered mode: the next bounce's extend queue from the marked slots.
+void launchNextQueue(const LaunchCtx* d, int sel, int grid, cudaStream_t s);
 void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, int nw, cudaStream_t s);
 void launchShade(const LaunchCtx* d, int sel, int iter, int grid, int nw, cudaStream_t s);
 void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, bool inst, cudaStream_t s);

@@ -83,7 +83,8 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_tonemap", "pt_exposure_multiplier", "pt_set_materials", "pt_backward",
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
                     "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift",
-                    "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune", "pt_measure_l2"]
+                    "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune", "pt_measure_l2",
+                    "pt_set_extend_mode"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -125,6 +126,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_set_profiling.argtypes = [vp, C.c_int]
     L.pt_get_profile.argtypes = [vp, C.POINTER(PtProfile)]
     L.pt_set_tuning.argtypes = [vp, C.c_int, C.c_int]
+    L.pt_set_extend_mode.argtypes = [vp, C.c_int]
     L.pt_batch_configure.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.pt_batch_set_mesh.argtypes = [vp, C.c_int, C.POINTER(PtMesh)]
     L.pt_batch_set_camera.argtypes = [vp, C.c_int, vp]
@@ -570,6 +572,10 @@ class PathTracer:
 
     def set_tuning(self, path_capacity: int = 0, blocks_per_sm: int = 0):
         self._check(self._lib.pt_set_tuning(self._h, int(path_capacity), int(blocks_per_sm)))
+
+    def set_extend_mode(self, mode: int):
+        """pt_set_extend_mode: 0 auto, 1 warp-fetch closest hit, 2 per-lane replacement (identical images)."""
+        self._check(self._lib.pt_set_extend_mode(self._h, int(mode)))
 
     def rng_tape(self, first_wave: int, waves: int, stride: int) -> np.ndarray:
         out = np.zeros((waves, self.width * self.height, stride), np.float32)
