@@ -7,12 +7,16 @@
 //
 //   generate   camera ray per (pixel, sample): curand_init with the reference
 //              seed, jitter + lens draws (PathTracer.cu:69-96)
-//   extend     closest hit for every live path            (pt_trace.cuh)
+//   extend     closest hit for every live path            (pt_trace.cuh);
+//              large flat scenes: per-lane ray replacement (k_extend_lane)
+//              + k_route, which splits the queue into miss and hit queues
 //   shade      pending NEE resolve, miss/env MIS, emission, environment and
 //              emissive NEE (shadow rays queued), BSDF sample, throughput,
 //              subsurface tier B, Russian roulette, continuation ray
 //   shadow     any-hit occlusion for the queued shadow rays
 //   finalize   paths that ended with shadow rays in flight
+//   next_queue (with k_extend_lane) the next bounce's extend queue in slot
+//              order, from the slots the shade kernels marked
 //   accumulate per pixel, the batch's samples in sample order: running mean,
 //              Welford luminance variance, convergence every 4 samples
 //              (PathTracer.cu:232-272)
@@ -811,9 +815,9 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
             float t, u, v;
             if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
                     f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
-                if (t < closest || tgroup.x + kt > best || best == 0xFFFFFFFFu) {
+                if (t < closest || __float_as_uint(tv.v0.w) > best || best == 0xFFFFFFFFu) {
                     closest = t;
-                    best = tgroup.x + kt;
+                    best = __float_as_uint(tv.v0.w); // original index: traceRay's tie rule
                     bu = u;
                     bv = v;
                 }
@@ -824,7 +828,7 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
                 // the ray is finished
                 const bool hit = best != 0xFFFFFFFFu && closest < kRayTMax;
                 if (hit) {
-                    c.paths.hit[i] = make_float4(closest, bu, bv, __ldg(&S->tris[best].v0.w));
+                    c.paths.hit[i] = make_float4(closest, bu, bv, __uint_as_float(best));
                 }
                 queue[k] = hit ? i : (i | 0x80000000u);
                 if (overflow && c.q.overflow != nullptr) {

@@ -6,9 +6,12 @@
 //   * triangles are intersected with the reference's Moller-Trumbore
 //     (:52-108), rounded exactly like the reference (no FMA contraction), and
 //     accepted when tMin <= t <= closest; of several hits at exactly the same t
-//     the one latest in leaf order wins (the reference keeps the last one its
-//     own traversal order meets; this rule does not depend on the order, so
-//     that the wavefront and the path-replay kernels agree);
+//     the one with the highest original triangle index wins (the reference
+//     keeps the last one its own traversal order meets).  The rule depends
+//     neither on the visiting order nor on the BVH's layout -- the parallel
+//     top-down collapse places nodes and leaves in an order that differs
+//     between builds -- so every kernel, and every build of the same scene,
+//     picks the same triangle;
 //   * a hit is reported only if the final t < tMax;
 //   * quirk Q1: a direction component with |d| <= 1e-8 gets a zero reciprocal
 //     in the reference, which turns every slab test into "does the box contain
@@ -265,18 +268,21 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
                     }
                 }
                 float t, u, v;
+                const uint32_t id = __float_as_uint(tv.v0.w);
                 if (inside && intersectTriExact(o, dn, v0, v1, v2, tMin, closest, t, u, v)) {
                     if (anyHit && t < tMax) {
                         out.t = t;
                         out.u = u;
                         out.v = v;
-                        out.tri = __float_as_uint(tv.v0.w);
+                        out.tri = id;
                         return true;
                     }
-                    closest = t;
-                    best = w1.y + off + k;
-                    bu = u;
-                    bv = v;
+                    if (t < closest || id > best || best == 0xFFFFFFFFu) {
+                        closest = t;
+                        best = id; // (original index; see the tie rule above)
+                        bu = u;
+                        bv = v;
+                    }
                 }
             }
         }
@@ -285,7 +291,7 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
         out.t = closest;
         out.u = bu;
         out.v = bv;
-        out.tri = __float_as_uint(S.tris[best].v0.w);
+        out.tri = best;
         return true;
     }
     return false;
@@ -296,7 +302,7 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
 // (o' = W2O o, d' = W2O d, unnormalised, so t is the same parameter) and the
 // object's BVH is traversed on the same stack above the top level's entries;
 // when those are used up the world ray is restored.  Exact-t ties go to the
-// larger (instance, leaf) pair.
+// larger (instance, original triangle index) pair.
 template <bool AnyHit, bool Count>
 __device__ __noinline__ bool traceInstanced(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, HitRec& out,
     unsigned int* overflowCounter, unsigned long long* visits, uint2* sstack, int sstride)
@@ -404,8 +410,8 @@ __device__ __noinline__ bool traceInstanced(const DevScene& S, float3 o, float3 
             }
             if (intersectTriExact(ro, rd, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
                     f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
-                const unsigned long long key =
-                    (static_cast<unsigned long long>(curInst) << 32) | static_cast<unsigned long long>(tgroup.x + k);
+                const unsigned long long key = (static_cast<unsigned long long>(curInst) << 32) |
+                    static_cast<unsigned long long>(__float_as_uint(tv.v0.w));
                 if (AnyHit) {
                     if (t < tMax) {
                         if (Count) {
@@ -569,11 +575,11 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
                         out.tri = __float_as_uint(tv.v0.w);
                         return true;
                     }
-                } else if (t < closest || tgroup.x + k > best || best == 0xFFFFFFFFu) {
-                    // an exact tie in t goes to the later leaf, whatever the visiting
-                    // order, so that every kernel that traces a ray picks the same triangle
+                } else if (t < closest || __float_as_uint(tv.v0.w) > best || best == 0xFFFFFFFFu) {
+                    // an exact tie in t goes to the higher original triangle index,
+                    // whatever the visiting order and the BVH's layout
                     closest = t;
-                    best = tgroup.x + k;
+                    best = __float_as_uint(tv.v0.w);
                     bu = u;
                     bv = v;
                 }
@@ -602,7 +608,7 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
         out.t = closest;
         out.u = bu;
         out.v = bv;
-        out.tri = __float_as_uint(__ldg(&S.tris[best].v0.w));
+        out.tri = best;
         return true;
     }
     return false;
