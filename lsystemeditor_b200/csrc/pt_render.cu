@@ -850,6 +850,8 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
 // both output ranges with one atomic each, and writes every entry to its rank
 // within the tile: two atomics per 2048 entries instead of two per warp.
 constexpr int kRouteRows = 8;
+// (blocks of 256 threads = 8 warps; warp 0 scans the 64 (row, warp) counts, two per lane)
+static_assert(kRouteRows * 8 == 64, "the tile scan covers exactly 64 (row, warp) counts");
 __global__ void __launch_bounds__(256) k_route(const LaunchCtx* __restrict__ cp, int sel, int iter)
 {
     const LaunchCtx& c = *cp;
