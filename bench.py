@@ -251,35 +251,16 @@ def workload_config(spec, name):
 # ---------------------------------------------------------------------------
 def run_b200(args):
     import torch
-    import torch.distributed as dist
 
     from lsystemeditor_b200.pathtracer import PROFILE_COUNT_VISITS, PROFILE_STAGE_TIMES, PathTracer
+    from lsystemeditor_b200.replicas import Replicas
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    # one replica of the workload per GPU; ranks meet only for the timing (NCCL)
+    reps = Replicas(backend="nccl", device="cuda", timeout_s=300.0)
+    world, rank = reps.world, reps.rank
+    barrier, max_over_ranks, sum_over_ranks = reps.barrier, reps.max, reps.sum
 
     spec = make_workload(args.config)
     nw = wavelengths(args)
@@ -456,8 +437,7 @@ def run_b200(args):
     if rank == 0:
         print(json.dumps(out))
     pt.close()
-    if world > 1:
-        dist.destroy_process_group()
+    reps.close()
     return 0
 
 
