@@ -815,9 +815,9 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
             float t, u, v;
             if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
                     f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
-                if (t < closest || __float_as_uint(tv.v0.w) > best || best == 0xFFFFFFFFu) {
-                    closest = t;
-                    best = __float_as_uint(tv.v0.w); // original index: traceRay's tie rule
+                if (t < closest || best == 0xFFFFFFFFu || leafId(S->tris, tgroup.x + kt) > leafId(S->tris, best)) {
+                    closest = t; // (traceRay's tie rule: the higher original triangle index)
+                    best = tgroup.x + kt;
                     bu = u;
                     bv = v;
                 }
@@ -828,7 +828,7 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
                 // the ray is finished
                 const bool hit = best != 0xFFFFFFFFu && closest < kRayTMax;
                 if (hit) {
-                    c.paths.hit[i] = make_float4(closest, bu, bv, __uint_as_float(best));
+                    c.paths.hit[i] = make_float4(closest, bu, bv, __uint_as_float(leafId(S->tris, best)));
                 }
                 queue[k] = hit ? i : (i | 0x80000000u);
                 if (overflow && c.q.overflow != nullptr) {

@@ -39,6 +39,12 @@ constexpr int kSharedStack = PT_SHARED_STACK;       // entries per thread of the
 constexpr int kPostponeLanes = PT_POSTPONE_LANES;   // postpone triangle tests when fewer lanes want them
 constexpr float kSlabWiden = 1.0000005f;
 
+// Original triangle index of the triangle at leaf position k.
+__device__ __forceinline__ uint32_t leafId(const TriVerts* __restrict__ tris, uint32_t k)
+{
+    return __float_as_uint(__ldg(&tris[k].v0.w));
+}
+
 struct HitRec {
     float t;
     float u;
@@ -575,11 +581,13 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
                         out.tri = __float_as_uint(tv.v0.w);
                         return true;
                     }
-                } else if (t < closest || __float_as_uint(tv.v0.w) > best || best == 0xFFFFFFFFu) {
+                } else if (t < closest || best == 0xFFFFFFFFu ||
+                           leafId(S.tris, tgroup.x + k) > leafId(S.tris, best)) {
                     // an exact tie in t goes to the higher original triangle index,
-                    // whatever the visiting order and the BVH's layout
+                    // whatever the visiting order and the BVH's layout (both ids are
+                    // read again only on a tie, which keeps no register live)
                     closest = t;
-                    best = __float_as_uint(tv.v0.w);
+                    best = tgroup.x + k;
                     bu = u;
                     bv = v;
                 }
@@ -608,7 +616,7 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
         out.t = closest;
         out.u = bu;
         out.v = bv;
-        out.tri = best;
+        out.tri = leafId(S.tris, best);
         return true;
     }
     return false;
