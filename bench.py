@@ -368,7 +368,11 @@ def run_b200(args):
         t, v = pinned(getattr(m, field))
         keep.append(t)
         setattr(pm, field, v)
+    # the step's result is read back into pinned host memory
     rgba_t = torch.empty((spec.height, spec.width, 4), dtype=torch.float32, pin_memory=True)
+    counts_t = torch.empty((spec.height, spec.width), dtype=torch.int32, pin_memory=True)
+    conv_t = torch.empty((spec.height, spec.width), dtype=torch.uint8, pin_memory=True)
+    out_bufs = (rgba_t.numpy(), counts_t.numpy().view(np.uint32), conv_t.numpy())
     h2d = sum(getattr(m, f).nbytes for f in ("positions", "normals", "uvs", "material_ids", "materials",
                                                 "textures")) + 80 + 64
     d2h = spec.width * spec.height * (16 + 4 + 1)
@@ -378,7 +382,7 @@ def run_b200(args):
         pt.set_camera(spec.camera)
         pt.set_params(spec.params)
         pt.render(0)
-        pt.readback()
+        pt.readback(out_bufs)
 
     for _ in range(2):
         e2e_step()

@@ -338,11 +338,21 @@ class PathTracer:
         """Traces `waves` full-resolution adaptive waves (<= 0: until every pixel is done)."""
         self._check(self._lib.pt_render(self._h, int(waves)))
 
-    def readback(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    def readback(self, out: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
+                 ) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """pt_readback: accumulated RGBA, sample counts and convergence flags of scene 0.  `out` reuses
+        caller-owned arrays (e.g. pinned host memory) of shapes (H, W, 4) float32, (H, W) uint32, (H, W) uint8."""
         P = self.width * self.height
-        rgba = np.empty((self.height, self.width, 4), np.float32)
-        counts = np.empty((self.height, self.width), np.uint32)
-        conv = np.empty((self.height, self.width), np.uint8)
+        if out is None:
+            rgba = np.empty((self.height, self.width, 4), np.float32)
+            counts = np.empty((self.height, self.width), np.uint32)
+            conv = np.empty((self.height, self.width), np.uint8)
+        else:
+            rgba, counts, conv = out
+            ok = (rgba.dtype == np.float32 and rgba.size == 4 * P and counts.dtype == np.uint32 and counts.size == P
+                  and conv.dtype == np.uint8 and conv.size == P and all(a.flags["C_CONTIGUOUS"] for a in out))
+            if not ok:
+                raise ValueError("readback: out arrays must be C-contiguous float32 (H, W, 4), uint32 and uint8 (H, W)")
         self._check(self._lib.pt_readback(self._h, _ptr(rgba, _fp), _ptr(counts, _u32p), _ptr(conv, _u8p)))
         assert rgba.size == 4 * P
         return rgba, counts, conv

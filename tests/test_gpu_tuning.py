@@ -6,6 +6,7 @@
 * pt_autotune returns knobs from its candidate sets, never a slower probe
   than the configuration it started from, and the image rendered with the
   chosen knobs is bit-identical to the one rendered with the defaults.
+* pt_readback fills caller-owned (e.g. pinned) arrays exactly like fresh ones.
 * The closest-hit stage renders the same image, sample counts and convergence
   flags in both its forms: one warp per 32 queued rays with pushes into the
   miss/hit and next-bounce queues, and per-lane ray replacement with
@@ -132,3 +133,21 @@ def test_extend_modes_batch():
         for x, y, what in zip(a, b, ("image", "sample counts", "convergence flags")):
             assert np.array_equal(x, y), f"scene {k}: {what} differ between the warp and lane forms"
         assert a[0][..., :3].max() > 0
+
+
+def test_readback_into_caller_buffers():
+    mesh = spectral_zoo_scene(n_per_mat=60, seed=12)
+    w, h = 40, 24
+    with PathTracer(0) as t:
+        t.configure(w, h, mesh)
+        t.set_camera(zoo_camera(w, h))
+        t.set_params(default_params(max_path_depth=4, min_samples=4, max_samples_per_pixel=4))
+        t.render(0)
+        fresh = t.readback()
+        out = (np.full((h, w, 4), -1.0, np.float32), np.zeros((h, w), np.uint32), np.full((h, w), 7, np.uint8))
+        got = t.readback(out)
+        assert all(g is o for g, o in zip(got, out))
+        for a, b in zip(fresh, out):
+            assert np.array_equal(a, b)
+        with pytest.raises(ValueError):
+            t.readback((np.zeros((h, w, 3), np.float32), out[1], out[2]))
