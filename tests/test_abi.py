@@ -63,3 +63,5 @@ def test_null_handle_errors_without_device():
     assert lib.pt_render(None, 1) == 1          # PT_ERR_INVALID_ARGUMENT
     assert lib.pt_destroy(None) == 1
     assert lib.pt_create(None, 0) == 1
+    lib.pt_set_extend_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    assert lib.pt_set_extend_mode(None, 0) == 1
