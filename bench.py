@@ -62,6 +62,8 @@ def parse_args():
                     default="plain-large")
     ap.add_argument("--opt-steps", type=int, default=200, help="Adam steps of the adjoint workload's optimisation")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the leg that times the reference's own CUDA kernels on this GPU")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: keep the default scheduling knobs")
     ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],
                     help="hero wavelengths per path: auto = the workload's own (plain-small 4, plain-large 8, "
@@ -183,6 +185,57 @@ def cpu_render_rate(spec, min_seconds: float = 10.0, max_pixels: int | None = No
     return {"value": samples / dt / 1e6, "unit": METRIC, "cores": int(threads), "kind": kind,
             "sample": f"{n} of {P} pixels x up to {spec.waves} samples, {reps} frame(s) ({samples} path samples, "
                       f"{dt:.1f} s), same scene/camera/params, PCG32 random numbers"}
+
+
+def reference_gpu_leg(spec, pt, stream, max_waves: int = 0):
+    """The reference's own megakernel (PathTracer.cu compiled unchanged for sm_100a,
+    oracle/_ref/libptref_gpu.so) on this GPU, driven by its render loop's wave
+    sequence, on the workload's scene, camera, resolution and sample budget with
+    the reference's estimator (RGB, relative std-dev stop test); beside it the
+    B200 path on exactly those parameters.  A baseline leg: reported, not the
+    headline value."""
+    import torch
+
+    from oracle.bindings import ReferenceGpu, reference_gpu_available
+    if not reference_gpu_available():
+        return {"unavailable": "oracle/_ref/libptref_gpu.so not built (no reference tree where build() ran)"}
+    params = np.array(spec.params, copy=True)
+    params["spectral_wavelengths"] = 0
+    params["adaptive_criterion"] = 0
+    rg = ReferenceGpu()
+    sc = rg.scene(spec.mesh)
+    sc.render(spec.camera, params, spec.width, spec.height, max_waves=4)  # warm-up: module load, first launches
+    torch.cuda.synchronize()
+    r = sc.render(spec.camera, params, spec.width, spec.height, max_waves=max_waves)
+    ref_value = r["samples"] / (r["device_ms"] / 1e3) / 1e6
+    # the B200 path on the same parameters (RGB, the reference's stop test)
+    saved = pt.params()
+    pt.set_params(params)
+    pt.reset_accumulation()
+    pt.render(max_waves)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pt.reset_accumulation()
+    a.record(stream)
+    pt.render(max_waves)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ours_ms = a.elapsed_time(b)
+    ours_samples = float(pt.stats()["samples"])
+    _, counts, _ = pt.readback()
+    pt.set_params(saved)
+    same_counts = float(np.mean(counts.reshape(-1) == r["counts"]))
+    return {
+        "value": ref_value, "unit": METRIC, "kind": "reference megakernel (PathTracer.cu sampleAdaptiveKernel, "
+        "unchanged, nvcc for sm_100a) driven by its render loop's wave sequence, per-wave host wait",
+        "estimator": "RGB, relative std-dev < %g, %d-%d spp" % (float(params["relative_error_threshold"]),
+                                                               int(params["min_samples"]),
+                                                               int(params["max_samples_per_pixel"])),
+        "frame_ms": r["device_ms"], "waves": r["waves"], "samples": r["samples"],
+        "host_bvh_build_ms": sc.build_ms, "bvh_nodes": sc.bvh_node_count(),
+        "b200_same_params": {"value": ours_samples / (ours_ms / 1e3) / 1e6, "unit": METRIC, "frame_ms": ours_ms,
+                             "samples": ours_samples, "pixels_with_equal_counts": same_counts},
+    }
 
 
 def run_reference(args):
@@ -410,6 +463,13 @@ def run_b200(args):
             cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
                    "sample": f"unavailable: {e}"}
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        try:
+            ref_gpu = reference_gpu_leg(spec, pt, stream)
+        except Exception as e:  # the baseline must not take the GPU number down with it
+            ref_gpu = {"unavailable": f"{type(e).__name__}: {e}"}
+
     st = pt.stats()
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -438,6 +498,8 @@ def run_b200(args):
         if nw > 0:
             cpu["sample"] += "; renders RGB (the reference has no spectral integrator)"
         out["cpu_baseline"] = cpu
+    if ref_gpu is not None:
+        out["reference_gpu"] = ref_gpu
     if rank == 0:
         print(json.dumps(out))
     pt.close()

@@ -4,6 +4,9 @@
   restatement of the reference render path (FP32 ``orc_*`` and FP64 ``orc64_*``).
 * ``Checker("ref")`` loads oracle/_ref/libptref.so -- the reference's own
   hot-path code compiled for the host (only where it could be built).
+* ``ReferenceGpu`` loads oracle/_ref/libptref_gpu.so -- the reference's own
+  CUDA render kernels (PathTracer.cu) compiled for sm_100a, driven by the wave
+  loop of its render loop; a GPU checker and the GPU bar of the benchmark.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module.  Both libraries expose the same entry points, so a test can run
@@ -21,7 +24,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libpt_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libptref.so")
-REF_ROOT = "/root/reference"
+REF_GPU_SO = os.path.join(HERE, "_ref", "libptref_gpu.so")
+# Where the reference checkout lies; only the build recipes read it (the built
+# libraries under oracle/_ref are used where the tree is absent).
+REF_ROOT = os.environ.get("LSYSTEM_REFERENCE_ROOT", "/root/reference")
 
 _fp = C.POINTER(C.c_float)
 _dp = C.POINTER(C.c_double)
@@ -68,6 +74,16 @@ def build_ref() -> Optional[str]:
     if not os.path.exists(REF_SO) or any(os.path.getmtime(s) > os.path.getmtime(REF_SO) for s in src):
         subprocess.run(["make", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"], check=True, stdout=subprocess.DEVNULL)
     return REF_SO
+
+
+def build_ref_gpu() -> Optional[str]:
+    """Compiles the reference's CUDA render kernels for sm_100a where the reference tree exists."""
+    if not os.path.isdir(REF_ROOT):
+        return REF_GPU_SO if os.path.exists(REF_GPU_SO) else None
+    src = [os.path.join(HERE, "ref_gpu_harness.cu"), os.path.join(HERE, "Makefile")]
+    if not os.path.exists(REF_GPU_SO) or any(os.path.getmtime(s) > os.path.getmtime(REF_GPU_SO) for s in src):
+        subprocess.run(["make", "-C", HERE, "refgpu", f"REF_ROOT={REF_ROOT}"], check=True, stdout=subprocess.DEVNULL)
+    return REF_GPU_SO
 
 
 class Checker:
@@ -486,3 +502,100 @@ def reference_available() -> bool:
         return build_ref() is not None and os.path.exists(REF_SO)
     except Exception:
         return False
+
+
+def reference_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+class ReferenceGpu:
+    """The reference's megakernel (PathTracer.cu, compiled unchanged for sm_100a)
+    driven through its launch wrappers by the wave loop of its render loop
+    (oracle/ref_gpu_harness.cu).  Needs a CUDA device."""
+
+    def __init__(self):
+        path = build_ref_gpu()
+        if path is None or not os.path.exists(path):
+            raise FileNotFoundError("reference GPU build unavailable")
+        L = self.lib = C.CDLL(path)
+        L.refgpu_scene_create.restype = C.c_void_p
+        L.refgpu_scene_create.argtypes = [C.c_int, _fp, _fp, _fp, _u32p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                          _dp]
+        L.refgpu_scene_destroy.argtypes = [C.c_void_p]
+        L.refgpu_scene_bvh_node_count.argtypes = [C.c_void_p]
+        L.refgpu_env_create.restype = C.c_void_p
+        L.refgpu_env_create.argtypes = [C.c_int, C.c_int, _fp, _fp, _fp]
+        L.refgpu_env_destroy.argtypes = [C.c_void_p]
+        L.refgpu_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, _fp,
+                                    _u32p, _fp, _fp, _u8p, _dp]
+
+    def scene(self, mesh) -> "ReferenceGpuScene":
+        return ReferenceGpuScene(self, mesh)
+
+    def env(self, rgb: np.ndarray, marginal: np.ndarray, row: np.ndarray) -> "ReferenceGpuEnv":
+        return ReferenceGpuEnv(self, rgb, marginal, row)
+
+
+class ReferenceGpuScene:
+    def __init__(self, rg: ReferenceGpu, mesh):
+        self.rg = rg
+        m = mesh.contiguous()
+        self.ms = np.zeros(2, np.float64)
+        self.h = rg.lib.refgpu_scene_create(m.triangle_count, _ptr(m.positions, _fp), _ptr(m.normals, _fp),
+                                            _ptr(m.uvs, _fp), _ptr(m.material_ids, _u32p), len(m.materials),
+                                            _vp(m.materials) if len(m.materials) else None, len(m.textures),
+                                            _vp(m.textures) if len(m.textures) else None, _ptr(self.ms, _dp))
+        if not self.h:
+            raise RuntimeError("reference GPU scene build failed")
+
+    @property
+    def build_ms(self) -> float:
+        """Host median-split BVH + scene build time of the reference (ms)."""
+        return float(self.ms[0])
+
+    @property
+    def upload_ms(self) -> float:
+        return float(self.ms[1])
+
+    def bvh_node_count(self) -> int:
+        return int(self.rg.lib.refgpu_scene_bvh_node_count(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.rg.lib.refgpu_scene_destroy(self.h)
+            self.h = None
+
+    def render(self, camera, params, width, height, max_waves=0, env=None):
+        """One frame from a cleared accumulator; returns the accumulation state
+        and the timing of the wave loop."""
+        camera_, params_ = _rec(camera), _rec(params)
+        P = width * height
+        st = dict(acc=np.zeros((P, 4), np.float32), counts=np.zeros(P, np.uint32), lum_mean=np.zeros(P, np.float32),
+                  m2=np.zeros(P, np.float32), converged=np.zeros(P, np.uint8))
+        out = np.zeros(5, np.float64)
+        rc = self.rg.lib.refgpu_render(self.h, env.h if env is not None else None, _vp(camera_), _vp(params_),
+                                       width, height, int(max_waves), _ptr(st["acc"], _fp), _ptr(st["counts"], _u32p),
+                                       _ptr(st["lum_mean"], _fp), _ptr(st["m2"], _fp), _ptr(st["converged"], _u8p),
+                                       _ptr(out, _dp))
+        if rc != 0:
+            raise RuntimeError(f"reference GPU render failed at step {rc}")
+        st.update(device_ms=float(out[0]), waves=int(out[1]), samples=float(out[2]), wall_ms=float(out[3]),
+                  compactions=int(out[4]))
+        return st
+
+
+class ReferenceGpuEnv:
+    def __init__(self, rg: ReferenceGpu, rgb, marginal, row):
+        self.rg = rg
+        h, w = rgb.shape[:2]
+        self.rgb = np.ascontiguousarray(rgb, np.float32)
+        self.marginal = np.ascontiguousarray(marginal, np.float32)
+        self.row = np.ascontiguousarray(row, np.float32)
+        self.h = rg.lib.refgpu_env_create(w, h, _ptr(self.rgb, _fp), _ptr(self.marginal, _fp), _ptr(self.row, _fp))
+        if not self.h:
+            raise RuntimeError("reference GPU environment upload failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.rg.lib.refgpu_env_destroy(self.h)
+            self.h = None
