@@ -495,17 +495,21 @@ int pt_reset_region(pt_renderer* r);
  * latency-critical callbacks such as a viewport's surface pick, for which
  * cudaMalloc/cudaFree cost an implicit device synchronisation each time.  Every input and output
  * is a DEVICE pointer supplied by the caller (positions 9 floats/triangle;
- * normals and uvs may be NULL; results as in pt_trace_rays); work runs on
- * `stream` (NULL = default stream) of the current device and the call returns
- * after the work is enqueued (the BVH build synchronises the stream once per
- * tree level).  All temporaries live in one 8 MiB device array that the
- * library reserves on every GPU it is loaded on, for the life of the process;
- * up to PT_NOALLOC_MAX_TRIANGLES triangles (larger inputs are rejected with
- * PT_ERR_INVALID_ARGUMENT and a message).  The first call on a device looks up
- * that array's device address -- make it before any stream capture.  Calls
- * share the array, so calls whose GPU work overlaps race and must be
- * serialised by the caller.  error_message (may be NULL) receives the reason
- * of a failure. */
+ * normals and uvs may be NULL: without normals the reported normal is the
+ * triangle's geometric normal facing the ray, without uvs the uv is 0; results
+ * as in pt_trace_rays); work runs on `stream` (NULL = default stream) of the
+ * current device.  The BVH build waits for `stream` once per tree level, so
+ * the call blocks the host until the build is done and returns with the
+ * traversal enqueued.  All temporaries live in one 8 MiB device array,
+ * reserved on a GPU when the library's module is first loaded there (at the
+ * latest at the first call) and kept for the life of the process; up to
+ * PT_NOALLOC_MAX_TRIANGLES triangles (larger inputs are rejected with
+ * PT_ERR_INVALID_ARGUMENT and a message).  The first call in a CUDA context
+ * (per device, and again after that context is destroyed and recreated, e.g.
+ * by cudaDeviceReset) looks up that array's device address -- make it before
+ * any stream capture.  Calls share the array, so calls whose GPU work overlaps
+ * race and must be serialised by the caller.  error_message (may be NULL)
+ * receives the reason of a failure. */
 int pt_trace_soup_noalloc(uint32_t triangle_count, const float* positions, const float* normals, const float* uvs,
     int n, const float* origins, const float* dirs, const float* tmin, const float* tmax, uint8_t* hit, float* t,
     uint32_t* tri, float* normal, float* uv, void* stream, char* error_message, size_t error_capacity);

@@ -8,15 +8,23 @@
 // would cost an implicit device synchronisation on every call.  They pass
 // device buffers for the triangles, rays and results; every temporary of the
 // BVH build and the traversal lives in one file-scope device array
-// (kScratchBytes, room for PT_NOALLOC_MAX_TRIANGLES triangles) that the module
-// reserves when the library is loaded and that every GPU which loads the
-// library keeps until the process exits.
+// (kScratchBytes, room for PT_NOALLOC_MAX_TRIANGLES triangles).  The array is
+// reserved on a device when this module is first loaded there (with CUDA's
+// lazy module loading, at the latest at the first call) and stays reserved
+// until the process exits.
 //
-// Set-up: the first call on a device, with that device current, looks up the
-// array's device address with cudaGetSymbolAddress and caches it; make that
-// first call before any stream capture on the device.
+// Set-up: the first call in a CUDA context (per device, and again if that
+// device's context is destroyed and created anew, e.g. after cudaDeviceReset,
+// or if the caller makes another context of the device current) looks up the
+// array's device address with cudaGetSymbolAddress while that context is
+// current, and keeps it keyed by the context's unique id; make that first call
+// before any stream capture in the context.
 //
-// Sharing: all calls on a device use the same array, which keeps the previous
+// Blocking: the BVH build waits for `stream` between its levels, so a call
+// returns to the host only once the build is done (the traversal is left
+// enqueued on `stream`).
+//
+// Sharing: all calls in a context use the same array, which keeps the previous
 // call's contents; everything that must start at zero or at a sentinel (the
 // bounds reduction, parent links, visit counters, work counters, the root
 // task) is written by the call itself before use.  Calls whose GPU work
@@ -26,7 +34,8 @@
 #include "pt_render.cuh"
 
 
-#include <atomic>
+#include <cuda.h> // CUcontext / CUresult types; the two driver calls are fetched through the runtime
+
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -39,12 +48,54 @@ constexpr size_t kScratchBytes = size_t(8) << 20; // 8 MiB per device
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-// Device address of g_scratch per device. In host code `g_scratch` names a
-// host-side stand-in, so the address is looked up once per device with
-// cudaGetSymbolAddress while that device is current.
+// Device address of g_scratch per device.  In host code `g_scratch` names a
+// host-side stand-in, so the address is looked up with cudaGetSymbolAddress
+// while the device's context is current.  A module global has a different
+// address in every context it is loaded into, so the cached address is keyed
+// by the unique id of the context it was looked up in (cuCtxGetId) and looked
+// up again when the current context's id differs.
 constexpr int kMaxDevices = 64;
-std::atomic<void*> g_scratchAddr[kMaxDevices];
+struct ScratchSlot {
+    unsigned long long context = 0; // cuCtxGetId of the context `address` belongs to (0 = none yet)
+    void* address = nullptr;
+};
+ScratchSlot g_scratchSlot[kMaxDevices];
 std::mutex g_setupMutex;
+
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+PfnCtxGetCurrent g_ctxGetCurrent = nullptr;
+PfnCtxGetId g_ctxGetId = nullptr;
+
+// Id of the calling thread's current context (0 if none is current); the
+// caller holds g_setupMutex.
+int currentContextId(unsigned long long* id, char* err, size_t errLen)
+{
+    if (g_ctxGetCurrent == nullptr || g_ctxGetId == nullptr) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa = cudaDriverEntryPointSymbolNotFound, qb = qa;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || a == nullptr || b == nullptr) {
+            std::snprintf(err, errLen, "driver entry points cuCtxGetCurrent/cuCtxGetId unavailable");
+            return PT_ERR_CUDA;
+        }
+        g_ctxGetCurrent = reinterpret_cast<PfnCtxGetCurrent>(a);
+        g_ctxGetId = reinterpret_cast<PfnCtxGetId>(b);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctxGetCurrent(&ctx) != CUDA_SUCCESS) {
+        std::snprintf(err, errLen, "cuCtxGetCurrent failed");
+        return PT_ERR_CUDA;
+    }
+    *id = 0;
+    if (ctx != nullptr && g_ctxGetId(ctx, id) != CUDA_SUCCESS) {
+        std::snprintf(err, errLen, "cuCtxGetId failed");
+        return PT_ERR_CUDA;
+    }
+    return PT_OK;
+}
 
 int scratchFor(int device, void** out, char* err, size_t errLen)
 {
@@ -52,20 +103,34 @@ int scratchFor(int device, void** out, char* err, size_t errLen)
         std::snprintf(err, errLen, "device %d out of range", device);
         return PT_ERR_INVALID_ARGUMENT;
     }
-    void* p = g_scratchAddr[device].load(std::memory_order_acquire);
-    if (p == nullptr) {
-        std::lock_guard<std::mutex> lock(g_setupMutex);
-        p = g_scratchAddr[device].load(std::memory_order_relaxed);
-        if (p == nullptr) {
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-            if (e != cudaSuccess || p == nullptr) {
-                std::snprintf(err, errLen, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
-                return PT_ERR_CUDA;
-            }
-            g_scratchAddr[device].store(p, std::memory_order_release);
-        }
+    std::lock_guard<std::mutex> lock(g_setupMutex);
+    unsigned long long ctx = 0;
+    int st = currentContextId(&ctx, err, errLen);
+    if (st != PT_OK) {
+        return st;
     }
-    *out = p;
+    ScratchSlot& slot = g_scratchSlot[device];
+    if (ctx == 0 || slot.context != ctx || slot.address == nullptr) {
+        // set-up in this context (the runtime makes the device's primary
+        // context current first if no context is current yet)
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            std::snprintf(err, errLen, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+            return PT_ERR_CUDA;
+        }
+        st = currentContextId(&ctx, err, errLen);
+        if (st != PT_OK) {
+            return st;
+        }
+        if (ctx == 0) {
+            std::snprintf(err, errLen, "no CUDA context is current after the symbol lookup");
+            return PT_ERR_CUDA;
+        }
+        slot.context = ctx;
+        slot.address = p;
+    }
+    *out = slot.address;
     return PT_OK;
 }
 
@@ -88,7 +153,10 @@ struct Carve {
     }
 };
 
-__global__ void k_soup_shade(const float* nrm, const float* uv, uint32_t n, TriShade* out)
+// Shading records of the soup.  Without vertex normals every vertex gets the
+// triangle's geometric normal (v1 - v0) x (v2 - v0), so the reported normal is
+// the face normal flipped to face the ray.
+__global__ void k_soup_shade(const float* pos, const float* nrm, const float* uv, uint32_t n, TriShade* out)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         TriShade s;
@@ -98,7 +166,14 @@ __global__ void k_soup_shade(const float* nrm, const float* uv, uint32_t n, TriS
             s.b = make_float4(a[3], a[4], a[5], 0.0f);
             s.c = make_float4(a[6], a[7], a[8], 0.0f);
         } else {
-            s.a = s.b = s.c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            // rounded products (no contraction): the same bits as a float32 host cross product
+            const float* p = pos + 9ull * i;
+            const float e1x = p[3] - p[0], e1y = p[4] - p[1], e1z = p[5] - p[2];
+            const float e2x = p[6] - p[0], e2y = p[7] - p[1], e2z = p[8] - p[2];
+            const float4 g = make_float4(__fsub_rn(__fmul_rn(e1y, e2z), __fmul_rn(e1z, e2y)),
+                __fsub_rn(__fmul_rn(e1z, e2x), __fmul_rn(e1x, e2z)),
+                __fsub_rn(__fmul_rn(e1x, e2y), __fmul_rn(e1y, e2x)), 0.0f);
+            s.a = s.b = s.c = g;
         }
         float t[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         if (uv != nullptr) {
@@ -194,7 +269,7 @@ extern "C" int pt_trace_soup_noalloc(uint32_t triangle_count, const float* posit
     }
     if (N > 0) {
         const int grid = static_cast<int>((N + 255) / 256);
-        k_soup_shade<<<grid, 256, 0, s>>>(normals, uvs, N, shade);
+        k_soup_shade<<<grid, 256, 0, s>>>(positions, normals, uvs, N, shade);
     }
     if (n > 0) {
         DevScene scene;

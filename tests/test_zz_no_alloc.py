@@ -10,6 +10,10 @@ This file is collected last on purpose, so that it also runs after every other
 test in the same process.
 """
 import ctypes as C
+import os
+import subprocess
+import sys
+import tempfile
 
 import numpy as np
 import pytest
@@ -34,13 +38,13 @@ def _lib():
 class _DeviceQuery:
     """Device copies of one soup and one ray batch plus result buffers."""
 
-    def __init__(self, mesh, o, d, tmin, tmax):
+    def __init__(self, mesh, o, d, tmin, tmax, with_normals=True):
         import torch
         dev = torch.device("cuda", 0)
         m = mesh.contiguous()
         self.triangles = m.triangle_count
         up = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32).reshape(-1)).to(dev)
-        self.pos, self.nrm, self.uvs = up(m.positions), up(m.normals), up(m.uvs)
+        self.pos, self.nrm, self.uvs = up(m.positions), up(m.normals) if with_normals else None, up(m.uvs)
         self.n = len(o)
         self.o, self.d, self.tmin, self.tmax = up(o), up(d), up(tmin), up(tmax)
         self.hit = torch.zeros(self.n, dtype=torch.uint8, device=dev)
@@ -54,7 +58,8 @@ class _DeviceQuery:
     def run(self, L):
         import torch
         err = C.create_string_buffer(256)
-        rc = L.pt_trace_soup_noalloc(self.triangles, self.pos.data_ptr(), self.nrm.data_ptr(), self.uvs.data_ptr(),
+        nrm = self.nrm.data_ptr() if self.nrm is not None else None
+        rc = L.pt_trace_soup_noalloc(self.triangles, self.pos.data_ptr(), nrm, self.uvs.data_ptr(),
                                      self.n, self.o.data_ptr(), self.d.data_ptr(), self.tmin.data_ptr(),
                                      self.tmax.data_ptr(), self.hit.data_ptr(), self.t.data_ptr(), self.tri.data_ptr(),
                                      self.normal.data_ptr(), self.uv.data_ptr(), C.c_void_p(self.stream.cuda_stream),
@@ -122,3 +127,56 @@ def test_noalloc_rejects_oversized_input():
                                  None, None, None, err, 256)
     assert rc == 1  # PT_ERR_INVALID_ARGUMENT
     assert b"exceed the maximum of 16384" in err.value
+
+
+def _face_normal_mesh(mesh):
+    """The soup with every vertex normal replaced by the float32 geometric normal (v1 - v0) x (v2 - v0)."""
+    m = mesh.contiguous()
+    p = m.positions.astype(np.float32)
+    e1, e2 = p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]
+    g = np.stack([e1[:, 1] * e2[:, 2] - e1[:, 2] * e2[:, 1], e1[:, 2] * e2[:, 0] - e1[:, 0] * e2[:, 2],
+                  e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0]], axis=1).astype(np.float32)
+    return type(m)(m.positions, np.repeat(g[:, None, :], 3, axis=1), m.uvs, m.material_ids, m.materials, m.textures)
+
+
+def test_noalloc_without_normals_reports_face_normals():
+    """normals = NULL: the reported normal is the triangle's geometric normal facing the ray, the same
+    as the allocating entry point gives for a soup whose vertex normals are the face normals."""
+    from lsystemeditor_b200.pathtracer import PathTracer
+    L = _lib()
+    mesh, o, d, tmin, tmax = _case(4000, 43)
+    q = _DeviceQuery(mesh, o, d, tmin, tmax, with_normals=False)
+    with PathTracer(0) as pt:
+        pt.configure(8, 8, _face_normal_mesh(mesh))
+        expect = pt.trace_rays(o, d, tmin, tmax)
+    q.run(L)
+    got = q.results()
+    assert expect["hit"].sum() > 1000
+    _compare(got, expect, "no normals")
+    assert np.allclose(np.linalg.norm(got["normal"][got["hit"]], axis=1), 1.0, atol=1e-5)
+
+
+def test_noalloc_scratch_follows_the_context():
+    """A module global has its own address in every CUDA context: the scratch address is looked up per
+    context (keyed by the context's id), so the query gives the same results in the primary context, in a
+    second context of the same device, and in the primary context again.  Runs in a child process that
+    drives the contexts through the driver API."""
+    from lsystemeditor_b200._build import LIB
+    from lsystemeditor_b200.pathtracer import PathTracer
+    mesh, o, d, tmin, tmax = _case(2000, 44, n_rays=20_000)
+    with PathTracer(0) as pt:
+        pt.configure(8, 8, _face_normal_mesh(mesh))
+        expect = pt.trace_rays(o, d, tmin, tmax)
+    with tempfile.TemporaryDirectory() as tmp:
+        inp, out = os.path.join(tmp, "in.npz"), os.path.join(tmp, "out.npz")
+        m = mesh.contiguous()
+        np.savez(inp, pos=m.positions, uvs=m.uvs, o=o, d=d, tmin=tmin, tmax=tmax, lib=LIB)
+        root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        r = subprocess.run([sys.executable, "-m", "tests.noalloc_contexts", inp, out], cwd=root,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        res = dict(np.load(out))
+    for tag in ("primary", "second", "again"):
+        got = dict(hit=res[f"{tag}_hit"].astype(bool), t=res[f"{tag}_t"], tri=res[f"{tag}_tri"],
+                   normal=res[f"{tag}_normal"].reshape(-1, 3), uv=res[f"{tag}_uv"].reshape(-1, 2))
+        _compare(got, expect, tag)
