@@ -434,6 +434,18 @@ int pt_autotune(pt_renderer* r, int waves, pt_tuning* out);
  * receives bytes read / time. */
 int pt_measure_l2(pt_renderer* r, uint64_t bytes, int reps, double* gb_per_s);
 
+/* Stable LSD radix sort of n (key, value) pairs of 32-bit unsigned integers on
+ * the low `bits` bits of the keys, over DEVICE buffers, on `stream` (no
+ * counterpart in the reference, whose BVH is a host median split; the GPU BVH
+ * build sorts its 30-bit Morton keys with it).  keys/vals are left unchanged,
+ * keys_out/vals_out (not aliasing them) receive the sorted pairs; temp is
+ * device scratch of at least pt_radix_sort_temp_bytes(n) bytes.  Returns
+ * PT_ERR_INVALID_ARGUMENT for null pointers, bits outside 1..32 or too little
+ * scratch. */
+size_t pt_radix_sort_temp_bytes(uint32_t n);
+int pt_radix_sort_pairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keys_out, uint32_t* vals_out, uint32_t n,
+    int bits, void* temp, size_t temp_bytes, void* stream);
+
 /* ---- Spectral mode (extension; the reference's integrator is RGB) ---------
  * With pt_render_params.spectral_wavelengths = 4 or 8, every path carries
  * that many wavelengths spread evenly over [380, 780] nm from a hero

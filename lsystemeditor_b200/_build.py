@@ -17,8 +17,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libpt_b200.so")
-SOURCES = ["pt_bvh.cu", "pt_render.cu", "pt_scene.cu", "pt_output.cu", "pt_adjoint.cu", "pt_api.cu", "pt_noalloc.cu", "pt_spectral.cu", "pt_l2probe.cu"]
-HEADERS = ["pt_common.cuh", "pt_bvh.cuh", "pt_render.cuh", "pt_trace.cuh", "pt_bsdf.cuh", "pt_scene.cuh", "pt_output.cuh", "pt_path.cuh", "pt_adjoint.cuh", "pt_spectral.cuh"]
+SOURCES = ["pt_bvh.cu", "pt_render.cu", "pt_scene.cu", "pt_output.cu", "pt_adjoint.cu", "pt_api.cu", "pt_noalloc.cu", "pt_spectral.cu", "pt_l2probe.cu",
+           "pt_sort.cu"]
+HEADERS = ["pt_common.cuh", "pt_bvh.cuh", "pt_render.cuh", "pt_trace.cuh", "pt_bsdf.cuh", "pt_scene.cuh", "pt_output.cuh", "pt_path.cuh", "pt_adjoint.cuh", "pt_spectral.cuh",
+           "pt_select.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--cudart", "static",
               "-Xcompiler", "-ffp-contract=off"]

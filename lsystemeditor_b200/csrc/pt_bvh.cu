@@ -20,7 +20,6 @@
 // builds whatever tree traverses fastest.
 #include "pt_bvh.cuh"
 
-#include <cub/device/device_radix_sort.cuh>
 
 #include <cfloat>
 #include <cmath>
@@ -665,14 +664,13 @@ int buildBvh(const float* dPositions, uint32_t n, BvhBuffers& out, cudaStream_t 
     PT_TRY(cudaMemcpyAsync(cbounds, init, sizeof(init), cudaMemcpyHostToDevice, stream));
     k_prepare<<<gridFor(n), kBlock, 0, stream>>>(dPositions, n, triLo, triHi, cbounds);
     k_morton<<<gridFor(n), kBlock, 0, stream>>>(triLo, triHi, n, cbounds, keys, vals);
-    size_t tempBytes = 0;
-    PT_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keysSorted, vals, valsSorted, N, 0, 30, stream));
+    const size_t tempBytes = radixSortTempBytes(n);
     void* temp = ar.getBytes(13, tempBytes);
     if (!ar.ok()) {
         std::snprintf(err, errLen, "radix sort scratch allocation failed");
         return PT_ERR_OUT_OF_MEMORY;
     }
-    PT_TRY(cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keysSorted, vals, valsSorted, N, 0, 30, stream));
+    PT_TRY(radixSortPairs(keys, vals, keysSorted, valsSorted, n, 30, temp, tempBytes, stream));
     PT_TRY(cudaMemsetAsync(parent, 0xff, sizeof(int) * nodesBin, stream));
     if (N > 1) {
         k_karras<<<gridFor(N - 1), kBlock, 0, stream>>>(keysSorted, N, child, parent);
@@ -749,10 +747,7 @@ namespace pt {
 
 size_t bvhSortTempBytes(uint32_t n)
 {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
-        static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 30);
-    return bytes;
+    return radixSortTempBytes(n);
 }
 
 // Same build as buildBvh, into caller-provided buffers: nothing is allocated.
@@ -769,15 +764,12 @@ int buildBvhInto(const float* dPositions, uint32_t n, const BvhScratch& sc, CwNo
     PT_TRY(cudaMemcpyAsync(sc.cbounds, init, sizeof(init), cudaMemcpyHostToDevice, stream));
     k_prepare<<<gridFor(n), kBlock, 0, stream>>>(dPositions, n, sc.triLo, sc.triHi, sc.cbounds);
     k_morton<<<gridFor(n), kBlock, 0, stream>>>(sc.triLo, sc.triHi, n, sc.cbounds, sc.keys, sc.vals);
-    size_t tempBytes = 0;
-    PT_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, sc.keys, sc.keysSorted, sc.vals, sc.valsSorted, N, 0, 30,
-        stream));
+    const size_t tempBytes = radixSortTempBytes(n);
     if (tempBytes > sc.sortTempBytes) {
         std::snprintf(err, errLen, "radix sort needs %zu scratch bytes, %zu reserved", tempBytes, sc.sortTempBytes);
         return PT_ERR_INVALID_ARGUMENT;
     }
-    PT_TRY(cub::DeviceRadixSort::SortPairs(sc.sortTemp, tempBytes, sc.keys, sc.keysSorted, sc.vals, sc.valsSorted, N, 0,
-        30, stream));
+    PT_TRY(radixSortPairs(sc.keys, sc.vals, sc.keysSorted, sc.valsSorted, n, 30, sc.sortTemp, tempBytes, stream));
     PT_TRY(cudaMemsetAsync(sc.parent, 0xff, sizeof(int) * nodesBin, stream));
     if (N > 1) {
         k_karras<<<gridFor(N - 1), kBlock, 0, stream>>>(sc.keysSorted, N, sc.child, sc.parent);

@@ -128,6 +128,13 @@ struct BvhScratch {
 // Radix-sort scratch bytes for n keys (a size query; nothing is launched).
 size_t bvhSortTempBytes(uint32_t n);
 
+// Stable LSD radix sort of n (key, value) pairs on the low `bits` bits of the
+// keys (pt_sort.cu); keys/vals are left unchanged, the sorted pairs go to
+// keysOut/valsOut.  temp needs radixSortTempBytes(n) bytes.
+size_t radixSortTempBytes(uint32_t n);
+cudaError_t radixSortPairs(const uint32_t* keys, const uint32_t* vals, uint32_t* keysOut, uint32_t* valsOut, uint32_t n,
+    int bits, void* temp, size_t tempBytes, cudaStream_t s);
+
 // The build of buildBvh into caller-provided buffers (outNodes: n + 1 nodes,
 // outTris: n records); performs no device allocation.
 int buildBvhInto(const float* dPositions, uint32_t n, const BvhScratch& scratch, CwNode* outNodes, TriVerts* outTris,

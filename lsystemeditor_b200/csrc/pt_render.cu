@@ -36,7 +36,7 @@
 #include "pt_trace.cuh"
 
 #include <cooperative_groups.h>
-#include <cub/device/device_select.cuh>
+#include "pt_select.cuh"
 #include <curand_kernel.h>
 
 namespace cg = cooperative_groups;
@@ -1465,8 +1465,6 @@ __global__ void __launch_bounds__(256) k_accumulate(const LaunchCtx* __restrict_
     }
 }
 
-// Ordered-within-block compaction of the active list (compactActiveListKernel,
-// PathTracer.cu:372-411, without per-element atomics).
 // Per-scene active ranges (the active list is sorted by pixel) and job
 // offsets of the current batch: scene s owns active entries
 // [sceneActiveStart[s], sceneActiveStart[s + 1]) and jobs
@@ -1505,6 +1503,8 @@ __global__ void k_scene_jobs(const LaunchCtx* __restrict__ cp, int sceneCount, i
     }
 }
 
+// A pixel stays on the active list until it converged or reached the sample
+// cap (the tests of compactActiveListKernel, PathTracer.cu:385-391).
 struct KeepActive {
     const uint8_t* converged;
     const uint32_t* counts;
@@ -1513,6 +1513,16 @@ struct KeepActive {
     {
         return converged[p] == 0 && !(maxSpp > 0 && counts[p] >= static_cast<uint32_t>(maxSpp));
     }
+};
+// Select predicate / value over the entries of an active list.
+struct KeepListed {
+    const int* list;
+    KeepActive keep;
+    __device__ __forceinline__ bool operator()(long long i) const { return keep(list[i]); }
+};
+struct ListedPixel {
+    const int* list;
+    __device__ __forceinline__ int operator()(long long i) const { return list[i]; }
 };
 
 __global__ void k_reset(const LaunchCtx* __restrict__ cp, int pixels)
@@ -1729,15 +1739,13 @@ void launchAccumulate(const LaunchCtx* c, int activeCount, int batch, cudaStream
 }
 size_t compactTempBytes(int n)
 {
-    size_t bytes = 0;
-    cub::DeviceSelect::If(nullptr, bytes, static_cast<const int*>(nullptr), static_cast<int*>(nullptr),
-        static_cast<int*>(nullptr), n, KeepActive{nullptr, nullptr, 0});
-    return bytes;
+    return selectTempBytes(n);
 }
 cudaError_t launchCompactStable(const int* in, int* out, int* outCount, int n, const uint8_t* converged,
     const uint32_t* counts, int maxSpp, void* temp, size_t tempBytes, cudaStream_t s)
 {
-    return cub::DeviceSelect::If(temp, tempBytes, in, out, outCount, n, KeepActive{converged, counts, maxSpp}, s);
+    return launchSelect(static_cast<long long>(n), KeepListed{in, KeepActive{converged, counts, maxSpp}},
+        ListedPixel{in}, out, outCount, temp, tempBytes, s);
 }
 void launchSceneJobs(const LaunchCtx* c, int sceneCount, int waves, cudaStream_t s)
 {

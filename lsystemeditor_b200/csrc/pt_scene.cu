@@ -13,8 +13,7 @@
 // light sampling picks the same triangle as the reference for every uniform.
 #include "pt_scene.cuh"
 
-#include <cub/device/device_select.cuh>
-#include <thrust/iterator/counting_iterator.h>
+#include "pt_select.cuh"
 
 namespace pt {
 
@@ -387,20 +386,28 @@ void launchEmissiveWeights(const float* positions, const uint32_t* materialIds, 
     }
 }
 
+namespace {
+struct FlaggedTriangle {
+    const uint8_t* flags;
+    __device__ __forceinline__ bool operator()(long long i) const { return flags[i] != 0; }
+};
+struct TriangleIndex {
+    __device__ __forceinline__ uint32_t operator()(long long i) const { return static_cast<uint32_t>(i); }
+};
+} // namespace
+
 size_t emissiveSelectTempBytes(uint32_t n)
 {
-    size_t bytes = 0;
-    cub::DeviceSelect::Flagged(nullptr, bytes, thrust::counting_iterator<uint32_t>(0u),
-        static_cast<const uint8_t*>(nullptr), static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
-        static_cast<int>(n));
-    return bytes;
+    return selectTempBytes(n);
 }
 
+// The emissive list in increasing triangle order (MeshAccelScene.cpp:62-95
+// walks the triangles in order and appends every emitter).
 cudaError_t emissiveSelect(void* temp, size_t tempBytes, const uint8_t* flags, uint32_t n, uint32_t* idx,
     uint32_t* dCount, cudaStream_t s)
 {
-    return cub::DeviceSelect::Flagged(temp, tempBytes, thrust::counting_iterator<uint32_t>(0u), flags, idx, dCount,
-        static_cast<int>(n), s);
+    return launchSelect(static_cast<long long>(n), FlaggedTriangle{flags}, TriangleIndex{}, idx, dCount, temp,
+        tempBytes, s);
 }
 
 void launchEmissiveCdf(const float* weights, const uint32_t* idx, const uint32_t* dCount, float* cdf, uint32_t* out,

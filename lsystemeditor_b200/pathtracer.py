@@ -84,7 +84,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
                     "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift",
                     "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune", "pt_measure_l2",
-                    "pt_set_extend_mode"]
+                    "pt_set_extend_mode", "pt_radix_sort_temp_bytes", "pt_radix_sort_pairs"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -152,6 +152,9 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_batch_share_scene.argtypes = [vp, C.c_int, C.c_int]
     L.pt_autotune.argtypes = [vp, C.c_int, C.POINTER(PtTuning)]
     L.pt_measure_l2.argtypes = [vp, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
+    L.pt_radix_sort_temp_bytes.argtypes = [C.c_uint32]
+    L.pt_radix_sort_temp_bytes.restype = C.c_size_t
+    L.pt_radix_sort_pairs.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_int, vp, C.c_size_t, vp]
     _LIB = L
     return L
 

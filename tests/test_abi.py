@@ -16,7 +16,7 @@ HEADER = os.path.join(_build.INCLUDE, "pt_b200.h")
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^(?:int|void|float|const char\*)\s+(pt_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:int|void|float|size_t|const char\*)\s+(pt_\w+)\s*\(", text, re.M)))
 
 
 def test_library_builds_and_exports_every_declared_symbol():
