@@ -194,7 +194,10 @@ int pt_get_camera(const pt_renderer* r, pt_camera* out);
 /* Snapshot of the setters setMaxSamplesPerPixel, setMinSamples,
  * setRelativeErrorThreshold, setRussianRouletteMinDepth, setBrdfDebugFlags,
  * setClearColor, setEnvironmentIntensity (PathTracer.h:73-124) as one record
- * (RenderParamsGpu, RenderTypes.h:15-28). Resets accumulation. */
+ * (RenderParamsGpu, RenderTypes.h:15-28). Resets accumulation.  Values are
+ * clamped as those setters clamp them (PathTracer.cpp:126-190): max spp to
+ * [0, 1e6], min spp to [1, 1e4], relative error threshold to [0.001, 1], RR
+ * depth to >= 0; pt_get_params returns the clamped record. */
 int pt_set_params(pt_renderer* r, const pt_render_params* params);
 int pt_get_params(const pt_renderer* r, pt_render_params* out);
 /* RenderParamsGpu{} defaults (RenderTypes.h:15-28) with a zero extension tail. */

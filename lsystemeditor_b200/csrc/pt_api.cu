@@ -1471,6 +1471,17 @@ int pt_set_params(pt_renderer* r, const pt_render_params* params)
             params->spectral_wavelengths);
     }
     r->params = *params;
+    // The ranges the reference's setters clamp to (PathTracer.cpp:126-190):
+    // max spp in [0, 1e6] (0 = no cap), min spp in [1, 1e4], relative error in
+    // [0.001, 1] (a NaN becomes the lower bound); the RR depth is not negative.
+    pt_render_params& p = r->params;
+    p.max_samples_per_pixel = std::min(std::max(p.max_samples_per_pixel, 0), 1000000);
+    p.min_samples = std::min(std::max(p.min_samples, 1), 10000);
+    if (!(p.relative_error_threshold >= 0.001f)) {
+        p.relative_error_threshold = 0.001f;
+    }
+    p.relative_error_threshold = std::min(p.relative_error_threshold, 1.0f);
+    p.russian_roulette_min_depth = std::max(p.russian_roulette_min_depth, 0);
     return resetAccum(r);
 }
 
