@@ -437,6 +437,16 @@ int pt_autotune(pt_renderer* r, int waves, pt_tuning* out);
  * receives bytes read / time. */
 int pt_measure_l2(pt_renderer* r, uint64_t bytes, int reps, double* gb_per_s);
 
+/* BVH build quality knob (no reference counterpart; the reference's host
+ * median split has none): the number of treelet SAH reordering passes of the
+ * GPU build (Karras & Aila 2013), 0 = the plain Karras LBVH; default 1.
+ * Applies to the following mesh / instance / batch builds. */
+int pt_set_bvh_options(pt_renderer* r, int treelet_passes);
+/* SAH cost of scene `scene`'s binary BVH as built (before the collapse to
+ * 8-wide nodes; one triangle per leaf): (1.2 * sum of inner node areas +
+ * sum of leaf areas) / root area.  A quality measure for tests and tuning. */
+int pt_bvh_sah_cost(pt_renderer* r, int scene, double* cost);
+
 /* Stable LSD radix sort of n (key, value) pairs of 32-bit unsigned integers on
  * the low `bits` bits of the keys, over DEVICE buffers, on `stream` (no
  * counterpart in the reference, whose BVH is a host median split; the GPU BVH

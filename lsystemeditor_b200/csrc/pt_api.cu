@@ -1967,6 +1967,55 @@ int pt_measure_l2(pt_renderer* r, uint64_t bytes, int reps, double* gb_per_s)
     return PT_OK;
 }
 
+int pt_set_bvh_options(pt_renderer* r, int treelet_passes)
+{
+    if (r == nullptr || treelet_passes < 0 || treelet_passes > 8) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_bvh_options: treelet_passes must be in 0..8");
+    }
+    r->bvhOptions.treeletPasses = treelet_passes;
+    return PT_OK;
+}
+
+// SAH cost of a scene's binary BVH as built (Karras hierarchy after the
+// treelet passes, one triangle per leaf): (C_node * sum of the internal nodes'
+// areas + C_tri * sum of the leaves' areas) / root area, with the builder's
+// costs.  Internal nodes are 0 .. n-2 (root 0), leaves n-1 .. 2n-2; the
+// refit stores each node's surface area in nodeHi.w.
+int pt_bvh_sah_cost(pt_renderer* r, int scene, double* cost)
+{
+    if (r == nullptr || cost == nullptr || scene < 0 || scene >= static_cast<int>(r->scenes.size())) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_bvh_sah_cost: bad arguments");
+    }
+    const SceneSlot& sl = r->scenes[static_cast<size_t>(scene)];
+    const uint32_t n = sl.bvh.triCount;
+    if (n == 0 || sl.bvh.nodes == nullptr) {
+        return fail(r, PT_ERR_NO_SCENE, "pt_bvh_sah_cost: scene %d has no flat BVH", scene);
+    }
+    if (n == 1) {
+        *cost = r->bvhOptions.costTriangle;
+        return PT_OK;
+    }
+    const size_t nodes = 2ull * n - 1;
+    const float4* nodeHi = static_cast<const float4*>(sl.bvh.scratch.ptr[10]);
+    if (nodeHi == nullptr || sl.bvh.scratch.bytes[10] < nodes * sizeof(float4)) {
+        return fail(r, PT_ERR_INTERNAL, "pt_bvh_sah_cost: the build's node bounds are not available");
+    }
+    PT_CHECK(r, cudaSetDevice(r->device));
+    std::vector<float4> hi(nodes);
+    PT_CHECK(r, cudaMemcpyAsync(hi.data(), nodeHi, nodes * sizeof(float4), cudaMemcpyDeviceToHost, r->stream));
+    PT_CHECK(r, cudaStreamSynchronize(r->stream));
+    double inner = 0.0, leaves = 0.0;
+    for (size_t i = 0; i < nodes; ++i) {
+        (i + 1 < n ? inner : leaves) += hi[i].w;
+    }
+    const double root = hi[0].w;
+    if (!(root > 0.0)) {
+        return fail(r, PT_ERR_INTERNAL, "pt_bvh_sah_cost: degenerate root box");
+    }
+    *cost = (r->bvhOptions.costNode * inner + r->bvhOptions.costTriangle * leaves) / root;
+    return PT_OK;
+}
+
 int pt_autotune(pt_renderer* r, int waves, pt_tuning* out)
 {
     if (r == nullptr || waves <= 0 || out == nullptr) {

@@ -84,7 +84,8 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_record_samples", "pt_set_preview_levels", "pt_render_previews", "pt_preview_readback", "pt_set_region",
                     "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift",
                     "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune", "pt_measure_l2",
-                    "pt_set_extend_mode", "pt_radix_sort_temp_bytes", "pt_radix_sort_pairs"]
+                    "pt_set_extend_mode", "pt_radix_sort_temp_bytes", "pt_radix_sort_pairs",
+                    "pt_set_bvh_options", "pt_bvh_sah_cost"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -152,6 +153,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_batch_share_scene.argtypes = [vp, C.c_int, C.c_int]
     L.pt_autotune.argtypes = [vp, C.c_int, C.POINTER(PtTuning)]
     L.pt_measure_l2.argtypes = [vp, C.c_uint64, C.c_int, C.POINTER(C.c_double)]
+    L.pt_set_bvh_options.argtypes = [vp, C.c_int]
+    L.pt_bvh_sah_cost.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
     L.pt_radix_sort_temp_bytes.argtypes = [C.c_uint32]
     L.pt_radix_sort_temp_bytes.restype = C.c_size_t
     L.pt_radix_sort_pairs.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_int, vp, C.c_size_t, vp]
@@ -585,6 +588,15 @@ class PathTracer:
 
     def set_tuning(self, path_capacity: int = 0, blocks_per_sm: int = 0):
         self._check(self._lib.pt_set_tuning(self._h, int(path_capacity), int(blocks_per_sm)))
+
+    def set_bvh_options(self, treelet_passes: int = 1):
+        """Treelet SAH reordering passes of the next BVH builds (0 = plain Karras LBVH)."""
+        self._check(self._lib.pt_set_bvh_options(self._h, int(treelet_passes)))
+
+    def bvh_sah_cost(self, scene: int = 0) -> float:
+        c = C.c_double()
+        self._check(self._lib.pt_bvh_sah_cost(self._h, int(scene), C.byref(c)))
+        return float(c.value)
 
     def set_extend_mode(self, mode: int):
         """pt_set_extend_mode: 0 auto, 1 warp-fetch closest hit, 2 per-lane replacement (identical images)."""
