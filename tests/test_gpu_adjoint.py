@@ -104,6 +104,48 @@ def test_adjoint_matches_finite_differences(tracer, name):
         assert abs(g[m, j] - fd) <= 1e-3 * abs(fd) + 1e-3, (name, m, g[m, j], fd)
 
 
+@pytest.mark.parametrize("name", ["roughness", "metallic"])
+def test_adjoint_matches_finite_differences_in_expectation(tracer, name):
+    """Roughness and metallic change how directions and lobes are sampled, so the
+    fixed-seed estimate is not a smooth function of them and the difference
+    quotient of one render is not their gradient.  For a loss linear in the image
+    (weights w), the path-replay gradient (sampling detached) and a central
+    difference of two renders with common random numbers are both unbiased
+    estimates of d E[loss] / d theta (the difference up to O(step^2)).  Over K
+    independent seed batches (hash seeds) their means must agree within four
+    combined standard errors plus 2%, and the gradient must be resolved."""
+    w = h = 32
+    spp, K, m, step = 16, 24, 8, 0.05
+    spec, params = _setup(tracer, w, h, spp, depth=5, rr_min=64)  # no Russian roulette
+    mats = spec.mesh.materials.copy()
+    mats[m]["roughness"] = 0.5   # the ground: half the image, away from the parameter bounds
+    mats[m]["metallic"] = 0.2
+    j = PARAMS.index(name)
+    wgt = np.random.default_rng(11).uniform(0.5, 1.5, (h, w, 3))
+    theta = theta_of(mats)
+    tp, tm = theta.copy(), theta.copy()
+    tp[m, j] += step
+    tm[m, j] -= step
+    dx = float(np.float32(tp[m, j])) - float(np.float32(tm[m, j]))
+    grads, fds = [], []
+    for k in range(K):
+        p = params.copy()
+        p["seed_mode"] = 1
+        p["seed_value"] = 1000 + k
+        tracer.set_params(p)
+        _render(tracer, mats, spp)
+        g, _ = tracer.backward(wgt.astype(np.float32), spp)
+        grads.append(float(g[m, j]))
+        lp = float((wgt * _render(tracer, apply_theta(mats, tp), spp)).sum())
+        lm = float((wgt * _render(tracer, apply_theta(mats, tm), spp)).sum())
+        fds.append((lp - lm) / dx)
+    grads, fds = np.array(grads), np.array(fds)
+    se = np.sqrt(grads.var(ddof=1) / K + fds.var(ddof=1) / K)
+    gm, fm = grads.mean(), fds.mean()
+    assert abs(gm) > 4.0 * grads.std(ddof=1) / np.sqrt(K), f"{name}: gradient not resolved ({gm} +- {grads.std()})"
+    assert abs(gm - fm) <= 4.0 * se + 0.02 * abs(fm), f"{name}: path replay {gm:.4f} vs difference {fm:.4f} (se {se:.4f})"
+
+
 def test_torch_autograd_reduces_loss(tracer):
     """Adam on the branch materials' base colours through torch.autograd
     (Russian roulette off, so the fixed-seed loss is smooth in them)."""
