@@ -27,8 +27,12 @@ views of 1920x1080 per launch; a step takes about a minute, so run it with
   cpu_baseline  the reference's own render code compiled for the host
          (oracle/_ref, OpenMP over pixels) on a bounded pixel sample.
 
-Multi-GPU: every rank renders its own copy of the workload (pixels and
-scenes are independent; no data-path collective) -> weak scaling.
+Multi-GPU: for the plain, adjoint and forest workloads every rank renders its
+own copy of the workload (pixels and scenes are independent; no data-path
+collective) -> weak scaling.  The batch workload is split by whole scenes over
+the ranks by estimated cost (lsystemeditor_b200/partition.py), each rank
+renders its scenes in one batch and every image is gathered once to rank 0
+inside the timed step -> strong scaling.
 """
 from __future__ import annotations
 
@@ -539,13 +543,26 @@ def run_batch(args):
             dist.barrier()
 
     t0 = time.perf_counter()
-    tubes, cams, sizes, params = batch_scenes()
+    all_tubes, all_cams, all_sizes, params = batch_scenes()
     gen_s = time.perf_counter() - t0
+    # scenes split over the ranks by estimated cost; each rank renders its own
+    # scenes in one batch and rank 0 gathers every image once (strong scaling)
+    from lsystemeditor_b200.partition import assign, gather_to_root, owners, scene_cost
+    spp_cap = int(params["max_samples_per_pixel"])
+    costs = [scene_cost(t.triangle_count, w * h, spp_cap) for t, (w, h) in zip(all_tubes, all_sizes)]
+    assignment = assign(costs, world)
+    mine = assignment[rank]
+    tubes = [all_tubes[k] for k in mine]
+    cams = [all_cams[k] for k in mine]
+    sizes = [all_sizes[k] for k in mine]
     n = len(tubes)
     stream = torch.cuda.current_stream()
     pt = PathTracer(local)
     pt.set_stream(stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    own = owners(assignment)
+    recv = {k: torch.empty((all_sizes[k][0] * all_sizes[k][1], 4), dtype=torch.float32, device="cuda")
+            for k in own if own[k] != 0} if (world > 1 and rank == 0) else {}
 
     def build_batch():
         pt.batch_configure(sizes)
@@ -553,6 +570,23 @@ def run_batch(args):
             pt.batch_set_tubes(k, tubes[k])
             pt.batch_set_camera(k, cams[k])
         pt.set_params(params)
+
+    def local_images():
+        """This rank's scene images as views of the renderer's device accumulator (scene after scene)."""
+        class _View:
+            def __init__(self, ptr, rows):
+                self.__cuda_array_interface__ = {"shape": (rows, 4), "typestr": "<f4", "data": (ptr, False),
+                                                 "strides": None, "version": 3}
+        ptr = pt.device_buffers()[0]
+        views, off = {}, 0
+        for k, (w, h) in zip(mine, sizes):
+            views[k] = torch.as_tensor(_View(ptr + 16 * off, w * h), device="cuda")
+            off += w * h
+        return views
+
+    def gather():
+        if world > 1:
+            gather_to_root(rank, assignment, local_images(), recv)
 
     tb = time.perf_counter()
     build_batch()
@@ -565,6 +599,7 @@ def run_batch(args):
     def step():
         pt.reset_accumulation()
         pt.render(0)
+        gather()
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -632,7 +667,7 @@ def run_batch(args):
     h2d = sum(t.ring_start.nbytes + t.points.nbytes + t.tangents.nbytes + t.radii.nbytes + t.materials.nbytes +
               t.leaves.nbytes + t.extra.positions.nbytes + t.extra.normals.nbytes + t.extra.uvs.nbytes +
               t.extra.material_ids.nbytes + t.extra.materials.nbytes for t in tubes)
-    d2h = sum(w * h * (16 + 4 + 1) for w, h in sizes)
+    d2h = sum(w * h * (16 + 4 + 1) for w, h in sizes) + sum(v.numel() * 4 for v in recv.values())
     torch.cuda.synchronize()
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -641,8 +676,12 @@ def run_batch(args):
     build_batch()
     pt.render(0)
     e_samples = pt.stats()["samples"]
-    for k in range(n):
-        pt.batch_readback(k)
+    gather()
+    if rank == 0:
+        for k in range(n):
+            pt.batch_readback(k)
+        for v in recv.values():
+            v.cpu()
     e1.record(stream)
     torch.cuda.synchronize()
     e_ms = reduce(float(e0.elapsed_time(e1)), "max")
@@ -658,13 +697,18 @@ def run_batch(args):
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"batch: {n} stochastic trees (iterations 4-8, seeds 100-{99 + n}), "
-                               f"{sum(t.triangle_count for t in tubes)} triangles, {sum(w * h for w, h in sizes)} "
-                               "pixels, adaptive 16-512 spp to relative std-error 0.03, depth 12",
-                   "scenes": n, "triangles": int(sum(t.triangle_count for t in tubes)),
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batch: {len(all_tubes)} stochastic trees (iterations 4-8, seeds "
+                               f"100-{99 + len(all_tubes)}), {sum(t.triangle_count for t in all_tubes)} triangles, "
+                               f"{sum(w * h for w, h in all_sizes)} pixels, adaptive 16-512 spp to relative "
+                               "std-error 0.03, depth 12",
+                   "scenes": len(all_tubes), "scenes_on_rank0": n,
+                   "triangles": int(sum(t.triangle_count for t in all_tubes)),
                    "autotune": tune, "frame_loop": "CUDA graphs of 4 bounce iterations",
-                   "pixels": int(sum(w * h for w, h in sizes)), "parallelism": f"replicas{world}",
+                   "pixels": int(sum(w * h for w, h in all_sizes)),
+                   "parallelism": f"scenes split over {world} rank(s) by estimated cost (pixels x spp x BVH depth), "
+                                  "each rank one batched render, every image gathered once to rank 0 "
+                                  "(NCCL point-to-point, inside the timed step)",
                    "l2": "flushed between timed steps (256 MiB write, untimed)",
                    "host_generation_s": round(gen_s, 2), "device_build_s": round(build_s, 2),
                    "batched_ms_per_render": total_ms / args.steps,
@@ -893,6 +937,7 @@ def run_forest(args):
     def step():
         pt.reset_accumulation()
         pt.render(0)
+        gather()
 
     for _ in range(max(args.warmup, 3)):
         step()
