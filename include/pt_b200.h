@@ -109,6 +109,14 @@ typedef struct pt_render_params {
     int32_t adaptive_criterion; /* 0: relative std-dev (reference); 1: relative std-error */
     int32_t samples_per_launch; /* waves traced per launch; 0 = automatic */
     int32_t spectral_wavelengths; /* 0: RGB (reference); 4 or 8: hero-wavelength spectral samples */
+    int32_t emitter_mis;        /* 0: reference emissive NEE (its shadow ray runs to 1e6 and the sampled
+                                   emitter blocks it, so emitters are found by BSDF sampling only);
+                                   1: at opaque vertices (no transmission, no subsurface, no BRDF debug
+                                   flags, flat scenes) the shadow ray stops short of the light sample and
+                                   BSDF-sampled emitter hits are balance-weighted against it: the same
+                                   expected image, far less noise from small lights (no reference
+                                   counterpart) */
+    int32_t reserved[3];        /* zero */
 } pt_render_params;
 
 /* Triangle soup in structure-of-arrays form: HostMesh + HostTriangle

@@ -70,6 +70,7 @@ struct SceneSlot {
     DevBuf<pt_texture> textures;
     DevBuf<uint32_t> emissiveIdx;
     DevBuf<float> emissiveCdf;
+    DevBuf<float> emitPdf; // per triangle, emitter MIS mode
     // spectral mode: host copies of the banks and their spectrum coefficients
     std::vector<pt_material> hostMats;
     std::vector<pt_texture> hostTex;
@@ -117,6 +118,7 @@ struct SceneSlot {
         textures.release();
         emissiveIdx.release();
         emissiveCdf.release();
+        emitPdf.release();
         matSpec.release();
         texSpec.release();
         specValid = false;
@@ -323,6 +325,7 @@ DevScene deviceScene(const SceneSlot* r)
     s.textures = r->textureCount ? r->textures.p : nullptr;
     s.emissiveIdx = r->emissiveIdx.p;
     s.emissiveCdf = r->emissiveCdf.p;
+    s.emitPdfArea = r->emissiveCount > 0 ? r->emitPdf.p : nullptr;
     s.matSpec = r->specValid ? r->matSpec.p : nullptr;
     s.texSpec = r->specValid ? r->texSpec.p : nullptr;
     if (r->instanceCount > 0) {
@@ -902,6 +905,12 @@ int buildEmissive(pt_renderer* r, SceneSlot& sl, uint32_t n)
     if (count > 0) {
         PT_CHECK(r, cudaMemcpyAsync(sl.emissiveIdx.p, r->eIdx.p, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         PT_CHECK(r, cudaMemcpyAsync(sl.emissiveCdf.p, r->eCdf.p, (count + 1ull) * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        if (!sl.emitPdf.ensure(n)) {
+            return fail(r, PT_ERR_OUT_OF_MEMORY, "emitter density allocation failed for %u triangles", n);
+        }
+        PT_CHECK(r, cudaMemsetAsync(sl.emitPdf.p, 0, n * sizeof(float), s));
+        launchEmitterPdf(sl.positions.p, sl.emissiveIdx.p, sl.emissiveCdf.p, count, sl.emitPdf.p, s);
+        PT_CHECK(r, cudaGetLastError());
     } else {
         PT_CHECK(r, cudaMemsetAsync(sl.emissiveCdf.p, 0, sizeof(float), s));
     }
@@ -1465,6 +1474,9 @@ int pt_set_params(pt_renderer* r, const pt_render_params* params)
 {
     if (r == nullptr || params == nullptr) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_params: null argument");
+    }
+    if (params->emitter_mis != 0 && params->emitter_mis != 1) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_params: emitter_mis must be 0 or 1 (got %d)", params->emitter_mis);
     }
     if (params->spectral_wavelengths != 0 && params->spectral_wavelengths != 4 && params->spectral_wavelengths != 8) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_params: spectral_wavelengths must be 0, 4 or 8 (got %d)",
@@ -2492,6 +2504,9 @@ int pt_backward(pt_renderer* r, const float* d_image, int channels, int spp, flo
     }
     if (r->params.spectral_wavelengths != 0) {
         return fail(r, PT_ERR_UNSUPPORTED, "pt_backward: the adjoint differentiates the RGB integrator only");
+    }
+    if (r->params.emitter_mis != 0) {
+        return fail(r, PT_ERR_UNSUPPORTED, "pt_backward: the adjoint replays the reference estimator (emitter_mis 0)");
     }
     if (r->scenes[0].instanceCount > 0 || r->sun.enabled) {
         return fail(r, PT_ERR_UNSUPPORTED, "pt_backward: instanced scenes and the distant light are not differentiated");

@@ -140,6 +140,9 @@ struct DevScene {
     const pt_texture* textures = nullptr;
     const uint32_t* emissiveIdx = nullptr;
     const float* emissiveCdf = nullptr;
+    // per original triangle: the probability density (per unit area) with which
+    // emissive NEE picks a point of it, 0 for non-emitters (emitter MIS mode)
+    const float* emitPdfArea = nullptr;
     // spectral mode: spectrum coefficients (c0, c1, c2, scale) of each
     // material's base colour [2 m] and scatter radii [2 m + 1], and of each
     // albedo texture's colours [2 t] (constant / grid colour 1), [2 t + 1] (grid colour 2)

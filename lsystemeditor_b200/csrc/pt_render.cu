@@ -1010,7 +1010,7 @@ __global__ void __launch_bounds__(256, PT_SHADE_MISS_MIN_BLOCKS) k_shade_miss(co
             const Col<NW> T = loadCol<NW>(c.paths.thr[i], c.paths.thrS, c.paths.capacity, i);
             const Col<NW> Le = sunOn ? skyCol<NW>(c, d, wv) : envCol<NW>(c, d, wv);
             const float lp = sunOn ? skyPdf(c, d) : envPdf(c.env, d);
-            const float w = misBalance(d4.w, lp);
+            const float w = misBalance(fabsf(d4.w), lp);
             L = cadd(L, cmul(T, cscl(Le, w)));
         }
         writeSample<NW>(c, i, L, wv);
@@ -1098,14 +1098,37 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
             cx.wo = scl3(d, -1.0f);
             cx.eta = eta;
             cx.debug = 0;
+            // Emitter MIS mode: at a vertex whose BSDF samples only its diffuse and
+            // specular lobes (their sample pdf is the pdf the NEE weight uses), the
+            // emissive NEE and the BSDF-sampled emitter hits share the light by the
+            // balance heuristic; elsewhere the reference's estimator is kept.
+            const bool emitterMis = c.params.emitter_mis == 1;
+            const bool misVertex = emitterMis && S.instanceCount == 0 && debugFlags == 0 &&
+                cx.w.transmit <= 0.0f && cx.w.subsurface <= 0.0f;
+            // weight of this hit's emission: the previous vertex took part (pdf > 0) and
+            // emissive NEE can pick this point (front face of a listed emitter)
+            float emitW = 1.0f;
+            if (emitterMis && depth > 0 && d4.w > 0.0f && S.emitPdfArea != nullptr && cx.m.emission != 0.0f) {
+                const float pa = S.emitPdfArea[tri];
+                if (pa > 0.0f) {
+                    const float3 ev0 = loadOrigVertex(S, tri, 0), ev1 = loadOrigVertex(S, tri, 1),
+                                 ev2 = loadOrigVertex(S, tri, 2);
+                    const float3 ng = normalize3(cross3(sub3(ev1, ev0), sub3(ev2, ev0)));
+                    const float cl = fmax2(0.0f, -dot3(ng, dn));
+                    if (cl > 0.0f) {
+                        const float lp = pa * (t * t * dot3(d, d)) / cl;
+                        emitW = misBalance(d4.w, lp);
+                    }
+                }
+            }
+            const float emission = cx.m.emission * emitW;
             // base colour at the path's wavelengths (spectral mode)
             Col<NW> rho;
             float4 scatterCoef = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if constexpr (NW == 0) {
                 rho.c = f3(cx.m.r, cx.m.g, cx.m.b);
                 // emission (PathIntegratorRandCore.h:248)
-                L = cadd(L, cmul(T, Col<0>{f3(cx.m.r * cx.m.emission, cx.m.g * cx.m.emission,
-                                               cx.m.b * cx.m.emission)}));
+                L = cadd(L, cmul(T, Col<0>{f3(cx.m.r * emission, cx.m.g * emission, cx.m.b * emission)}));
             } else {
                 float4 baseCoef;
                 matCoefs(S, mi, srcMat, tu, tv, baseCoef, scatterCoef);
@@ -1123,7 +1146,7 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                 // emission (PathIntegratorRandCore.h:248)
 #pragma unroll
                 for (int q = 0; q < NW; ++q) {
-                    Lm.v[q] = Lm.v[q] + T.v[q] * (rho.v[q] * cx.m.emission);
+                    Lm.v[q] = Lm.v[q] + T.v[q] * (rho.v[q] * emission);
                 }
                 storeCol<NW>(nullptr, c.paths.radS, cap, i, Lm, 0.0f);
             }
@@ -1198,7 +1221,12 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                             const float3 so = add3(pos, scl3(wi, kShadowBias));
                             const float3 sdn = xnormalize(wi);
                             bool occludedBySelf = false;
-                            if (!isDegenerateDir(sdn)) {
+                            // emitter MIS: the shadow ray ends just short of the light
+                            // sample, so the emitter (and coplanar neighbours) never block it
+                            float shadowTMax = 0.0f; // 0: the reference's kRayTMax
+                            if (misVertex) {
+                                shadowTMax = (sqrtf(d2) - kShadowBias) * (1.0f - 1.0e-4f);
+                            } else if (!isDegenerateDir(sdn)) {
                                 float th, tu2, tv2;
                                 occludedBySelf = intersectTriExact(so, sdn, ev0, ev1, ev2, kShadowBias, kRayTMax, th,
                                                      tu2, tv2) && th < kRayTMax;
@@ -1225,7 +1253,7 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                                     const uint32_t s = warpPush(&c.q.counts[2]);
                                     c.q.shadowPath[s] = i | 0x80000000u;
                                     c.q.shadowOrig[s] = make_float4(so.x, so.y, so.z, 0.0f);
-                                    c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, 0.0f);
+                                    c.q.shadowDir[s] = make_float4(wi.x, wi.y, wi.z, shadowTMax);
                                     pendEmis = true;
                                 }
                             }
@@ -1288,7 +1316,10 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                         const float sign = dot3(n, smp.dir) >= 0.0f ? 1.0f : -1.0f;
                         const float3 no = xadd(pos, xscl(n, __fmul_rn(sign, bias)));
                         c.paths.orig[i] = make_float4(no.x, no.y, no.z, bias);
-                        c.paths.dir[i] = make_float4(smp.dir.x, smp.dir.y, smp.dir.z, smp.pdf);
+                        // emitter MIS mode: a negative pdf marks a vertex that does not
+                        // take part (the next hit's emission keeps weight 1)
+                        c.paths.dir[i] = make_float4(smp.dir.x, smp.dir.y, smp.dir.z,
+                            (emitterMis && !misVertex) ? -smp.pdf : smp.pdf);
                         storeCol<NW>(c.paths.thr, c.paths.thrS, cap, i, T, eta);
                         cont = true;
                     }
@@ -1367,7 +1398,8 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const LaunchCtx* __restrict__
         const float4 d4 = c.q.shadowDir[k];
         const float3 dn = xnormalize(f3(d4.x, d4.y, d4.z));
         HitRec h;
-        const bool occluded = traceRay<true, Count, Inst>(sceneOf(c, e & 0x7FFFFFFFu), f3(o4.x, o4.y, o4.z), dn, kShadowBias, kRayTMax, h,
+        const float tMax = d4.w > 0.0f ? d4.w : kRayTMax; // emitter MIS rays end short of the light
+        const bool occluded = traceRay<true, Count, Inst>(sceneOf(c, e & 0x7FFFFFFFu), f3(o4.x, o4.y, o4.z), dn, kShadowBias, tMax, h,
             c.q.overflow, c.q.visits + 2, smemStack + threadIdx.x, blockDim.x);
         if (!occluded) {
             const uint32_t i = e & 0x7FFFFFFFu;

@@ -410,6 +410,32 @@ cudaError_t emissiveSelect(void* temp, size_t tempBytes, const uint8_t* flags, u
         tempBytes, s);
 }
 
+namespace {
+// Per emitter of the list: the area density with which sampleEmissive picks a
+// point of it, ((cdf[e+1] - cdf[e]) / total) / area, in the same operations.
+__global__ void k_emitter_pdf(const float* __restrict__ positions, const uint32_t* __restrict__ idx,
+    const float* __restrict__ cdf, uint32_t count, float* __restrict__ out)
+{
+    const float total = cdf[count];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const uint32_t tri = idx[e];
+        const float* p = positions + 9ull * tri;
+        const float3 v0 = f3(p[0], p[1], p[2]), v1 = f3(p[3], p[4], p[5]), v2 = f3(p[6], p[7], p[8]);
+        const float3 cr = cross3(sub3(v1, v0), sub3(v2, v0));
+        const float area = 0.5f * sqrtf(dot3(cr, cr));
+        out[tri] = (total > kMinPdf && area > kMinPdf) ? ((cdf[e + 1] - cdf[e]) / total) / area : 0.0f;
+    }
+}
+} // namespace
+
+void launchEmitterPdf(const float* positions, const uint32_t* idx, const float* cdf, uint32_t count, float* out,
+    cudaStream_t s)
+{
+    if (count > 0) {
+        k_emitter_pdf<<<gridFor(count), kBlock, 0, s>>>(positions, idx, cdf, count, out);
+    }
+}
+
 void launchEmissiveCdf(const float* weights, const uint32_t* idx, const uint32_t* dCount, float* cdf, uint32_t* out,
     cudaStream_t s)
 {

@@ -46,6 +46,10 @@ size_t emissiveSelectTempBytes(uint32_t n);
 cudaError_t emissiveSelect(void* temp, size_t tempBytes, const uint8_t* flags, uint32_t n, uint32_t* idx,
     uint32_t* dCount, cudaStream_t s);
 // cdf[0] = 0, cdf[k + 1] = sum of weights[idx[0..k]]; out[0] = count, out[1] = bits of the total.
+// Per-triangle area density of emissive NEE's point sampling (0 for non-emitters;
+// out must be zeroed first).
+void launchEmitterPdf(const float* positions, const uint32_t* idx, const float* cdf, uint32_t count, float* out,
+    cudaStream_t s);
 void launchEmissiveCdf(const float* weights, const uint32_t* idx, const uint32_t* dCount, float* cdf, uint32_t* out,
     cudaStream_t s);
 

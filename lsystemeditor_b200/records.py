@@ -10,7 +10,7 @@ record              bytes  reference struct
 MATERIAL_DTYPE        96   ``MaterialGpu``      PathTracerLib/src/MeshAccel/MeshAccelTypes.h:49-86
 TEXTURE_DTYPE         64   ``TextureDescGpu``   PathTracerLib/src/MeshAccel/MeshAccelTypes.h:22-28
 CAMERA_DTYPE          80   ``CameraGpu``        PathTracerLib/src/CameraGpu.h:5-16
-PARAMS_DTYPE          64   ``RenderParamsGpu``  PathTracerLib/src/RenderTypes.h:15-28 (44 B) + extensions
+PARAMS_DTYPE          80   ``RenderParamsGpu``  PathTracerLib/src/RenderTypes.h:15-28 (44 B) + extensions
 ==================  =====  ==============================================================
 
 ``MATERIAL_DTYPE`` uses the reference's 4 tail-padding bytes for ``sheen``
@@ -68,8 +68,10 @@ PARAMS_DTYPE = np.dtype([
     ("adaptive_criterion", "<i4"),   # 0: relative std-dev (reference), 1: relative std-error
     ("samples_per_launch", "<i4"),   # 0: automatic batch of waves per launch
     ("spectral_wavelengths", "<i4"), # 0: RGB (reference); 4 or 8 hero wavelengths
+    ("emitter_mis", "<i4"),          # 0: reference emissive NEE; 1: MIS-complete emitters at opaque vertices
+    ("reserved", "<i4", (3,)),
 ])
-assert PARAMS_DTYPE.itemsize == 64
+assert PARAMS_DTYPE.itemsize == 80
 
 REFERENCE_PARAMS_BYTES = 44
 

@@ -147,6 +147,7 @@ class Checker:
             L.orc64_render_spectral.argtypes = spec + [_dp, _u32p, _dp, _dp, _u8p, C.c_int]
             L.orc_spec_eval.restype = C.c_float
             L.orc_spec_eval.argtypes = [_fp, C.c_float]
+            L.orc_scene_set_emitter_mis.argtypes = [C.c_void_p, C.c_int]
             L.orc_scene_set_sun.argtypes = [C.c_void_p, C.c_int, _fp, C.c_float, _fp, C.c_float, C.c_float, _fp, _fp]
             L.orc_hero_lambda.restype = C.c_float
             L.orc_hero_lambda.argtypes = [C.c_uint, C.c_int, C.c_int]
@@ -377,6 +378,12 @@ class CheckerScene:
                                         _ptr(state["converged"], _u8p), int(threads))
         state["tape_errors"] = int(err)
         return state
+
+    def set_emitter_mis(self, on: bool = True):
+        """The emitter MIS estimator (the product's emitter_mis = 1) for this scene's renders."""
+        assert self.chk.kind == "oracle"
+        self.chk.lib.orc_scene_set_emitter_mis(self.h, 1 if on else 0)
+        return self
 
     def set_sun(self, direction=None, half_angle=0.0, radiance=(0.0, 0.0, 0.0), temperature_k=0.0, luminance=1.0,
                 resp=None, coef=None):

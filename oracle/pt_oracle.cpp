@@ -454,6 +454,13 @@ int orc64_render_spectral(void* scene, void* env, const void* cam, const void* p
 // temperature scaled to Rec. 709 luminance `luminance` through the response
 // table resp (401 x 3, 1 nm from 380 nm); spectral coefficients of the RGB
 // radiance `coef` (4 floats) for temperature <= 0.  enabled = 0 removes it.
+// Emitter MIS mode of the renders of this scene (extension; the product's
+// pt_render_params.emitter_mis = 1): 0 = the reference estimator.
+void orc_scene_set_emitter_mis(void* h, int on)
+{
+    setEmitterMis(*static_cast<Scene*>(h), on != 0);
+}
+
 void orc_scene_set_sun(void* h, int enabled, const float* dir, float halfAngle, const float* rgb, float temperature,
     float luminance, const float* resp, const float* coef)
 {

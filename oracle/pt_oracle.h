@@ -150,6 +150,12 @@ struct Scene {
     uint32_t root = 0;
     std::vector<uint32_t> emissiveIdx;
     std::vector<float> emissiveCdf;
+    // Emitter MIS mode (extension; no reference counterpart): at opaque
+    // vertices emissive NEE's shadow ray stops short of the light sample and
+    // BSDF-sampled emitter hits are balance-weighted against it.  emitIndex[t]
+    // is triangle t's position in the emissive list (-1 if none).
+    bool emitterMis = false;
+    std::vector<int> emitIndex;
 };
 
 struct Env {
@@ -1294,9 +1300,9 @@ template <class R> inline V3<R> skyEval(const Scene& s, const Env* e, const Para
     return L;
 }
 
-template <class R> inline bool occluded(const Scene& s, V3<R> origin, V3<R> wi)
+template <class R> inline bool occluded(const Scene& s, V3<R> origin, V3<R> wi, R tMax = R(1.0e6f))
 {
-    return traceRay(s, origin, wi, R(1.0e-4f), R(1.0e6f)).hit;
+    return traceRay(s, origin, wi, R(1.0e-4f), tMax).hit;
 }
 
 inline const MaterialRec& fetchMaterial(const Scene& s, uint32_t tri, MaterialRec& fallback)
@@ -1532,7 +1538,8 @@ inline V3<R> neeEnvironment(const Scene& s, const Env* e, const ParamsRec* p, V3
 }
 
 template <class R>
-inline V3<R> neeEmissive(const Scene& s, V3<R> pos, V3<R> n, V3<R> wo, const Mat<R>& m, R eta, Rng& rng)
+inline V3<R> neeEmissive(const Scene& s, V3<R> pos, V3<R> n, V3<R> wo, const Mat<R>& m, R eta, Rng& rng,
+    bool misVertex = false)
 {
     if (s.emissiveIdx.empty()) {
         return mk(R(0), R(0), R(0));
@@ -1556,7 +1563,10 @@ inline V3<R> neeEmissive(const Scene& s, V3<R> pos, V3<R> n, V3<R> wo, const Mat
     if (ct <= R(0) || cl <= R(0)) {
         return mk(R(0), R(0), R(0));
     }
-    if (occluded(s, add(pos, scl(wi, R(1.0e-4f))), wi)) {
+    // Q12: the reference's shadow ray runs to 1e6 and meets the sampled emitter;
+    // in emitter MIS mode it ends just short of the light sample
+    const R tMax = misVertex ? (std::sqrt(d2) - R(1.0e-4f)) * (R(1) - R(1.0e-4f)) : R(1.0e6f);
+    if (occluded(s, add(pos, scl(wi, R(1.0e-4f))), wi, tMax)) {
         return mk(R(0), R(0), R(0));
     }
     const R lp = ap * d2 / cl;
@@ -1600,6 +1610,55 @@ inline V3<R> subsurfaceTierB(V3<R> tp, const Mat<R>& m, V3<R> n, const Sample<R>
     return tp;
 }
 
+// Emitter MIS mode: the vertex samples only its diffuse and specular lobes
+// (whose sample pdf is the pdf the NEE weight uses).
+template <class R> inline bool emitterMisVertex(const Scene& s, const Ctx<R>& c)
+{
+    if (!s.emitterMis || c.debug != 0) {
+        return false;
+    }
+    const Lobes<R> w = lobes(c);
+    return w.transmit <= R(0) && w.subsurface <= R(0);
+}
+
+// Balance weight of the emission of an emitter hit at distance t along the
+// BSDF-sampled direction d (pdf bsdfPdfPrev) against emissive NEE's density
+// of picking that point: pick probability / area * t^2 |d|^2 / cos at the light.
+template <class R> inline R emitterHitWeight(const Scene& s, uint32_t tri, V3<R> d, R t, R bsdfPdfPrev)
+{
+    using std::sqrt;
+    if (tri >= s.emitIndex.size() || s.emitIndex[tri] < 0) {
+        return R(1);
+    }
+    const size_t e = static_cast<size_t>(s.emitIndex[tri]);
+    const uint32_t E = static_cast<uint32_t>(s.emissiveIdx.size());
+    const R total = R(s.emissiveCdf[E]);
+    const TriRec& tr = s.tris[tri];
+    const V3<R> cr = cross(sub(vtx<R>(tr, 1), vtx<R>(tr, 0)), sub(vtx<R>(tr, 2), vtx<R>(tr, 0)));
+    const R area = R(0.5f) * len(cr);
+    if (total <= Kc<R>::minPdf || area <= Kc<R>::minPdf) {
+        return R(1);
+    }
+    const R pa = ((R(s.emissiveCdf[e + 1]) - R(s.emissiveCdf[e])) / total) / area;
+    const R cl = mx(R(0), -dot(nrm(cr), nrm(d)));
+    if (pa <= R(0) || cl <= R(0)) {
+        return R(1);
+    }
+    const R lp = pa * (t * t * dot(d, d)) / cl;
+    return misBalance(bsdfPdfPrev, lp);
+}
+
+inline void setEmitterMis(Scene& s, bool on)
+{
+    s.emitterMis = on;
+    s.emitIndex.assign(s.tris.size(), -1);
+    for (size_t e = 0; e < s.emissiveIdx.size(); ++e) {
+        if (s.emissiveIdx[e] < s.tris.size()) {
+            s.emitIndex[s.emissiveIdx[e]] = static_cast<int>(e);
+        }
+    }
+}
+
 template <class R>
 inline V3<R> tracePath(const Scene& s, const Env* e, const ParamsRec* p, V3<R> ro, V3<R> rd, Rng& rng)
 {
@@ -1626,15 +1685,20 @@ inline V3<R> tracePath(const Scene& s, const Env* e, const ParamsRec* p, V3<R> r
     Hit<R> h = first;
     R eta = R(1);
     MaterialRec fb = defaultFetchMaterial();
+    R prevPdf = R(0);
+    bool prevMis = false;
     for (int depth = 0; depth < maxDepth; ++depth) {
         const V3<R> pos = add(o, scl(d, h.t));
         const V3<R> n = h.normal;
         const V3<R> wo = scl(d, R(-1));
         const Mat<R> m = resolve<R>(fetchMaterial(s, h.tri, fb), h.uv, s.textures);
-        L = add(L, mul(T, mk(m.r * m.emission, m.g * m.emission, m.b * m.emission)));
-        L = add(L, mul(T, neeEnvironment(s, e, p, pos, n, wo, m, eta, rng)));
-        L = add(L, mul(T, neeEmissive(s, pos, n, wo, m, eta, rng)));
         const Ctx<R> c{n, wo, m, eta, debug};
+        const bool misV = emitterMisVertex(s, c);
+        const R ew = (prevMis && depth > 0 && m.emission != R(0)) ? emitterHitWeight(s, h.tri, d, h.t, prevPdf) : R(1);
+        const R em = m.emission * ew;
+        L = add(L, mul(T, mk(m.r * em, m.g * em, m.b * em)));
+        L = add(L, mul(T, neeEnvironment(s, e, p, pos, n, wo, m, eta, rng)));
+        L = add(L, mul(T, neeEmissive(s, pos, n, wo, m, eta, rng, misV)));
         const R u1 = R(rng.next());
         const R u2 = R(rng.next());
         const Sample<R> smp = bsdfSample(c, u1, u2);
@@ -1659,6 +1723,8 @@ inline V3<R> tracePath(const Scene& s, const Env* e, const ParamsRec* p, V3<R> r
             T = scl(T, R(1) / surv);
         }
         eta = smp.nextEta;
+        prevPdf = smp.pdf;
+        prevMis = misV;
         const R bias = mx(R(1.0e-4f), R(1.0e-3f) * h.t);
         const R sign = dot(n, smp.dir) >= R(0) ? R(1) : R(-1);
         o = add(pos, scl(n, sign * bias));

@@ -36,10 +36,10 @@ def test_library_builds_and_exports_every_declared_symbol():
 def test_record_layouts_match_header():
     text = open(HEADER).read()
     assert MATERIAL_DTYPE.itemsize == 96 and TEXTURE_DTYPE.itemsize == 64 and CAMERA_DTYPE.itemsize == 80
-    assert PARAMS_DTYPE.itemsize == 64
+    assert PARAMS_DTYPE.itemsize == 80
     # field order of the params record follows the header
     body = re.search(r"typedef struct pt_render_params \{(.*?)\} pt_render_params;", text, re.S).group(1)
-    names = re.findall(r"(\w+)(?:\s*,\s*(\w+))?(?:\s*,\s*(\w+))?;", re.sub(r"/\*.*?\*/", "", body, flags=re.S))
+    names = re.findall(r"(\w+)(?:\s*,\s*(\w+))?(?:\s*,\s*(\w+))?;", re.sub(r"\[\d+\]", "", re.sub(r"/\*.*?\*/", "", body, flags=re.S)))
     flat = [n for tup in names for n in tup if n]
     assert list(PARAMS_DTYPE.names) == flat
     assert ctypes.sizeof(PtStats) == 72 and ctypes.sizeof(PtProfile) == 15 * 8
