@@ -69,6 +69,13 @@ def parse_args():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the leg that times the reference's own CUDA kernels on this GPU")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: keep the default scheduling knobs")
+    ap.add_argument("--estimator", choices=["mis", "reference"], default="mis",
+                    help="batch workload: the emitter MIS estimator (reaches the relative-MSE target) or the "
+                         "reference's estimator (emitters found by BSDF sampling only)")
+    ap.add_argument("--rel-err", type=float, default=0.025,
+                    help="batch workload: per-pixel relative standard error at which a pixel stops")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="batch workload: skip the FP64-oracle check of the batch's relative MSE")
     ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],
                     help="hero wavelengths per path: auto = the workload's own (plain-small 4, plain-large 8, "
                          "batch and adjoint RGB), 0 = RGB like the reference's integrator")
@@ -511,6 +518,61 @@ def run_b200(args):
     return 0
 
 
+def batch_accuracy_scenes(tubes, count: int = 4, seed: int = 9):
+    """Scenes of the batch whose images are checked: the smallest, the largest
+    and seeded others."""
+    order = np.argsort([t.triangle_count for t in tubes])
+    pick = {int(order[0]), int(order[-1])}
+    rng = np.random.default_rng(seed)
+    for k in rng.permutation(len(tubes)):
+        if len(pick) >= min(count, len(tubes)):
+            break
+        pick.add(int(k))
+    return sorted(pick)
+
+
+def batch_accuracy(tubes, cams, sizes, params, images, pixels_per_scene: int = 128, ref_spp: int = 4096,
+                   seed: int = 11):
+    """Relative MSE of the batch's images against the FP64 oracle.
+
+    Per checked scene, pixels are drawn uniformly over the image (independently
+    of the image under test); the FP64 oracle renders them with ref_spp samples
+    of its own random numbers (PCG32) and the same estimator.  Pixels whose
+    reference luminance is below 1e-4 (background) are dropped.  The relative
+    MSE is of the luminance, corrected for the reference's own variance:
+    mean(((x - r)^2 - var(r)) / r^2)."""
+    from oracle.bindings import Checker
+    chk = Checker("oracle")
+    threads = chk.max_threads()
+    rng = np.random.default_rng(seed)
+    lum = np.array([0.2126, 0.7152, 0.0722])
+    terms, per_scene = [], {}
+    t0 = time.perf_counter()
+    for k, img in images.items():
+        w, h = sizes[k]
+        pix = np.sort(rng.choice(w * h, size=min(pixels_per_scene, w * h), replace=False)).astype(np.int32)
+        sc = chk.scene(tubes[k].host_mesh())
+        if int(params["emitter_mis"]) == 1:
+            sc.set_emitter_mis(True)
+        p = params.copy()
+        p["min_samples"] = p["max_samples_per_pixel"] = ref_spp
+        p["adaptive_criterion"] = 0
+        st = sc.render(cams[k], p, w, h, ref_spp, seed_base=900_001, pixels=pix, threads=threads, fp64=True)
+        r = st["lum_mean"][pix]
+        var_r = st["m2"][pix] / float(ref_spp) / float(ref_spp)
+        x = img[..., :3].reshape(-1, 3).astype(np.float64)[pix] @ lum
+        keep = r > 1e-4
+        t = ((x - r) ** 2 - var_r)[keep] / (r[keep] ** 2)
+        terms.append(t)
+        per_scene[int(k)] = {"pixels": int(keep.sum()), "relmse": float(t.mean()) if keep.any() else None,
+                             "triangles": int(tubes[k].triangle_count)}
+    allt = np.concatenate(terms) if terms else np.zeros(0)
+    return {"relmse": float(allt.mean()) if len(allt) else None, "pixels": int(len(allt)),
+            "scenes": per_scene, "reference": f"FP64 oracle, {ref_spp} samples per pixel, independent random "
+            f"numbers, {threads} host threads", "measure": "luminance relative MSE, reference variance "
+            "subtracted", "oracle_s": round(time.perf_counter() - t0, 1)}
+
+
 def run_batch(args):
     """The batching workload: 64 scenes built on the device and rendered in one
     pt_render (value), against the same scenes rendered one per pt_render
@@ -543,7 +605,8 @@ def run_batch(args):
             dist.barrier()
 
     t0 = time.perf_counter()
-    all_tubes, all_cams, all_sizes, params = batch_scenes()
+    all_tubes, all_cams, all_sizes, params = batch_scenes(rel_err=args.rel_err)
+    params["emitter_mis"] = 1 if args.estimator == "mis" else 0
     gen_s = time.perf_counter() - t0
     # scenes split over the ranks by estimated cost; each rank renders its own
     # scenes in one batch and rank 0 gathers every image once (strong scaling)
@@ -648,6 +711,10 @@ def run_batch(args):
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
 
     # the same scenes one per render (the plain drop-in), device-built likewise
+    # images of the scenes whose accuracy is checked against the FP64 oracle
+    acc_scenes = batch_accuracy_scenes(all_tubes) if (world == 1 and not args.no_accuracy) else []
+    acc_images = {k: pt.batch_readback(k)[0] for k in acc_scenes}
+
     plain_ms, plain_samples, plain_build_ms = 0.0, 0, 0.0
     for k in range(n):
         w, h = sizes[k]
@@ -687,6 +754,23 @@ def run_batch(args):
     e_ms = reduce(float(e0.elapsed_time(e1)), "max")
     e_value = reduce(float(e_samples), "sum") / (e_ms / 1e3) / 1e6
 
+    accuracy = None
+    if acc_scenes:
+        try:
+            accuracy = batch_accuracy(all_tubes, all_cams, all_sizes, params, acc_images)
+        except Exception as e:  # the check must not take the GPU number down with it
+            accuracy = {"unavailable": f"{type(e).__name__}: {e}"}
+        batched_s = build_s + total_ms / args.steps / 1e3
+        plain_s = plain_build_ms / 1e3 + plain_ms / 1e3
+        accuracy["time_to_target"] = {
+            "batched_s": batched_s, "plain_s": plain_s,
+            "note": "wall time of one pass over all scenes to the per-pixel stop criterion, device builds "
+                    "(loft + BVH) included; batched and plain images are identical, so both reach the same "
+                    "relative MSE"}
+        if "relmse" in accuracy:
+            accuracy["target_met"] = bool(accuracy["relmse"] <= 1e-3)
+            accuracy["batched_faster"] = bool(batched_s < plain_s)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -715,7 +799,11 @@ def run_batch(args):
                    "plain_ms_per_render": plain_ms, "plain_msamples_per_s": plain_samples / plain_ms / 1e3,
                    "plain_build_ms": plain_build_ms,
                    "stage_ms_per_step": {k[3:]: round(v, 2) for k, v in prof.items() if k.startswith("ms_")},
-                   "images": "every scene identical in the batched and the plain form"},
+                   "images": "every scene identical in the batched and the plain form",
+                   "estimator": ("emitter MIS (emitter_mis = 1: short emissive shadow rays, balance-weighted "
+                                 "BSDF emitter hits at opaque vertices; the reference estimator's expectation)"
+                                 if args.estimator == "mis" else "the reference's (emitters by BSDF sampling only)"),
+                   "accuracy": accuracy},
         "e2e": {"value": e_value, "unit": METRIC, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "steps": 1},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",

@@ -82,3 +82,37 @@ def test_batch_scene_accuracy_vs_fp64_oracle(oracle):
     print(f"  bias without the 2% largest errors: GPU {tg:+.4f}, FP64 oracle at 512 spp {tc:+.4f}")
     assert 1.0 / 1.5 <= mg / mc <= 1.5
     assert abs(tg - tc) <= 0.05
+
+
+def test_batch_scene_reaches_the_relative_mse_target_with_emitter_mis(oracle):
+    """With the emitter MIS estimator (emitter_mis = 1) and the bench's stop
+    criterion (relative standard error 0.025, 16-512 spp) a batch scene reaches
+    the workload's relative MSE target of 1e-3 against the FP64 oracle's
+    4096-sample estimate of the same integral (independent random numbers;
+    luminance, the reference's variance subtracted), on a seeded sample of the
+    pixels (background pixels, whose reference is below 1e-4, dropped)."""
+    tubes, cams, sizes, params = batch_scenes(count=4, rel_err=0.025)
+    params["emitter_mis"] = 1
+    k = int(np.argmin([t.triangle_count for t in tubes]))
+    w, h = sizes[k]
+    mesh = tubes[k].host_mesh()
+    with PathTracer(0) as t:
+        t.configure(w, h, mesh)
+        t.set_camera(cams[k])
+        t.set_params(params)
+        t.render(0)
+        img, counts, _ = t.readback()
+    lum = img[..., :3].reshape(-1, 3).astype(np.float64) @ LUM
+    rng = np.random.default_rng(13)
+    pix = np.sort(rng.choice(w * h, size=1500, replace=False)).astype(np.int32)
+    sc = oracle.scene(mesh).set_emitter_mis(True)
+    st = sc.render(cams[k], _fixed(params, 4096), w, h, 4096, seed_base=7919, pixels=pix, fp64=True)
+    r = st["lum_mean"][pix]
+    var_r = st["m2"][pix] / 4096.0 / 4096.0
+    keep = r > 1e-4
+    assert keep.sum() > 100
+    rel = ((lum[pix] - r) ** 2 - var_r)[keep] / r[keep] ** 2
+    relmse = float(rel.mean())
+    print(f"scene {k}: GPU mean spp {counts.reshape(-1)[pix][keep].mean():.0f}, relative MSE {relmse:.3e} over "
+          f"{keep.sum()} pixels")
+    assert relmse <= 1e-3
