@@ -86,6 +86,21 @@ def build_ref_gpu() -> Optional[str]:
     return REF_GPU_SO
 
 
+WRAPPER_BIN = os.path.join(HERE, "_ref", "wrapper_check")
+
+
+def build_wrapper() -> Optional[str]:
+    """Compiles the C++ PathTracer-shaped wrapper (tests/cpp) against the reference's headers."""
+    if not os.path.isdir(REF_ROOT):
+        return WRAPPER_BIN if os.path.exists(WRAPPER_BIN) else None
+    root = os.path.dirname(HERE)
+    src = [os.path.join(root, "tests", "cpp", f) for f in ("wrapper_check.cpp", "PathTracerB200.h")] + \
+        [os.path.join(root, "include", "pt_b200.h")]
+    if not os.path.exists(WRAPPER_BIN) or any(os.path.getmtime(s) > os.path.getmtime(WRAPPER_BIN) for s in src):
+        subprocess.run(["make", "-C", HERE, "wrapper", f"REF_ROOT={REF_ROOT}"], check=True, stdout=subprocess.DEVNULL)
+    return WRAPPER_BIN
+
+
 class Checker:
     def __init__(self, kind: str = "oracle"):
         if kind == "oracle":
