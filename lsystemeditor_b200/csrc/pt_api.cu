@@ -1870,7 +1870,9 @@ int pt_trace_rays(pt_renderer* r, int n, const float* origins, const float* dirs
     // one staging allocation: inputs 8 floats, outputs 1 byte + 7 words per ray
     const size_t bytes = N * (8 * sizeof(float) + 7 * sizeof(float) + 16);
     void* buf = nullptr;
-    PT_CHECK(r, cudaMallocAsync(&buf, bytes, r->stream));
+    PT_CHECK(r, cudaMallocAsync(&buf, bytes + 16, r->stream));
+    // traversal stack overflows of this query (pt_stats.stack_overflows)
+    unsigned int* dOverflow = reinterpret_cast<unsigned int*>(static_cast<char*>(buf) + ((bytes + 15) & ~size_t(15)));
     float* dO = static_cast<float*>(buf);
     float* dD = dO + 3 * N;
     float* dTmin = dD + 3 * N;
@@ -1882,14 +1884,17 @@ int pt_trace_rays(pt_renderer* r, int n, const float* origins, const float* dirs
     uint8_t* dHit = reinterpret_cast<uint8_t*>(dUv + 2 * N);
     cudaStream_t s = r->stream;
     int rc = PT_OK;
-    cudaError_t e = cudaMemcpyAsync(dO, origins, 3 * N * sizeof(float), cudaMemcpyHostToDevice, s);
+    unsigned int overflow = 0;
+    cudaError_t e = cudaMemsetAsync(dOverflow, 0, sizeof(unsigned int), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dO, origins, 3 * N * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dD, dirs, 3 * N * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dTmin, tmin, N * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dTmax, tmax, N * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-        launchTraceRays(deviceScene(&r->scenes[0]), n, dO, dD, dTmin, dTmax, dHit, dT, dTri, dN, dUv, s);
+        launchTraceRays(deviceScene(&r->scenes[0]), n, dO, dD, dTmin, dTmax, dHit, dT, dTri, dN, dUv, s, dOverflow);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, dOverflow, sizeof(overflow), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hit, dHit, N, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && t) e = cudaMemcpyAsync(t, dT, N * sizeof(float), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && tri) e = cudaMemcpyAsync(tri, dTri, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
@@ -1902,6 +1907,8 @@ int pt_trace_rays(pt_renderer* r, int n, const float* origins, const float* dirs
     }
     if (e != cudaSuccess) {
         rc = cudaFail(r, e, "pt_trace_rays");
+    } else {
+        r->stats.stack_overflows += static_cast<int32_t>(overflow);
     }
     return rc;
 }

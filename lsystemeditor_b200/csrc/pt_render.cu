@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
                 bool hit = false;
                 h.tri = 0xFFFFFFFFu;
                 if (S->nodeCount != 0) {
-                    hit = traceQ1(*S, o, dn, tMin, kRayTMax, false, h);
+                    hit = traceQ1(*S, o, dn, tMin, kRayTMax, false, h, c.q.overflow);
                 }
                 if (hit) {
                     c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
@@ -1575,13 +1575,13 @@ __global__ void k_reset(const LaunchCtx* __restrict__ cp, int pixels)
 }
 
 __global__ void __launch_bounds__(256) k_trace_rays(DevScene S, int n, const float* o, const float* d, const float* tmin,
-    const float* tmax, uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv)
+    const float* tmax, uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, unsigned int* overflow)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float3 ro = f3(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
         const float3 dn = xnormalize(f3(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
         HitRec h;
-        const bool ok = traceRay<false, false, true>(S, ro, dn, tmin[i], tmax[i], h);
+        const bool ok = traceRay<false, false, true>(S, ro, dn, tmin[i], tmax[i], h, overflow);
         hit[i] = ok ? 1 : 0;
         float3 nn = f3(0.0f, 0.0f, 0.0f);
         float tu = 0.0f, tv = 0.0f;
@@ -1785,9 +1785,9 @@ void launchSceneJobs(const LaunchCtx* c, int sceneCount, int waves, cudaStream_t
 }
 void launchResetAccum(const LaunchCtx* c, int pixels, cudaStream_t s) { k_reset<<<gridFor(pixels), 256, 0, s>>>(c, pixels); }
 void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,
-    uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s)
+    uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s, unsigned int* overflow)
 {
-    k_trace_rays<<<gridFor(n), 256, 0, s>>>(S, n, o, d, tmin, tmax, hit, t, tri, normal, uv);
+    k_trace_rays<<<gridFor(n), 256, 0, s>>>(S, n, o, d, tmin, tmax, hit, t, tri, normal, uv, overflow);
 }
 void launchRngTape(int width, int height, int firstWave, int waves, int stride, int seedOffset, float* out,
     cudaStream_t s)

@@ -177,7 +177,7 @@ cudaError_t launchCompactStable(const int* in, int* out, int* outCount, int n, c
 void launchSceneJobs(const LaunchCtx* d, int sceneCount, int waves, cudaStream_t s);
 void launchResetAccum(const LaunchCtx* d, int pixels, cudaStream_t s);
 void launchTraceRays(const DevScene& S, int n, const float* o, const float* d, const float* tmin, const float* tmax,
-    uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s);
+    uint8_t* hit, float* t, uint32_t* tri, float* normal, float* uv, cudaStream_t s, unsigned int* overflow = nullptr);
 // Resident blocks per SM of the stage kernels (occupancy calculator).
 void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks);
 void launchRngTape(int width, int height, int firstWave, int waves, int stride, int seedOffset, float* out,

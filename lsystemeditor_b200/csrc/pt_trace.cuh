@@ -205,7 +205,7 @@ __device__ __forceinline__ uint32_t intersectChildren(const CwNode* __restrict__
 
 // Slow path for quirk Q1 (degenerate direction components); see the file comment.
 static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 dn, float tMin, float tMax, bool anyHit,
-    HitRec& out)
+    HitRec& out, unsigned int* overflowCounter)
 {
     out.tri = 0xFFFFFFFFu;
     out.inst = 0xFFFFFFFFu;
@@ -215,6 +215,7 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
     const bool useX = fabsf(dn.x) > 1.0e-8f, useY = fabsf(dn.y) > 1.0e-8f, useZ = fabsf(dn.z) > 1.0e-8f;
     uint32_t stack[kTraversalStack * 2];
     int sp = 0;
+    bool dropped = false;
     stack[sp++] = 0;
     float closest = tMax;
     uint32_t best = 0xFFFFFFFFu;
@@ -248,8 +249,12 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
                 pass = lo <= oo[a] && oo[a] <= hi;
             }
             if (inner) {
-                if (pass && sp < kTraversalStack * 2) {
-                    stack[sp++] = w1.x + rank;
+                if (pass) {
+                    if (sp < kTraversalStack * 2) {
+                        stack[sp++] = w1.x + rank;
+                    } else {
+                        dropped = true; // a full stack drops the child, like the reference's 64-entry stack
+                    }
                 }
                 ++rank;
                 continue;
@@ -292,6 +297,9 @@ static __device__ __noinline__ bool traceQ1(const DevScene& S, float3 o, float3 
                 }
             }
         }
+    }
+    if (dropped && overflowCounter != nullptr) {
+        atomicAdd(overflowCounter, 1u);
     }
     if (best != 0xFFFFFFFFu && closest < tMax) {
         out.t = closest;
@@ -505,7 +513,7 @@ __device__ __forceinline__ bool traceRay(const DevScene& S, float3 o, float3 dn,
         return false;
     }
     if (isDegenerateDir(dn)) {
-        return traceQ1(S, o, dn, tMin, tMax, AnyHit, out);
+        return traceQ1(S, o, dn, tMin, tMax, AnyHit, out, overflowCounter);
     }
     const float3 idir = f3(__frcp_rn(dn.x), __frcp_rn(dn.y), __frcp_rn(dn.z));
     const uint32_t oct = (dn.x < 0.0f ? 4u : 0u) | (dn.y < 0.0f ? 2u : 0u) | (dn.z < 0.0f ? 1u : 0u);
