@@ -106,7 +106,8 @@ typedef struct pt_render_params {
     /* --- extensions --- */
     int32_t seed_mode;          /* 0: reference seed (Sampling/RandCore.h:7-12); 1: hash(x, y, seed_value) */
     uint32_t seed_value;
-    int32_t adaptive_criterion; /* 0: relative std-dev (reference); 1: relative std-error */
+    int32_t adaptive_criterion; /* 0: relative std-dev (reference); 1: relative std-error; 2: as 1, and a
+                                   pixel all of whose samples are black stops after max(min_samples, 64) */
     int32_t samples_per_launch; /* waves traced per launch; 0 = automatic */
     int32_t spectral_wavelengths; /* 0: RGB (reference); 4 or 8: hero-wavelength spectral samples */
     int32_t emitter_mis;        /* 0: reference emissive NEE (its shadow ray runs to 1e6 and the sampled

@@ -500,6 +500,32 @@ __device__ __forceinline__ float pdfSpecular(const Ctx& c, float3 wi)
     return c.w.specular * (ggxD(cH, a) * cH) / fmax2(4.0f * cHo, 1.0e-8f);
 }
 
+// The reference's transmit lobe is a pair of narrow cones (cosine > 0.999
+// with the mirror and with the transmitted direction; evalTransmit and
+// pdfTransmit) that its sampler produces as exact directions.  The emitter MIS
+// mode leaves directions in those cones to BSDF sampling alone.
+__device__ __forceinline__ bool inTransmitCones(const Ctx& c, float3 wi)
+{
+    if (c.w.transmit == 0.0f) {
+        return false;
+    }
+    const float cOs = dot3(c.n, c.wo);
+    if (!transmitValid(c, cOs)) {
+        return false;
+    }
+    if (dot3(wi, mirrorOut(c.wo, c.n)) > 0.999f) {
+        return true;
+    }
+    float3 td;
+    float ne = 1.0f;
+    if (clamp01(c.m.thin) > 0.5f) {
+        td = normalize3(scl3(c.wo, -1.0f));
+    } else if (!refractDir(c, td, ne)) {
+        return false;
+    }
+    return dot3(wi, td) > 0.999f;
+}
+
 __device__ __forceinline__ float pdfTransmit(const Ctx& c, float3 wi)
 {
     const float cOs = dot3(c.n, c.wo);
@@ -736,6 +762,16 @@ static __device__ __noinline__ BsdfSample bsdfSample(const Ctx& c, float u1, flo
 __device__ __forceinline__ bool skipsEnvNee(const Mat& m)
 {
     return fmax2(0.0f, fmin2(1.0f, m.transmission)) > 0.99f && fmax2(0.0f, fmin2(1.0f, m.metallic)) < 0.01f;
+}
+
+// Emitter MIS mode: a vertex takes part when its BSDF samples the upper
+// hemisphere with the mixture pdf the NEE weight uses and its throughput is
+// f cos / pdf: no subsurface lobe, not the pure transmit lobe (whose throughput
+// drops the cosine), outside any medium.  Directions in the transmit cones and
+// below the surface stay with BSDF sampling alone.
+__device__ __forceinline__ bool emitterMisVertex(const Ctx& c)
+{
+    return c.w.subsurface <= 0.0f && !skipsEnvNee(c.m) && c.eta == 1.0f;
 }
 
 // Throughput rule of the sampled lobe (BrdfDispatch.h:42-76): the new

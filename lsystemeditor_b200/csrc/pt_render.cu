@@ -1098,13 +1098,12 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
             cx.wo = scl3(d, -1.0f);
             cx.eta = eta;
             cx.debug = 0;
-            // Emitter MIS mode: at a vertex whose BSDF samples only its diffuse and
-            // specular lobes (their sample pdf is the pdf the NEE weight uses), the
+            // Emitter MIS mode: at a vertex that takes part (emitterMisVertex), the
             // emissive NEE and the BSDF-sampled emitter hits share the light by the
-            // balance heuristic; elsewhere the reference's estimator is kept.
+            // balance heuristic, outside the transmit cones and above the surface;
+            // elsewhere the reference's estimator is kept.
             const bool emitterMis = c.params.emitter_mis == 1;
-            const bool misVertex = emitterMis && S.instanceCount == 0 && debugFlags == 0 &&
-                cx.w.transmit <= 0.0f && cx.w.subsurface <= 0.0f;
+            const bool misVertex = emitterMis && S.instanceCount == 0 && debugFlags == 0 && emitterMisVertex(cx);
             // weight of this hit's emission: the previous vertex took part (pdf > 0) and
             // emissive NEE can pick this point (front face of a listed emitter)
             float emitW = 1.0f;
@@ -1224,7 +1223,7 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                             // emitter MIS: the shadow ray ends just short of the light
                             // sample, so the emitter (and coplanar neighbours) never block it
                             float shadowTMax = 0.0f; // 0: the reference's kRayTMax
-                            if (misVertex) {
+                            if (misVertex && !inTransmitCones(cx, wi)) {
                                 shadowTMax = (sqrtf(d2) - kShadowBias) * (1.0f - 1.0e-4f);
                             } else if (!isDegenerateDir(sdn)) {
                                 float th, tu2, tv2;
@@ -1318,8 +1317,10 @@ __global__ void __launch_bounds__(256, NW == 0 ? PT_SHADE_MIN_BLOCKS : PT_SHADE_
                         c.paths.orig[i] = make_float4(no.x, no.y, no.z, bias);
                         // emitter MIS mode: a negative pdf marks a vertex that does not
                         // take part (the next hit's emission keeps weight 1)
+                        const bool misSample = misVertex && !smp.transmitted && !smp.sss &&
+                            dot3(n, smp.dir) > 0.0f && !inTransmitCones(cx, smp.dir);
                         c.paths.dir[i] = make_float4(smp.dir.x, smp.dir.y, smp.dir.z,
-                            (emitterMis && !misVertex) ? -smp.pdf : smp.pdf);
+                            (emitterMis && !misSample) ? -smp.pdf : smp.pdf);
                         storeCol<NW>(c.paths.thr, c.paths.thrS, cap, i, T, eta);
                         cont = true;
                     }
@@ -1443,7 +1444,10 @@ __global__ void __launch_bounds__(256) k_accumulate(const LaunchCtx* __restrict_
     const int maxSpp = c.params.max_samples_per_pixel;
     const int minSpp = c.params.min_samples;
     const float thr = c.params.relative_error_threshold;
-    const bool stdErr = c.params.adaptive_criterion == 1;
+    const bool stdErr = c.params.adaptive_criterion == 1 || c.params.adaptive_criterion == 2;
+    // criterion 2: a pixel all of whose samples are black stops after max(min spp, 64) samples
+    const bool blackStops = c.params.adaptive_criterion == 2;
+    const uint32_t blackSpp = static_cast<uint32_t>(minSpp > 64 ? minSpp : 64);
     for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < activeCount; li += gridDim.x * blockDim.x) {
         const int p = active[li];
         uint8_t conv = c.acc.converged[p];
@@ -1487,6 +1491,8 @@ __global__ void __launch_bounds__(256) k_accumulate(const LaunchCtx* __restrict_
                 if (rel < thr) {
                     conv = 1;
                 }
+            } else if (blackStops && n >= blackSpp && mean == 0.0f && m2 == 0.0f) {
+                conv = 1;
             }
         }
         c.acc.counts[p] = n;

@@ -65,7 +65,7 @@ PARAMS_DTYPE = np.dtype([
     # --- extensions (zero = reference behaviour) ---
     ("seed_mode", "<i4"),            # 0: reference seed formula, 1: hash(x, y, seed_value)
     ("seed_value", "<u4"),
-    ("adaptive_criterion", "<i4"),   # 0: relative std-dev (reference), 1: relative std-error
+    ("adaptive_criterion", "<i4"),   # 0: relative std-dev (reference), 1: relative std-error, 2: as 1 + black stops
     ("samples_per_launch", "<i4"),   # 0: automatic batch of waves per launch
     ("spectral_wavelengths", "<i4"), # 0: RGB (reference); 4 or 8 hero wavelengths
     ("emitter_mis", "<i4"),          # 0: reference emissive NEE; 1: MIS-complete emitters at opaque vertices

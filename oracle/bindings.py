@@ -163,6 +163,7 @@ class Checker:
             L.orc_spec_eval.restype = C.c_float
             L.orc_spec_eval.argtypes = [_fp, C.c_float]
             L.orc_scene_set_emitter_mis.argtypes = [C.c_void_p, C.c_int]
+            L.orc_scene_set_adaptive_criterion.argtypes = [C.c_void_p, C.c_int]
             L.orc_scene_set_sun.argtypes = [C.c_void_p, C.c_int, _fp, C.c_float, _fp, C.c_float, C.c_float, _fp, _fp]
             L.orc_hero_lambda.restype = C.c_float
             L.orc_hero_lambda.argtypes = [C.c_uint, C.c_int, C.c_int]
@@ -398,6 +399,12 @@ class CheckerScene:
         """The emitter MIS estimator (the product's emitter_mis = 1) for this scene's renders."""
         assert self.chk.kind == "oracle"
         self.chk.lib.orc_scene_set_emitter_mis(self.h, 1 if on else 0)
+        return self
+
+    def set_adaptive_criterion(self, criterion: int):
+        """The product's stop test (adaptive_criterion 0, 1 or 2) for this scene's adaptive renders."""
+        assert self.chk.kind == "oracle"
+        self.chk.lib.orc_scene_set_adaptive_criterion(self.h, int(criterion))
         return self
 
     def set_sun(self, direction=None, half_angle=0.0, radiance=(0.0, 0.0, 0.0), temperature_k=0.0, luminance=1.0,

@@ -171,7 +171,7 @@ int renderImpl(void* sceneHandle, void* envHandle, const void* cameraBytes, cons
                 continue;
             }
             if (isConverged(nc, static_cast<float>(nm), static_cast<float>(m2[idx]), p.minSamples,
-                    p.relativeErrorThreshold)) {
+                    p.relativeErrorThreshold, s.adaptiveCriterion)) {
                 converged[idx] = 1;
             }
         }
@@ -237,7 +237,7 @@ int renderSpectralImpl(void* sceneHandle, void* envHandle, const void* cameraByt
                 continue;
             }
             if (isConverged(nc, static_cast<float>(nm), static_cast<float>(m2[idx]), p.minSamples,
-                    p.relativeErrorThreshold)) {
+                    p.relativeErrorThreshold, s.adaptiveCriterion)) {
                 converged[idx] = 1;
             }
         }
@@ -459,6 +459,13 @@ int orc64_render_spectral(void* scene, void* env, const void* cam, const void* p
 void orc_scene_set_emitter_mis(void* h, int on)
 {
     setEmitterMis(*static_cast<Scene*>(h), on != 0);
+}
+
+// Stop test of this scene's adaptive renders (the product's
+// pt_render_params.adaptive_criterion): 0 = the reference's.
+void orc_scene_set_adaptive_criterion(void* h, int criterion)
+{
+    static_cast<Scene*>(h)->adaptiveCriterion = criterion;
 }
 
 void orc_scene_set_sun(void* h, int enabled, const float* dir, float halfAngle, const float* rgb, float temperature,

@@ -156,6 +156,8 @@ struct Scene {
     // is triangle t's position in the emissive list (-1 if none).
     bool emitterMis = false;
     std::vector<int> emitIndex;
+    // the product's stop-test extensions (isConverged); 0 = the reference's
+    int adaptiveCriterion = 0;
 };
 
 struct Env {
@@ -1565,7 +1567,8 @@ inline V3<R> neeEmissive(const Scene& s, V3<R> pos, V3<R> n, V3<R> wo, const Mat
     }
     // Q12: the reference's shadow ray runs to 1e6 and meets the sampled emitter;
     // in emitter MIS mode it ends just short of the light sample
-    const R tMax = misVertex ? (std::sqrt(d2) - R(1.0e-4f)) * (R(1) - R(1.0e-4f)) : R(1.0e6f);
+    const bool misLight = misVertex && !inTransmitCones(Ctx<R>{n, wo, m, eta, 0}, wi);
+    const R tMax = misLight ? (std::sqrt(d2) - R(1.0e-4f)) * (R(1) - R(1.0e-4f)) : R(1.0e6f);
     if (occluded(s, add(pos, scl(wi, R(1.0e-4f))), wi, tMax)) {
         return mk(R(0), R(0), R(0));
     }
@@ -1610,15 +1613,42 @@ inline V3<R> subsurfaceTierB(V3<R> tp, const Mat<R>& m, V3<R> n, const Sample<R>
     return tp;
 }
 
-// Emitter MIS mode: the vertex samples only its diffuse and specular lobes
-// (whose sample pdf is the pdf the NEE weight uses).
+// Emitter MIS mode: a vertex takes part when its BSDF samples the upper
+// hemisphere with the mixture pdf the NEE weight uses and its throughput is
+// f cos / pdf: no subsurface lobe, not the pure transmit lobe (whose throughput
+// drops the cosine), outside any medium, no BRDF debug flags.
 template <class R> inline bool emitterMisVertex(const Scene& s, const Ctx<R>& c)
 {
     if (!s.emitterMis || c.debug != 0) {
         return false;
     }
     const Lobes<R> w = lobes(c);
-    return w.transmit <= R(0) && w.subsurface <= R(0);
+    return w.subsurface <= R(0) && !skipsEnvNee(c.m) && c.eta == R(1);
+}
+
+// The transmit lobe's two narrow cones (evalTransmit: cosine > 0.999 with the
+// mirror and the transmitted direction), left to BSDF sampling alone.
+template <class R> inline bool inTransmitCones(const Ctx<R>& c, V3<R> wi)
+{
+    const Lobes<R> w = lobes(c);
+    if (w.transmit == R(0)) {
+        return false;
+    }
+    const R cOs = dot(c.n, c.wo);
+    if (!transmitValid(c, cOs)) {
+        return false;
+    }
+    if (dot(wi, mirrorOut(c.wo, c.n)) > R(0.999f)) {
+        return true;
+    }
+    V3<R> td{R(0), R(0), R(0)};
+    R ne = R(1);
+    if (clamp01(c.m.thin) > R(0.5f)) {
+        td = nrm(scl(c.wo, R(-1)));
+    } else if (!refractDir(c, td, ne)) {
+        return false;
+    }
+    return dot(wi, td) > R(0.999f);
 }
 
 // Balance weight of the emission of an emitter hit at distance t along the
@@ -1724,7 +1754,7 @@ inline V3<R> tracePath(const Scene& s, const Env* e, const ParamsRec* p, V3<R> r
         }
         eta = smp.nextEta;
         prevPdf = smp.pdf;
-        prevMis = misV;
+        prevMis = misV && !smp.transmitted && !smp.sss && dot(n, smp.dir) > R(0) && !inTransmitCones(c, smp.dir);
         const R bias = mx(R(1.0e-4f), R(1.0e-3f) * h.t);
         const R sign = dot(n, smp.dir) >= R(0) ? R(1) : R(-1);
         o = add(pos, scl(n, sign * bias));
@@ -2170,19 +2200,27 @@ inline V3<R> tracePixelSpectral(const Scene& s, const Env* e, const CameraRec& c
     return spectralSampleRgb(sp, lam, L);
 }
 
-// PathTracerAdaptiveSampling.h:16-40.
-inline bool isConverged(uint32_t n, float mean, float m2, int minSamples, float thr)
+// PathTracerAdaptiveSampling.h:16-40 (criterion 0).  The product's extensions:
+// criterion 1 divides the relative std-dev by sqrt(n) (relative std-error);
+// criterion 2 is criterion 1 plus: a pixel all of whose samples are black
+// (mean and M2 exactly 0) stops after max(minSamples, 64) samples.
+inline bool isConverged(uint32_t n, float mean, float m2, int minSamples, float thr, int criterion = 0)
 {
     if (n < static_cast<uint32_t>(minSamples) || n == 0) {
         return false;
     }
     if (mean < 1.0e-5f) {
-        return false;
+        const uint32_t blackSpp = static_cast<uint32_t>(minSamples > 64 ? minSamples : 64);
+        return criterion == 2 && n >= blackSpp && mean == 0.0f && m2 == 0.0f;
     }
     const float var = m2 / static_cast<float>(n);
     const float sd = std::sqrt(var);
     const float den = std::fmax(mean, 1.0e-4f);
-    return sd / den < thr;
+    float rel = sd / den;
+    if (criterion == 1 || criterion == 2) {
+        rel = rel / std::sqrt(static_cast<float>(n));
+    }
+    return rel < thr;
 }
 
 // ---------------------------------------------------------------------------

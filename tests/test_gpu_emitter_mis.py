@@ -61,13 +61,18 @@ def test_emitter_mis_parity_config0(tracer, oracle, config0):
 
 @pytest.mark.parametrize("nw", [0, 4])
 def test_emitter_mis_keeps_the_expectation(tracer, config0, nw):
+    """Both modes over 8 independent seed batches (hash seeds): the image's mean
+    luminance agrees within 4.5 standard errors, and on the pixels lit by the
+    small light (not seeing it directly) the per-pixel batch-to-batch variance
+    of MIS mode is far lower."""
     w = h = 64
     spp, batches = 64, 8
     cam = config0.camera.copy()
     cam["aspect"] = 1.0
     tracer.configure(w, h, config0.mesh)
     tracer.set_camera(cam)
-    means = {}
+    lum = np.array([0.2126, 0.7152, 0.0722])
+    imgs = {}
     for mode in (0, 1):
         vals = []
         for b in range(batches):
@@ -81,13 +86,17 @@ def test_emitter_mis_keeps_the_expectation(tracer, config0, nw):
             tracer.reset_accumulation()
             tracer.render(0)
             rgba, _, _ = tracer.readback()
-            c = rgba[..., :3].reshape(-1, 3).astype(np.float64)
-            vals.append(float((c @ np.array([0.2126, 0.7152, 0.0722])).mean()))
-        means[mode] = np.array(vals)
+            vals.append(rgba[..., :3].reshape(-1, 3).astype(np.float64) @ lum)
+        imgs[mode] = np.array(vals)  # (batches, pixels)
+    means = {m: imgs[m].mean(axis=1) for m in imgs}
     m0, m1 = means[0].mean(), means[1].mean()
     se = np.sqrt(means[0].var(ddof=1) / batches + means[1].var(ddof=1) / batches)
     assert abs(m0 - m1) <= 4.5 * se, f"mean luminance {m0} (reference) vs {m1} (MIS), se {se}"
-    assert means[1].std() < means[0].std()
+    pix_mean = 0.5 * (imgs[0].mean(0) + imgs[1].mean(0))
+    lit = (pix_mean > 1e-3) & (pix_mean < 1.0)  # lit geometry, not the emitter itself
+    assert lit.sum() > 100
+    v0, v1 = imgs[0].var(axis=0, ddof=1)[lit], imgs[1].var(axis=0, ddof=1)[lit]
+    assert np.median(v1 / np.maximum(v0, 1e-30)) < 0.25, "MIS mode did not lower the per-pixel variance"
 
 
 def test_backward_rejects_emitter_mis(tracer, config0):

@@ -183,3 +183,35 @@ def test_environment_tables_built_on_device_match_reference_build(tracer, oracle
         assert np.array_equal(marg, np.asarray(m_ref).reshape(-1)), chk
         assert np.array_equal(row.reshape(-1), np.asarray(r_ref).reshape(-1)), chk
     tracer.set_environment(None)
+
+
+@pytest.mark.parametrize("criterion", [1, 2])
+def test_render_parity_adaptive_std_error_criteria(tracer, oracle, criterion):
+    """The stop tests the product adds (adaptive_criterion 1: relative std-error;
+    2: the same, and all-black pixels stop after max(min spp, 64)): per-pixel
+    stop decisions and images match the oracle's restatement of them."""
+    mesh = zoo_scene(n_per_mat=150, seed=4)
+    w, h, waves = 40, 32, 96
+    params = default_params(background_r=0.0, background_g=0.0, background_b=0.0, max_path_depth=5,
+                            min_samples=8, max_samples_per_pixel=96, relative_error_threshold=0.08,
+                            adaptive_criterion=criterion)
+    tracer.configure(w, h, mesh)
+    tracer.set_camera(zoo_camera(w, h))
+    tracer.set_params(params)
+    tracer.set_environment(None)
+    tape = tracer.rng_tape(0, waves, 100)
+    tracer.reset_accumulation()
+    tracer.render(waves)
+    rgba, counts, conv = tracer.readback()
+    sc = oracle.scene(mesh).set_adaptive_criterion(criterion)
+    st = sc.render(zoo_camera(w, h), params, w, h, waves, seed_base=1, tape=tape, tape_stride=100)
+    assert st["tape_errors"] == 0
+    counts, rgba = counts.reshape(-1), rgba.reshape(-1, 4)
+    assert len(np.unique(counts)) > 2, "the stop test stopped no pixel early"
+    if criterion == 2:
+        assert np.any(counts == 64), "no black pixel stopped at 64 samples"
+    agree = np.mean(counts == st["counts"])
+    assert agree > 0.995, f"stop decisions agree on {agree:.4f} of pixels"
+    sel = counts == st["counts"]
+    err = rel_rmse(rgba[sel, :3], st["acc"][sel, :3])
+    assert np.all(err <= IMAGE_REL_RMSE), f"relative RMSE {err}"
