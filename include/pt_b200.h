@@ -308,8 +308,12 @@ int pt_batch_readback(pt_renderer* r, int scene, float* rgba, uint32_t* counts, 
  * (side quads to the next ring, a flat cap at each tube end) and every leaf a
  * two-triangle quad of size leaf_size * leaf[9] spanning (tangent x up) and
  * the tangent.  The mesh is [tubes in order, leaves in order, extra]; all
- * material ids index the material bank of `extra`.  cos_sin may be NULL (the
- * library then tabulates cos / sin of k * 2 pi / sides itself). */
+ * material ids index the material bank of `extra`.  Per tube the triangles
+ * follow buildLoftHostMeshFromFrames: side walls ring by ring (the seam vertex
+ * shared with side 0), then start and end caps interleaved per side with rim
+ * uvs 0.5 + 0.5 (sin, cos).  cos_sin may be NULL (the library then tabulates
+ * the reference's angles k * 6.283185307f / sides, cosine and sine rounded to
+ * single precision). */
 typedef struct pt_tubes {
     uint32_t tube_count;
     uint32_t sides;
@@ -323,6 +327,10 @@ typedef struct pt_tubes {
     const double* leaves;         /* 10 per leaf: position, tangent, up, size */
     double leaf_size;
     uint32_t leaf_material;
+    const double* frames;         /* 6 per ring: unit normal, unit binormal (e.g. the reference's
+                                     spline frames, Spline.cpp:102-255), or NULL: a frame derived
+                                     from the ring tangent (+Y reference axis, the last ring of a
+                                     tube takes the tangent of the one before it) */
 } pt_tubes;
 
 /* Builds scene `scene` (0 for a single-scene renderer) from tubes, leaves and

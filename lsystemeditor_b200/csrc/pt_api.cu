@@ -154,6 +154,7 @@ struct pt_renderer {
     DevBuf<unsigned char> eTemp;
     DevBuf<uint32_t> tRingStart, tMaterials;
     DevBuf<double> tPoints, tTangents, tRadii, tCosSin, tLeaves, tFrames;
+    DevBuf<double> tGivenFrames; // given ring frames (pt_tubes.frames)
     BvhBuildOptions bvhOptions;
 
     // environment
@@ -1335,6 +1336,7 @@ int pt_destroy(pt_renderer* r)
     r->tCosSin.release();
     r->tLeaves.release();
     r->tFrames.release();
+    r->tGivenFrames.release();
     r->envPixels.release();
     r->envMarginal.release();
     r->envRow.release();
@@ -2286,18 +2288,22 @@ int pt_batch_set_tubes(pt_renderer* r, int scene, const pt_tubes* tubes, const p
         std::vector<double> cs;
         const double* csp = tubes->cos_sin;
         if (csp == nullptr && S > 0) {
+            // the reference's angles (Loft.cpp:25): k * 6.283185307f / sides in single
+            // precision, cosine and sine rounded to single precision; entry S = entry 0
             cs.resize(2ull * (S + 1));
-            const double step = 2.0 * 3.14159265358979323846 / static_cast<double>(S);
             for (uint32_t k = 0; k <= S; ++k) {
-                cs[2 * k] = std::cos(static_cast<double>(k) * step);
-                cs[2 * k + 1] = std::sin(static_cast<double>(k) * step);
+                const uint32_t kk = k == S ? 0u : k;
+                const float ang = (static_cast<float>(kk) * 6.283185307f) / static_cast<float>(S);
+                cs[2 * k] = static_cast<double>(static_cast<float>(std::cos(static_cast<double>(ang))));
+                cs[2 * k + 1] = static_cast<double>(static_cast<float>(std::sin(static_cast<double>(ang))));
             }
             csp = cs.data();
         }
         const size_t R = rings;
         if (!r->tRingStart.ensure(T + 1ull) || !r->tMaterials.ensure(std::max<uint32_t>(T, 1)) ||
             !r->tPoints.ensure(3 * R + 1) || !r->tTangents.ensure(3 * R + 1) || !r->tRadii.ensure(R + 1) ||
-            !r->tCosSin.ensure(2ull * (S + 1)) || !r->tLeaves.ensure(10ull * Lc + 1) || !r->tFrames.ensure(9 * R + 1)) {
+            !r->tCosSin.ensure(2ull * (S + 1)) || !r->tLeaves.ensure(10ull * Lc + 1) || !r->tFrames.ensure(9 * R + 1) ||
+            (tubes->frames != nullptr && !r->tGivenFrames.ensure(6 * R + 1))) {
             return fail(r, PT_ERR_OUT_OF_MEMORY, "tube upload failed (%u rings, %u leaves)", rings, Lc);
         }
         if (T > 0) {
@@ -2307,6 +2313,10 @@ int pt_batch_set_tubes(pt_renderer* r, int scene, const pt_tubes* tubes, const p
             PT_CHECK(r, cudaMemcpyAsync(r->tTangents.p, tubes->tangents, 3 * R * sizeof(double), cudaMemcpyHostToDevice, s));
             PT_CHECK(r, cudaMemcpyAsync(r->tRadii.p, tubes->radii, R * sizeof(double), cudaMemcpyHostToDevice, s));
             PT_CHECK(r, cudaMemcpyAsync(r->tCosSin.p, csp, 2ull * (S + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+            if (tubes->frames != nullptr) {
+                PT_CHECK(r, cudaMemcpyAsync(r->tGivenFrames.p, tubes->frames, 6 * R * sizeof(double),
+                    cudaMemcpyHostToDevice, s));
+            }
         }
         if (Lc > 0) {
             PT_CHECK(r, cudaMemcpyAsync(r->tLeaves.p, tubes->leaves, 10ull * Lc * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -2321,6 +2331,7 @@ int pt_batch_set_tubes(pt_renderer* r, int scene, const pt_tubes* tubes, const p
         d.radii = r->tRadii.p;
         d.materials = r->tMaterials.p;
         d.cosSin = r->tCosSin.p;
+        d.frames = (tubes->frames != nullptr && T > 0) ? r->tGivenFrames.p : nullptr;
         d.leafCount = Lc;
         d.leaves = r->tLeaves.p;
         d.leafSize = tubes->leaf_size;

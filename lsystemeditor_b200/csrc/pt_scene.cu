@@ -77,15 +77,24 @@ __device__ __forceinline__ uint32_t tubeOfRing(const uint32_t* ringStart, uint32
 __global__ void k_ring_frames(TubeSetDev T, double* frames)
 {
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < T.ringCount; g += gridDim.x * blockDim.x) {
-        const uint32_t t = tubeOfRing(T.ringStart, T.tubeCount, g);
-        const uint32_t first = T.ringStart[t], last = T.ringStart[t + 1] - 1;
-        const uint32_t src = (g == last && last > first) ? g - 1 : g;
-        const D3 tan = dload(T.tangents + 3ull * src);
-        const D3 u = ddiv(tan, dnorm(tan));
-        const D3 ref = fabs(u.y) < 0.99 ? D3{0.0, 1.0, 0.0} : D3{1.0, 0.0, 0.0};
-        D3 a = dcross(ref, u);
-        a = ddiv(a, dnorm(a));
-        const D3 b = dcross(u, a);
+        D3 u, a, b;
+        if (T.frames != nullptr) {
+            // given frames (the spline's): the ring's own unit tangent, normal and binormal
+            const D3 tan = dload(T.tangents + 3ull * g);
+            u = ddiv(tan, dnorm(tan));
+            a = dload(T.frames + 6ull * g);
+            b = dload(T.frames + 6ull * g + 3);
+        } else {
+            const uint32_t t = tubeOfRing(T.ringStart, T.tubeCount, g);
+            const uint32_t first = T.ringStart[t], last = T.ringStart[t + 1] - 1;
+            const uint32_t src = (g == last && last > first) ? g - 1 : g;
+            const D3 tan = dload(T.tangents + 3ull * src);
+            u = ddiv(tan, dnorm(tan));
+            const D3 ref = fabs(u.y) < 0.99 ? D3{0.0, 1.0, 0.0} : D3{1.0, 0.0, 0.0};
+            a = dcross(ref, u);
+            a = ddiv(a, dnorm(a));
+            b = dcross(u, a);
+        }
         double* f = frames + 9ull * g;
         f[0] = u.x;
         f[1] = u.y;
@@ -131,6 +140,7 @@ __global__ void k_loft(TubeSetDev T, const double* frames, float* positions, flo
                 const uint32_t r = static_cast<uint32_t>(local / sides2);
                 const uint32_t rem = static_cast<uint32_t>(local % sides2);
                 const uint32_t k = rem >> 1;
+                const uint32_t k1 = (k + 1 == T.sides) ? 0u : k + 1; // the seam vertex is side 0's
                 const double u0 = __ddiv_rn(static_cast<double>(k), static_cast<double>(T.sides));
                 const double u1 = __ddiv_rn(static_cast<double>(k + 1), static_cast<double>(T.sides));
                 const double span = static_cast<double>(R - 1 > 1 ? R - 1 : 1);
@@ -138,7 +148,7 @@ __global__ void k_loft(TubeSetDev T, const double* frames, float* positions, flo
                 const double v1 = __ddiv_rn(static_cast<double>(r + 1), span);
                 if ((rem & 1u) == 0u) {
                     ringVertex(T, frames, first + r, k, n[0], p[0]);
-                    ringVertex(T, frames, first + r, k + 1, n[1], p[1]);
+                    ringVertex(T, frames, first + r, k1, n[1], p[1]);
                     ringVertex(T, frames, first + r + 1, k, n[2], p[2]);
                     const float q[6] = {__double2float_rn(u0), __double2float_rn(v0), __double2float_rn(u1),
                         __double2float_rn(v0), __double2float_rn(u0), __double2float_rn(v1)};
@@ -146,8 +156,8 @@ __global__ void k_loft(TubeSetDev T, const double* frames, float* positions, flo
                         uv[i] = q[i];
                     }
                 } else {
-                    ringVertex(T, frames, first + r, k + 1, n[0], p[0]);
-                    ringVertex(T, frames, first + r + 1, k + 1, n[1], p[1]);
+                    ringVertex(T, frames, first + r, k1, n[0], p[0]);
+                    ringVertex(T, frames, first + r + 1, k1, n[1], p[1]);
                     ringVertex(T, frames, first + r + 1, k, n[2], p[2]);
                     const float q[6] = {__double2float_rn(u1), __double2float_rn(v0), __double2float_rn(u1),
                         __double2float_rn(v1), __double2float_rn(u0), __double2float_rn(v1)};
@@ -156,24 +166,32 @@ __global__ void k_loft(TubeSetDev T, const double* frames, float* positions, flo
                     }
                 }
             } else {
-                // caps: start (centre, k+1, k) facing -u, then end (centre, k, k+1) facing +u
+                // caps, interleaved per side (Loft.cpp:141-152): start (centre, k+1, k)
+                // facing -u, end (centre, k, k+1) facing +u; rim uvs 0.5 + 0.5 (sin, cos)
                 const uint32_t c = static_cast<uint32_t>(local - sides2 * (R - 1));
-                const bool start = c < T.sides;
-                const uint32_t k = start ? c : c - T.sides;
+                const bool start = (c & 1u) == 0u;
+                const uint32_t k = c >> 1;
+                const uint32_t k1 = (k + 1 == T.sides) ? 0u : k + 1;
                 const uint32_t ring = start ? first : first + R - 1;
                 D3 d0, d1, r0, r1;
                 ringVertex(T, frames, ring, k, d0, r0);
-                ringVertex(T, frames, ring, k + 1, d1, r1);
+                ringVertex(T, frames, ring, k1, d1, r1);
                 p[0] = dload(T.points + 3ull * ring);
                 p[1] = start ? r1 : r0;
                 p[2] = start ? r0 : r1;
                 const double* f = frames + 9ull * ring;
                 const D3 u = D3{f[0], f[1], f[2]};
                 n[0] = n[1] = n[2] = start ? dneg(u) : u;
-                const float q[6] = {0.5f, 0.5f, 1.0f, 0.0f, 0.0f, 1.0f};
-                for (int i = 0; i < 6; ++i) {
-                    uv[i] = q[i];
-                }
+                const float ua = __double2float_rn(__dadd_rn(0.5, __dmul_rn(0.5, T.cosSin[2 * k + 1])));
+                const float va = __double2float_rn(__dadd_rn(0.5, __dmul_rn(0.5, T.cosSin[2 * k])));
+                const float ub = __double2float_rn(__dadd_rn(0.5, __dmul_rn(0.5, T.cosSin[2 * k1 + 1])));
+                const float vb = __double2float_rn(__dadd_rn(0.5, __dmul_rn(0.5, T.cosSin[2 * k1])));
+                uv[0] = 0.5f;
+                uv[1] = 0.5f;
+                uv[2] = start ? ub : ua;
+                uv[3] = start ? vb : va;
+                uv[4] = start ? ua : ub;
+                uv[5] = start ? va : vb;
             }
         } else {
             // leaf quad spanning (tangent x up) and the tangent: (p00 p10 p11) (p00 p11 p01)

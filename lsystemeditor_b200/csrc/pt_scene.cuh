@@ -16,7 +16,8 @@ struct TubeSetDev {
     const double* tangents = nullptr;     // 3 per ring
     const double* radii = nullptr;        // 1 per ring
     const uint32_t* materials = nullptr;  // per tube
-    const double* cosSin = nullptr;       // 2 * (sides + 1): cos, sin of k * 2 pi / sides
+    const double* cosSin = nullptr;       // 2 * (sides + 1): cos, sin of side k's angle (entry sides = entry 0)
+    const double* frames = nullptr;       // 6 per ring: normal, binormal (given frames) or null
     uint32_t leafCount = 0;
     const double* leaves = nullptr;       // 10 per leaf: position, tangent, up, size
     double leafSize = 0.0;

@@ -38,7 +38,7 @@ class PtTubes(C.Structure):
     _fields_ = [("tube_count", C.c_uint32), ("sides", C.c_uint32), ("ring_start", C.c_void_p),
                 ("points", C.c_void_p), ("tangents", C.c_void_p), ("radii", C.c_void_p), ("materials", C.c_void_p),
                 ("cos_sin", C.c_void_p), ("leaf_count", C.c_uint32), ("leaves", C.c_void_p),
-                ("leaf_size", C.c_double), ("leaf_material", C.c_uint32)]
+                ("leaf_size", C.c_double), ("leaf_material", C.c_uint32), ("frames", C.c_void_p)]
 
 
 class PtProfile(C.Structure):
@@ -429,8 +429,10 @@ class PathTracer:
         cs = np.ascontiguousarray(tubes.cos_sin(), np.float64)
         lv = np.ascontiguousarray(tubes.leaves, np.float64)
         addr = lambda a: C.c_void_p(a.ctypes.data) if a.size else None
+        fr = None if tubes.frames is None else np.ascontiguousarray(tubes.frames, np.float64)
         t = PtTubes(len(mat), int(tubes.sides), addr(rs), addr(pts), addr(tan), addr(rad), addr(mat), addr(cs),
-                    len(lv), addr(lv), float(tubes.leaf_size), int(tubes.leaf_material))
+                    len(lv), addr(lv), float(tubes.leaf_size), int(tubes.leaf_material),
+                    addr(fr) if fr is not None else None)
         m, ms = self._pt_mesh(tubes.extra)
         self._check(self._lib.pt_batch_set_tubes(self._h, int(scene), C.byref(t), C.byref(ms)))
 

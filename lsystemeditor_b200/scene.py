@@ -10,9 +10,13 @@ the benchmark scenes.  It follows the reference's turtle conventions
 (Application/src/Procedural/Turtle.cpp:12-282): the turtle starts at the
 origin heading -Z with up +Y, ``Yaw`` turns about up, ``Pitch`` about
 right = up x tangent, ``Roll`` about the tangent, ``F`` appends a state and
-brackets / ``f`` close the current segment.  Each segment is lofted as an
-n-gon tube with rings at its states and flat caps (Loft.cpp:108-155).  It is a
-scene generator only; the path tracer consumes whatever mesh it is given.
+brackets / ``f`` close the current segment.  Each segment's rings and their
+frames come from the reference's Hermite spline and parallel transport
+(Spline.cpp:102-255, ``spline_frames``), the tree is rotated by the root
+transform (ProceduralMeshBuilder.cpp:211-253, ``rotate_turtle_output``) and
+every segment is lofted as an n-gon tube with rings at its frames and flat caps
+(Loft.cpp:108-155, ``loft``).  It is a scene generator only; the path tracer
+consumes whatever mesh it is given.
 """
 from __future__ import annotations
 
@@ -129,6 +133,10 @@ class Segment:
     radii: List[float]
     material: int
     tag: int  # caller-defined (branch depth for leaves, etc.)
+    # ring frames (unit normal and binormal per ring) from spline_frames; None:
+    # the loft derives a frame from each ring's tangent
+    normals: Optional[List[np.ndarray]] = None
+    binormals: Optional[List[np.ndarray]] = None
 
 
 def turtle(word: List[Module], start_tangent=(0.0, 0.0, -1.0), start_up=(0.0, 1.0, 0.0),
@@ -188,6 +196,268 @@ def turtle(word: List[Module], start_tangent=(0.0, 0.0, -1.0), start_up=(0.0, 1.
 
 
 # ---------------------------------------------------------------------------
+# Spline frames (Spline.cpp:102-255), restated in single precision with the
+# reference's operation order: Hermite spans between the turtle states,
+# interior samples only on spans that are not straight, parallel-transported
+# frames starting from a normal perpendicular to world up.
+# ---------------------------------------------------------------------------
+_F = np.float32
+
+
+def _v3(x) -> np.ndarray:
+    return np.asarray(x, np.float32).reshape(3)
+
+
+def _dot(a, b):
+    """x*x' + y*y' + z*z' in single precision, left to right (rows of (..., 3))."""
+    return (a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1]).astype(np.float32) + (a[..., 2] * b[..., 2])
+
+
+def _len(a):
+    return np.sqrt(_dot(a, a).astype(np.float32)).astype(np.float32)
+
+
+def _nrm(a) -> np.ndarray:
+    """vecNormalize3: v * (1 / |v|), (0, 0, -1) for a zero vector."""
+    a = np.asarray(a, np.float32)
+    l = _len(a)
+    inv = (np.float32(1.0) / np.where(l > 0, l, np.float32(1.0))).astype(np.float32)
+    out = (a * inv[..., None]).astype(np.float32)
+    return np.where((l > 0)[..., None], out, np.array([0.0, 0.0, -1.0], np.float32))
+
+
+def _cross(a, b) -> np.ndarray:
+    return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1], a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                     a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], -1).astype(np.float32)
+
+
+def _initial_normal(t) -> np.ndarray:
+    t = _nrm(t)
+    up = np.broadcast_to(np.array([0.0, 1.0, 0.0], np.float32), t.shape)
+    up = np.where((np.abs(_dot(t, up)) > np.float32(0.95))[..., None], np.array([1.0, 0.0, 0.0], np.float32), up)
+    return _nrm(_cross(up, t))
+
+
+def _transport(t_prev, t_next, n_prev) -> np.ndarray:
+    t0, t1 = _nrm(t_prev), _nrm(t_next)
+    axis = _cross(t0, t1)
+    al = _len(axis)
+    if al <= _F(1e-6):
+        return n_prev
+    n = (axis * _F(_F(1.0) / al)).astype(np.float32)
+    ang = _F(np.arcsin(np.float64(min(max(al, _F(-1.0)), _F(1.0)))))
+    c, s_ = _F(np.cos(np.float64(ang))), _F(np.sin(np.float64(ang)))
+    omc = _F(_F(1.0) - c)
+    x, y, z = (_F(v) for v in n_prev)
+    m = lambda a, b: _F(a * b)
+    # rotation matrix of Spline.cpp:28-36, entry by entry in the reference's order
+    r00 = _F(c + m(m(n[0], n[0]), omc)); r01 = _F(m(m(n[0], n[1]), omc) - m(n[2], s_))
+    r02 = _F(m(m(n[0], n[2]), omc) + m(n[1], s_))
+    r10 = _F(m(m(n[1], n[0]), omc) + m(n[2], s_)); r11 = _F(c + m(m(n[1], n[1]), omc))
+    r12 = _F(m(m(n[1], n[2]), omc) - m(n[0], s_))
+    r20 = _F(m(m(n[2], n[0]), omc) - m(n[1], s_)); r21 = _F(m(m(n[2], n[1]), omc) + m(n[0], s_))
+    r22 = _F(c + m(m(n[2], n[2]), omc))
+    return _nrm(np.array([_F(_F(m(r00, x) + m(r01, y)) + m(r02, z)), _F(_F(m(r10, x) + m(r11, y)) + m(r12, z)),
+                          _F(_F(m(r20, x) + m(r21, y)) + m(r22, z))], np.float32))
+
+
+def _hermite(p0, p1, m0, m1, t):
+    t = _F(t)
+    t2 = _F(t * t)
+    t3 = _F(t2 * t)
+    h00 = _F(_F(_F(2.0) * t3) - _F(_F(3.0) * t2)) + _F(1.0)
+    h10 = _F(t3 - _F(_F(2.0) * t2)) + t
+    h01 = _F(_F(-2.0) * t3) + _F(_F(3.0) * t2)
+    h11 = _F(t3 - t2)
+    return ((p0 * h00 + m0 * h10).astype(np.float32) + (p1 * h01 + m1 * h11).astype(np.float32)).astype(np.float32)
+
+
+def _hermite_tangent(p0, p1, m0, m1, t):
+    t = _F(t)
+    t2 = _F(t * t)
+    d00 = _F(_F(6.0) * t2) - _F(_F(6.0) * t)
+    d10 = _F(_F(_F(3.0) * t2) - _F(_F(4.0) * t)) + _F(1.0)
+    d01 = _F(_F(-6.0) * t2) + _F(_F(6.0) * t)
+    d11 = _F(_F(3.0) * t2) - _F(_F(2.0) * t)
+    return _nrm(((p0 * d00 + m0 * d10).astype(np.float32) + (p1 * d01 + m1 * d11).astype(np.float32)).astype(np.float32))
+
+
+def spline_frames(seg: "Segment", samples_per_span: int = 4, tension: float = 1.0) -> Optional["Segment"]:
+    """SplinePath::buildFromSegment + computeLoftFrames (Spline.cpp:102-255) of one
+    turtle segment: returns the segment with its loft rings (positions, unit
+    tangents, radii) and ring frames, or None when its spline has no length
+    (the reference then builds a sphere, which is not generated here)."""
+    if len(seg.points) < 2:
+        return None
+    ten = _F(tension if tension > 0 else 1.0)
+    spans = []
+    for i in range(len(seg.points) - 1):
+        p0, p1 = _v3(seg.points[i]), _v3(seg.points[i + 1])
+        cl = _len((p1 - p0).astype(np.float32))
+        spans.append((p0, p1, (_nrm(_v3(seg.tangents[i])) * _F(cl * ten)).astype(np.float32),
+                      (_nrm(_v3(seg.tangents[i + 1])) * _F(cl * ten)).astype(np.float32),
+                      _F(seg.radii[i]), _F(seg.radii[i + 1]), cl))
+    if sum(float(sp[6]) for sp in spans) <= 1e-6:  # totalArcLength
+        return None
+    per = max(2, samples_per_span)
+    pts: List[Tuple[np.ndarray, np.ndarray, np.float32]] = []
+
+    def append(p, t, r):
+        if pts and _len((p - pts[-1][0]).astype(np.float32)) <= _F(1e-6):
+            return
+        pts.append((p, t, r))
+
+    for k, (p0, p1, m0, m1, r0, r1, cl) in enumerate(spans):
+        if k == 0:
+            append(p0, _nrm(m0), r0)
+        refine = False
+        if per > 2 and cl > _F(1e-6):
+            cd = ((p1 - p0) * _F(_F(1.0) / cl)).astype(np.float32)
+            t0, t1 = _nrm(m0), _nrm(m1)
+            if _dot(t0, cd) < _F(0.999) or _dot(t1, cd) < _F(0.999) or _dot(t0, t1) < _F(0.999):
+                refine = True
+            else:
+                mid = _hermite(p0, p1, m0, m1, 0.5)
+                lin = ((p0 + p1) * _F(0.5)).astype(np.float32)
+                refine = _len((mid - lin).astype(np.float32)) > _F(_F(1e-4) * cl)
+        if refine:
+            for step in range(1, per - 1):
+                t = _F(_F(step) / _F(per - 1))
+                append(_hermite(p0, p1, m0, m1, t), _hermite_tangent(p0, p1, m0, m1, t), _F(r0 + _F(r1 - r0) * t))
+        append(p1, _nrm(m1), r1)
+    normals, binormals = [], []
+    n = _initial_normal(pts[0][1])
+    for i, (p, t, r) in enumerate(pts):
+        if i > 0:
+            n = _transport(pts[i - 1][1], t, n)
+        tn = _nrm(t)
+        b = _nrm(_cross(tn, n))
+        n = _nrm(_cross(b, tn))
+        normals.append(n)
+        binormals.append(b)
+    return Segment([q[0].astype(np.float64) for q in pts], [_nrm(q[1]).astype(np.float64) for q in pts],
+                   [float(q[2]) for q in pts], seg.material, seg.tag,
+                   [v.astype(np.float64) for v in normals], [v.astype(np.float64) for v in binormals])
+
+
+def spline_frames_all(segments: Sequence["Segment"], samples_per_span: int = 4,
+                      tension: float = 1.0) -> List["Segment"]:
+    """``spline_frames`` of every segment (segments whose spline has no length
+    dropped), vectorised over segments with the same state count whose spans
+    are all straight -- every span's end tangents within the reference's 0.999
+    of its chord and of each other and its Hermite midpoint within 1e-4 chord
+    lengths of the chord's (spanNeedsRefinement false), consecutive states
+    more than 1e-6 apart, and every transport step a rotation below 1e-6 --
+    which then give one ring per state; other segments take the scalar path.
+    The operations are the scalar path's, element by element."""
+    F = np.float32
+    out: List[Optional[Segment]] = [None] * len(segments)
+    slow: List[int] = []
+    groups: Dict[int, List[int]] = {}
+    for i, sg in enumerate(segments):
+        groups.setdefault(len(sg.points), []).append(i)
+    ten = F(tension if tension > 0 else 1.0)
+    for R, idxs in groups.items():
+        if R < 2 or max(2, samples_per_span) <= 2:
+            slow += idxs
+            continue
+        P = np.array([np.asarray(segments[i].points, np.float64).reshape(R, 3) for i in idxs]).astype(np.float32)
+        T = np.array([np.asarray(segments[i].tangents, np.float64).reshape(R, 3) for i in idxs]).astype(np.float32)
+        rad = np.array([np.asarray(segments[i].radii, np.float64).reshape(R) for i in idxs]).astype(np.float32)
+        chord = (P[:, 1:] - P[:, :-1]).astype(np.float32)
+        cl = _len(chord)                                              # (N, R-1)
+        k = (cl * ten).astype(np.float32)[..., None]
+        m0 = (_nrm(T[:, :-1]) * k).astype(np.float32)
+        m1 = (_nrm(T[:, 1:]) * k).astype(np.float32)
+        inv = (F(1.0) / np.where(cl > 0, cl, F(1.0))).astype(np.float32)
+        cd = (chord * inv[..., None]).astype(np.float32)
+        t0, t1 = _nrm(m0), _nrm(m1)
+        mid = _hermite(P[:, :-1], P[:, 1:], m0, m1, 0.5)
+        lin = ((P[:, :-1] + P[:, 1:]) * F(0.5)).astype(np.float32)
+        straight = ((cl > F(1e-6)) & (_dot(t0, cd) >= F(0.999)) & (_dot(t1, cd) >= F(0.999)) &
+                    (_dot(t0, t1) >= F(0.999)) & (_len((mid - lin).astype(np.float32)) <= (F(1e-4) * cl)))
+        ok = straight.all(axis=1)
+        # loft points: state 0 with the first span's start tangent, then every span's end
+        tan = np.concatenate([_nrm(m0[:, :1]), _nrm(m1)], axis=1)      # (N, R, 3)
+        n = _initial_normal(tan[:, 0])
+        normals = np.empty_like(tan)
+        binormals = np.empty_like(tan)
+        for r in range(R):
+            if r > 0:
+                a0, a1 = _nrm(tan[:, r - 1]), _nrm(tan[:, r])
+                ok &= _len(_cross(a0, a1)) <= F(1e-6)  # transport keeps the normal
+            tn = _nrm(tan[:, r])
+            b = _nrm(_cross(tn, n))
+            n = _nrm(_cross(b, tn))
+            normals[:, r] = n
+            binormals[:, r] = b
+        for j, i in enumerate(idxs):
+            if not ok[j]:
+                slow.append(i)
+                continue
+            sg = segments[i]
+            out[i] = Segment([q for q in P[j].astype(np.float64)], [q for q in _nrm(tan[j]).astype(np.float64)],
+                             [float(v) for v in rad[j]], sg.material, sg.tag,
+                             [q for q in normals[j].astype(np.float64)], [q for q in binormals[j].astype(np.float64)])
+    for i in slow:
+        out[i] = spline_frames(segments[i], samples_per_span, tension)
+    return [sg for sg in out if sg is not None]
+
+
+def _rotate_about(v: np.ndarray, axis, deg: float) -> np.ndarray:
+    """rotateAroundAxis (ProceduralMeshBuilder.cpp:213-226) in double, rows of v."""
+    a = np.asarray(axis, np.float64)
+    ang = float(np.float32(deg) * np.float32(0.0174532925))
+    c, s_ = math.cos(ang), math.sin(ang)
+    d = v @ a
+    return v * c + np.cross(a, v) * s_ + np.outer(d, a) * (1.0 - c)
+
+
+def rotate_yaw_pitch_roll(v: np.ndarray, rotation_deg) -> np.ndarray:
+    """rotateYawPitchRoll (ProceduralMeshBuilder.cpp:228-241): yaw about +Y, then
+    pitch about +X, then roll about +Z (angles in degrees, skipped when ~0)."""
+    v = np.asarray(v, np.float64).reshape(-1, 3)
+    for deg, axis in zip(rotation_deg, ((0.0, 1.0, 0.0), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0))):
+        if abs(deg) > 1e-6:
+            v = _rotate_about(v, axis, deg)
+    return v
+
+
+def rotate_turtle_output(segments: Sequence["Segment"], leaves, rotation_deg) -> Tuple[List["Segment"], list]:
+    """The root transform of ProceduralMeshBuilder (applyRootTransform,
+    ProceduralMeshBuilder.cpp:243-253) applied to ring centres, tangents and
+    frames, and to leaf frames, instead of to the lofted vertices (a rotation
+    commutes with the loft)."""
+    out = []
+    for sg in segments:
+        rot = lambda xs: [r for r in rotate_yaw_pitch_roll(np.array(xs), rotation_deg)] if xs is not None else None
+        out.append(Segment(rot(sg.points), rot(sg.tangents), list(sg.radii), sg.material, sg.tag, rot(sg.normals),
+                           rot(sg.binormals)))
+    lv = []
+    for (p, t, u, size) in leaves:
+        q = rotate_yaw_pitch_roll(np.array([p, t, u]), rotation_deg)
+        lv.append((q[0], q[1], q[2], size))
+    return out, lv
+
+
+def frame_tree(segments: Sequence["Segment"], leaves, rotation_deg=(0.0, 90.0, 0.0), samples_per_span: int = 4):
+    """Spline frames of turtle output in the reference's start pose, then the
+    root rotation (the default +90 degree pitch turns heading -Z to +Y)."""
+    return rotate_turtle_output(spline_frames_all(segments, samples_per_span), leaves, rotation_deg)
+
+
+def reference_tree(word: List[Module], rotation_deg=(0.0, 90.0, 0.0), samples_per_span: int = 4,
+                   leaf_symbol: Optional[str] = None, refine: Optional[Callable] = None):
+    """The reference's procedural pipeline on a symbol string: turtle from its
+    default pose (heading -Z, up +Y), optional ring refinement, spline frames,
+    root rotation (the default pitch of +90 degrees turns the heading to +Y)."""
+    segs, leaves = turtle(word, leaf_symbol=leaf_symbol)
+    if refine is not None:
+        segs = refine(segs)
+    return rotate_turtle_output(spline_frames_all(segs, samples_per_span), leaves, rotation_deg)
+
+
+# ---------------------------------------------------------------------------
 # Loft (Loft.cpp:108-155): rings at every state, side quads as two triangles,
 # flat caps at both ends.  Vectorised over all segments that have the same
 # number of rings.
@@ -201,57 +471,87 @@ def _perp_frames(tangents: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     return a, b
 
 
+def angle_table(sides: int) -> Tuple[np.ndarray, np.ndarray]:
+    """cos / sin of side k's angle k * 6.283185307f / sides, the angle in single
+    precision as Loft.cpp:25 computes it, the cosine and sine rounded to single
+    precision; returned in double (the loft's arithmetic)."""
+    k = np.arange(sides, dtype=np.float32)
+    ang = ((k * np.float32(6.283185307)) / np.float32(sides)).astype(np.float64)
+    return (np.cos(ang).astype(np.float32).astype(np.float64), np.sin(ang).astype(np.float32).astype(np.float64))
+
+
 def loft(segments: Sequence[Segment], sides: int = 8, material_ids: Optional[Sequence[int]] = None) -> HostMesh:
+    """buildLoftHostMeshFromFrames (Loft.cpp:108-155) of every segment, in double:
+    per ring, vertex k = centre + radius (normal cos_k + binormal sin_k) with the
+    segment's frames (or, for a segment without frames, a frame derived from the
+    ring tangent); side walls ring by ring (two triangles per side, the seam
+    vertex shared with side 0, u = k / sides, v = ring / (rings - 1)), then the
+    start and end caps interleaved per side (normals -/+ the unit tangent, rim
+    uvs 0.5 + 0.5 (sin, cos), centre 0.5).  Vectorised over segments with the
+    same ring count; the device loft (pt_batch_set_tubes) computes the same."""
     groups: Dict[int, List[int]] = {}
+    order: List[int] = []
     for i, s in enumerate(segments):
         groups.setdefault(len(s.points), []).append(i)
-    parts_pos, parts_nrm, parts_uv, parts_mid = [], [], [], []
-    ang = np.arange(sides + 1) * (2.0 * math.pi / sides)
-    cs, sn = np.cos(ang), np.sin(ang)
+    cs, sn = angle_table(sides)
+    nxt = (np.arange(sides) + 1) % sides
+    cap_uv = np.stack([(0.5 + 0.5 * sn).astype(np.float32), (0.5 + 0.5 * cs).astype(np.float32)], -1)  # (sides, 2)
+    per_seg_pos, per_seg_nrm, per_seg_uv = {}, {}, {}
     for rings, idxs in groups.items():
-        P = np.array([[segments[i].points[k] for k in range(rings)] for i in idxs])      # (S, R, 3)
-        T = np.array([[segments[i].tangents[k] for k in range(rings)] for i in idxs])
-        Rr = np.array([[segments[i].radii[k] for k in range(rings)] for i in idxs])     # (S, R)
-        T[:, -1] = T[:, -2] if rings > 1 else T[:, -1]
-        A, B = _perp_frames(T)
-        # Parallel-transport-free approximation: per-ring frame from the ring tangent.
-        dirs = A[:, :, None, :] * cs[None, None, :, None] + B[:, :, None, :] * sn[None, None, :, None]  # (S,R,C+1,3)
+        P = np.array([[segments[i].points[k] for k in range(rings)] for i in idxs], np.float64)      # (S, R, 3)
+        T = np.array([[segments[i].tangents[k] for k in range(rings)] for i in idxs], np.float64)
+        Rr = np.array([[segments[i].radii[k] for k in range(rings)] for i in idxs], np.float64)     # (S, R)
+        framed = segments[idxs[0]].normals is not None
+        if framed:
+            A = np.array([[segments[i].normals[k] for k in range(rings)] for i in idxs], np.float64)
+            B = np.array([[segments[i].binormals[k] for k in range(rings)] for i in idxs], np.float64)
+            U = T / np.linalg.norm(T, axis=-1, keepdims=True)
+        else:
+            if rings > 1:
+                T[:, -1] = T[:, -2]
+            A, B = _perp_frames(T)
+            U = T / np.linalg.norm(T, axis=-1, keepdims=True)
+        dirs = A[:, :, None, :] * cs[None, None, :, None] + B[:, :, None, :] * sn[None, None, :, None]  # (S,R,C,3)
         ringp = P[:, :, None, :] + dirs * Rr[:, :, None, None]
         S = len(idxs)
         tris_pos, tris_nrm, tris_uv = [], [], []
+        span = float(max(rings - 1, 1))
         for r in range(rings - 1):
-            v0, v1 = r / max(rings - 1, 1), (r + 1) / max(rings - 1, 1)
+            v0, v1 = r / span, (r + 1) / span
             for k in range(sides):
-                a00, a01 = ringp[:, r, k], ringp[:, r, k + 1]
-                a10, a11 = ringp[:, r + 1, k], ringp[:, r + 1, k + 1]
-                n00, n01 = dirs[:, r, k], dirs[:, r, k + 1]
-                n10, n11 = dirs[:, r + 1, k], dirs[:, r + 1, k + 1]
+                k1 = int(nxt[k])
                 u0, u1 = k / sides, (k + 1) / sides
-                tris_pos += [np.stack([a00, a01, a10], 1), np.stack([a01, a11, a10], 1)]
-                tris_nrm += [np.stack([n00, n01, n10], 1), np.stack([n01, n11, n10], 1)]
-                uvq = np.array([[[u0, v0], [u1, v0], [u0, v1]], [[u1, v0], [u1, v1], [u0, v1]]], np.float32)
+                tris_pos += [np.stack([ringp[:, r, k], ringp[:, r, k1], ringp[:, r + 1, k]], 1),
+                             np.stack([ringp[:, r, k1], ringp[:, r + 1, k1], ringp[:, r + 1, k]], 1)]
+                tris_nrm += [np.stack([dirs[:, r, k], dirs[:, r, k1], dirs[:, r + 1, k]], 1),
+                             np.stack([dirs[:, r, k1], dirs[:, r + 1, k1], dirs[:, r + 1, k]], 1)]
+                uvq = np.array([[[u0, v0], [u1, v0], [u0, v1]], [[u1, v0], [u1, v1], [u0, v1]]], np.float64)
+                uvq = uvq.astype(np.float32)
                 tris_uv += [np.broadcast_to(uvq[0], (S, 3, 2)), np.broadcast_to(uvq[1], (S, 3, 2))]
-        # caps
-        for end, sign in ((0, -1.0), (rings - 1, 1.0)):
-            tn = T[:, end] / np.linalg.norm(T[:, end], axis=-1, keepdims=True) * sign
-            c = P[:, end]
-            for k in range(sides):
-                r0, r1 = ringp[:, end, k], ringp[:, end, k + 1]
-                tri = np.stack([c, r1, r0] if sign < 0 else [c, r0, r1], 1)
-                tris_pos.append(tri)
-                tris_nrm.append(np.broadcast_to(tn[:, None, :], (S, 3, 3)))
-                tris_uv.append(np.broadcast_to(np.array([[0.5, 0.5], [1.0, 0.0], [0.0, 1.0]], np.float32), (S, 3, 2)))
-        pos = np.stack(tris_pos, 1).reshape(-1, 3, 3)     # segment-major
-        nrm = np.stack(tris_nrm, 1).reshape(-1, 3, 3)
-        uv = np.stack(tris_uv, 1).reshape(-1, 3, 2)
-        per = len(tris_pos)
-        mids = np.repeat(np.array([segments[i].material if material_ids is None else material_ids[i]
-                                   for i in idxs], np.uint32), per)
-        parts_pos.append(pos); parts_nrm.append(nrm); parts_uv.append(uv); parts_mid.append(mids)
-    if not parts_pos:
+        c0, c1 = P[:, 0], P[:, rings - 1]
+        n0 = np.broadcast_to(-U[:, 0][:, None, :], (S, 3, 3))
+        n1 = np.broadcast_to(U[:, rings - 1][:, None, :], (S, 3, 3))
+        for k in range(sides):
+            k1 = int(nxt[k])
+            tris_pos.append(np.stack([c0, ringp[:, 0, k1], ringp[:, 0, k]], 1))
+            tris_nrm.append(n0)
+            tris_uv.append(np.broadcast_to(np.array([[0.5, 0.5], cap_uv[k1], cap_uv[k]], np.float32), (S, 3, 2)))
+            tris_pos.append(np.stack([c1, ringp[:, rings - 1, k], ringp[:, rings - 1, k1]], 1))
+            tris_nrm.append(n1)
+            tris_uv.append(np.broadcast_to(np.array([[0.5, 0.5], cap_uv[k], cap_uv[k1]], np.float32), (S, 3, 2)))
+        pos = np.stack(tris_pos, 1)     # (S, per, 3, 3)
+        nrm = np.stack(tris_nrm, 1)
+        uv = np.stack(tris_uv, 1)
+        for j, i in enumerate(idxs):
+            per_seg_pos[i], per_seg_nrm[i], per_seg_uv[i] = pos[j], nrm[j], uv[j]
+    if not segments:
         return HostMesh.empty()
-    return HostMesh(np.concatenate(parts_pos).astype(np.float32), np.concatenate(parts_nrm).astype(np.float32),
-                    np.concatenate(parts_uv).astype(np.float32), np.concatenate(parts_mid).astype(np.uint32),
+    order = list(range(len(segments)))
+    mids = np.concatenate([np.full(len(per_seg_pos[i]), segments[i].material if material_ids is None
+                                   else material_ids[i], np.uint32) for i in order])
+    return HostMesh(np.concatenate([per_seg_pos[i] for i in order]).astype(np.float32),
+                    np.concatenate([per_seg_nrm[i] for i in order]).astype(np.float32),
+                    np.concatenate([per_seg_uv[i] for i in order]).astype(np.float32), mids,
                     np.zeros(0, MATERIAL_DTYPE), np.zeros(0, TEXTURE_DTYPE))
 
 
@@ -293,6 +593,7 @@ class TubeSet:
     leaf_size: float
     leaf_material: int
     extra: HostMesh          # appended triangles; its material bank is the scene's
+    frames: Optional[np.ndarray] = None  # (R, 6) float64 ring normal + binormal, or None
 
     @staticmethod
     def from_turtle(segments: Sequence[Segment], leaves, sides: int, leaf_size: float, leaf_material: int,
@@ -308,24 +609,32 @@ class TubeSet:
             pts = np.zeros((0, 3)); tans = np.zeros((0, 3)); rad = np.zeros(0)
         mats = np.array([sg.material + tube_material_offset for sg in segments], np.uint32)
         lv = np.array([np.concatenate([l[0], l[1], l[2], [l[3]]]) for l in leaves], np.float64).reshape(-1, 10)
+        frames = None
+        if segments and all(sg.normals is not None for sg in segments):
+            frames = np.concatenate([np.concatenate([np.array(sg.normals, np.float64).reshape(-1, 3),
+                                                     np.array(sg.binormals, np.float64).reshape(-1, 3)], 1)
+                                     for sg in segments])
         return TubeSet(ring_start, pts, tans, rad, mats, int(sides), lv, float(leaf_size), int(leaf_material),
-                       extra)
+                       extra, frames)
 
     @property
     def triangle_count(self) -> int:
         return 2 * self.sides * len(self.radii) + 2 * len(self.leaves) + self.extra.triangle_count
 
     def cos_sin(self) -> np.ndarray:
-        """The loft's angle table (same expression as ``loft``)."""
-        ang = np.arange(self.sides + 1) * (2.0 * math.pi / self.sides)
-        return np.stack([np.cos(ang), np.sin(ang)], -1).reshape(-1)
+        """The loft's angle table (``angle_table``), interleaved cos / sin, with
+        entry `sides` repeating entry 0 (the seam)."""
+        cs, sn = angle_table(self.sides)
+        t = np.stack([cs, sn], -1)
+        return np.concatenate([t, t[:1]]).reshape(-1)
 
     def segments(self) -> List[Segment]:
         out = []
         for t in range(len(self.materials)):
             a, b = int(self.ring_start[t]), int(self.ring_start[t + 1])
+            nb = (None, None) if self.frames is None else (list(self.frames[a:b, 0:3]), list(self.frames[a:b, 3:6]))
             out.append(Segment(list(self.points[a:b]), list(self.tangents[a:b]), list(self.radii[a:b]),
-                               int(self.materials[t]), 0))
+                               int(self.materials[t]), 0, nb[0], nb[1]))
         return out
 
     def host_mesh(self) -> HostMesh:
@@ -372,16 +681,24 @@ def bracketed_ol_tree(iterations: int = 4, angle: float = 25.7, length: float = 
                       sides: int = 8) -> HostMesh:
     """F(h,r) -> F(h,r)[Yaw(a)F(h,r)]F(h,r)[Yaw(-a)F(h,r)]F(h,r) in the XY plane (5^n segments).
 
-    The turtle heads +Y with up +Z so that Yaw bends the branches in the XY plane
-    (the reference reaches the same orientation with a +90 degree instance pitch).
+    The reference pipeline (``reference_tree``): the turtle starts heading -Z
+    with up +Y, the spline frames and the loft follow Spline.cpp / Loft.cpp, and
+    the root transform's +90 degree pitch turns the tree to head +Y with up +Z,
+    so Yaw bends the branches in the XY plane.
     """
+    return loft(bracketed_ol_segments(iterations, angle, length, radius), sides)
+
+
+def bracketed_ol_segments(iterations: int = 4, angle: float = 25.7, length: float = 0.1,
+                          radius: float = 0.02) -> List[Segment]:
+    """The framed, root-rotated tube segments of ``bracketed_ol_tree``."""
     def rule(args, _rng):
         h, r = args
         F = ("F", (h, r))
         return [F, ("[", ()), ("Yaw", (angle,)), F, ("]", ()), F, ("[", ()), ("Yaw", (-angle,)), F, ("]", ()), F]
     word = expand([("F", (length, radius))], {"F": rule}, iterations)
-    segs, _ = turtle(word, start_tangent=(0.0, 1.0, 0.0), start_up=(0.0, 0.0, 1.0))
-    return loft(segs, sides)
+    segs, _ = reference_tree(word)
+    return segs
 
 
 def stochastic_tree(iterations: int = 7, seed: int = 7, angle: float = 22.5, jitter: float = 5.0,
@@ -392,7 +709,9 @@ def stochastic_tree(iterations: int = 7, seed: int = 7, angle: float = 22.5, jit
     with + / - = Yaw(+-a), & / ^ = Pitch(+-a), / = Roll(a), a = angle +- uniform jitter
     (drawn per symbol from a seeded generator and baked into the successor), segment
     length x length_decay and radius x radius_decay per depth.  Terminal A's carry
-    a leaf.  Returns (segments, leaves) from the turtle (heading +Y, up +Z).
+    a leaf.  Returns (segments, leaves) from the turtle in the reference's start
+    pose (heading -Z, up +Y); ``frame_tree`` adds the spline frames and the root
+    rotation that turns it to head +Y.
     """
     def rot(name, rng, sign=1.0):
         return (name, (sign * (angle + rng.uniform(-jitter, jitter)),))
@@ -412,7 +731,7 @@ def stochastic_tree(iterations: int = 7, seed: int = 7, angle: float = 22.5, jit
 
     word = expand([("A", (0,))], {"A": rule}, iterations, seed=seed)
     word = [("Leaf", (1.0,)) if name == "A" else (name, a) for name, a in word]
-    return turtle(word, start_tangent=(0.0, 1.0, 0.0), start_up=(0.0, 0.0, 1.0), leaf_symbol="Leaf")
+    return turtle(word, leaf_symbol="Leaf")
 
 
 def refine_segments(segments: Sequence[Segment], rings: int, taper: float) -> List[Segment]:
@@ -444,7 +763,7 @@ def tree_tubes(iterations: int = 7, seed: int = 7, sides: int = 64, rings: int =
     """The stochastic tree as a TubeSet: bark tubes (material 0), leaf quads
     (material 1), the ground (2) and the light (3) of the plain scenes."""
     segs, leaves = stochastic_tree(iterations=iterations, seed=seed)
-    segs = refine_segments(segs, rings, taper=taper)
+    segs, leaves = frame_tree(refine_segments(segs, rings, taper=taper), leaves)
     ground = quad_mesh((0, 0, 0), (10, 0, 0), (0, 0, -10),
                        default_material(r=0.5, g=0.5, b=0.5, roughness=1.0), normal=(0, 1, 0))
     light = quad_mesh((0, 5, 1.5), (1, 0, 0), (0, 0, 1),
@@ -541,7 +860,7 @@ def config3_scene(width: int = 512, height: int = 512, spp: int = 64, seed: int 
         a = 25.7
         return [F, ("[", ()), ("Yaw", (a,)), F, ("]", ()), F, ("[", ()), ("Yaw", (-a,)), F, ("]", ()), F]
     word = expand([("F", (0.1, 0.02))], {"F": rule}, 4)
-    segs, _ = turtle(word, start_tangent=(0.0, 1.0, 0.0), start_up=(0.0, 0.0, 1.0))
+    segs, _ = reference_tree(word)
     dist = np.array([float(np.linalg.norm(sg.points[0])) for sg in segs])
     band = np.minimum((dist / max(dist.max(), 1e-9) * 8.0).astype(int), 7)
     tree = loft(segs, 8, material_ids=[int(b) for b in band])
@@ -570,14 +889,16 @@ def config0_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth:
     light at height 5 (emission 10, white) offset 1.5 units in z so that the trunk
     does not pass through it; black background; 64 spp fixed (min = max); max depth 8.
     """
-    tree = bracketed_ol_tree()
-    tree.materials = np.array([default_material(r=0.35, g=0.22, b=0.12, roughness=0.8, metallic=0.0)],
-                              MATERIAL_DTYPE)
+    segs = bracketed_ol_segments()
+    bark = default_material(r=0.35, g=0.22, b=0.12, roughness=0.8, metallic=0.0)
+    tree = loft(segs, 8)
+    tree.materials = np.array([bark], MATERIAL_DTYPE)
     ground = quad_mesh((0, 0, 0), (10, 0, 0), (0, 0, -10),
                        default_material(r=0.5, g=0.5, b=0.5, roughness=1.0), normal=(0, 1, 0))
     light = quad_mesh((0, 5, 1.5), (1, 0, 0), (0, 0, 1),
                       default_material(r=1.0, g=1.0, b=1.0, emission=10.0), normal=(0, -1, 0))
     mesh = HostMesh.concat([tree, ground, light])
+    tubes = TubeSet.from_turtle(segs, [], 8, 0.0, 0, extra=HostMesh.concat([_bank([bark]), ground, light]))
     lo, hi = tree.bounds()
     center = (lo + hi) * 0.5
     extent = float(np.max(hi - lo))
@@ -587,7 +908,7 @@ def config0_scene(width: int = 256, height: int = 256, spp: int = 64, max_depth:
     params = default_params(background_r=0.0, background_g=0.0, background_b=0.0, max_path_depth=max_depth,
                             russian_roulette_min_depth=3, min_samples=spp, max_samples_per_pixel=spp)
     return SceneSpec("plain-small: 2D bracketed OL-system, 625 segments, 256x256, 64 spp, depth 8",
-                     mesh, cam, params, width, height, spp)
+                     mesh, cam, params, width, height, spp, tubes)
 
 
 @dataclasses.dataclass
@@ -658,7 +979,7 @@ def forest_scene(width: int = 1920, height: int = 1080, trees: int = 12, instanc
     objects = []
     for k in range(trees):
         segs, leaves = stochastic_tree(iterations=int(its[k]), seed=seed + k)
-        segs = refine_segments(segs, rings, taper=0.85)
+        segs, leaves = frame_tree(refine_segments(segs, rings, taper=0.85), leaves)
         ts = TubeSet.from_turtle(segs, leaves, sides, 0.18, leaf_material=1, extra=_bank([bark, leaf, ground_mat]))
         objects.append(ts.host_mesh())
     ground = quad_mesh((0, 0, 0), (extent, 0, 0), (0, 0, -extent), ground_mat, normal=(0, 1, 0))

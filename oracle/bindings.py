@@ -4,6 +4,8 @@
   restatement of the reference render path (FP32 ``orc_*`` and FP64 ``orc64_*``).
 * ``Checker("ref")`` loads oracle/_ref/libptref.so -- the reference's own
   hot-path code compiled for the host (only where it could be built).
+* ``ReferenceGenerator`` loads oracle/_ref/libptref_gen.so -- the reference's
+  L-system, turtle and spline code with its loft restated (scene generator).
 * ``ReferenceGpu`` loads oracle/_ref/libptref_gpu.so -- the reference's own
   CUDA render kernels (PathTracer.cu) compiled for sm_100a, driven by the wave
   loop of its render loop; a GPU checker and the GPU bar of the benchmark.
@@ -86,7 +88,18 @@ def build_ref_gpu() -> Optional[str]:
     return REF_GPU_SO
 
 
+REF_GEN_SO = os.path.join(HERE, "_ref", "libptref_gen.so")
 WRAPPER_BIN = os.path.join(HERE, "_ref", "wrapper_check")
+
+
+def build_ref_gen() -> Optional[str]:
+    """Compiles the reference's scene generator (LSystemLib, Turtle.cpp, Spline.cpp) for the host."""
+    if not os.path.isdir(REF_ROOT):
+        return REF_GEN_SO if os.path.exists(REF_GEN_SO) else None
+    src = [os.path.join(HERE, "ref_gen_harness.cpp"), os.path.join(HERE, "Makefile")]
+    if not os.path.exists(REF_GEN_SO) or any(os.path.getmtime(s) > os.path.getmtime(REF_GEN_SO) for s in src):
+        subprocess.run(["make", "-C", HERE, "refgen", f"REF_ROOT={REF_ROOT}"], check=True, stdout=subprocess.DEVNULL)
+    return REF_GEN_SO
 
 
 def build_wrapper() -> Optional[str]:
@@ -628,3 +641,64 @@ class ReferenceGpuEnv:
         if getattr(self, "h", None):
             self.rg.lib.refgpu_env_destroy(self.h)
             self.h = None
+
+
+def reference_generator_available() -> bool:
+    return os.path.exists(REF_GEN_SO)
+
+
+class ReferenceGenerator:
+    """The reference's procedural pipeline on the host (oracle/ref_gen_harness.cpp):
+    LSystemEvaluator::evaluate -> turtleExecute -> SplinePath::computeLoftFrames
+    -> loft -> root transform."""
+
+    def __init__(self):
+        path = build_ref_gen()
+        if path is None or not os.path.exists(path):
+            raise FileNotFoundError("reference generator build unavailable")
+        L = self.lib = C.CDLL(path)
+        L.refgen_build.restype = C.c_void_p
+        L.refgen_build.argtypes = [C.c_char_p, C.c_int, C.c_ulonglong, _fp, _fp, C.c_int, C.c_int, C.c_float,
+                                   C.c_float, C.c_float]
+        L.refgen_destroy.argtypes = [C.c_void_p]
+        L.refgen_error.restype = C.c_char_p
+        L.refgen_error.argtypes = [C.c_void_p]
+        L.refgen_counts.argtypes = [C.c_void_p, _i32p]
+        L.refgen_times.argtypes = [C.c_void_p, _dp]
+        L.refgen_triangles.argtypes = [C.c_void_p, _fp, _fp, _fp, _u32p]
+        L.refgen_frames.argtypes = [C.c_void_p, _fp, _u32p, _u32p]
+
+    def build(self, definition: str, iterations: int, seed: int = 0xC0FFEE, rotation_deg=(0.0, 0.0, 0.0),
+              translation=(0.0, 0.0, 0.0), sides: int = 32, samples_per_span: int = 4, tension: float = 1.0,
+              default_step: float = 500.0, default_radius: float = 100.0) -> dict:
+        """Mesh (positions (N,3,3), normals, uvs (N,3,2), segment per triangle), loft frames before the root
+        transform ((F,13): position, tangent, normal, binormal, radius; frame_start per lofted segment),
+        stage times in ms (lsystem, turtle, spline, loft) and counts."""
+        rot = np.ascontiguousarray(rotation_deg, np.float32)
+        tr = np.ascontiguousarray(translation, np.float32)
+        h = self.lib.refgen_build(definition.encode(), int(iterations), int(seed), _ptr(rot, _fp), _ptr(tr, _fp),
+                                  int(sides), int(samples_per_span), float(tension), float(default_step),
+                                  float(default_radius))
+        try:
+            err = self.lib.refgen_error(h).decode()
+            if err:
+                raise ValueError(f"reference L-system: {err}")
+            c = np.zeros(5, np.int32)
+            self.lib.refgen_counts(h, _ptr(c, _i32p))
+            n, segs, nf = int(c[0]), int(c[1]), int(c[2])
+            pos = np.zeros((n, 3, 3), np.float32)
+            nrm = np.zeros((n, 3, 3), np.float32)
+            uv = np.zeros((n, 3, 2), np.float32)
+            seg = np.zeros(max(n, 1), np.uint32)
+            self.lib.refgen_triangles(h, _ptr(pos, _fp), _ptr(nrm, _fp), _ptr(uv, _fp), _ptr(seg, _u32p))
+            frames = np.zeros((max(nf, 1), 13), np.float32)
+            start = np.zeros(segs + 1, np.uint32)
+            mats = np.zeros(max(segs, 1), np.uint32)
+            self.lib.refgen_frames(h, _ptr(frames, _fp), _ptr(start, _u32p), _ptr(mats, _u32p))
+            ms = np.zeros(4, np.float64)
+            self.lib.refgen_times(h, _ptr(ms, _dp))
+        finally:
+            self.lib.refgen_destroy(h)
+        return dict(positions=pos, normals=nrm, uvs=uv, segment=seg[:n], frames=frames[:nf], frame_start=start,
+                    materials=mats[:segs], skipped=int(c[3]), symbols=int(c[4]),
+                    ms=dict(lsystem=ms[0], turtle=ms[1], spline=ms[2], loft=ms[3]))

@@ -118,3 +118,27 @@ def test_exposure_multiplier():
         i = max(f32(iso), f32(1.0))
         want = f32(sh) * (i / f32(100.0)) / (f * f)
         assert PathTracer.exposure_multiplier(fs, sh, iso) == float(want)
+
+
+def test_device_loft_of_config0_is_the_reference_generator_mesh(tracer):
+    """Config 0 built on the device from its tube set (pt_batch_set_tubes with the
+    spline frames): bit for bit the host generator's mesh, and -- where the
+    reference's own generator is available -- its triangles in its order
+    (positions within 1e-5, normals within 1e-4, uvs exactly)."""
+    from lsystemeditor_b200.scene import config0_scene
+    spec = config0_scene()
+    tracer.configure(16, 16)
+    tracer.batch_set_tubes(0, spec.tubes)
+    dev = tracer.export_mesh(0)
+    for f in ("positions", "normals", "uvs", "material_ids"):
+        assert np.array_equal(getattr(dev, f), getattr(spec.mesh, f)), f
+    from oracle.bindings import ReferenceGenerator, reference_generator_available
+    if not reference_generator_available():
+        pytest.skip("reference generator build unavailable")
+    ref = ReferenceGenerator().build("F(0.1,0.02)\nF(h,r) -> F(h,r)[Yaw(25.7)F(h,r)]F(h,r)[Yaw(0-25.7)F(h,r)]F(h,r)",
+                                     4, rotation_deg=(0.0, 90.0, 0.0), sides=8)
+    n = ref["positions"].shape[0]
+    assert n == 20000
+    assert np.abs(dev.positions[:n] - ref["positions"]).max() < 1e-5
+    assert np.abs(dev.normals[:n] - ref["normals"]).max() < 1e-4
+    assert np.array_equal(dev.uvs[:n], ref["uvs"])

@@ -18,7 +18,7 @@ def test_config0_scene_layout():
     n = np.linalg.norm(m.normals, axis=-1)
     assert np.allclose(n, 1.0, atol=1e-5)
     lo, hi = m.bounds()
-    assert hi[1] > 8.0 and lo[1] == 0.0
+    assert hi[1] > 8.0 and abs(lo[1]) < 1e-6  # the root pitch of 90 degrees in single precision
     assert int(spec.params["min_samples"]) == int(spec.params["max_samples_per_pixel"]) == 64
     assert int(spec.params["max_path_depth"]) == 8
 
