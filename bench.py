@@ -165,11 +165,36 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's render code on the host cores
 # ---------------------------------------------------------------------------
+CONFIG0_GRAMMAR = "F(0.1,0.02)\nF(h,r) -> F(h,r)[Yaw(25.7)F(h,r)]F(h,r)[Yaw(0-25.7)F(h,r)]F(h,r)"
+
+
+def host_stage_times(chk, spec) -> dict:
+    """The reference's host stages: its L-system evaluator, turtle, spline frames
+    and loft on the plain-small grammar (the reference's syntax, 4 iterations,
+    8 sides; oracle/_ref/libptref_gen.so), and its BVH + emissive-CDF build
+    (MeshAccelScene::build, meshAccelBuildBvh) of the workload's mesh."""
+    out = {}
+    try:
+        from oracle.bindings import ReferenceGenerator, reference_generator_available
+        if reference_generator_available():
+            g = ReferenceGenerator().build(CONFIG0_GRAMMAR, 4, rotation_deg=(0.0, 90.0, 0.0), sides=8)
+            out["plain_small_generator"] = {k: round(float(v), 3) for k, v in g["ms"].items()}
+            out["plain_small_generator"]["triangles"] = int(g["positions"].shape[0])
+    except Exception as e:  # reported, never fatal
+        out["plain_small_generator"] = f"unavailable: {e}"
+    t0 = time.perf_counter()
+    sc = chk.scene(spec.mesh)
+    out["bvh_and_scene_build"] = {"ms": round((time.perf_counter() - t0) * 1e3, 1),
+                                  "triangles": int(spec.mesh.triangle_count), "nodes": sc.bvh_node_count()}
+    return out
+
+
 def cpu_render_rate(spec, min_seconds: float = 10.0, max_pixels: int | None = None, seed: int = 0):
     """Times the host render (reference build when present, else the oracle port) on a pixel sample."""
     from oracle.bindings import Checker, reference_available
     kind = "reference" if reference_available() else "port"
     chk = Checker("ref" if kind == "reference" else "oracle")
+    stages = host_stage_times(chk, spec)
     sc = chk.scene(spec.mesh)
     threads = chk.max_threads()
     P = spec.width * spec.height
@@ -198,7 +223,8 @@ def cpu_render_rate(spec, min_seconds: float = 10.0, max_pixels: int | None = No
             break
     return {"value": samples / dt / 1e6, "unit": METRIC, "cores": int(threads), "kind": kind,
             "sample": f"{n} of {P} pixels x up to {spec.waves} samples, {reps} frame(s) ({samples} path samples, "
-                      f"{dt:.1f} s), same scene/camera/params, PCG32 random numbers"}
+                      f"{dt:.1f} s), same scene/camera/params, PCG32 random numbers",
+            "host_stages_ms": stages}
 
 
 def reference_gpu_leg(spec, pt, stream, max_waves: int = 0):
