@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 IMAGE_REL_RMSE = 1e-3
 
 
-def _spectral_pair(tracer, oracle, mesh, camera, params, w, h, waves, stride, env=None, fp64=False):
+def _spectral_pair(tracer, oracle, mesh, camera, params, w, h, waves, stride, env=None, fp64=False, criterion=0):
     tracer.configure(w, h, mesh)
     tracer.set_camera(camera)
     tracer.set_params(params)
@@ -31,7 +31,7 @@ def _spectral_pair(tracer, oracle, mesh, camera, params, w, h, waves, stride, en
     tracer.reset_accumulation()
     tracer.render(waves)
     rgba, counts, conv = tracer.readback()
-    sc = oracle.scene(mesh)
+    sc = oracle.scene(mesh).set_adaptive_criterion(criterion)
     oenv = oracle.env(env) if env is not None else None
     sp = spectral_inputs(mesh, params, int(params["spectral_wavelengths"]), env)
     st = sc.render_spectral(camera, params, w, h, waves, sp, seed_base=1, tape=tape, tape_stride=stride, env=oenv)
@@ -59,6 +59,34 @@ def test_spectral_parity_zoo(tracer, oracle, nw):
     assert np.all(err64 <= 1e-2), f"relative RMSE vs FP64 oracle {err64}"
     # the spectral render is a different image from the RGB one (colours interreflect per wavelength)
     assert np.abs(rgba[:, :3]).sum() > 0
+
+
+def test_spectral_parity_config1_mesh_std_error_adaptive(tracer, oracle):
+    """The headline configuration's path on its own scene: the config-1 tree
+    (972k triangles, so the per-lane closest-hit kernel), 8 hero wavelengths,
+    depth 12 and the relative std-error stop (adaptive_criterion 1), at 48x48
+    and 8-32 spp, against the spectral oracle replaying the GPU's numbers: stop
+    decisions and images."""
+    from lsystemeditor_b200.scene import config1_scene
+    spec = config1_scene()
+    w = h = 48
+    waves = 32
+    cam = spec.camera.copy()
+    cam["aspect"] = 1.0
+    params = spec.params.copy()
+    params["min_samples"] = 8
+    params["max_samples_per_pixel"] = waves
+    params["relative_error_threshold"] = 0.15
+    assert int(params["spectral_wavelengths"]) in (0, 8) and int(params["adaptive_criterion"]) == 1
+    params["spectral_wavelengths"] = 8
+    rgba, counts, st, _ = _spectral_pair(tracer, oracle, spec.mesh, cam, params, w, h, waves, 180, criterion=1)
+    assert tracer.stats()["bvh_nodes"] >= 32768, "the per-lane closest-hit kernel was not used"
+    assert len(np.unique(counts)) > 2
+    agree = np.mean(counts == st["counts"])
+    assert agree > 0.99, f"stop decisions agree on {agree:.4f} of pixels"
+    sel = counts == st["counts"]
+    err = rel_rmse(rgba[sel, :3], st["acc"][sel, :3])
+    assert np.all(err <= IMAGE_REL_RMSE), f"relative RMSE {err}"
 
 
 def test_spectral_parity_environment_map(tracer, oracle):
