@@ -743,103 +743,123 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
         ++sp;
         return true;
     };
+    // Every iteration is warp-synchronous: the idle lanes fetch together at the
+    // top (one ballot, one atomic), the lanes with a ray take one traversal step,
+    // and the warp leaves the loop only when the queue is drained for every lane
+    // and no lane holds a ray.  The full-mask ballot and vote reconverge the warp
+    // once per step, so lanes that took different branches do not go on as
+    // separately scheduled groups.
+    const unsigned int lane = threadIdx.x & 31u;
+    bool drained = false;
     for (;;) {
-        if (!active) {
-            // lanes without a ray take the next queue entries together (one atomic)
-            cg::coalesced_group g = cg::coalesced_threads();
+        const bool want = !active && !drained;
+        const unsigned int wantMask = __ballot_sync(0xFFFFFFFFu, want);
+        if (wantMask != 0u) {
+            const int leader = __ffs(wantMask) - 1;
             unsigned int base = 0;
-            if (g.thread_rank() == 0) {
-                base = atomicAdd(fetch, g.size());
+            if (static_cast<int>(lane) == leader) {
+                base = atomicAdd(fetch, static_cast<unsigned int>(__popc(wantMask)));
             }
-            k = g.shfl(base, 0) + g.thread_rank();
-            if (k >= count) {
-                break; // the queue is drained
-            }
-            i = identity ? k : queue[k];
-            S = &sceneOf(c, i);
-            const float4 o4 = c.paths.orig[i];
-            const float4 d4 = c.paths.dir[i];
-            o = f3(o4.x, o4.y, o4.z);
-            tMin = o4.w;
-            dn = xnormalize(f3(d4.x, d4.y, d4.z));
-            if (S->nodeCount == 0 || isDegenerateDir(dn)) {
-                // empty scene, or quirk Q1: decided here without the wide traversal
-                HitRec h;
-                bool hit = false;
-                h.tri = 0xFFFFFFFFu;
-                if (S->nodeCount != 0) {
-                    hit = traceQ1(*S, o, dn, tMin, kRayTMax, false, h, c.q.overflow);
-                }
-                if (hit) {
-                    c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
-                }
-                queue[k] = hit ? i : (i | 0x80000000u);
-                continue;
-            }
-            idir = f3(__frcp_rn(dn.x), __frcp_rn(dn.y), __frcp_rn(dn.z));
-            const uint32_t oct = (dn.x < 0.0f ? 4u : 0u) | (dn.y < 0.0f ? 2u : 0u) | (dn.z < 0.0f ? 1u : 0u);
-            octinv = 7u - oct;
-            ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
-            tgroup = make_uint2(0u, 0u);
-            sp = 0;
-            closest = kRayTMax;
-            best = 0xFFFFFFFFu;
-            bu = bv = 0.0f;
-            active = true;
-        }
-        // one traversal step (traceRay's loop body)
-        if (ngroup.y > 0x00FFFFFFu) {
-            const uint32_t bit = 31u - __clz(ngroup.y);
-            ngroup.y &= ~(1u << bit);
-            const uint32_t slot = (bit - 24u) ^ octinv;
-            const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
-            if (ngroup.y > 0x00FFFFFFu && !push(ngroup)) {
-                overflow = true;
-            }
-            uint32_t childBase, triBase, imask;
-            const uint32_t hits =
-                intersectChildren(S->nodes, child, o, idir, octinv, tMin, closest, childBase, triBase, imask);
-            ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
-            tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
-        } else {
-            tgroup = ngroup;
-            ngroup = make_uint2(0u, 0u);
-        }
-        while (tgroup.y != 0u) {
-            if (ngroup.y > 0x00FFFFFFu && __popc(__activemask()) < kPostponeLanes && push(tgroup)) {
-                break;
-            }
-            const int kt = __ffs(tgroup.y) - 1;
-            tgroup.y &= tgroup.y - 1u;
-            const TriVerts tv = S->tris[tgroup.x + kt];
-            float t, u, v;
-            if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
-                    f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
-                if (t < closest || best == 0xFFFFFFFFu || leafId(S->tris, tgroup.x + kt) > leafId(S->tris, best)) {
-                    closest = t; // (traceRay's tie rule: the higher original triangle index)
-                    best = tgroup.x + kt;
-                    bu = u;
-                    bv = v;
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (want) {
+                k = base + __popc(wantMask & ((1u << lane) - 1u));
+                if (k >= count) {
+                    drained = true; // the queue is drained
+                } else {
+                    i = identity ? k : queue[k];
+                    S = &sceneOf(c, i);
+                    const float4 o4 = c.paths.orig[i];
+                    const float4 d4 = c.paths.dir[i];
+                    o = f3(o4.x, o4.y, o4.z);
+                    tMin = o4.w;
+                    dn = xnormalize(f3(d4.x, d4.y, d4.z));
+                    if (S->nodeCount == 0 || isDegenerateDir(dn)) {
+                        // empty scene, or quirk Q1: decided here without the wide
+                        // traversal; the lane fetches again next iteration
+                        HitRec h;
+                        bool hit = false;
+                        h.tri = 0xFFFFFFFFu;
+                        if (S->nodeCount != 0) {
+                            hit = traceQ1(*S, o, dn, tMin, kRayTMax, false, h, c.q.overflow);
+                        }
+                        if (hit) {
+                            c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+                        }
+                        queue[k] = hit ? i : (i | 0x80000000u);
+                    } else {
+                        idir = f3(__frcp_rn(dn.x), __frcp_rn(dn.y), __frcp_rn(dn.z));
+                        const uint32_t oct =
+                            (dn.x < 0.0f ? 4u : 0u) | (dn.y < 0.0f ? 2u : 0u) | (dn.z < 0.0f ? 1u : 0u);
+                        octinv = 7u - oct;
+                        ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
+                        tgroup = make_uint2(0u, 0u);
+                        sp = 0;
+                        closest = kRayTMax;
+                        best = 0xFFFFFFFFu;
+                        bu = bv = 0.0f;
+                        active = true;
+                    }
                 }
             }
         }
-        if (ngroup.y <= 0x00FFFFFFu) {
-            if (sp == 0) {
-                // the ray is finished
-                const bool hit = best != 0xFFFFFFFFu && closest < kRayTMax;
-                if (hit) {
-                    c.paths.hit[i] = make_float4(closest, bu, bv, __uint_as_float(leafId(S->tris, best)));
+        if (!__any_sync(0xFFFFFFFFu, active || !drained)) {
+            break;
+        }
+        if (active) {
+            // one traversal step (traceRay's loop body)
+            if (ngroup.y > 0x00FFFFFFu) {
+                const uint32_t bit = 31u - __clz(ngroup.y);
+                ngroup.y &= ~(1u << bit);
+                const uint32_t slot = (bit - 24u) ^ octinv;
+                const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
+                if (ngroup.y > 0x00FFFFFFu && !push(ngroup)) {
+                    overflow = true;
                 }
-                queue[k] = hit ? i : (i | 0x80000000u);
-                if (overflow && c.q.overflow != nullptr) {
-                    atomicAdd(c.q.overflow, 1u); // rays whose stack overflowed, as traceRay counts them
-                }
-                overflow = false;
-                active = false;
-                continue;
+                uint32_t childBase, triBase, imask;
+                const uint32_t hits =
+                    intersectChildren(S->nodes, child, o, idir, octinv, tMin, closest, childBase, triBase, imask);
+                ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
+                tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
+            } else {
+                tgroup = ngroup;
+                ngroup = make_uint2(0u, 0u);
             }
-            --sp;
-            ngroup = sp < kSharedStack ? sstack[sp * sstride] : stack[sp - kSharedStack];
+            while (tgroup.y != 0u) {
+                if (ngroup.y > 0x00FFFFFFu && __popc(__activemask()) < kPostponeLanes && push(tgroup)) {
+                    break;
+                }
+                const int kt = __ffs(tgroup.y) - 1;
+                tgroup.y &= tgroup.y - 1u;
+                const TriVerts tv = S->tris[tgroup.x + kt];
+                float t, u, v;
+                if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                        f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
+                    if (t < closest || best == 0xFFFFFFFFu || leafId(S->tris, tgroup.x + kt) > leafId(S->tris, best)) {
+                        closest = t; // (traceRay's tie rule: the higher original triangle index)
+                        best = tgroup.x + kt;
+                        bu = u;
+                        bv = v;
+                    }
+                }
+            }
+            if (ngroup.y <= 0x00FFFFFFu) {
+                if (sp == 0) {
+                    // the ray is finished
+                    const bool hit = best != 0xFFFFFFFFu && closest < kRayTMax;
+                    if (hit) {
+                        c.paths.hit[i] = make_float4(closest, bu, bv, __uint_as_float(leafId(S->tris, best)));
+                    }
+                    queue[k] = hit ? i : (i | 0x80000000u);
+                    if (overflow && c.q.overflow != nullptr) {
+                        atomicAdd(c.q.overflow, 1u); // rays whose stack overflowed, as traceRay counts them
+                    }
+                    overflow = false;
+                    active = false;
+                } else {
+                    --sp;
+                    ngroup = sp < kSharedStack ? sstack[sp * sstride] : stack[sp - kSharedStack];
+                }
+            }
         }
     }
 }
