@@ -575,7 +575,7 @@ def batch_accuracy(tubes, cams, sizes, params, images, pixels_per_scene: int = 1
     threads = chk.max_threads()
     rng = np.random.default_rng(seed)
     lum = np.array([0.2126, 0.7152, 0.0722])
-    terms, per_scene = [], {}
+    terms, caps, per_scene = [], [], {}
     t0 = time.perf_counter()
     for k, img in images.items():
         w, h = sizes[k]
@@ -589,14 +589,22 @@ def batch_accuracy(tubes, cams, sizes, params, images, pixels_per_scene: int = 1
         st = sc.render(cams[k], p, w, h, ref_spp, seed_base=900_001, pixels=pix, threads=threads, fp64=True)
         r = st["lum_mean"][pix]
         var_r = st["m2"][pix] / float(ref_spp) / float(ref_spp)
-        x = img[..., :3].reshape(-1, 3).astype(np.float64)[pix] @ lum
+        rgba, counts = img
+        x = rgba[..., :3].reshape(-1, 3).astype(np.float64)[pix] @ lum
         keep = r > 1e-4
         t = ((x - r) ** 2 - var_r)[keep] / (r[keep] ** 2)
+        capped = (counts.reshape(-1)[pix] >= int(params["max_samples_per_pixel"]))[keep]
         terms.append(t)
+        caps.append(capped)
         per_scene[int(k)] = {"pixels": int(keep.sum()), "relmse": float(t.mean()) if keep.any() else None,
-                             "triangles": int(tubes[k].triangle_count)}
+                             "at_cap": int(capped.sum()), "triangles": int(tubes[k].triangle_count)}
     allt = np.concatenate(terms) if terms else np.zeros(0)
+    allc = np.concatenate(caps) if caps else np.zeros(0, bool)
     return {"relmse": float(allt.mean()) if len(allt) else None, "pixels": int(len(allt)),
+            "median_sq_rel_err": float(np.median(allt)) if len(allt) else None,
+            "pixels_at_cap": int(allc.sum()),
+            "relmse_pixels_at_cap": float(allt[allc].mean()) if allc.any() else None,
+            "relmse_pixels_stopped": float(allt[~allc].mean()) if (~allc).any() else None,
             "scenes": per_scene, "reference": f"FP64 oracle, {ref_spp} samples per pixel, independent random "
             f"numbers, {threads} host threads", "measure": "luminance relative MSE, reference variance "
             "subtracted", "oracle_s": round(time.perf_counter() - t0, 1)}
@@ -743,7 +751,7 @@ def run_batch(args):
     # the same scenes one per render (the plain drop-in), device-built likewise
     # images of the scenes whose accuracy is checked against the FP64 oracle
     acc_scenes = batch_accuracy_scenes(all_tubes) if (world == 1 and not args.no_accuracy) else []
-    acc_images = {k: pt.batch_readback(k)[0] for k in acc_scenes}
+    acc_images = {k: pt.batch_readback(k)[:2] for k in acc_scenes}
 
     plain_ms, plain_samples, plain_build_ms = 0.0, 0, 0.0
     for k in range(n):

@@ -223,8 +223,10 @@ struct pt_renderer {
     DevBuf<unsigned int> qOverflow;
     int gridExtend = 0, gridShade = 0, gridShadow = 0;
     int gridExtendLane = 0;          // grid of the per-lane closest-hit kernel
+    int gridShadowLane = 0;          // grid of the per-lane shadow kernel
     int gridShadeMiss = 0;           // grid of the miss shader (its own occupancy)
     bool extendLane = false;         // per-lane ray replacement in this render's closest-hit stage
+    bool sceneBinning = true;        // batches: next-bounce queue grouped by scene per tile
     int extendMode = PT_EXTEND_MODE_AUTO;
     // CUDA graphs of four bounce iterations (the first block of a batch, later
     // blocks) and the launch configuration they were captured for
@@ -375,6 +377,7 @@ int ensurePaths(pt_renderer* r, int capacity)
 // whose queue order does not matter to it, the shade kernels read consecutive
 // slots' path state.
 bool slotOrdered(const pt_renderer* r) { return PT_SLOT_ORDER && r->extendLane; }
+bool sceneBinned(const pt_renderer* r) { return slotOrdered(r) && r->sceneBinning && r->scenes.size() > 1; }
 
 LaunchCtx makeCtx(pt_renderer* r)
 {
@@ -1207,6 +1210,10 @@ int extendGrid(const pt_renderer* r, bool count, bool inst)
 {
     return (r->extendLane && !count && !inst) ? r->gridExtendLane : r->gridExtend;
 }
+int shadowGrid(const pt_renderer* r, bool count, bool inst)
+{
+    return (r->extendLane && !count && !inst) ? r->gridShadowLane : r->gridShadow;
+}
 
 // The graphs of four bounce iterations for this launch configuration
 // (captured on first use; false: run without graphs, e.g. when the caller's
@@ -1216,8 +1223,10 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
     const unsigned long long key[6] = {reinterpret_cast<unsigned long long>(c), static_cast<unsigned long long>(r->gridExtend),
         static_cast<unsigned long long>(r->gridShade), static_cast<unsigned long long>(r->gridShadow),
         static_cast<unsigned long long>(inst ? 1 : 0) | (static_cast<unsigned long long>(nw) << 1) |
+            (static_cast<unsigned long long>(sceneBinned(r) ? 1 : 0) << 6) |
             (static_cast<unsigned long long>(r->extendLane ? 1 : 0) << 8) |
             (static_cast<unsigned long long>(r->gridExtendLane) << 9) |
+            (static_cast<unsigned long long>(r->gridShadowLane) << 22) |
             (static_cast<unsigned long long>(r->gridShadeMiss) << 36),
         reinterpret_cast<unsigned long long>(r->stream)};
     if (r->bounceGraph[0] != nullptr && std::equal(key, key + 6, r->bounceKey)) {
@@ -1240,10 +1249,10 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
             launchExtend(c, sel, g == 0 && it == 0, it, extendGrid(r, false, inst), false, inst, r->extendLane, s);
             launchShadeMiss(c, it, sel, r->gridShadeMiss, nw, s);
             launchShade(c, sel, it, r->gridShade, nw, s);
-            launchShadow(c, it, r->gridShadow, false, inst, s);
+            launchShadow(c, it, shadowGrid(r, false, inst), false, inst, r->extendLane, s);
             launchFinalize(c, sel, r->gridShadow, nw, s);
             if (slotOrdered(r)) {
-                launchNextQueue(c, sel, r->gridShadow, s);
+                launchNextQueue(c, sel, r->gridShadow, sceneBinned(r), s);
             }
             sel ^= 1;
         }
@@ -1301,6 +1310,7 @@ int pt_create(pt_renderer** out, int device)
     r->gridShade = r->smCount * std::max(bs, 1);
     r->gridShadow = r->smCount * std::max(bsh, 1);
     r->gridExtendLane = r->smCount * extendLaneOccupancy();
+    r->gridShadowLane = r->smCount * shadowLaneOccupancy();
     r->gridShadeMiss = r->smCount * shadeMissOccupancy();
     *out = r;
     return PT_OK;
@@ -1699,13 +1709,13 @@ int pt_render(pt_renderer* r, int waves)
             }
             {
                 StageTimer tm(r, kShadow);
-                launchShadow(c, iter, r->gridShadow, countVisits, inst, s);
+                launchShadow(c, iter, shadowGrid(r, countVisits, inst), countVisits, inst, r->extendLane, s);
             }
             {
                 StageTimer tm(r, kFinalize);
                 launchFinalize(c, sel, r->gridShadow, nw, s);
                 if (slotOrdered(r)) {
-                    launchNextQueue(c, sel, r->gridShadow, s);
+                    launchNextQueue(c, sel, r->gridShadow, sceneBinned(r), s);
                 }
             }
             launches += 4 + extendKernels(countVisits, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0);
@@ -1952,6 +1962,15 @@ int pt_set_extend_mode(pt_renderer* r, int mode)
     return PT_OK;
 }
 
+int pt_set_scene_binning(pt_renderer* r, int on)
+{
+    if (r == nullptr || (on != 0 && on != 1)) {
+        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_scene_binning: on must be 0 or 1");
+    }
+    r->sceneBinning = on != 0;
+    return PT_OK;
+}
+
 int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
 {
     if (r == nullptr || path_capacity < 0 || blocks_per_sm < 0 || path_capacity > (1 << 26)) {
@@ -1962,6 +1981,7 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
     if (blocks_per_sm > 0) {
         r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
         r->gridExtendLane = r->smCount * std::min(blocks_per_sm, extendLaneOccupancy());
+        r->gridShadowLane = r->smCount * std::min(blocks_per_sm, shadowLaneOccupancy());
         r->gridShadeMiss = r->smCount * std::min(blocks_per_sm, shadeMissOccupancy());
     } else {
         int be = 1, bs = 1, bsh = 1;
@@ -1970,6 +1990,7 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
         r->gridShade = r->smCount * std::max(bs, 1);
         r->gridShadow = r->smCount * std::max(bsh, 1);
         r->gridExtendLane = r->smCount * extendLaneOccupancy();
+        r->gridShadowLane = r->smCount * shadowLaneOccupancy();
         r->gridShadeMiss = r->smCount * shadeMissOccupancy();
     }
     return PT_OK;

@@ -685,45 +685,46 @@ __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const Laun
 #ifndef PT_EXTEND_LANE_MIN_BLOCKS
 #define PT_EXTEND_LANE_MIN_BLOCKS 3
 #endif
+#ifndef PT_SHADOW_LANE_MIN_BLOCKS
+#define PT_SHADOW_LANE_MIN_BLOCKS 4
+#endif
 
-// Closest hit with per-lane ray replacement (Aila & Laine 2009, "dynamic
-// fetch"): a lane whose ray is finished takes the next queue entry at once,
-// while the other lanes of its warp go on traversing, so a warp is not held
-// by its longest ray.  One loop iteration is one step of traceRay's
-// traversal (a node's children, then the triangles of that node), with the
-// same postponing, stacks and tie rule, so the hits are traceRay's.  Rays
-// finish in no particular order; the result of queue entry k goes back into
-// entry k (path index, bit 31 set for a miss) and k_route splits the queue
-// into the miss and hit queues in queue order afterwards.  Flat scenes only
-// (no instances, no visit counting).
-__global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLOCKS)
-    k_extend_lane(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
+// A ray of the per-lane traversal: its scene, origin, normalised direction and
+// the parametric interval it is tested on.
+struct LaneRay {
+    const DevScene* S;
+    float3 o;
+    float3 dn;
+    float tMin;
+    float tMax;
+};
+
+// Per-lane ray replacement (Aila & Laine 2009, "dynamic fetch") over a queue of
+// `count` rays of flat scenes: a lane whose ray is finished takes the next
+// queue entry at once, while the other lanes of its warp go on traversing, so
+// a warp is not held by its longest ray.  One loop iteration is one step of
+// traceRay's traversal (a node's children, then the triangles of that node),
+// with the same postponing, stacks and tie rule, so the results are
+// traceRay's.  Every iteration is warp-synchronous: the idle lanes fetch
+// together at the top (one ballot, one atomic), the lanes with a ray take one
+// traversal step, and the warp leaves the loop only when the queue is drained
+// for every lane and no lane holds a ray; the full-mask ballot and vote
+// reconverge the warp once per step, so lanes that took different branches do
+// not go on as separately scheduled groups.
+//   load(k, ray) -> bool: reads queue entry k into `ray`; false when the entry
+//     was decided without the wide traversal (and its result written).
+//   finish(k, hit, t, u, v, tri): the result of entry k (tri = original
+//     triangle index; for AnyHit, hit means occluded and t, u, v, tri are unset).
+// Rays finish in no particular order.
+template <bool AnyHit, class Load, class Finish>
+__device__ __forceinline__ void laneTraversal(unsigned int count, unsigned int* fetch, uint2* sstack, int sstride,
+    unsigned int* overflowCounter, Load load, Finish finish)
 {
-    const LaunchCtx& c = *cp;
-    extern __shared__ uint2 smemStack[];
-    const unsigned int count = c.q.counts[sel];
-    const int par = iter & 1;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        atomicAdd(&c.q.rays[0], static_cast<unsigned long long>(count));
-        c.q.counts[sel ^ 1] = 0u;
-        c.q.counts[2] = 0u;
-        c.q.counts[3] = 0u;
-        c.q.counts[4 + 2 * (par ^ 1)] = 0u;
-        c.q.counts[5 + 2 * (par ^ 1)] = 0u;
-        c.q.counts[8 + (par ^ 1)] = 0u;
-    }
-    uint32_t* queue = c.q.extend[sel];
-    unsigned int* fetch = &c.q.counts[8 + par];
-    uint2* sstack = smemStack + threadIdx.x;
-    const int sstride = blockDim.x;
     uint2 stack[kTraversalStack];
-
     bool active = false;
     unsigned int k = 0;
-    uint32_t i = 0;
-    const DevScene* S = nullptr;
-    float3 o = f3(0.0f, 0.0f, 0.0f), dn = o, idir = o;
-    float tMin = 0.0f;
+    LaneRay r{nullptr, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), 0.0f, 0.0f};
+    float3 idir = r.o;
     uint32_t octinv = 0;
     uint2 ngroup = make_uint2(0u, 0u), tgroup = make_uint2(0u, 0u);
     int sp = 0;
@@ -743,12 +744,14 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
         ++sp;
         return true;
     };
-    // Every iteration is warp-synchronous: the idle lanes fetch together at the
-    // top (one ballot, one atomic), the lanes with a ray take one traversal step,
-    // and the warp leaves the loop only when the queue is drained for every lane
-    // and no lane holds a ray.  The full-mask ballot and vote reconverge the warp
-    // once per step, so lanes that took different branches do not go on as
-    // separately scheduled groups.
+    auto done = [&](bool hit) {
+        finish(k, hit, closest, bu, bv, hit && !AnyHit ? leafId(r.S->tris, best) : 0xFFFFFFFFu);
+        if (overflow && overflowCounter != nullptr) {
+            atomicAdd(overflowCounter, 1u); // rays whose stack overflowed, as traceRay counts them
+        }
+        overflow = false;
+        active = false;
+    };
     const unsigned int lane = threadIdx.x & 31u;
     bool drained = false;
     for (;;) {
@@ -765,41 +768,20 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
                 k = base + __popc(wantMask & ((1u << lane) - 1u));
                 if (k >= count) {
                     drained = true; // the queue is drained
-                } else {
-                    i = identity ? k : queue[k];
-                    S = &sceneOf(c, i);
-                    const float4 o4 = c.paths.orig[i];
-                    const float4 d4 = c.paths.dir[i];
-                    o = f3(o4.x, o4.y, o4.z);
-                    tMin = o4.w;
-                    dn = xnormalize(f3(d4.x, d4.y, d4.z));
-                    if (S->nodeCount == 0 || isDegenerateDir(dn)) {
-                        // empty scene, or quirk Q1: decided here without the wide
-                        // traversal; the lane fetches again next iteration
-                        HitRec h;
-                        bool hit = false;
-                        h.tri = 0xFFFFFFFFu;
-                        if (S->nodeCount != 0) {
-                            hit = traceQ1(*S, o, dn, tMin, kRayTMax, false, h, c.q.overflow);
-                        }
-                        if (hit) {
-                            c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
-                        }
-                        queue[k] = hit ? i : (i | 0x80000000u);
-                    } else {
-                        idir = f3(__frcp_rn(dn.x), __frcp_rn(dn.y), __frcp_rn(dn.z));
-                        const uint32_t oct =
-                            (dn.x < 0.0f ? 4u : 0u) | (dn.y < 0.0f ? 2u : 0u) | (dn.z < 0.0f ? 1u : 0u);
-                        octinv = 7u - oct;
-                        ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
-                        tgroup = make_uint2(0u, 0u);
-                        sp = 0;
-                        closest = kRayTMax;
-                        best = 0xFFFFFFFFu;
-                        bu = bv = 0.0f;
-                        active = true;
-                    }
+                } else if (load(k, r)) {
+                    idir = f3(__frcp_rn(r.dn.x), __frcp_rn(r.dn.y), __frcp_rn(r.dn.z));
+                    const uint32_t oct =
+                        (r.dn.x < 0.0f ? 4u : 0u) | (r.dn.y < 0.0f ? 2u : 0u) | (r.dn.z < 0.0f ? 1u : 0u);
+                    octinv = 7u - oct;
+                    ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
+                    tgroup = make_uint2(0u, 0u);
+                    sp = 0;
+                    closest = r.tMax;
+                    best = 0xFFFFFFFFu;
+                    bu = bv = 0.0f;
+                    active = true;
                 }
+                // (an entry decided by load leaves the lane idle: it fetches again)
             }
         }
         if (!__any_sync(0xFFFFFFFFu, active || !drained)) {
@@ -817,24 +799,31 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
                 }
                 uint32_t childBase, triBase, imask;
                 const uint32_t hits =
-                    intersectChildren(S->nodes, child, o, idir, octinv, tMin, closest, childBase, triBase, imask);
+                    intersectChildren(r.S->nodes, child, r.o, idir, octinv, r.tMin, closest, childBase, triBase, imask);
                 ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
                 tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
             } else {
                 tgroup = ngroup;
                 ngroup = make_uint2(0u, 0u);
             }
+            bool occluded = false;
             while (tgroup.y != 0u) {
                 if (ngroup.y > 0x00FFFFFFu && __popc(__activemask()) < kPostponeLanes && push(tgroup)) {
                     break;
                 }
                 const int kt = __ffs(tgroup.y) - 1;
                 tgroup.y &= tgroup.y - 1u;
-                const TriVerts tv = S->tris[tgroup.x + kt];
+                const TriVerts tv = r.S->tris[tgroup.x + kt];
                 float t, u, v;
-                if (intersectTriExact(o, dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
-                        f3(tv.v2.x, tv.v2.y, tv.v2.z), tMin, closest, t, u, v)) {
-                    if (t < closest || best == 0xFFFFFFFFu || leafId(S->tris, tgroup.x + kt) > leafId(S->tris, best)) {
+                if (intersectTriExact(r.o, r.dn, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                        f3(tv.v2.x, tv.v2.y, tv.v2.z), r.tMin, closest, t, u, v)) {
+                    if (AnyHit) {
+                        if (t < r.tMax) {
+                            occluded = true; // traceRay's any-hit: the first hit below tMax ends the ray
+                            break;
+                        }
+                    } else if (t < closest || best == 0xFFFFFFFFu ||
+                               leafId(r.S->tris, tgroup.x + kt) > leafId(r.S->tris, best)) {
                         closest = t; // (traceRay's tie rule: the higher original triangle index)
                         best = tgroup.x + kt;
                         bu = u;
@@ -842,19 +831,12 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
                     }
                 }
             }
-            if (ngroup.y <= 0x00FFFFFFu) {
+            if (occluded) {
+                done(true);
+            } else if (ngroup.y <= 0x00FFFFFFu) {
                 if (sp == 0) {
                     // the ray is finished
-                    const bool hit = best != 0xFFFFFFFFu && closest < kRayTMax;
-                    if (hit) {
-                        c.paths.hit[i] = make_float4(closest, bu, bv, __uint_as_float(leafId(S->tris, best)));
-                    }
-                    queue[k] = hit ? i : (i | 0x80000000u);
-                    if (overflow && c.q.overflow != nullptr) {
-                        atomicAdd(c.q.overflow, 1u); // rays whose stack overflowed, as traceRay counts them
-                    }
-                    overflow = false;
-                    active = false;
+                    done(!AnyHit && best != 0xFFFFFFFFu && closest < r.tMax);
                 } else {
                     --sp;
                     ngroup = sp < kSharedStack ? sstack[sp * sstride] : stack[sp - kSharedStack];
@@ -862,6 +844,119 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
             }
         }
     }
+}
+
+// Closest hit of every queued path by the per-lane traversal.  The result of
+// queue entry k goes back into entry k (path index, bit 31 set for a miss) and
+// k_route splits the queue into the miss and hit queues in queue order
+// afterwards.  Flat scenes only (no instances, no visit counting).
+__global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLOCKS)
+    k_extend_lane(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
+{
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
+    const unsigned int count = c.q.counts[sel];
+    const int par = iter & 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&c.q.rays[0], static_cast<unsigned long long>(count));
+        c.q.counts[sel ^ 1] = 0u;
+        c.q.counts[2] = 0u;
+        c.q.counts[3] = 0u;
+        c.q.counts[4 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[5 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[8 + (par ^ 1)] = 0u;
+    }
+    uint32_t* queue = c.q.extend[sel];
+    uint32_t i = 0;
+    laneTraversal<false>(count, &c.q.counts[8 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
+        c.q.overflow,
+        [&](unsigned int k, LaneRay& r) -> bool {
+            i = identity ? k : queue[k];
+            r.S = &sceneOf(c, i);
+            const float4 o4 = c.paths.orig[i];
+            const float4 d4 = c.paths.dir[i];
+            r.o = f3(o4.x, o4.y, o4.z);
+            r.tMin = o4.w;
+            r.tMax = kRayTMax;
+            r.dn = xnormalize(f3(d4.x, d4.y, d4.z));
+            if (r.S->nodeCount != 0 && !isDegenerateDir(r.dn)) {
+                return true;
+            }
+            // empty scene, or quirk Q1: decided here without the wide traversal
+            HitRec h;
+            bool hit = false;
+            h.tri = 0xFFFFFFFFu;
+            if (r.S->nodeCount != 0) {
+                hit = traceQ1(*r.S, r.o, r.dn, r.tMin, kRayTMax, false, h, c.q.overflow);
+            }
+            if (hit) {
+                c.paths.hit[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+            }
+            queue[k] = hit ? i : (i | 0x80000000u);
+            return false;
+        },
+        [&](unsigned int k, bool hit, float t, float u, float v, uint32_t tri) {
+            if (hit) {
+                c.paths.hit[i] = make_float4(t, u, v, __uint_as_float(tri));
+            }
+            queue[k] = hit ? i : (i | 0x80000000u);
+        });
+}
+
+// Occlusion of every queued shadow ray by the per-lane traversal (any hit
+// below the ray's tMax); unoccluded rays mark their path's pending NEE
+// contribution visible.  Flat scenes only (no instances, no visit counting).
+__global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_SHADOW_LANE_MIN_BLOCKS)
+    k_shadow_lane(const LaunchCtx* __restrict__ cp, int iter)
+{
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
+    const unsigned int count = c.q.counts[2];
+    const int par = iter & 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&c.q.rays[1], static_cast<unsigned long long>(count));
+        c.q.counts[10 + (par ^ 1)] = 0u; // next shadow stage's fetch counter
+    }
+    uint32_t e = 0;
+    laneTraversal<true>(count, &c.q.counts[10 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
+        c.q.overflow,
+        [&](unsigned int k, LaneRay& r) -> bool {
+            e = c.q.shadowPath[k];
+            r.S = &sceneOf(c, e & 0x7FFFFFFFu);
+            const float4 o4 = c.q.shadowOrig[k];
+            const float4 d4 = c.q.shadowDir[k];
+            r.o = f3(o4.x, o4.y, o4.z);
+            r.dn = xnormalize(f3(d4.x, d4.y, d4.z));
+            r.tMin = kShadowBias;
+            r.tMax = d4.w > 0.0f ? d4.w : kRayTMax; // emitter MIS rays end short of the light
+            bool occluded = false;
+            if (r.S->nodeCount != 0) {
+                if (!isDegenerateDir(r.dn)) {
+                    return true;
+                }
+                HitRec h;
+                occluded = traceQ1(*r.S, r.o, r.dn, r.tMin, r.tMax, true, h, c.q.overflow);
+            }
+            if (!occluded) {
+                const uint32_t i = e & 0x7FFFFFFFu;
+                if (e & 0x80000000u) {
+                    c.paths.visEmis[i] = 1;
+                } else {
+                    c.paths.visEnv[i] = 1;
+                }
+            }
+            return false;
+        },
+        [&](unsigned int, bool occluded, float, float, float, uint32_t) {
+            if (!occluded) {
+                const uint32_t i = e & 0x7FFFFFFFu;
+                if (e & 0x80000000u) {
+                    c.paths.visEmis[i] = 1;
+                } else {
+                    c.paths.visEnv[i] = 1;
+                }
+            }
+        });
 }
 
 // Splits the queue that k_extend_lane marked into the miss and hit queues of
@@ -990,6 +1085,71 @@ __global__ void __launch_bounds__(256) k_next_queue(const LaunchCtx* __restrict_
             if ((mask[r] >> lane) & 1u) {
                 out[sBase + sOff[r * 8 + warp] + __popc(mask[r] & below)] =
                     t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Batches of several scenes: the same tile pass, with each tile's entries
+// written grouped by scene (a counting sort of the tile in shared memory over
+// the scene index modulo kSceneBins), so that the warps of the next extend and
+// shade stages mostly hold paths of one scene and read one scene's records.
+// Paths in flight span several scenes because a recycled slot takes the next
+// job in scene-major order whenever its path ends.  Within a bin the entries
+// keep no particular order; no result depends on the queue order.
+constexpr int kSceneBins = 256;
+static_assert(kSceneBins == 256, "k_next_queue_binned clears and scans one bin per thread of its 256-thread blocks");
+__global__ void __launch_bounds__(256) k_next_queue_binned(const LaunchCtx* __restrict__ cp, int sel)
+{
+    const LaunchCtx& c = *cp;
+    const unsigned int n = static_cast<unsigned int>(c.q.batch->slotCount);
+    uint8_t* flag = c.q.nextFlag;
+    uint32_t* out = c.q.extend[sel ^ 1];
+    __shared__ unsigned int sBin[kSceneBins];
+    __shared__ unsigned int sWarp[8];
+    __shared__ unsigned int sBase;
+    const unsigned int lane = threadIdx.x & 31u;
+    const unsigned int below = (1u << lane) - 1u;
+    const unsigned int tile = 256u * kRouteRows;
+    for (unsigned int t0 = blockIdx.x * tile; t0 < n; t0 += gridDim.x * tile) {
+        sBin[threadIdx.x] = 0u;
+        __syncthreads();
+        unsigned int bin[kRouteRows], rank[kRouteRows];
+#pragma unroll
+        for (int r = 0; r < kRouteRows; ++r) {
+            const unsigned int k = t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
+            const bool on = k < n && flag[k] != 0;
+            if (on) {
+                flag[k] = 0;
+            }
+            const unsigned int b = on ? (static_cast<unsigned int>(c.paths.scene[k]) & (kSceneBins - 1u)) : 0xFFFFFFFFu;
+            // lanes of one bin take consecutive ranks with one shared atomic
+            const unsigned int peers = __match_any_sync(0xFFFFFFFFu, b);
+            unsigned int rk = 0u;
+            if (on) {
+                const int leader = __ffs(peers) - 1;
+                unsigned int base = 0u;
+                if (static_cast<int>(lane) == leader) {
+                    base = atomicAdd(&sBin[b], static_cast<unsigned int>(__popc(peers)));
+                }
+                rk = __shfl_sync(peers, base, leader) + __popc(peers & below);
+            }
+            bin[r] = b;
+            rank[r] = rk;
+        }
+        __syncthreads();
+        unsigned int total = 0u;
+        const unsigned int start = blockExclusiveScan(sBin[threadIdx.x], sWarp, &total);
+        sBin[threadIdx.x] = start;
+        if (threadIdx.x == 0) {
+            sBase = total ? atomicAdd(&c.q.counts[sel ^ 1], total) : 0u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kRouteRows; ++r) {
+            if (bin[r] != 0xFFFFFFFFu) {
+                out[sBase + sBin[bin[r]] + rank[r]] = t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
             }
         }
         __syncthreads();
@@ -1721,9 +1881,20 @@ int extendKernels(bool count, bool inst, bool lane)
 {
     return (!inst && !count && lane) ? 2 : 1;
 }
-void launchNextQueue(const LaunchCtx* c, int sel, int grid, cudaStream_t s)
+void launchNextQueue(const LaunchCtx* c, int sel, int grid, bool binned, cudaStream_t s)
 {
-    k_next_queue<<<grid, 256, 0, s>>>(c, sel);
+    if (binned) {
+        k_next_queue_binned<<<grid, 256, 0, s>>>(c, sel);
+    } else {
+        k_next_queue<<<grid, 256, 0, s>>>(c, sel);
+    }
+}
+int shadowLaneOccupancy()
+{
+    int blocks = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_shadow_lane, PT_EXTEND_LANE_THREADS,
+        sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS);
+    return blocks > 0 ? blocks : 1;
 }
 int shadeMissOccupancy()
 {
@@ -1758,10 +1929,13 @@ void launchShade(const LaunchCtx* c, int sel, int iter, int grid, int nw, cudaSt
         k_shade<0><<<grid, 256, 0, s>>>(c, sel, iter);
     }
 }
-void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, bool inst, cudaStream_t s)
+void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, bool inst, bool lane, cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
-    if (inst) {
+    if (lane && !inst && !count) {
+        k_shadow_lane<<<grid, PT_EXTEND_LANE_THREADS, sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS, s>>>(c,
+            iter);
+    } else if (inst) {
         if (count) {
             k_shadow<true, true><<<grid, 256, smem, s>>>(c, iter);
         } else {

@@ -160,11 +160,14 @@ int extendKernels(bool count, bool inst, bool lane);
 // Resident blocks per SM of the per-lane closest-hit kernel and of the miss shader.
 int extendLaneOccupancy();
 int shadeMissOccupancy();
+int shadowLaneOccupancy();
 // Slot-ordered mode: the next bounce's extend queue from the marked slots.
-void launchNextQueue(const LaunchCtx* d, int sel, int grid, cudaStream_t s);
+void launchNextQueue(const LaunchCtx* d, int sel, int grid, bool binned, cudaStream_t s);
 void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, int nw, cudaStream_t s);
 void launchShade(const LaunchCtx* d, int sel, int iter, int grid, int nw, cudaStream_t s);
-void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, bool inst, cudaStream_t s);
+// Shadow stage.  lane: per-lane ray replacement (k_shadow_lane; flat scenes,
+// no visit counting), else one warp per 32 queued rays (k_shadow).
+void launchShadow(const LaunchCtx* d, int iter, int grid, bool count, bool inst, bool lane, cudaStream_t s);
 void launchFinalize(const LaunchCtx* d, int sel, int grid, int nw, cudaStream_t s);
 void launchAccumulate(const LaunchCtx* d, int activeCount, int batch, cudaStream_t s);
 // Stable compaction of the active list (pixels neither converged nor at the

@@ -7,9 +7,10 @@
 //
 //   wrapper_check <scene.bin> <image.bin>
 //
-// scene.bin: int32 w, h, spp, triangle count n, material count m; then n
-// HostTriangle-equivalents as 24 floats (v0 v1 v2 n0 n1 n2 uv0 uv1 uv2) + one
-// uint32 material index each; m MaterialGpu records; one CameraGpu.
+// scene.bin: int32 w, h, spp, triangle count n, material count m, texture
+// count t; then n HostTriangle-equivalents as 24 floats (v0 v1 v2 n0 n1 n2 uv0
+// uv1 uv2) + one uint32 material index each; m MaterialGpu records; t
+// TextureDescGpu records; one CameraGpu.
 #include "PathTracerB200.h"
 
 #include <cstdio>
@@ -25,8 +26,9 @@ int main(int argc, char** argv)
     if (f == nullptr) {
         return 2;
     }
-    int32_t hdr[5] = {};
-    if (std::fread(hdr, sizeof(int32_t), 5, f) != 5 || hdr[0] <= 0 || hdr[1] <= 0 || hdr[3] < 0 || hdr[4] < 0) {
+    int32_t hdr[6] = {};
+    if (std::fread(hdr, sizeof(int32_t), 6, f) != 6 || hdr[0] <= 0 || hdr[1] <= 0 || hdr[3] < 0 || hdr[4] < 0 ||
+        hdr[5] < 0) {
         return 2;
     }
     HostMesh mesh;
@@ -51,6 +53,11 @@ int main(int argc, char** argv)
     mesh.materials.resize(static_cast<size_t>(hdr[4]));
     if (hdr[4] > 0 && std::fread(mesh.materials.data(), sizeof(MaterialGpu), mesh.materials.size(), f) !=
             mesh.materials.size()) {
+        return 2;
+    }
+    mesh.textures.resize(static_cast<size_t>(hdr[5]));
+    if (hdr[5] > 0 && std::fread(mesh.textures.data(), sizeof(TextureDescGpu), mesh.textures.size(), f) !=
+            mesh.textures.size()) {
         return 2;
     }
     CameraGpu cam{};

@@ -26,7 +26,8 @@ def test_cxx_wrapper_renders_like_the_python_binding(tracer):
     with tempfile.TemporaryDirectory() as tmp:
         scene, image = os.path.join(tmp, "scene.bin"), os.path.join(tmp, "image.bin")
         with open(scene, "wb") as f:
-            np.array([w, h, spp, mesh.triangle_count, len(mesh.materials)], np.int32).tofile(f)
+            textures = mesh.textures if mesh.textures is not None else np.zeros(0, np.uint8)
+            np.array([w, h, spp, mesh.triangle_count, len(mesh.materials), len(textures)], np.int32).tofile(f)
             tri = np.concatenate([mesh.positions.reshape(-1, 9), mesh.normals.reshape(-1, 9),
                                   mesh.uvs.reshape(-1, 6)], axis=1).astype(np.float32)
             rec = np.zeros(mesh.triangle_count, [("f", "<f4", (24,)), ("m", "<u4")])
@@ -34,6 +35,7 @@ def test_cxx_wrapper_renders_like_the_python_binding(tracer):
             rec["m"] = mesh.material_ids
             rec.tofile(f)
             mesh.materials.tofile(f)
+            textures.tofile(f)
             np.asarray(cam).tofile(f)
         r = subprocess.run([WRAPPER_BIN, scene, image], capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stdout + r.stderr
@@ -43,6 +45,7 @@ def test_cxx_wrapper_renders_like_the_python_binding(tracer):
     params = default_params(background_r=0.1, background_g=0.1, background_b=0.1, max_path_depth=6,
                             min_samples=spp, max_samples_per_pixel=spp)
     tracer.configure(w, h, mesh)
+    tracer.set_environment(None)
     tracer.set_camera(cam)
     tracer.set_params(params)
     tracer.reset_accumulation()

@@ -76,7 +76,9 @@ def test_spectral_parity_config1_mesh_std_error_adaptive(tracer, oracle):
     params = spec.params.copy()
     params["min_samples"] = 8
     params["max_samples_per_pixel"] = waves
-    params["relative_error_threshold"] = 0.15
+    # (most pixels of this view are foliage or in shadow and run to the cap at
+    # any useful threshold; 0.8 stops a few dozen of them at different counts)
+    params["relative_error_threshold"] = 0.8
     assert int(params["spectral_wavelengths"]) in (0, 8) and int(params["adaptive_criterion"]) == 1
     params["spectral_wavelengths"] = 8
     rgba, counts, st, _ = _spectral_pair(tracer, oracle, spec.mesh, cam, params, w, h, waves, 180, criterion=1)
