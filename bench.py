@@ -70,13 +70,14 @@ def parse_args():
                     help="skip the leg that times the reference's own CUDA kernels on this GPU")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: keep the default scheduling knobs")
     ap.add_argument("--estimator", choices=["mis", "reference"], default="mis",
-                    help="batch workload: the emitter MIS estimator (reaches the relative-MSE target) or the "
+                    help="batch workload: the emitter MIS estimator (short emissive shadow rays) or the "
                          "reference's estimator (emitters found by BSDF sampling only)")
     ap.add_argument("--rel-err", type=float, default=0.02,
                     help="batch workload: per-pixel relative standard error at which a pixel stops")
-    ap.add_argument("--spp-cap", type=int, default=4096,
+    ap.add_argument("--spp-cap", type=int, default=512,
                     help="batch workload: samples per pixel at which a pixel stops at the latest (the workload "
-                         "definition's 512 leaves the noisiest pixels above the relative-MSE target)")
+                         "definition's 512; pixels lit through the foliage stay above the relative-MSE target "
+                         "at 4096 too)")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="batch workload: skip the FP64-oracle check of the batch's relative MSE")
     ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],

@@ -276,12 +276,6 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
 enum pt_extend_mode { PT_EXTEND_MODE_AUTO = 0, PT_EXTEND_MODE_WARP = 1, PT_EXTEND_MODE_LANE = 2 };
 int pt_set_extend_mode(pt_renderer* r, int mode);
 
-/* Batches with the slot-ordered queue (no reference counterpart; images are
- * identical either way): 1 (the default) writes each tile of 2048 slots of the
- * next-bounce queue grouped by scene, so that warps mostly trace and shade
- * paths of one scene; 0 keeps plain slot order. */
-int pt_set_scene_binning(pt_renderer* r, int on);
-
 /* Parity hook (no reference counterpart): writes, for waves [first_wave,
  * first_wave + waves) and every pixel, the first `stride` uniforms that the
  * renderer's generator draws for that (pixel, sample) -- curand_init /

@@ -226,7 +226,6 @@ struct pt_renderer {
     int gridShadowLane = 0;          // grid of the per-lane shadow kernel
     int gridShadeMiss = 0;           // grid of the miss shader (its own occupancy)
     bool extendLane = false;         // per-lane ray replacement in this render's closest-hit stage
-    bool sceneBinning = true;        // batches: next-bounce queue grouped by scene per tile
     int extendMode = PT_EXTEND_MODE_AUTO;
     // CUDA graphs of four bounce iterations (the first block of a batch, later
     // blocks) and the launch configuration they were captured for
@@ -377,7 +376,6 @@ int ensurePaths(pt_renderer* r, int capacity)
 // whose queue order does not matter to it, the shade kernels read consecutive
 // slots' path state.
 bool slotOrdered(const pt_renderer* r) { return PT_SLOT_ORDER && r->extendLane; }
-bool sceneBinned(const pt_renderer* r) { return slotOrdered(r) && r->sceneBinning && r->scenes.size() > 1; }
 
 LaunchCtx makeCtx(pt_renderer* r)
 {
@@ -1223,7 +1221,6 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
     const unsigned long long key[6] = {reinterpret_cast<unsigned long long>(c), static_cast<unsigned long long>(r->gridExtend),
         static_cast<unsigned long long>(r->gridShade), static_cast<unsigned long long>(r->gridShadow),
         static_cast<unsigned long long>(inst ? 1 : 0) | (static_cast<unsigned long long>(nw) << 1) |
-            (static_cast<unsigned long long>(sceneBinned(r) ? 1 : 0) << 6) |
             (static_cast<unsigned long long>(r->extendLane ? 1 : 0) << 8) |
             (static_cast<unsigned long long>(r->gridExtendLane) << 9) |
             (static_cast<unsigned long long>(r->gridShadowLane) << 22) |
@@ -1252,7 +1249,7 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
             launchShadow(c, it, shadowGrid(r, false, inst), false, inst, r->extendLane, s);
             launchFinalize(c, sel, r->gridShadow, nw, s);
             if (slotOrdered(r)) {
-                launchNextQueue(c, sel, r->gridShadow, sceneBinned(r), s);
+                launchNextQueue(c, sel, r->gridShadow, s);
             }
             sel ^= 1;
         }
@@ -1715,7 +1712,7 @@ int pt_render(pt_renderer* r, int waves)
                 StageTimer tm(r, kFinalize);
                 launchFinalize(c, sel, r->gridShadow, nw, s);
                 if (slotOrdered(r)) {
-                    launchNextQueue(c, sel, r->gridShadow, sceneBinned(r), s);
+                    launchNextQueue(c, sel, r->gridShadow, s);
                 }
             }
             launches += 4 + extendKernels(countVisits, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0);
@@ -1959,15 +1956,6 @@ int pt_set_extend_mode(pt_renderer* r, int mode)
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_extend_mode: mode must be 0 (auto), 1 (warp) or 2 (lane)");
     }
     r->extendMode = mode;
-    return PT_OK;
-}
-
-int pt_set_scene_binning(pt_renderer* r, int on)
-{
-    if (r == nullptr || (on != 0 && on != 1)) {
-        return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_scene_binning: on must be 0 or 1");
-    }
-    r->sceneBinning = on != 0;
     return PT_OK;
 }
 

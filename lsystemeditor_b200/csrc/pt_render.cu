@@ -688,6 +688,15 @@ __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const Laun
 #ifndef PT_SHADOW_LANE_MIN_BLOCKS
 #define PT_SHADOW_LANE_MIN_BLOCKS 4
 #endif
+#ifndef PT_EXTEND_LANE_SYNC
+#define PT_EXTEND_LANE_SYNC false
+#endif
+#ifndef PT_SHADOW_LANE_SYNC
+#define PT_SHADOW_LANE_SYNC false
+#endif
+#ifndef PT_SHADOW_LANE
+#define PT_SHADOW_LANE 1
+#endif
 
 // A ray of the per-lane traversal: its scene, origin, normalised direction and
 // the parametric interval it is tested on.
@@ -705,18 +714,21 @@ struct LaneRay {
 // a warp is not held by its longest ray.  One loop iteration is one step of
 // traceRay's traversal (a node's children, then the triangles of that node),
 // with the same postponing, stacks and tie rule, so the results are
-// traceRay's.  Every iteration is warp-synchronous: the idle lanes fetch
-// together at the top (one ballot, one atomic), the lanes with a ray take one
-// traversal step, and the warp leaves the loop only when the queue is drained
-// for every lane and no lane holds a ray; the full-mask ballot and vote
-// reconverge the warp once per step, so lanes that took different branches do
-// not go on as separately scheduled groups.
+// traceRay's.  Two loop forms:
+//   Sync = false: a lane fetches as soon as it is idle (the idle lanes of the
+//     moment share one atomic) and the lanes of a warp are not reconverged, so
+//     the scheduler can issue from the lanes that fetch while the others wait
+//     on node loads.  On the 972k-triangle tree this form's closest-hit stage
+//     took 629 ms per frame against 678 ms for Sync = true.
+//   Sync = true: every iteration is warp-synchronous (one ballot fetch for the
+//     idle lanes at the top, a full-warp vote to leave), so the lanes of a
+//     warp step together.
 //   load(k, ray) -> bool: reads queue entry k into `ray`; false when the entry
 //     was decided without the wide traversal (and its result written).
 //   finish(k, hit, t, u, v, tri): the result of entry k (tri = original
 //     triangle index; for AnyHit, hit means occluded and t, u, v, tri are unset).
 // Rays finish in no particular order.
-template <bool AnyHit, class Load, class Finish>
+template <bool AnyHit, bool Sync, class Load, class Finish>
 __device__ __forceinline__ void laneTraversal(unsigned int count, unsigned int* fetch, uint2* sstack, int sstride,
     unsigned int* overflowCounter, Load load, Finish finish)
 {
@@ -752,40 +764,59 @@ __device__ __forceinline__ void laneTraversal(unsigned int count, unsigned int* 
         overflow = false;
         active = false;
     };
+    auto begin = [&]() {
+        idir = f3(__frcp_rn(r.dn.x), __frcp_rn(r.dn.y), __frcp_rn(r.dn.z));
+        const uint32_t oct = (r.dn.x < 0.0f ? 4u : 0u) | (r.dn.y < 0.0f ? 2u : 0u) | (r.dn.z < 0.0f ? 1u : 0u);
+        octinv = 7u - oct;
+        ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
+        tgroup = make_uint2(0u, 0u);
+        sp = 0;
+        closest = r.tMax;
+        best = 0xFFFFFFFFu;
+        bu = bv = 0.0f;
+        active = true;
+    };
     const unsigned int lane = threadIdx.x & 31u;
     bool drained = false;
     for (;;) {
-        const bool want = !active && !drained;
-        const unsigned int wantMask = __ballot_sync(0xFFFFFFFFu, want);
-        if (wantMask != 0u) {
-            const int leader = __ffs(wantMask) - 1;
-            unsigned int base = 0;
-            if (static_cast<int>(lane) == leader) {
-                base = atomicAdd(fetch, static_cast<unsigned int>(__popc(wantMask)));
-            }
-            base = __shfl_sync(0xFFFFFFFFu, base, leader);
-            if (want) {
-                k = base + __popc(wantMask & ((1u << lane) - 1u));
-                if (k >= count) {
-                    drained = true; // the queue is drained
-                } else if (load(k, r)) {
-                    idir = f3(__frcp_rn(r.dn.x), __frcp_rn(r.dn.y), __frcp_rn(r.dn.z));
-                    const uint32_t oct =
-                        (r.dn.x < 0.0f ? 4u : 0u) | (r.dn.y < 0.0f ? 2u : 0u) | (r.dn.z < 0.0f ? 1u : 0u);
-                    octinv = 7u - oct;
-                    ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
-                    tgroup = make_uint2(0u, 0u);
-                    sp = 0;
-                    closest = r.tMax;
-                    best = 0xFFFFFFFFu;
-                    bu = bv = 0.0f;
-                    active = true;
+        if constexpr (Sync) {
+            const bool want = !active && !drained;
+            const unsigned int wantMask = __ballot_sync(0xFFFFFFFFu, want);
+            if (wantMask != 0u) {
+                const int leader = __ffs(wantMask) - 1;
+                unsigned int base = 0;
+                if (static_cast<int>(lane) == leader) {
+                    base = atomicAdd(fetch, static_cast<unsigned int>(__popc(wantMask)));
                 }
-                // (an entry decided by load leaves the lane idle: it fetches again)
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (want) {
+                    k = base + __popc(wantMask & ((1u << lane) - 1u));
+                    if (k >= count) {
+                        drained = true; // the queue is drained
+                    } else if (load(k, r)) {
+                        begin();
+                    }
+                    // (an entry decided by load leaves the lane idle: it fetches again)
+                }
             }
-        }
-        if (!__any_sync(0xFFFFFFFFu, active || !drained)) {
-            break;
+            if (!__any_sync(0xFFFFFFFFu, active || !drained)) {
+                break;
+            }
+        } else if (!active) {
+            // the lanes without a ray take the next queue entries together (one atomic)
+            cg::coalesced_group g = cg::coalesced_threads();
+            unsigned int base = 0;
+            if (g.thread_rank() == 0) {
+                base = atomicAdd(fetch, g.size());
+            }
+            k = g.shfl(base, 0) + g.thread_rank();
+            if (k >= count) {
+                break; // the queue is drained
+            }
+            if (!load(k, r)) {
+                continue; // decided without the wide traversal
+            }
+            begin();
         }
         if (active) {
             // one traversal step (traceRay's loop body)
@@ -868,7 +899,7 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLO
     }
     uint32_t* queue = c.q.extend[sel];
     uint32_t i = 0;
-    laneTraversal<false>(count, &c.q.counts[8 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
+    laneTraversal<false, PT_EXTEND_LANE_SYNC>(count, &c.q.counts[8 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
         c.q.overflow,
         [&](unsigned int k, LaneRay& r) -> bool {
             i = identity ? k : queue[k];
@@ -918,7 +949,7 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_SHADOW_LANE_MIN_BLO
         c.q.counts[10 + (par ^ 1)] = 0u; // next shadow stage's fetch counter
     }
     uint32_t e = 0;
-    laneTraversal<true>(count, &c.q.counts[10 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
+    laneTraversal<true, PT_SHADOW_LANE_SYNC>(count, &c.q.counts[10 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
         c.q.overflow,
         [&](unsigned int k, LaneRay& r) -> bool {
             e = c.q.shadowPath[k];
@@ -1085,71 +1116,6 @@ __global__ void __launch_bounds__(256) k_next_queue(const LaunchCtx* __restrict_
             if ((mask[r] >> lane) & 1u) {
                 out[sBase + sOff[r * 8 + warp] + __popc(mask[r] & below)] =
                     t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// Batches of several scenes: the same tile pass, with each tile's entries
-// written grouped by scene (a counting sort of the tile in shared memory over
-// the scene index modulo kSceneBins), so that the warps of the next extend and
-// shade stages mostly hold paths of one scene and read one scene's records.
-// Paths in flight span several scenes because a recycled slot takes the next
-// job in scene-major order whenever its path ends.  Within a bin the entries
-// keep no particular order; no result depends on the queue order.
-constexpr int kSceneBins = 256;
-static_assert(kSceneBins == 256, "k_next_queue_binned clears and scans one bin per thread of its 256-thread blocks");
-__global__ void __launch_bounds__(256) k_next_queue_binned(const LaunchCtx* __restrict__ cp, int sel)
-{
-    const LaunchCtx& c = *cp;
-    const unsigned int n = static_cast<unsigned int>(c.q.batch->slotCount);
-    uint8_t* flag = c.q.nextFlag;
-    uint32_t* out = c.q.extend[sel ^ 1];
-    __shared__ unsigned int sBin[kSceneBins];
-    __shared__ unsigned int sWarp[8];
-    __shared__ unsigned int sBase;
-    const unsigned int lane = threadIdx.x & 31u;
-    const unsigned int below = (1u << lane) - 1u;
-    const unsigned int tile = 256u * kRouteRows;
-    for (unsigned int t0 = blockIdx.x * tile; t0 < n; t0 += gridDim.x * tile) {
-        sBin[threadIdx.x] = 0u;
-        __syncthreads();
-        unsigned int bin[kRouteRows], rank[kRouteRows];
-#pragma unroll
-        for (int r = 0; r < kRouteRows; ++r) {
-            const unsigned int k = t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
-            const bool on = k < n && flag[k] != 0;
-            if (on) {
-                flag[k] = 0;
-            }
-            const unsigned int b = on ? (static_cast<unsigned int>(c.paths.scene[k]) & (kSceneBins - 1u)) : 0xFFFFFFFFu;
-            // lanes of one bin take consecutive ranks with one shared atomic
-            const unsigned int peers = __match_any_sync(0xFFFFFFFFu, b);
-            unsigned int rk = 0u;
-            if (on) {
-                const int leader = __ffs(peers) - 1;
-                unsigned int base = 0u;
-                if (static_cast<int>(lane) == leader) {
-                    base = atomicAdd(&sBin[b], static_cast<unsigned int>(__popc(peers)));
-                }
-                rk = __shfl_sync(peers, base, leader) + __popc(peers & below);
-            }
-            bin[r] = b;
-            rank[r] = rk;
-        }
-        __syncthreads();
-        unsigned int total = 0u;
-        const unsigned int start = blockExclusiveScan(sBin[threadIdx.x], sWarp, &total);
-        sBin[threadIdx.x] = start;
-        if (threadIdx.x == 0) {
-            sBase = total ? atomicAdd(&c.q.counts[sel ^ 1], total) : 0u;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < kRouteRows; ++r) {
-            if (bin[r] != 0xFFFFFFFFu) {
-                out[sBase + sBin[bin[r]] + rank[r]] = t0 + static_cast<unsigned int>(r) * 256u + threadIdx.x;
             }
         }
         __syncthreads();
@@ -1881,13 +1847,9 @@ int extendKernels(bool count, bool inst, bool lane)
 {
     return (!inst && !count && lane) ? 2 : 1;
 }
-void launchNextQueue(const LaunchCtx* c, int sel, int grid, bool binned, cudaStream_t s)
+void launchNextQueue(const LaunchCtx* c, int sel, int grid, cudaStream_t s)
 {
-    if (binned) {
-        k_next_queue_binned<<<grid, 256, 0, s>>>(c, sel);
-    } else {
-        k_next_queue<<<grid, 256, 0, s>>>(c, sel);
-    }
+    k_next_queue<<<grid, 256, 0, s>>>(c, sel);
 }
 int shadowLaneOccupancy()
 {
@@ -1932,7 +1894,7 @@ void launchShade(const LaunchCtx* c, int sel, int iter, int grid, int nw, cudaSt
 void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, bool inst, bool lane, cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
-    if (lane && !inst && !count) {
+    if (PT_SHADOW_LANE && lane && !inst && !count) {
         k_shadow_lane<<<grid, PT_EXTEND_LANE_THREADS, sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS, s>>>(c,
             iter);
     } else if (inst) {

@@ -162,7 +162,7 @@ int extendLaneOccupancy();
 int shadeMissOccupancy();
 int shadowLaneOccupancy();
 // Slot-ordered mode: the next bounce's extend queue from the marked slots.
-void launchNextQueue(const LaunchCtx* d, int sel, int grid, bool binned, cudaStream_t s);
+void launchNextQueue(const LaunchCtx* d, int sel, int grid, cudaStream_t s);
 void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, int nw, cudaStream_t s);
 void launchShade(const LaunchCtx* d, int sel, int iter, int grid, int nw, cudaStream_t s);
 // Shadow stage.  lane: per-lane ray replacement (k_shadow_lane; flat scenes,

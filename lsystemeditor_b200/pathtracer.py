@@ -85,7 +85,7 @@ EXPORTED_SYMBOLS = ["pt_create", "pt_destroy", "pt_last_error", "pt_configure", 
                     "pt_reset_region", "pt_environment_tables", "pt_spectral_response", "pt_spectral_uplift",
                     "pt_set_instances", "pt_set_distant_light", "pt_batch_share_scene", "pt_autotune", "pt_measure_l2",
                     "pt_set_extend_mode", "pt_radix_sort_temp_bytes", "pt_radix_sort_pairs",
-                    "pt_set_bvh_options", "pt_bvh_sah_cost", "pt_set_scene_binning"]
+                    "pt_set_bvh_options", "pt_bvh_sah_cost"]
 
 _LIB: Optional[C.CDLL] = None
 
@@ -128,7 +128,6 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     L.pt_get_profile.argtypes = [vp, C.POINTER(PtProfile)]
     L.pt_set_tuning.argtypes = [vp, C.c_int, C.c_int]
     L.pt_set_extend_mode.argtypes = [vp, C.c_int]
-    L.pt_set_scene_binning.argtypes = [vp, C.c_int]
     L.pt_batch_configure.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.pt_batch_set_mesh.argtypes = [vp, C.c_int, C.POINTER(PtMesh)]
     L.pt_batch_set_camera.argtypes = [vp, C.c_int, vp]
@@ -604,11 +603,6 @@ class PathTracer:
     def set_extend_mode(self, mode: int):
         """pt_set_extend_mode: 0 auto, 1 warp-fetch closest hit, 2 per-lane replacement (identical images)."""
         self._check(self._lib.pt_set_extend_mode(self._h, int(mode)))
-
-    def set_scene_binning(self, on: bool):
-        """pt_set_scene_binning: batches group each tile of the next-bounce queue by scene (default on;
-        identical images either way)."""
-        self._check(self._lib.pt_set_scene_binning(self._h, 1 if on else 0))
 
     def rng_tape(self, first_wave: int, waves: int, stride: int) -> np.ndarray:
         out = np.zeros((waves, self.width * self.height, stride), np.float32)

@@ -99,28 +99,23 @@ def test_batch_argument_errors(tracer):
         tracer.render(1)  # scene 1 has no mesh yet
 
 
-@pytest.mark.parametrize("binning", [True, False])
-def test_batch_per_lane_queue_orders(tracer, binning):
-    """The per-lane closest-hit form with its slot-ordered next-bounce queue, the
-    queue grouped by scene per tile (the default for batches) or in plain slot
-    order: every scene still equals its render alone, at a path capacity small
-    enough that slots are recycled across scene boundaries many times."""
-    from lsystemeditor_b200.pathtracer import PathTracerError
+def test_batch_per_lane_kernels(tracer):
+    """The per-lane closest-hit and shadow kernels with the slot-ordered
+    next-bounce queue: every scene still equals its render alone, at a path
+    capacity small enough that slots are recycled across scene boundaries many
+    times."""
     scenes = _scenes()
     params = default_params(background_r=0.2, background_g=0.2, background_b=0.25, max_path_depth=5,
-                            min_samples=4, max_samples_per_pixel=24, relative_error_threshold=0.3)
+                            min_samples=4, max_samples_per_pixel=24, relative_error_threshold=0.3,
+                            emitter_mis=1)
     tracer.set_extend_mode(2)
     tracer.set_tuning(4096, 0)
-    tracer.set_scene_binning(binning)
     try:
         alone = _plain(tracer, scenes, params, None)
         together = _batched(tracer, scenes, params, None)
     finally:
-        tracer.set_scene_binning(True)
         tracer.set_tuning(0, 0)
         tracer.set_extend_mode(0)
     for k, ((ra, ca, va), (rb, cb, vb)) in enumerate(zip(alone, together)):
         assert np.array_equal(ca, cb), f"scene {k}: sample counts differ"
         assert np.array_equal(ra, rb), f"scene {k}: image differs"
-    with pytest.raises(PathTracerError):
-        tracer._check(tracer._lib.pt_set_scene_binning(tracer._h, 2))

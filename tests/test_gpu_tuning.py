@@ -77,13 +77,15 @@ def _render_all(t):
     return rgba.copy(), counts.copy(), conv.copy()
 
 
-@pytest.mark.parametrize("nw", [0, 8])
-def test_extend_modes_render_the_same_image(nw):
+@pytest.mark.parametrize("nw, mis", [(0, 0), (8, 0), (0, 1)])
+def test_extend_modes_render_the_same_image(nw, mis):
+    """Closest-hit and shadow stages in the warp-fetch and per-lane forms; with
+    emitter MIS the emissive shadow rays end short of the light (tMax)."""
     mesh = spectral_zoo_scene(n_per_mat=150, seed=11)
     w, h = 64, 48
     params = default_params(background_r=0.1, background_g=0.12, background_b=0.2, max_path_depth=8,
                             min_samples=8, max_samples_per_pixel=32, relative_error_threshold=0.3,
-                            spectral_wavelengths=nw)
+                            spectral_wavelengths=nw, emitter_mis=mis)
     with PathTracer(0) as t:
         t.configure(w, h, mesh)
         t.set_camera(zoo_camera(w, h))
