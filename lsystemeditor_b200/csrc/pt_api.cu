@@ -1208,6 +1208,13 @@ int extendGrid(const pt_renderer* r, bool count, bool inst)
 {
     return (r->extendLane && !count && !inst) ? r->gridExtendLane : r->gridExtend;
 }
+// Grid of the hit shader: RGB and spectral forms differ in registers, and a
+// grid above one form's occupancy leaves a partial second wave of blocks.
+int shadeGrid(const pt_renderer* r, int nw)
+{
+    const int occ = shadeOccupancy(nw);
+    return r->smCount * (r->blocksPerSmOverride > 0 ? std::min(r->blocksPerSmOverride, occ) : occ);
+}
 int shadowGrid(const pt_renderer* r, bool count, bool inst)
 {
     return (r->extendLane && !count && !inst) ? r->gridShadowLane : r->gridShadow;
@@ -1245,7 +1252,7 @@ bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
         for (int it = 0; it < 4; ++it) {
             launchExtend(c, sel, g == 0 && it == 0, it, extendGrid(r, false, inst), false, inst, r->extendLane, s);
             launchShadeMiss(c, it, sel, r->gridShadeMiss, nw, s);
-            launchShade(c, sel, it, r->gridShade, nw, s);
+            launchShade(c, sel, it, shadeGrid(r, nw), nw, s);
             launchShadow(c, it, shadowGrid(r, false, inst), false, inst, r->extendLane, s);
             launchFinalize(c, sel, r->gridShadow, nw, s);
             if (slotOrdered(r)) {
@@ -1702,7 +1709,7 @@ int pt_render(pt_renderer* r, int waves)
             {
                 StageTimer tm(r, kShade);
                 launchShadeMiss(c, iter, sel, r->gridShadeMiss, nw, s);
-                launchShade(c, sel, iter, r->gridShade, nw, s);
+                launchShade(c, sel, iter, shadeGrid(r, nw), nw, s);
             }
             {
                 StageTimer tm(r, kShadow);

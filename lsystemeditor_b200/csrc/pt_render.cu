@@ -633,7 +633,10 @@ template <bool Count, bool Inst>
 #define PT_SHADE_MIN_BLOCKS 4
 #endif
 #ifndef PT_SHADE_SPEC_MIN_BLOCKS
-#define PT_SHADE_SPEC_MIN_BLOCKS 3
+// (spectral shade at 4 blocks per SM, 64 registers: 531 -> 474 ms per frame on
+// the 972k-triangle tree with 8 wavelengths, each form on a grid of its own
+// occupancy)
+#define PT_SHADE_SPEC_MIN_BLOCKS 4
 #endif
 __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
 {
@@ -1912,6 +1915,24 @@ void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, bool inst,
     } else {
         k_shadow<false, false><<<grid, 256, smem, s>>>(c, iter);
     }
+}
+int shadeOccupancy(int nw)
+{
+    // (one value per instantiation; every device here is the same part)
+    static int occ[3] = {0, 0, 0};
+    const int k = nw == 8 ? 2 : (nw == 4 ? 1 : 0);
+    if (occ[k] == 0) {
+        int b = 1;
+        if (nw == 8) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<8>, 256, 0);
+        } else if (nw == 4) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<4>, 256, 0);
+        } else {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<0>, 256, 0);
+        }
+        occ[k] = b > 0 ? b : 1;
+    }
+    return occ[k];
 }
 void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
 {

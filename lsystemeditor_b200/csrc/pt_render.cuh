@@ -161,6 +161,8 @@ int extendKernels(bool count, bool inst, bool lane);
 int extendLaneOccupancy();
 int shadeMissOccupancy();
 int shadowLaneOccupancy();
+// Resident blocks per SM of the hit shader for nw wavelengths (0 = RGB).
+int shadeOccupancy(int nw);
 // Slot-ordered mode: the next bounce's extend queue from the marked slots.
 void launchNextQueue(const LaunchCtx* d, int sel, int grid, cudaStream_t s);
 void launchShadeMiss(const LaunchCtx* d, int iter, int sel, int grid, int nw, cudaStream_t s);
