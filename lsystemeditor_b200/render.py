@@ -38,6 +38,8 @@ def main(argv=None) -> int:
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--spectral", default="auto", choices=["auto", "0", "4", "8"],
                     help="hero wavelengths per path (auto: plain-small 4, plain-large 8; 0 = RGB)")
+    ap.add_argument("--emitter-mis", action="store_true",
+                    help="emitter MIS estimator (short emissive shadow rays; not the reference's estimator)")
     ap.add_argument("--save", default="")
     ap.add_argument("--stage-times", action="store_true",
                     help="time every stage launch with CUDA events and print the per-stage totals and ray counts")
@@ -53,6 +55,8 @@ def main(argv=None) -> int:
     if a.spp > 0:
         params["min_samples"] = a.spp
         params["max_samples_per_pixel"] = a.spp
+    if a.emitter_mis:
+        params["emitter_mis"] = 1
     t0 = time.perf_counter()
     with PathTracer(a.device) as pt:
         if a.capacity:
