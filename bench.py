@@ -754,7 +754,12 @@ def run_batch(args):
     acc_scenes = batch_accuracy_scenes(all_tubes) if (world == 1 and not args.no_accuracy) else []
     acc_images = {k: pt.batch_readback(k)[:2] for k in acc_scenes}
 
+    # (host wall time of the whole loop too: per scene its configure, tube
+    # upload, device build, render and image readback, as a caller of the plain
+    # drop-in would run it)
     plain_ms, plain_samples, plain_build_ms = 0.0, 0, 0.0
+    torch.cuda.synchronize()
+    pw0 = time.perf_counter()
     for k in range(n):
         w, h = sizes[k]
         pt.configure(w, h)
@@ -767,6 +772,9 @@ def run_batch(args):
         s = pt.stats()
         plain_ms += s["render_ms"]
         plain_samples += s["samples"]
+        pt.readback()
+    torch.cuda.synchronize()
+    plain_wall_s = time.perf_counter() - pw0
 
     # end to end through the public API: tube arrays from host memory, device
     # loft + BVH builds, render, read back every image (one step)
@@ -778,6 +786,7 @@ def run_batch(args):
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    bw0 = time.perf_counter()
     e0.record(stream)
     build_batch()
     pt.render(0)
@@ -790,6 +799,7 @@ def run_batch(args):
             v.cpu()
     e1.record(stream)
     torch.cuda.synchronize()
+    batched_wall_s = time.perf_counter() - bw0
     e_ms = reduce(float(e0.elapsed_time(e1)), "max")
     e_value = reduce(float(e_samples), "sum") / (e_ms / 1e3) / 1e6
 
@@ -803,12 +813,16 @@ def run_batch(args):
         plain_s = plain_build_ms / 1e3 + plain_ms / 1e3
         accuracy["time_to_target"] = {
             "batched_s": batched_s, "plain_s": plain_s,
-            "note": "wall time of one pass over all scenes to the per-pixel stop criterion, device builds "
-                    "(loft + BVH) included; batched and plain images are identical, so both reach the same "
-                    "relative MSE"}
+            "batched_wall_s": batched_wall_s, "plain_wall_s": plain_wall_s,
+            "note": "one pass over all scenes to the per-pixel stop criterion; *_s: device time of the device "
+                    "builds (loft + BVH) plus the render; *_wall_s: host wall time from the first tube upload to "
+                    "the last image read back (batched: one renderer call sequence for all scenes; plain: one "
+                    "configure / upload / build / render / readback per scene); batched and plain images are "
+                    "identical, so both reach the same relative MSE"}
+        accuracy["batched_faster_device"] = bool(batched_s < plain_s)
+        accuracy["batched_faster"] = bool(batched_wall_s < plain_wall_s)
         if "relmse" in accuracy:
             accuracy["target_met"] = bool(accuracy["relmse"] <= 1e-3)
-            accuracy["batched_faster"] = bool(batched_s < plain_s)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
