@@ -224,6 +224,8 @@ struct pt_renderer {
     int gridExtend = 0, gridShade = 0, gridShadow = 0;
     int gridExtendLane = 0;          // grid of the per-lane closest-hit kernel
     int gridShadowLane = 0;          // grid of the per-lane shadow kernel
+    int gridExtendLaneInst = 0;      // grids of the per-lane kernels of instanced scenes
+    int gridShadowLaneInst = 0;
     int gridShadeMiss = 0;           // grid of the miss shader (its own occupancy)
     bool extendLane = false;         // per-lane ray replacement in this render's closest-hit stage
     int extendMode = PT_EXTEND_MODE_AUTO;
@@ -1206,7 +1208,10 @@ void releaseBounceGraphs(pt_renderer* r)
 // Grid of the closest-hit stage: the per-lane kernel has its own occupancy.
 int extendGrid(const pt_renderer* r, bool count, bool inst)
 {
-    return (r->extendLane && !count && !inst) ? r->gridExtendLane : r->gridExtend;
+    if (r->extendLane && !count) {
+        return inst ? r->gridExtendLaneInst : r->gridExtendLane;
+    }
+    return r->gridExtend;
 }
 // Grid of the hit shader: RGB and spectral forms differ in registers, and a
 // grid above one form's occupancy leaves a partial second wave of blocks.
@@ -1217,7 +1222,10 @@ int shadeGrid(const pt_renderer* r, int nw)
 }
 int shadowGrid(const pt_renderer* r, bool count, bool inst)
 {
-    return (r->extendLane && !count && !inst) ? r->gridShadowLane : r->gridShadow;
+    if (r->extendLane && !count) {
+        return inst ? r->gridShadowLaneInst : r->gridShadowLane;
+    }
+    return r->gridShadow;
 }
 
 // The graphs of four bounce iterations for this launch configuration
@@ -1226,7 +1234,9 @@ int shadowGrid(const pt_renderer* r, bool count, bool inst)
 bool ensureBounceGraphs(pt_renderer* r, const LaunchCtx* c, bool inst, int nw)
 {
     const unsigned long long key[6] = {reinterpret_cast<unsigned long long>(c), static_cast<unsigned long long>(r->gridExtend),
-        static_cast<unsigned long long>(r->gridShade), static_cast<unsigned long long>(r->gridShadow),
+        static_cast<unsigned long long>(r->gridShade) | (static_cast<unsigned long long>(r->gridExtendLaneInst) << 16) |
+            (static_cast<unsigned long long>(r->gridShadowLaneInst) << 32),
+        static_cast<unsigned long long>(r->gridShadow),
         static_cast<unsigned long long>(inst ? 1 : 0) | (static_cast<unsigned long long>(nw) << 1) |
             (static_cast<unsigned long long>(r->extendLane ? 1 : 0) << 8) |
             (static_cast<unsigned long long>(r->gridExtendLane) << 9) |
@@ -1315,6 +1325,8 @@ int pt_create(pt_renderer** out, int device)
     r->gridShadow = r->smCount * std::max(bsh, 1);
     r->gridExtendLane = r->smCount * extendLaneOccupancy();
     r->gridShadowLane = r->smCount * shadowLaneOccupancy();
+    r->gridExtendLaneInst = r->smCount * extendLaneInstOccupancy();
+    r->gridShadowLaneInst = r->smCount * shadowLaneInstOccupancy();
     r->gridShadeMiss = r->smCount * shadeMissOccupancy();
     *out = r;
     return PT_OK;
@@ -1614,9 +1626,8 @@ int pt_render(pt_renderer* r, int waves)
     }
     // Per-lane ray replacement pays where traversals are long (large trees);
     // on small scenes the extra routing launch costs more than it saves.
-    r->extendLane = !inst && (r->extendMode == PT_EXTEND_MODE_LANE ||
-                                 (r->extendMode == PT_EXTEND_MODE_AUTO &&
-                                     maxNodes >= static_cast<uint32_t>(PT_EXTEND_LANE_MIN_NODES)));
+    r->extendLane = r->extendMode == PT_EXTEND_MODE_LANE ||
+        (r->extendMode == PT_EXTEND_MODE_AUTO && !inst && maxNodes >= static_cast<uint32_t>(PT_EXTEND_LANE_MIN_NODES));
     const int nw = r->params.spectral_wavelengths;
     if (nw > 0) {
         const int st = prepareSpectral(r, nw);
@@ -1977,6 +1988,8 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
         r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
         r->gridExtendLane = r->smCount * std::min(blocks_per_sm, extendLaneOccupancy());
         r->gridShadowLane = r->smCount * std::min(blocks_per_sm, shadowLaneOccupancy());
+        r->gridExtendLaneInst = r->smCount * std::min(blocks_per_sm, extendLaneInstOccupancy());
+        r->gridShadowLaneInst = r->smCount * std::min(blocks_per_sm, shadowLaneInstOccupancy());
         r->gridShadeMiss = r->smCount * std::min(blocks_per_sm, shadeMissOccupancy());
     } else {
         int be = 1, bs = 1, bsh = 1;
@@ -1986,6 +1999,8 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
         r->gridShadow = r->smCount * std::max(bsh, 1);
         r->gridExtendLane = r->smCount * extendLaneOccupancy();
         r->gridShadowLane = r->smCount * shadowLaneOccupancy();
+    r->gridExtendLaneInst = r->smCount * extendLaneInstOccupancy();
+    r->gridShadowLaneInst = r->smCount * shadowLaneInstOccupancy();
         r->gridShadeMiss = r->smCount * shadeMissOccupancy();
     }
     return PT_OK;

@@ -765,8 +765,8 @@ __device__ __forceinline__ void laneTraversal(unsigned int count, unsigned int* 
     };
     auto done = [&](bool hit) {
         finish(k, hit, closest, bu, bv, hit && !AnyHit ? leafId(r.S->tris, best) : 0xFFFFFFFFu);
-        if (overflow && overflowCounter != nullptr) {
-            atomicAdd(overflowCounter, 1u); // rays whose stack overflowed, as traceRay counts them
+        if (overflow && overflowCounter != nullptr && !(AnyHit && hit)) {
+            atomicAdd(overflowCounter, 1u); // rays whose stack overflowed, as traceRay counts them (an occluded any-hit ray is not counted)
         }
         overflow = false;
         active = false;
@@ -884,6 +884,194 @@ __device__ __forceinline__ void laneTraversal(unsigned int count, unsigned int* 
     }
 }
 
+// Per-lane ray replacement over the two-level BVH of an instanced scene: the
+// free-running loop of laneTraversal around traceInstanced's step (top-level
+// leaves are instances; on reaching one the ray goes to the object's space on
+// the same stack above the top level's entries, and comes back when those are
+// used up), with traceInstanced's postponing, overflow and tie rule, so the
+// results are traceInstanced's.  finish(k, hit, t, u, v, tri, inst): tri is
+// the shading-record index (object base + object triangle), inst the instance.
+template <bool AnyHit, class Load, class Finish>
+__device__ __forceinline__ void laneTraversalInst(unsigned int count, unsigned int* fetch, uint2* sstack, int sstride,
+    unsigned int* overflowCounter, Load load, Finish finish)
+{
+    uint2 stack[kTraversalStack];
+    bool active = false;
+    unsigned int k = 0;
+    LaneRay r{nullptr, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f), 0.0f, 0.0f};
+    float3 ro = r.o, rd = r.o, idir = r.o;
+    uint32_t oct = 0, octinv = 7;
+    const CwNode* nodes = nullptr;
+    const TriVerts* leaves = nullptr;
+    int level = 0, base = 0;
+    uint32_t curInst = 0, curTriBase = 0;
+    uint2 ngroup = make_uint2(0u, 0u), tgroup = make_uint2(0u, 0u);
+    int sp = 0;
+    float closest = kRayTMax;
+    unsigned long long bestKey = ~0ull;
+    uint32_t bestTri = 0xFFFFFFFFu, bestInst = 0xFFFFFFFFu;
+    float bu = 0.0f, bv = 0.0f;
+    bool overflow = false;
+
+    auto setRay = [&](float3 a, float3 d) {
+        ro = a;
+        const float dx = fabsf(d.x) < 1.0e-20f ? copysignf(1.0e-20f, d.x) : d.x;
+        const float dy = fabsf(d.y) < 1.0e-20f ? copysignf(1.0e-20f, d.y) : d.y;
+        const float dz = fabsf(d.z) < 1.0e-20f ? copysignf(1.0e-20f, d.z) : d.z;
+        idir = f3(__frcp_rn(dx), __frcp_rn(dy), __frcp_rn(dz));
+        oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+        octinv = 7u - oct;
+    };
+    auto push = [&](uint2 g) -> bool {
+        if (sp < kSharedStack) {
+            sstack[sp * sstride] = g;
+        } else if (sp < kSharedStack + kTraversalStack) {
+            stack[sp - kSharedStack] = g;
+        } else {
+            return false;
+        }
+        ++sp;
+        return true;
+    };
+    auto done = [&](bool hit) {
+        finish(k, hit, closest, bu, bv, bestTri, bestInst);
+        if (overflow && overflowCounter != nullptr && !(AnyHit && hit)) {
+            atomicAdd(overflowCounter, 1u); // rays whose stack overflowed, as traceInstanced counts them
+        }
+        overflow = false;
+        active = false;
+    };
+    for (;;) {
+        if (!active) {
+            // the lanes without a ray take the next queue entries together (one atomic)
+            cg::coalesced_group g = cg::coalesced_threads();
+            unsigned int b = 0;
+            if (g.thread_rank() == 0) {
+                b = atomicAdd(fetch, g.size());
+            }
+            k = g.shfl(b, 0) + g.thread_rank();
+            if (k >= count) {
+                break; // the queue is drained
+            }
+            if (!load(k, r)) {
+                continue; // decided without the wide traversal
+            }
+            setRay(r.o, r.dn);
+            rd = r.dn;
+            nodes = r.S->tlasNodes;
+            leaves = r.S->tlasLeaves;
+            level = 0;
+            base = 0;
+            curInst = 0;
+            curTriBase = 0;
+            ngroup = make_uint2(0u, 0x80000000u | (1u << oct));
+            tgroup = make_uint2(0u, 0u);
+            sp = 0;
+            closest = r.tMax;
+            bestKey = ~0ull;
+            bestTri = bestInst = 0xFFFFFFFFu;
+            bu = bv = 0.0f;
+            active = true;
+        }
+        // one step of traceInstanced's loop
+        if (ngroup.y > 0x00FFFFFFu) {
+            const uint32_t bit = 31u - __clz(ngroup.y);
+            ngroup.y &= ~(1u << bit);
+            const uint32_t slot = (bit - 24u) ^ octinv;
+            const uint32_t child = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << slot) - 1u));
+            if (ngroup.y > 0x00FFFFFFu && !push(ngroup)) {
+                overflow = true;
+            }
+            uint32_t childBase, triBase, imask;
+            const uint32_t hits = intersectChildren(nodes, child, ro, idir, octinv, r.tMin, closest, childBase, triBase,
+                imask);
+            ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
+            tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
+        } else {
+            tgroup = ngroup;
+            ngroup = make_uint2(0u, 0u);
+        }
+        bool occluded = false;
+        while (tgroup.y != 0u) {
+            if (level == 0) {
+                // an instance: descend into its object
+                const int kt = __ffs(tgroup.y) - 1;
+                tgroup.y &= tgroup.y - 1u;
+                const uint32_t inst = __float_as_uint(__ldg(&leaves[tgroup.x + kt].v0.w));
+                bool saved = true;
+                if (ngroup.y > 0x00FFFFFFu) {
+                    saved = push(ngroup);
+                }
+                if (saved && tgroup.y != 0u) {
+                    saved = push(tgroup);
+                }
+                if (!saved) {
+                    overflow = true; // the rest of this top-level group is dropped
+                }
+                const DevInstance& I = r.S->instances[inst];
+                const DevBlas B = r.S->blases[I.meta.x];
+                curInst = inst;
+                curTriBase = B.triBase;
+                nodes = B.nodes;
+                leaves = B.tris;
+                rd = xformVector(I.w2o, r.dn);
+                setRay(xformPoint(I.w2o, r.o), rd);
+                level = 1;
+                base = sp;
+                ngroup = make_uint2(0u, B.nodeCount > 0 ? (0x80000000u | (1u << oct)) : 0u);
+                tgroup = make_uint2(0u, 0u);
+                break;
+            }
+            if (ngroup.y > 0x00FFFFFFu && __popc(__activemask()) < kPostponeLanes && push(tgroup)) {
+                break;
+            }
+            const int kt = __ffs(tgroup.y) - 1;
+            tgroup.y &= tgroup.y - 1u;
+            const TriVerts tv = leaves[tgroup.x + kt];
+            float t, u, v;
+            if (intersectTriExact(ro, rd, f3(tv.v0.x, tv.v0.y, tv.v0.z), f3(tv.v1.x, tv.v1.y, tv.v1.z),
+                    f3(tv.v2.x, tv.v2.y, tv.v2.z), r.tMin, closest, t, u, v)) {
+                const unsigned long long key = (static_cast<unsigned long long>(curInst) << 32) |
+                    static_cast<unsigned long long>(__float_as_uint(tv.v0.w));
+                if (AnyHit) {
+                    if (t < r.tMax) {
+                        occluded = true; // the first hit below tMax ends the ray
+                        break;
+                    }
+                } else if (t < closest || key > bestKey || bestKey == ~0ull) {
+                    closest = t;
+                    bestKey = key;
+                    bestTri = curTriBase + __float_as_uint(tv.v0.w);
+                    bestInst = curInst;
+                    bu = u;
+                    bv = v;
+                }
+            }
+        }
+        if (occluded) {
+            done(true);
+            continue;
+        }
+        if (ngroup.y <= 0x00FFFFFFu) {
+            if (level == 1 && sp == base) {
+                // the object is done: back to the top level in world space
+                level = 0;
+                nodes = r.S->tlasNodes;
+                leaves = r.S->tlasLeaves;
+                rd = r.dn;
+                setRay(r.o, r.dn);
+            }
+            if (sp == 0) {
+                // the ray is finished
+                done(!AnyHit && bestTri != 0xFFFFFFFFu && closest < r.tMax);
+            } else {
+                --sp;
+                ngroup = sp < kSharedStack ? sstack[sp * sstride] : stack[sp - kSharedStack];
+            }
+        }
+    }
+}
+
 // Closest hit of every queued path by the per-lane traversal.  The result of
 // queue entry k goes back into entry k (path index, bit 31 set for a miss) and
 // k_route splits the queue into the miss and hit queues in queue order
@@ -986,6 +1174,87 @@ __global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_SHADOW_LANE_MIN_BLO
             return false;
         },
         [&](unsigned int, bool occluded, float, float, float, uint32_t) {
+            if (!occluded) {
+                const uint32_t i = e & 0x7FFFFFFFu;
+                if (e & 0x80000000u) {
+                    c.paths.visEmis[i] = 1;
+                } else {
+                    c.paths.visEnv[i] = 1;
+                }
+            }
+        });
+}
+
+// Closest hit of every queued path of an instanced scene by the two-level
+// per-lane traversal; results and routing as k_extend_lane.
+__global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_EXTEND_LANE_MIN_BLOCKS)
+    k_extend_lane_inst(const LaunchCtx* __restrict__ cp, int sel, bool identity, int iter)
+{
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
+    const unsigned int count = c.q.counts[sel];
+    const int par = iter & 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&c.q.rays[0], static_cast<unsigned long long>(count));
+        c.q.counts[sel ^ 1] = 0u;
+        c.q.counts[2] = 0u;
+        c.q.counts[3] = 0u;
+        c.q.counts[4 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[5 + 2 * (par ^ 1)] = 0u;
+        c.q.counts[8 + (par ^ 1)] = 0u;
+    }
+    uint32_t* queue = c.q.extend[sel];
+    uint32_t i = 0;
+    laneTraversalInst<false>(count, &c.q.counts[8 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
+        c.q.overflow,
+        [&](unsigned int k, LaneRay& r) -> bool {
+            i = identity ? k : queue[k];
+            r.S = &sceneOf(c, i);
+            const float4 o4 = c.paths.orig[i];
+            const float4 d4 = c.paths.dir[i];
+            r.o = f3(o4.x, o4.y, o4.z);
+            r.tMin = o4.w;
+            r.tMax = kRayTMax;
+            r.dn = xnormalize(f3(d4.x, d4.y, d4.z));
+            return true;
+        },
+        [&](unsigned int k, bool hit, float t, float u, float v, uint32_t tri, uint32_t inst) {
+            if (hit) {
+                c.paths.hit[i] = make_float4(t, u, v, __uint_as_float(tri));
+                c.paths.hitInst[i] = inst;
+            }
+            queue[k] = hit ? i : (i | 0x80000000u);
+        });
+}
+
+// Occlusion of every queued shadow ray of an instanced scene by the two-level
+// per-lane traversal; results as k_shadow_lane.
+__global__ void __launch_bounds__(PT_EXTEND_LANE_THREADS, PT_SHADOW_LANE_MIN_BLOCKS)
+    k_shadow_lane_inst(const LaunchCtx* __restrict__ cp, int iter)
+{
+    const LaunchCtx& c = *cp;
+    extern __shared__ uint2 smemStack[];
+    const unsigned int count = c.q.counts[2];
+    const int par = iter & 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&c.q.rays[1], static_cast<unsigned long long>(count));
+        c.q.counts[10 + (par ^ 1)] = 0u; // next shadow stage's fetch counter
+    }
+    uint32_t e = 0;
+    laneTraversalInst<true>(count, &c.q.counts[10 + par], smemStack + threadIdx.x, static_cast<int>(blockDim.x),
+        c.q.overflow,
+        [&](unsigned int k, LaneRay& r) -> bool {
+            e = c.q.shadowPath[k];
+            r.S = &sceneOf(c, e & 0x7FFFFFFFu);
+            const float4 o4 = c.q.shadowOrig[k];
+            const float4 d4 = c.q.shadowDir[k];
+            r.o = f3(o4.x, o4.y, o4.z);
+            r.dn = xnormalize(f3(d4.x, d4.y, d4.z));
+            r.tMin = kShadowBias;
+            r.tMax = d4.w > 0.0f ? d4.w : kRayTMax; // emitter MIS rays end short of the light
+            return true;
+        },
+        [&](unsigned int, bool occluded, float, float, float, uint32_t, uint32_t) {
             if (!occluded) {
                 const uint32_t i = e & 0x7FFFFFFFu;
                 if (e & 0x80000000u) {
@@ -1837,6 +2106,10 @@ void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid
     if (inst) {
         if (count) {
             k_extend<true, true><<<grid, 256, smem, s>>>(c, sel, identity, iter);
+        } else if (lane) {
+            k_extend_lane_inst<<<grid, PT_EXTEND_LANE_THREADS, sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS,
+                s>>>(c, sel, identity, iter);
+            k_route<<<grid, 256, 0, s>>>(c, sel, iter);
         } else {
             k_extend<false, true><<<grid, 256, smem, s>>>(c, sel, identity, iter);
         }
@@ -1852,11 +2125,25 @@ void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid
 }
 int extendKernels(bool count, bool inst, bool lane)
 {
-    return (!inst && !count && lane) ? 2 : 1;
+    return (!count && lane) ? 2 : 1;
 }
 void launchNextQueue(const LaunchCtx* c, int sel, int grid, cudaStream_t s)
 {
     k_next_queue<<<grid, 256, 0, s>>>(c, sel);
+}
+int extendLaneInstOccupancy()
+{
+    int blocks = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_extend_lane_inst, PT_EXTEND_LANE_THREADS,
+        sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS);
+    return blocks > 0 ? blocks : 1;
+}
+int shadowLaneInstOccupancy()
+{
+    int blocks = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_shadow_lane_inst, PT_EXTEND_LANE_THREADS,
+        sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS);
+    return blocks > 0 ? blocks : 1;
 }
 int shadowLaneOccupancy()
 {
@@ -1901,9 +2188,14 @@ void launchShade(const LaunchCtx* c, int sel, int iter, int grid, int nw, cudaSt
 void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, bool inst, bool lane, cudaStream_t s)
 {
     const size_t smem = sizeof(uint2) * kSharedStack * 256;
-    if (PT_SHADOW_LANE && lane && !inst && !count) {
-        k_shadow_lane<<<grid, PT_EXTEND_LANE_THREADS, sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS, s>>>(c,
-            iter);
+    if (PT_SHADOW_LANE && lane && !count) {
+        if (inst) {
+            k_shadow_lane_inst<<<grid, PT_EXTEND_LANE_THREADS, sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS,
+                s>>>(c, iter);
+        } else {
+            k_shadow_lane<<<grid, PT_EXTEND_LANE_THREADS, sizeof(uint2) * kSharedStack * PT_EXTEND_LANE_THREADS, s>>>(c,
+                iter);
+        }
     } else if (inst) {
         if (count) {
             k_shadow<true, true><<<grid, 256, smem, s>>>(c, iter);

@@ -161,6 +161,8 @@ int extendKernels(bool count, bool inst, bool lane);
 int extendLaneOccupancy();
 int shadeMissOccupancy();
 int shadowLaneOccupancy();
+int extendLaneInstOccupancy();
+int shadowLaneInstOccupancy();
 // Resident blocks per SM of the hit shader for nw wavelengths (0 = RGB).
 int shadeOccupancy(int nw);
 // Slot-ordered mode: the next bounce's extend queue from the marked slots.

@@ -164,3 +164,38 @@ def test_shared_views_match_plain_renders():
         t.render(0)
         for k in range(2):
             assert np.array_equal(t.batch_readback(k)[0], plain[k]), f"view {k} differs from its plain render"
+
+
+@pytest.mark.parametrize("nw", [0, 8])
+def test_instanced_extend_modes_render_the_same_image(nw):
+    """Closest-hit and shadow stages of an instanced scene (two-level BVH, sun
+    light) in the warp-fetch and the per-lane forms, with many recycled path
+    slots: identical images, sample counts and trace results."""
+    scene, cams, params, sun = _small_forest(views=1, w=64, h=48)
+    params = params.copy()
+    params["spectral_wavelengths"] = nw
+    params["min_samples"] = 4
+    params["max_samples_per_pixel"] = 12
+    params["relative_error_threshold"] = 0.3
+    out = {}
+    with PathTracer(0) as t:
+        t.configure(64, 48)
+        t.set_instances(scene.objects, scene.instances)
+        t.set_camera(cams[0])
+        t.set_params(params)
+        if sun is not None:
+            t.set_distant_light(**sun)
+        for mode, cap in ((1, 0), (2, 0), (2, 4096)):
+            t.set_extend_mode(mode)
+            t.set_tuning(cap, 0)
+            t.reset_accumulation()
+            t.render(0)
+            rgba, counts, conv = t.readback()
+            out[(mode, cap)] = (rgba.copy(), counts.copy(), conv.copy())
+        t.set_tuning(0, 0)
+        t.set_extend_mode(0)
+    ref = out[(1, 0)]
+    assert ref[0][..., :3].max() > 0
+    for key, got in out.items():
+        for a, b, what in zip(ref, got, ("image", "sample counts", "convergence flags")):
+            assert np.array_equal(a, b), f"mode {key}: {what} differ from the warp form"
