@@ -634,7 +634,8 @@ inline int gridFor(long long n, int block = kBlock)
 int buildBvh(const float* dPositions, uint32_t n, BvhBuffers& out, cudaStream_t stream, const BvhBuildOptions& opt,
     char* err, size_t errLen)
 {
-    out.release();
+    out.nodeCount = out.triCount = 0;
+    out.levels = 0;
     if (n == 0) {
         return PT_OK;
     }
@@ -691,8 +692,7 @@ int buildBvh(const float* dPositions, uint32_t n, BvhBuffers& out, cudaStream_t 
     // Collapse. Upper bounds: nodes <= n (every compressed node has >= 2 children or is the root),
     // triangles == n.
     const size_t maxNodes = static_cast<size_t>(n) + 1;
-    if (cudaMalloc(&out.nodes, maxNodes * sizeof(CwNode)) != cudaSuccess ||
-        cudaMalloc(&out.tris, static_cast<size_t>(n) * sizeof(TriVerts)) != cudaSuccess) {
+    if (!out.reserve(maxNodes, static_cast<size_t>(n))) {
         std::snprintf(err, errLen, "BVH output allocation failed (%u triangles)", n);
         out.release();
         return PT_ERR_OUT_OF_MEMORY;

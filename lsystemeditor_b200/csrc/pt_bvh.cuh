@@ -83,8 +83,41 @@ struct BvhBuffers {
     uint32_t nodeCount = 0;
     uint32_t triCount = 0;
     int levels = 0;
+    size_t nodeCapacity = 0; // allocated entries, kept across builds
+    size_t triCapacity = 0;
     DeviceArena scratch;
 
+    // Output arrays for at least `n` nodes and `t` triangles; arrays that are
+    // large enough are reused, so a rebuild of a scene that does not grow
+    // neither frees nor allocates (cudaFree waits for the whole device).
+    bool reserve(size_t n, size_t t)
+    {
+        if (n > nodeCapacity) {
+            if (nodes != nullptr) {
+                cudaFree(nodes);
+            }
+            nodes = nullptr;
+            nodeCapacity = 0;
+            if (cudaMalloc(&nodes, n * sizeof(CwNode)) != cudaSuccess) {
+                nodes = nullptr;
+                return false;
+            }
+            nodeCapacity = n;
+        }
+        if (t > triCapacity) {
+            if (tris != nullptr) {
+                cudaFree(tris);
+            }
+            tris = nullptr;
+            triCapacity = 0;
+            if (cudaMalloc(&tris, t * sizeof(TriVerts)) != cudaSuccess) {
+                tris = nullptr;
+                return false;
+            }
+            triCapacity = t;
+        }
+        return true;
+    }
     void release()
     {
         if (nodes != nullptr) {
@@ -95,6 +128,7 @@ struct BvhBuffers {
         }
         nodes = nullptr;
         tris = nullptr;
+        nodeCapacity = triCapacity = 0;
         nodeCount = triCount = 0;
         levels = 0;
     }
