@@ -268,11 +268,12 @@ int pt_get_profile(const pt_renderer* r, pt_profile* out);
  * (0 = from the occupancy calculator). */
 int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
 
-/* Closest-hit scheduling (no reference counterpart; images are identical in
- * every mode).  AUTO: per-lane ray replacement with a slot-ordered next-bounce
- * queue when the largest flat scene has at least 32768 BVH nodes, else one
- * warp per 32 queued rays.  WARP / LANE force either form (instanced scenes
- * always use the warp form). */
+/* Closest-hit and shadow-ray scheduling (no reference counterpart; images are
+ * identical in every mode).  AUTO: per-lane ray replacement (closest hit and
+ * shadow rays) with a slot-ordered next-bounce queue when the largest flat
+ * scene has at least 32768 BVH nodes, else one warp per 32 queued rays.  WARP
+ * / LANE force either form; LANE also runs instanced scenes through the
+ * two-level per-lane traversal. */
 enum pt_extend_mode { PT_EXTEND_MODE_AUTO = 0, PT_EXTEND_MODE_WARP = 1, PT_EXTEND_MODE_LANE = 2 };
 int pt_set_extend_mode(pt_renderer* r, int mode);
 
