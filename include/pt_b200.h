@@ -270,10 +270,10 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
 
 /* Closest-hit and shadow-ray scheduling (no reference counterpart; images are
  * identical in every mode).  AUTO: per-lane ray replacement (closest hit and
- * shadow rays) with a slot-ordered next-bounce queue when the largest flat
- * scene has at least 32768 BVH nodes, else one warp per 32 queued rays.  WARP
- * / LANE force either form; LANE also runs instanced scenes through the
- * two-level per-lane traversal. */
+ * shadow rays; two-level traversal in instanced scenes) with a slot-ordered
+ * next-bounce queue when the largest flat scene or instanced object has at
+ * least 32768 BVH nodes, else one warp per 32 queued rays.  WARP / LANE force
+ * either form. */
 enum pt_extend_mode { PT_EXTEND_MODE_AUTO = 0, PT_EXTEND_MODE_WARP = 1, PT_EXTEND_MODE_LANE = 2 };
 int pt_set_extend_mode(pt_renderer* r, int mode);
 

@@ -1623,11 +1623,15 @@ int pt_render(pt_renderer* r, int waves)
     for (const SceneSlot& sl : r->scenes) {
         inst = inst || sl.instanceCount > 0;
         maxNodes = std::max(maxNodes, sl.bvh.nodeCount);
+        for (const BvhBuffers& b : sl.objBvh) {
+            maxNodes = std::max(maxNodes, b.nodeCount); // an instanced scene's objects
+        }
     }
-    // Per-lane ray replacement pays where traversals are long (large trees);
-    // on small scenes the extra routing launch costs more than it saves.
+    // Per-lane ray replacement pays where traversals are long (large trees, and
+    // instanced scenes of large objects: the two-level traversal); on small
+    // scenes the extra routing launch costs more than it saves.
     r->extendLane = r->extendMode == PT_EXTEND_MODE_LANE ||
-        (r->extendMode == PT_EXTEND_MODE_AUTO && !inst && maxNodes >= static_cast<uint32_t>(PT_EXTEND_LANE_MIN_NODES));
+        (r->extendMode == PT_EXTEND_MODE_AUTO && maxNodes >= static_cast<uint32_t>(PT_EXTEND_LANE_MIN_NODES));
     const int nw = r->params.spectral_wavelengths;
     if (nw > 0) {
         const int st = prepareSpectral(r, nw);
