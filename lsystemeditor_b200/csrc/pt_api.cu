@@ -580,6 +580,9 @@ void collectStageTimes(pt_renderer* r)
 // Results do not depend on it; a pixel that converges inside a batch leaves
 // the rest of the batch's samples unused, so the batch grows when few pixels
 // stopped during the previous one.
+#ifndef PT_SAMPLE_BUFFER_BYTES
+#define PT_SAMPLE_BUFFER_BYTES (1ll << 30)
+#endif
 int chooseBatch(const pt_renderer* r, int remaining)
 {
     const pt_render_params& p = r->params;
@@ -597,8 +600,8 @@ int chooseBatch(const pt_renderer* r, int remaining)
     if (remaining > 0) {
         B = std::min<int64_t>(B, remaining);
     }
-    // cap the sample buffer at ~1 GiB
-    const int64_t cap = std::max<int64_t>(1, (int64_t(1) << 30) / (16 * std::max(1, r->hostActive)));
+    // cap the sample buffer (one float4 per active pixel and wave of the batch)
+    const int64_t cap = std::max<int64_t>(1, static_cast<int64_t>(PT_SAMPLE_BUFFER_BYTES) / (16 * std::max(1, r->hostActive)));
     B = std::min<int64_t>(B, std::min<int64_t>(cap, 1024));
     return static_cast<int>(std::max<int64_t>(B, 1));
 }
