@@ -1078,7 +1078,6 @@ def run_forest(args):
     def step():
         pt.reset_accumulation()
         pt.render(0)
-        gather()
 
     for _ in range(max(args.warmup, 3)):
         step()
