@@ -581,7 +581,11 @@ void collectStageTimes(pt_renderer* r)
 // the rest of the batch's samples unused, so the batch grows when few pixels
 // stopped during the previous one.
 #ifndef PT_SAMPLE_BUFFER_BYTES
-#define PT_SAMPLE_BUFFER_BYTES (1ll << 30)
+// (8 GiB: on the 64-tree batch, 31 M pixels, a 1 GiB buffer held batches to 2
+// waves, so every pass put ~16 scenes' paths in flight and drained often; at
+// 8 GiB the render took 20.9 s instead of 22.0 s, extend and shadow 7% and 11%
+// faster; renders of up to 1 M pixels are unaffected)
+#define PT_SAMPLE_BUFFER_BYTES (8ll << 30)
 #endif
 int chooseBatch(const pt_renderer* r, int remaining)
 {
