@@ -110,6 +110,22 @@ struct SceneSlot {
         instanceCount = 0;
     }
 
+    // Forgets the slot's scene but keeps its device arrays for the next one
+    // (they are reused where large enough: a batch reconfigured with scenes of
+    // the same sizes allocates nothing).
+    void clearScene()
+    {
+        hostMats.clear();
+        hostTex.clear();
+        specValid = false;
+        releaseInstances();
+        bvh.nodeCount = bvh.triCount = 0;
+        bvh.levels = 0;
+        shareFrom = -1;
+        triCount = materialCount = textureCount = emissiveCount = 0;
+        hasScene = false;
+    }
+
     void release()
     {
         positions.release();
@@ -2197,11 +2213,16 @@ int pt_batch_configure(pt_renderer* r, int scene_count, const int* widths, const
     }
     PT_CHECK(r, cudaSetDevice(r->device));
     PT_CHECK(r, cudaStreamSynchronize(r->stream));
-    for (SceneSlot& sl : r->scenes) {
-        sl.release();
+    // slots beyond the new count are freed; the others keep their device
+    // arrays for the new scenes (freeing waits for the device, and a batch
+    // rebuilt with the same scenes would allocate it all again)
+    const size_t n = static_cast<size_t>(scene_count);
+    for (size_t k = n; k < r->scenes.size(); ++k) {
+        r->scenes[k].release();
     }
-    r->scenes.assign(static_cast<size_t>(scene_count), SceneSlot{});
+    r->scenes.resize(n);
     for (SceneSlot& sl : r->scenes) {
+        sl.clearScene();
         sl.camera = defaultCamera();
     }
     return configureLayout(r, widths, heights);
