@@ -62,10 +62,15 @@ def test_instanced_trace_matches_flattened(tracer):
     assert np.mean(dots[same] > 0.999) > 0.999
 
 
-def test_instanced_render_matches_oracle(tracer, oracle):
+@pytest.mark.parametrize("mode", [0, 2])
+def test_instanced_render_matches_oracle(tracer, oracle, mode):
+    """Instanced render (warp-fetch form in the automatic mode on this small
+    forest, and the two-level per-lane form) against the oracle's render of
+    the flattened scene, replaying the GPU's random numbers."""
     scene, cams, params, sun = _small_forest()
     w, h, waves, stride = 48, 32, 4, 160
     params = params.copy()
+    tracer.set_extend_mode(mode)
     tracer.configure(w, h)
     tracer.set_instances(scene.objects, scene.instances)
     tracer.set_camera(cams[0])
@@ -75,6 +80,7 @@ def test_instanced_render_matches_oracle(tracer, oracle):
     tracer.reset_accumulation()
     tracer.render(waves)
     rgba = tracer.readback()[0].reshape(-1, 4)
+    tracer.set_extend_mode(0)
     st = oracle.scene(scene.flatten()).render(cams[0], params, w, h, waves, tape=tape, tape_stride=stride)
     assert st["tape_errors"] == 0
     err = rel_rmse(rgba[:, :3], st["acc"][:, :3])
