@@ -363,22 +363,60 @@ __device__ void treeletOptimize(int root, int n, int2* child, int* parent, float
 
 // One warp per leaf climbs towards the root; the warp that reaches a node
 // second (both subtrees final) optimises the treelet rooted there.
+// Bottom-up pass of the subtrees too small for treelets, one thread per leaf
+// (as the refit): the SAH cost of every subtree with fewer than minLeaves
+// triangles, and the list of the nodes where treelet work starts (at least
+// minLeaves triangles, both children finished here).  The second thread to
+// reach a node goes on; the first stops.
+__global__ void k_treelet_leaves(int n, const int2* child, const int* parent, const float4* nodeLo,
+    const float4* nodeHi, int* visits, float* subtreeCost, int minLeaves, float costTri, float costNode,
+    int* frontier, unsigned int* frontierCount)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int leaf = n - 1 + j;
+        __stcg(&subtreeCost[leaf], costTri * __ldcg(&nodeHi[leaf]).w);
+        __threadfence();
+        int p = __ldcg(&parent[leaf]);
+        while (p >= 0) {
+            if (atomicAdd(&visits[p], 1) == 0) {
+                break;
+            }
+            __threadfence();
+            if (__float_as_int(__ldcg(&nodeLo[p]).w) >= minLeaves) {
+                frontier[atomicAdd(frontierCount, 1u)] = p;
+                break;
+            }
+            const int2 c = __ldcg(&child[p]);
+            __stcg(&subtreeCost[p],
+                costNode * __ldcg(&nodeHi[p]).w + __ldcg(&subtreeCost[c.x]) + __ldcg(&subtreeCost[c.y]));
+            __threadfence();
+            p = __ldcg(&parent[p]);
+        }
+    }
+}
+
+// Treelet reordering (Karras & Aila 2013), one warp per node of the frontier
+// list and then up the tree: a node is optimised by the second warp to reach it
+// (its first arrival may have come from k_treelet_leaves, for a small child).
+// Every node from the frontier up has at least minLeaves triangles.
 __global__ void k_treelet(int n, int2* child, int* parent, float4* nodeLo, float4* nodeHi, int* visits,
-    float* subtreeCost, int minLeaves, float costTri, float costNode)
+    float* subtreeCost, float costNode, const int* frontier, const unsigned int* frontierCount)
 {
     __shared__ TreeletScratch scratch[kBlock / 32];
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     TreeletScratch& s = scratch[threadIdx.x >> 5];
-    for (int j = warp; j < n; j += warps) {
-        const int leaf = n - 1 + j;
-        if (lane == 0) {
-            __stcg(&subtreeCost[leaf], costTri * __ldcg(&nodeHi[leaf]).w);
-        }
-        __threadfence();
-        int p = __ldcg(&parent[leaf]);
-        while (p >= 0) {
+    const int count = static_cast<int>(*frontierCount);
+    for (int f = warp; f < count; f += warps) {
+        int p = frontier[f];
+        for (;;) {
+            treeletOptimize(p, n, child, parent, nodeLo, nodeHi, subtreeCost, s, costNode);
+            __threadfence();
+            p = __shfl_sync(0xffffffffu, lane == 0 ? __ldcg(&parent[p]) : 0, 0);
+            if (p < 0) {
+                break;
+            }
             int arrived = 0;
             if (lane == 0) {
                 arrived = atomicAdd(&visits[p], 1);
@@ -388,18 +426,33 @@ __global__ void k_treelet(int n, int2* child, int* parent, float4* nodeLo, float
                 break;
             }
             __threadfence();
-            const int leaves = __float_as_int(__ldcg(&nodeLo[p]).w);
-            if (leaves >= minLeaves) {
-                treeletOptimize(p, n, child, parent, nodeLo, nodeHi, subtreeCost, s, costNode);
-            } else if (lane == 0) {
-                const int2 c = __ldcg(&child[p]);
-                __stcg(&subtreeCost[p],
-                    costNode * __ldcg(&nodeHi[p]).w + __ldcg(&subtreeCost[c.x]) + __ldcg(&subtreeCost[c.y]));
-            }
-            __threadfence();
-            p = __shfl_sync(0xffffffffu, lane == 0 ? __ldcg(&parent[p]) : 0, 0);
         }
     }
+}
+
+// The treelet passes of a build: per pass, the small subtrees bottom-up (one
+// thread per leaf), then the treelets from the frontier up (one warp per
+// frontier node, a grid of resident warps).
+static cudaError_t runTreelets(int N, int2* child, int* parent, float4* nodeLo, float4* nodeHi, int* visits,
+    float* subCost, int* frontier, unsigned int* frontierCount, const BvhBuildOptions& opt, cudaStream_t stream)
+{
+    for (int pass = 0; pass < opt.treeletPasses; ++pass) {
+        cudaError_t e = cudaMemsetAsync(visits, 0, sizeof(int) * (N - 1), stream);
+        if (e == cudaSuccess) {
+            e = cudaMemsetAsync(frontierCount, 0, sizeof(unsigned int), stream);
+        }
+        if (e != cudaSuccess) {
+            return e;
+        }
+        k_treelet_leaves<<<(N + kBlock - 1) / kBlock, kBlock, 0, stream>>>(N, child, parent, nodeLo, nodeHi, visits, subCost,
+            opt.treeletMinLeaves, opt.costTriangle, opt.costNode, frontier, frontierCount);
+        int dev = 0, sms = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        k_treelet<<<sms * 4, kBlock, 0, stream>>>(N, child, parent, nodeLo, nodeHi, visits, subCost, opt.costNode,
+            frontier, frontierCount);
+    }
+    return cudaGetLastError();
 }
 
 // (7) Collapse to 8-wide compressed nodes. One thread per task (binary node ->
@@ -679,13 +732,13 @@ int buildBvh(const float* dPositions, uint32_t n, BvhBuffers& out, cudaStream_t 
     }
     k_refit<<<gridFor(N), kBlock, 0, stream>>>(valsSorted, triLo, triHi, N, child, parent, nodeLo, nodeHi, visits);
     if (N > 1 && opt.treeletPasses > 0) {
-        for (int pass = 0; pass < opt.treeletPasses; ++pass) {
-            PT_TRY(cudaMemsetAsync(visits, 0, sizeof(int) * (N - 1), stream));
-            const int warps = N;
-            long long threads = static_cast<long long>(warps) * 32;
-            k_treelet<<<gridFor(threads), kBlock, 0, stream>>>(N, child, parent, nodeLo, nodeHi, visits, subCost,
-                opt.treeletMinLeaves, opt.costTriangle, opt.costNode);
+        int* frontier = ar.get<int>(17, static_cast<size_t>(N - 1));
+        unsigned int* frontierCount = ar.get<unsigned int>(18, 1);
+        if (!ar.ok()) {
+            std::snprintf(err, errLen, "treelet scratch allocation failed");
+            return PT_ERR_OUT_OF_MEMORY;
         }
+        PT_TRY(runTreelets(N, child, parent, nodeLo, nodeHi, visits, subCost, frontier, frontierCount, opt, stream));
     }
     PT_TRY(cudaGetLastError());
 
@@ -778,11 +831,8 @@ int buildBvhInto(const float* dPositions, uint32_t n, const BvhScratch& sc, CwNo
     k_refit<<<gridFor(N), kBlock, 0, stream>>>(sc.valsSorted, sc.triLo, sc.triHi, N, sc.child, sc.parent, sc.nodeLo,
         sc.nodeHi, sc.visits);
     if (N > 1 && opt.treeletPasses > 0) {
-        for (int pass = 0; pass < opt.treeletPasses; ++pass) {
-            PT_TRY(cudaMemsetAsync(sc.visits, 0, sizeof(int) * (N - 1), stream));
-            k_treelet<<<gridFor(static_cast<long long>(N) * 32), kBlock, 0, stream>>>(N, sc.child, sc.parent, sc.nodeLo,
-                sc.nodeHi, sc.visits, sc.subCost, opt.treeletMinLeaves, opt.costTriangle, opt.costNode);
-        }
+        PT_TRY(runTreelets(N, sc.child, sc.parent, sc.nodeLo, sc.nodeHi, sc.visits, sc.subCost, sc.frontier,
+            sc.frontierCount, opt, stream));
     }
     PT_TRY(cudaGetLastError());
     const unsigned int cinit[4] = {1u, 0u, 0u, 0u};

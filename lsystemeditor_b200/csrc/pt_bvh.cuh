@@ -136,7 +136,7 @@ struct BvhBuffers {
 
 // Caller-provided scratch for buildBvhInto (n = triangle count):
 //   triLo, triHi: n float4; cbounds: 8; keys, vals, keysSorted, valsSorted: n;
-//   child: n int2; parent: 2n int; nodeLo, nodeHi: 2n float4; visits: n;
+//   child: n int2; parent: 2n int; nodeLo, nodeHi: 2n float4; visits: n; frontier: n; frontierCount: 1;
 //   subCost: 2n; taskA, taskB: n + 1 int2; counters: 4; sortTemp: sortTempBytes.
 struct BvhScratch {
     float4* triLo;
@@ -152,6 +152,8 @@ struct BvhScratch {
     float4* nodeHi;
     int* visits;
     float* subCost;
+    int* frontier;               // n: nodes where treelet work starts
+    unsigned int* frontierCount; // 1
     int2* taskA;
     int2* taskB;
     unsigned int* counters;

@@ -246,6 +246,8 @@ extern "C" int pt_trace_soup_noalloc(uint32_t triangle_count, const float* posit
     sc.nodeHi = cv.take<float4>(2 * Nn);
     sc.visits = cv.take<int>(Nn);
     sc.subCost = cv.take<float>(2 * Nn);
+    sc.frontier = cv.take<int>(Nn);
+    sc.frontierCount = cv.take<unsigned int>(1);
     sc.taskA = cv.take<int2>(Nn + 1);
     sc.taskB = cv.take<int2>(Nn + 1);
     sc.counters = cv.take<unsigned int>(4);
