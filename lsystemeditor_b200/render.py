@@ -1,4 +1,4 @@
-"""Command-line renderer for the named plain-method workloads.
+"""Command-line renderer for the named workloads (plain methods and one view of the instanced forest).
 
   python -m lsystemeditor_b200.render --workload plain-large --width 512 --height 512 --spp 8 --frames 3
 
@@ -29,7 +29,7 @@ def make_spec(workload: str, width: int = 0, height: int = 0):
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--workload", choices=["plain-small", "plain-large"], default="plain-small")
+    ap.add_argument("--workload", choices=["plain-small", "plain-large", "forest"], default="plain-small")
     ap.add_argument("--width", type=int, default=0, help="image width (0 = the workload's)")
     ap.add_argument("--height", type=int, default=0, help="image height (0 = the workload's)")
     ap.add_argument("--spp", type=int, default=0, help="fixed samples per pixel (0 = the workload's min/max)")
@@ -48,10 +48,23 @@ def main(argv=None) -> int:
         ap.error("--width and --height go together")
 
     from .pathtracer import PROFILE_STAGE_TIMES, PathTracer
-    spec = make_spec(a.workload, a.width, a.height)
+    forest = None
+    if a.workload == "forest":
+        # one view of the instanced forest (objects, instances, sun + sky)
+        from .scene import forest_scene
+        fw, fh = (a.width, a.height) if a.width else (1920, 1080)
+        scene, cams, fparams, sun = forest_scene(width=fw, height=fh, views=1)
+        forest = (scene, cams[0], sun)
+
+        class _Spec:
+            name = "forest: one view"
+            width, height, params, camera, mesh = fw, fh, fparams, cams[0], None
+        spec = _Spec()
+    else:
+        spec = make_spec(a.workload, a.width, a.height)
     params = spec.params.copy()
-    params["spectral_wavelengths"] = {"plain-small": 4, "plain-large": 8}[a.workload] if a.spectral == "auto" \
-        else int(a.spectral)
+    params["spectral_wavelengths"] = {"plain-small": 4, "plain-large": 8, "forest": 8}[a.workload] \
+        if a.spectral == "auto" else int(a.spectral)
     if a.spp > 0:
         params["min_samples"] = a.spp
         params["max_samples_per_pixel"] = a.spp
@@ -61,14 +74,21 @@ def main(argv=None) -> int:
     with PathTracer(a.device) as pt:
         if a.capacity:
             pt.set_tuning(a.capacity, 0)
-        pt.configure(spec.width, spec.height, spec.mesh)
+        if forest is None:
+            pt.configure(spec.width, spec.height, spec.mesh)
+            triangles = spec.mesh.triangle_count
+        else:
+            pt.configure(spec.width, spec.height)
+            pt.set_instances(forest[0].objects, forest[0].instances)
+            pt.set_distant_light(**forest[2])
+            triangles = sum(o.triangle_count for o in forest[0].objects)
         pt.set_camera(spec.camera)
         pt.set_params(params)
         if a.stage_times:
             pt.set_profiling(PROFILE_STAGE_TIMES)
         nw = int(params["spectral_wavelengths"])
         colour = f"{nw} wavelengths" if nw else "RGB"
-        print(f"{spec.name}: {spec.mesh.triangle_count} triangles, {spec.width}x{spec.height}, "
+        print(f"{spec.name}: {triangles} triangles, {spec.width}x{spec.height}, "
               f"{colour}, "
               f"scene ready in {time.perf_counter() - t0:.2f} s", flush=True)
         launched = pt.stats()["launches"]
