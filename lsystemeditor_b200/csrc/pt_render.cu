@@ -35,6 +35,7 @@
 #include "pt_spectral.cuh"
 #include "pt_trace.cuh"
 
+#include <atomic>
 #include <cooperative_groups.h>
 #include "pt_select.cuh"
 #include <curand_kernel.h>
@@ -2210,10 +2211,11 @@ void launchShadow(const LaunchCtx* c, int iter, int grid, bool count, bool inst,
 }
 int shadeOccupancy(int nw)
 {
-    // (one value per instantiation; every device here is the same part)
-    static int occ[3] = {0, 0, 0};
+    // (one value per instantiation, computed once per process; renderers on
+    // several host threads may race to fill it, with the same value)
+    static std::atomic<int> occ[3] = {{0}, {0}, {0}};
     const int k = nw == 8 ? 2 : (nw == 4 ? 1 : 0);
-    if (occ[k] == 0) {
+    if (occ[k].load(std::memory_order_relaxed) == 0) {
         int b = 1;
         if (nw == 8) {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<8>, 256, 0);
@@ -2222,9 +2224,9 @@ int shadeOccupancy(int nw)
         } else {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<0>, 256, 0);
         }
-        occ[k] = b > 0 ? b : 1;
+        occ[k].store(b > 0 ? b : 1, std::memory_order_relaxed);
     }
-    return occ[k];
+    return occ[k].load(std::memory_order_relaxed);
 }
 void stageOccupancy(int& extendBlocks, int& shadeBlocks, int& shadowBlocks)
 {
