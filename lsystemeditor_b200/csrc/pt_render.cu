@@ -705,9 +705,6 @@ __global__ void __launch_bounds__(256, PT_EXTEND_MIN_BLOCKS) k_extend(const Laun
 #ifndef PT_SHADOW_LANE
 #define PT_SHADOW_LANE 1
 #endif
-#ifndef PT_PREFETCH_NODE
-#define PT_PREFETCH_NODE 0
-#endif
 
 // A ray of the per-lane traversal: its scene, origin, normalised direction and
 // the parametric interval it is tested on.
@@ -844,18 +841,6 @@ __device__ __forceinline__ void laneTraversal(unsigned int count, unsigned int* 
                     intersectChildren(r.S->nodes, child, r.o, idir, octinv, r.tMin, closest, childBase, triBase, imask);
                 ngroup = make_uint2(childBase, (hits & 0xFF000000u) | imask);
                 tgroup = make_uint2(triBase, hits & 0x00FFFFFFu);
-#if PT_PREFETCH_NODE
-                if (ngroup.y > 0x00FFFFFFu && tgroup.y != 0u) {
-                    // the nearest child hit is the next node step: start its loads
-                    // while this node's triangles are tested
-                    const uint32_t nb = 31u - __clz(ngroup.y);
-                    const uint32_t ns = (nb - 24u) ^ octinv;
-                    const uint32_t nc = ngroup.x + __popc(ngroup.y & 0xffu & ((1u << ns) - 1u));
-                    const char* np = reinterpret_cast<const char*>(r.S->nodes + nc);
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(np));
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(np + 79));
-                }
-#endif
             } else {
                 tgroup = ngroup;
                 ngroup = make_uint2(0u, 0u);
