@@ -264,7 +264,7 @@ int pt_set_profiling(pt_renderer* r, int flags);
 int pt_get_profile(const pt_renderer* r, pt_profile* out);
 
 /* Work-size tuning (no reference counterpart): paths in flight per launch
- * (0 = default 2^23) and resident blocks per SM of the persistent stage grids
+ * (0 = default 2^24) and resident blocks per SM of the persistent stage grids
  * (0 = from the occupancy calculator). */
 int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm);
 
@@ -430,7 +430,7 @@ int pt_set_distant_light(pt_renderer* r, const pt_distant_light* light);
 
 /* ---- Autotuner (no reference counterpart) ---------------------------------
  * Chooses the scheduling knobs for the current scene(s), camera(s) and
- * parameters: path capacity (paths in flight, 2^20 .. 2^23), blocks per SM of
+ * parameters: path capacity (paths in flight, 2^21 .. 2^24), blocks per SM of
  * the stage kernels (occupancy calculator, 2, 3, 4) and waves per launch
  * (pt_render_params.samples_per_launch: automatic, 4, 16, 64), one knob at a
  * time from the current configuration, each candidate timed on the device

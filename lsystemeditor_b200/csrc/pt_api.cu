@@ -250,7 +250,7 @@ struct pt_renderer {
     cudaGraphExec_t bounceGraph[2] = {nullptr, nullptr};
     unsigned long long bounceKey[6] = {0, 0, 0, 0, 0, 0};
     bool useGraphs = true;
-    int capacityWanted = 1 << 23;     // paths in flight per launch (one chunk for most frames)
+    int capacityWanted = 1 << 24;     // paths in flight per launch (one chunk for most frames)
     int blocksPerSmOverride = 0;
 
     DevBuf<LaunchCtx> dctx;               // device copy of the launch context
@@ -2009,7 +2009,7 @@ int pt_set_tuning(pt_renderer* r, int path_capacity, int blocks_per_sm)
     if (r == nullptr || path_capacity < 0 || blocks_per_sm < 0 || path_capacity > (1 << 26)) {
         return fail(r, PT_ERR_INVALID_ARGUMENT, "pt_set_tuning: bad arguments");
     }
-    r->capacityWanted = path_capacity > 0 ? path_capacity : (1 << 23);
+    r->capacityWanted = path_capacity > 0 ? path_capacity : (1 << 24);
     r->blocksPerSmOverride = blocks_per_sm;
     if (blocks_per_sm > 0) {
         r->gridExtend = r->gridShade = r->gridShadow = r->smCount * blocks_per_sm;
@@ -2135,7 +2135,7 @@ int pt_autotune(pt_renderer* r, int waves, pt_tuning* out)
     out->ms_default = ms;
     Knobs best = cur;
     double bestMs = ms;
-    const int capacities[4] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
+    const int capacities[4] = {1 << 21, 1 << 22, 1 << 23, 1 << 24};
     const int blocks[4] = {0, 2, 3, 4};
     const int perLaunch[4] = {0, 4, 16, 64};
     for (int knob = 0; knob < 3; ++knob) {

@@ -61,7 +61,7 @@ def test_autotune_keeps_the_image():
         t.render(0)
         before = t.readback()[0].copy()
         tune = t.autotune(waves=4)
-        assert tune["path_capacity"] in (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+        assert tune["path_capacity"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24)
         assert tune["blocks_per_sm"] in (0, 2, 3, 4)
         assert tune["samples_per_launch"] in (0, 4, 16, 64)
         assert tune["trials"] >= 2 and tune["ms_best"] <= tune["ms_default"]
