@@ -2156,7 +2156,9 @@ int pt_autotune(pt_renderer* r, int waves, pt_tuning* out)
             if (st != PT_OK) {
                 return st;
             }
-            if (ms < bestMs) {
+            // (a knob moves only for a gain above the probes' run-to-run noise:
+            // a few waves are a short sample of the full render)
+            if (ms < 0.99 * bestMs) {
                 bestMs = ms;
                 best = k;
             }
