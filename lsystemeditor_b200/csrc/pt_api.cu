@@ -596,6 +596,9 @@ void collectStageTimes(pt_renderer* r)
 // Results do not depend on it; a pixel that converges inside a batch leaves
 // the rest of the batch's samples unused, so the batch grows when few pixels
 // stopped during the previous one.
+#ifndef PT_PATH_GENERATIONS
+#define PT_PATH_GENERATIONS 0
+#endif
 #ifndef PT_SAMPLE_BUFFER_BYTES
 // (8 GiB: on the 64-tree batch, 31 M pixels, a 1 GiB buffer held batches to 2
 // waves, so every pass put ~16 scenes' paths in flight and drained often; at
@@ -1690,7 +1693,9 @@ int pt_render(pt_renderer* r, int waves)
         const long long jobs = static_cast<long long>(active) * B;
         const int slots = static_cast<int>(std::min<long long>(std::min(r->capacity, r->capacityWanted), jobs));
         r->hbatch.jobs = static_cast<unsigned long long>(jobs);
-        r->hbatch.nextJob = static_cast<unsigned long long>(slots);
+        // generations: no slot takes a second job; each generation of `slots`
+        // jobs drains before the next one starts
+        r->hbatch.nextJob = static_cast<unsigned long long>(PT_PATH_GENERATIONS ? jobs : slots);
         r->hbatch.activeCount = active;
         r->hbatch.waveBase = static_cast<uint32_t>(r->wavesDone);
         r->hbatch.slotCount = slots;
@@ -1707,70 +1712,76 @@ int pt_render(pt_renderer* r, int waves)
             launchSceneJobs(c, static_cast<int>(r->scenes.size()), B, s);
             ++launches;
         }
-        {
-            StageTimer tm(r, kGenerate);
-            launchGenerate(c, slots, 0, nw, s);
-        }
-        ++launches;
-        // Every live path advances one bounce per iteration and a finished path's
-        // slot takes the next job, so iterations <= bounce-steps / slots + drain.
-        const long long maxIters =
-            (jobs * (maxDepthEff + 1) + slots - 1) / std::max(slots, 1) + maxDepthEff + 8;
-        int sel = 0;
-        const bool graphs = r->useGraphs && r->profileFlags == 0 && ensureBounceGraphs(r, c, inst, nw);
-        for (long long it = 0; graphs; it += 4) {
-            // the same four iterations as below, replayed from a graph: sel is 0
-            // again after four, and the kernels use only the parity of `iter`
-            if (it > maxIters) {
-                return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
-            }
-            PT_CHECK(r, cudaGraphLaunch(r->bounceGraph[it == 0 ? 0 : 1], s));
-            launches += 4 * (4 + extendKernels(false, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0));
-            r->profile.launches_extend += 4;
-            r->profile.launches_shadow += 4;
-            unsigned int live = 0;
-            PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-            PT_CHECK(r, cudaStreamSynchronize(s));
-            if (live == 0) {
-                break;
-            }
-        }
-        for (long long it = 0; !graphs; ++it) {
-            if (it > maxIters) {
-                return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
-            }
-            const int iter = static_cast<int>(it & 0x7fffffff);
+        for (long long jobOffset = 0; jobOffset < jobs; jobOffset += slots) {
+            const int genCount = static_cast<int>(std::min<long long>(slots, jobs - jobOffset));
             {
-                StageTimer tm(r, kExtend);
-                launchExtend(c, sel, it == 0, iter, extendGrid(r, countVisits, inst), countVisits, inst, r->extendLane, s);
+                StageTimer tm(r, kGenerate);
+                launchGenerate(c, genCount, 0, nw, s, static_cast<unsigned long long>(jobOffset));
             }
-            {
-                StageTimer tm(r, kShade);
-                launchShadeMiss(c, iter, sel, r->gridShadeMiss, nw, s);
-                launchShade(c, sel, iter, shadeGrid(r, nw), nw, s);
-            }
-            {
-                StageTimer tm(r, kShadow);
-                launchShadow(c, iter, shadowGrid(r, countVisits, inst), countVisits, inst, r->extendLane, s);
-            }
-            {
-                StageTimer tm(r, kFinalize);
-                launchFinalize(c, sel, r->gridShadow, nw, s);
-                if (slotOrdered(r)) {
-                    launchNextQueue(c, sel, r->gridShadow, s);
+            ++launches;
+            // Every live path advances one bounce per iteration and a finished path's
+            // slot takes the next job, so iterations <= bounce-steps / slots + drain.
+            const long long maxIters =
+                (jobs * (maxDepthEff + 1) + slots - 1) / std::max(slots, 1) + maxDepthEff + 8;
+            int sel = 0;
+            const bool graphs = r->useGraphs && r->profileFlags == 0 && ensureBounceGraphs(r, c, inst, nw);
+            for (long long it = 0; graphs; it += 4) {
+                // the same four iterations as below, replayed from a graph: sel is 0
+                // again after four, and the kernels use only the parity of `iter`
+                if (it > maxIters) {
+                    return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
                 }
-            }
-            launches += 4 + extendKernels(countVisits, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0);
-            r->profile.launches_extend += 1;
-            r->profile.launches_shadow += 1;
-            sel ^= 1;
-            if ((it & 3) == 3) {
+                PT_CHECK(r, cudaGraphLaunch(r->bounceGraph[it == 0 ? 0 : 1], s));
+                launches += 4 * (4 + extendKernels(false, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0));
+                r->profile.launches_extend += 4;
+                r->profile.launches_shadow += 4;
                 unsigned int live = 0;
-                PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p + sel, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+                PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
                 PT_CHECK(r, cudaStreamSynchronize(s));
                 if (live == 0) {
                     break;
                 }
+            }
+            for (long long it = 0; !graphs; ++it) {
+                if (it > maxIters) {
+                    return fail(r, PT_ERR_INTERNAL, "path queue did not drain after %lld iterations", it);
+                }
+                const int iter = static_cast<int>(it & 0x7fffffff);
+                {
+                    StageTimer tm(r, kExtend);
+                    launchExtend(c, sel, it == 0, iter, extendGrid(r, countVisits, inst), countVisits, inst, r->extendLane, s);
+                }
+                {
+                    StageTimer tm(r, kShade);
+                    launchShadeMiss(c, iter, sel, r->gridShadeMiss, nw, s);
+                    launchShade(c, sel, iter, shadeGrid(r, nw), nw, s);
+                }
+                {
+                    StageTimer tm(r, kShadow);
+                    launchShadow(c, iter, shadowGrid(r, countVisits, inst), countVisits, inst, r->extendLane, s);
+                }
+                {
+                    StageTimer tm(r, kFinalize);
+                    launchFinalize(c, sel, r->gridShadow, nw, s);
+                    if (slotOrdered(r)) {
+                        launchNextQueue(c, sel, r->gridShadow, s);
+                    }
+                }
+                launches += 4 + extendKernels(countVisits, inst, r->extendLane) + (slotOrdered(r) ? 1 : 0);
+                r->profile.launches_extend += 1;
+                r->profile.launches_shadow += 1;
+                sel ^= 1;
+                if ((it & 3) == 3) {
+                    unsigned int live = 0;
+                    PT_CHECK(r, cudaMemcpyAsync(&live, r->qCounts.p + sel, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+                    PT_CHECK(r, cudaStreamSynchronize(s));
+                    if (live == 0) {
+                        break;
+                    }
+                }
+            }
+            if (!PT_PATH_GENERATIONS) {
+                break; // one pass: finished paths' slots took the batch's later jobs
             }
         }
         PT_CHECK(r, cudaGetLastError());

@@ -598,9 +598,11 @@ __device__ __forceinline__ void recyclePath(const LaunchCtx& c, uint32_t i, unsi
     }
 }
 
-// First `count` jobs of a batch into slots 0..count-1 (extend queue = identity).
+// Jobs jobOffset .. jobOffset + count - 1 of a batch into slots 0..count-1
+// (extend queue = identity).
 template <int NW>
-__global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ cp, int count, int extendSel)
+__global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ cp, int count, int extendSel,
+    unsigned long long jobOffset)
 {
     const LaunchCtx& c = *cp;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -614,7 +616,7 @@ __global__ void __launch_bounds__(256) k_generate(const LaunchCtx* __restrict__ 
         c.q.counts[10] = 0u;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        initPath<NW>(c, static_cast<uint32_t>(i), static_cast<unsigned long long>(i));
+        initPath<NW>(c, static_cast<uint32_t>(i), jobOffset + static_cast<unsigned long long>(i));
     }
 }
 
@@ -2090,14 +2092,14 @@ inline int gridFor(long long n, int block = 256, int cap = 148 * 16)
 
 } // namespace
 
-void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s)
+void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s, unsigned long long jobOffset)
 {
     if (nw == 8) {
-        k_generate<8><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
+        k_generate<8><<<gridFor(count), 256, 0, s>>>(d, count, extendSel, jobOffset);
     } else if (nw == 4) {
-        k_generate<4><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
+        k_generate<4><<<gridFor(count), 256, 0, s>>>(d, count, extendSel, jobOffset);
     } else {
-        k_generate<0><<<gridFor(count), 256, 0, s>>>(d, count, extendSel);
+        k_generate<0><<<gridFor(count), 256, 0, s>>>(d, count, extendSel, jobOffset);
     }
 }
 void launchExtend(const LaunchCtx* c, int sel, bool identity, int iter, int grid, bool count, bool inst, bool lane,

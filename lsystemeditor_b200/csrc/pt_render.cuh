@@ -149,7 +149,8 @@ struct LaunchCtx {
 // taken by reference would be copied to local memory by every thread.
 // `grid` is a persistent-style grid; kernels loop over device-side counts.
 // `nw` (generate, shade-miss, shade, finalize): wavelengths per path, 0 = RGB.
-void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s);
+void launchGenerate(const LaunchCtx* d, int count, int extendSel, int nw, cudaStream_t s,
+    unsigned long long jobOffset = 0);
 // inst: compile-time instanced-scene traversal (any scene of the context instanced).
 // Closest-hit stage.  lane: per-lane ray replacement (k_extend_lane + k_route;
 // flat scenes, no visit counting), else one warp-fetch k_extend.
