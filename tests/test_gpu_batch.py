@@ -102,8 +102,8 @@ def test_batch_argument_errors(tracer):
 def test_batch_per_lane_kernels(tracer):
     """The per-lane closest-hit and shadow kernels with the slot-ordered
     next-bounce queue: every scene still equals its render alone, at a path
-    capacity small enough that slots are recycled across scene boundaries many
-    times."""
+    capacity small enough that a batch runs in many generations of slots that
+    cross scene boundaries."""
     scenes = _scenes()
     params = default_params(background_r=0.2, background_g=0.2, background_b=0.25, max_path_depth=5,
                             min_samples=4, max_samples_per_pixel=24, relative_error_threshold=0.3,
