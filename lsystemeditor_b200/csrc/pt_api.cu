@@ -596,15 +596,6 @@ void collectStageTimes(pt_renderer* r)
 // Results do not depend on it; a pixel that converges inside a batch leaves
 // the rest of the batch's samples unused, so the batch grows when few pixels
 // stopped during the previous one.
-#ifndef PT_PATH_GENERATIONS
-// Jobs of a batch run in generations of the slot count, each drained before
-// the next, instead of refilling each finished path's slot with the next job:
-// the launches of a generation hold paths of the same depth (camera rays
-// together, then first bounces, ...).  Same images; plain-large 1106 -> 1068
-// ms per frame, a 1920x1080 forest view 10.59 -> 10.47 s, the 64-tree batch
-// 20.71 -> 18.37 s.
-#define PT_PATH_GENERATIONS 1
-#endif
 #ifndef PT_SAMPLE_BUFFER_BYTES
 // (8 GiB: on the 64-tree batch, 31 M pixels, a 1 GiB buffer held batches to 2
 // waves, so every pass put ~16 scenes' paths in flight and drained often; at

@@ -585,6 +585,15 @@ __device__ __forceinline__ void queueNext(const LaunchCtx& c, uint32_t i, unsign
 template <int NW>
 __device__ __forceinline__ void recyclePath(const LaunchCtx& c, uint32_t i, unsigned int* nextCount, uint32_t* nextQueue)
 {
+#if PT_PATH_GENERATIONS
+    // (generations: a finished path's slot stays empty until the next
+    // generation; the batch's job counter is not touched per path)
+    (void)c;
+    (void)i;
+    (void)nextCount;
+    (void)nextQueue;
+    return;
+#endif
     cg::coalesced_group g = cg::coalesced_threads();
     unsigned long long base = 0;
     if (g.thread_rank() == 0) {
