@@ -9,7 +9,8 @@
 // the launches of a generation hold paths of the same depth (camera rays
 // together, then first bounces, ...).  Same images; plain-large 1106 -> 1068
 // ms per frame, a 1920x1080 forest view 10.59 -> 10.47 s, the 64-tree batch
-// 20.71 -> 18.37 s.
+// 20.71 -> 18.37 s; and 1068 -> 1035 ms once finished paths stopped claiming
+// jobs from the batch's counter.
 #define PT_PATH_GENERATIONS 1
 #endif
 
