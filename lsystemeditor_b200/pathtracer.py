@@ -419,6 +419,15 @@ class PathTracer:
         return rgba, counts, conv
 
     # -- scene generation on the device, export, display --------------------
+    def set_procedural(self, instances, params=None, scene: int = 0):
+        """meshSceneBuild (MeshSceneContent.h:16-20) over ProceduralInstance records: the
+        instances' turtle output in world space (procedural.build_tubes) lofted and built
+        on the device into scene `scene` (pt_batch_set_tubes).  Returns the TubeSet."""
+        from .procedural import build_tubes
+        tubes = build_tubes(instances, params)
+        self.batch_set_tubes(scene, tubes)
+        return tubes
+
     def batch_set_tubes(self, scene: int, tubes: TubeSet):
         """Lofts tubes and leaves on the GPU (pt_batch_set_tubes) and builds scene `scene`."""
         rs = np.ascontiguousarray(tubes.ring_start, np.uint32)
