@@ -123,3 +123,92 @@ def _empty_mesh(bank: np.ndarray) -> S.HostMesh:
     e = S.HostMesh.empty()
     e.materials = np.asarray(bank)
     return e
+
+
+# ---------------------------------------------------------------------------
+# Stochastic rule choice as the reference's evaluator makes it
+# (LSystemEvaluator.cpp:308-347, 386-425, 433-448): one 64-bit Mersenne
+# Twister seeded with the evaluation seed; for every symbol, in string order,
+# that some rule matches, one uniform draw in [0, total weight) picks the rule
+# whose running weight first reaches it.  A symbol without a matching rule is
+# copied and draws nothing.
+# ---------------------------------------------------------------------------
+class ReferenceRng:
+    """MT19937-64 (Matsumoto & Nishimura, the std::mt19937_64 parameters) with
+    the uniform real draw of std::uniform_real_distribution<double> over it:
+    one 64-bit output rounded to double and scaled by 2^-64, then a + u (b - a)."""
+
+    _N, _M = 312, 156
+    _MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int):
+        mt = [0] * self._N
+        mt[0] = seed & self._MASK
+        for i in range(1, self._N):
+            prev = mt[i - 1]
+            mt[i] = (6364136223846793005 * (prev ^ (prev >> 62)) + i) & self._MASK
+        self._mt = mt
+        self._i = self._N
+
+    def _twist(self):
+        mt, n, m = self._mt, self._N, self._M
+        upper, lower = 0xFFFFFFFF80000000, 0x7FFFFFFF
+        for i in range(n):
+            y = (mt[i] & upper) | (mt[(i + 1) % n] & lower)
+            v = mt[(i + m) % n] ^ (y >> 1)
+            if y & 1:
+                v ^= 0xB5026F5AA96619E9
+            mt[i] = v
+        self._i = 0
+
+    def next_u64(self) -> int:
+        if self._i >= self._N:
+            self._twist()
+        x = self._mt[self._i]
+        self._i += 1
+        x ^= (x >> 29) & 0x5555555555555555
+        x ^= (x << 17) & 0x71D67FFFEDA60000
+        x ^= (x << 37) & 0xFFF7EEE000000000
+        x ^= x >> 43
+        return x & self._MASK
+
+    def uniform(self, a: float, b: float) -> float:
+        u = float(self.next_u64()) / 18446744073709551616.0
+        if u >= 1.0:
+            u = np.nextafter(1.0, 0.0)
+        return u * (b - a) + a
+
+
+StochasticRules = Dict[str, List[Tuple[float, Callable[[tuple], List[Module]]]]]
+
+
+def expand_stochastic(axiom: List[Module], rules: StochasticRules, iterations: int, seed: int) -> List[Module]:
+    """Rewrites `axiom` `iterations` times; rules[name] lists the (probability,
+    successor(args)) pairs of the rules whose predecessor is `name`, in the
+    order the grammar lists them."""
+    rng = ReferenceRng(seed)
+    word = list(axiom)
+    for _ in range(int(iterations)):
+        out: List[Module] = []
+        for name, args in word:
+            cands = rules.get(name)
+            if not cands:
+                out.append((name, args))
+                continue
+            weights = [p if (np.isfinite(p) and p > 0.0) else 0.0 for p, _ in cands]
+            total = 0.0
+            for w in weights:
+                total += w
+            pick = 0
+            if total > 0.0:
+                selected = rng.uniform(0.0, total)
+                running = 0.0
+                pick = len(cands) - 1
+                for k, w in enumerate(weights):
+                    running += w
+                    if selected <= running:
+                        pick = k
+                        break
+            out.extend(cands[pick][1](args))
+        word = out
+    return word
